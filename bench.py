@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark: milliseconds per 60k-DOF plate solve at FP64-checked error 1e-6.
+
+One step = one complete solve of the plate_q4_141 workload (141x141 Q4
+Mindlin, 60,492 DOF, seeded synthetic loads and column supports): element
+stiffness and block-Jacobi set-up on the GPU, then the persistent PCG
+launch, inputs resident in HBM.  ``value`` is milliseconds per solve for the
+whole job (lower is better); ``e2e`` is the same through the public C ABI
+(pg_solve) from host buffers, copies included.  L2 is flushed (256 MiB
+write) between timed steps; each step is timed with CUDA events on the
+solver's stream.
+
+Multi-GPU: a single plate does not shard (the solve is bound by grid-wide
+synchronisation latency), so --gpus N runs N independent replicas, one per
+rank, and ``value`` = max-over-ranks time / (N * steps).
+
+--impl reference times the reference's CPU algorithm (the oracle's
+restatement of solvePCG + applyGlobalK in reference precision; the
+TypeScript original cannot run here) on the host.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpu-gauntlet_b200"))
+
+METRIC = "ms per 60k-DOF plate solve at 1e-6 FP64-checked error: learned/mixed vs plain PCG"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["plategpu", "reference"], default="plategpu")
+    ap.add_argument("--workload", default="plate_q4_141")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--tol", type=float, default=7e-7,
+                    help="relative recursive-residual tolerance (||r||/||b||)")
+    ap.add_argument("--ctas", type=int, default=0)
+    ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas)
+# ---------------------------------------------------------------------------
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, value, local):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.4)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, copy burst)"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback (6.65 TB/s earlier measurement on this pool)"
+
+
+def ncu_traffic(kernel_tag, workload):
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", f"{kernel_tag}_{workload}.txt")
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# checker (the oracle, test infrastructure) -- cpu_baseline leg only
+# ---------------------------------------------------------------------------
+
+def oracle_checks(wl, want_baseline=True):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+
+    m, mat = wl.mesh, wl.material
+    npe = m.nodesPerElement
+    F = wl.F.astype(np.float64)
+    ke64 = O.all_ke(m.nodes, m.elements, npe, mat.E, mat.nu, mat.t, elem_t=mat.elem_t,
+                    mode=O.FP64)
+    xs, rel = O.truth_solve(m.nodeCount, m.elements, npe, ke64, wl.cons_mask, F)
+    A = O.assemble(m.nodeCount, m.elements, npe, ke64, wl.cons_mask)
+    out = {"truth": xs, "A": A}
+    if want_baseline:
+        keR = O.all_ke(m.nodes, m.elements, npe, mat.E, mat.nu, mat.t, elem_t=mat.elem_t,
+                       mode=O.REF)
+        offs, flat = wl.coloring.flat()
+        t0 = time.perf_counter()
+        bd = O.invert_block_diag(O.block_diag(m.nodeCount, m.elements, npe, keR, O.REF),
+                                 wl.cons_mask, O.REF)
+        xr, it, res, conv = O.solve_pcg(m.nodeCount, m.elements, npe, keR, offs, flat,
+                                        wl.cons_mask, bd, F, 1e-6, 20000, O.REF)
+        ms = (time.perf_counter() - t0) * 1e3
+        out.update(ref_x=xr, ref_iters=it, ref_conv=conv, ref_ms=ms)
+    return out
+
+
+def accuracy(x, chk):
+    import numpy as np
+
+    xs, A = chk["truth"], chk["A"]
+    e = x - xs
+    res = {"rel_l2_vs_fp64_truth": float(np.linalg.norm(e) / np.linalg.norm(xs)),
+           "energy_norm_rel": float(np.sqrt(abs(e @ (A @ e)) / abs(xs @ (A @ xs)))),
+           "max_w_rel_vs_fp64_truth": None, "max_w_rel_vs_reference_cpu": None}
+    w, ws = x[0::3], xs[0::3]
+    mw, mws = w[np.argmax(np.abs(w))], ws[np.argmax(np.abs(ws))]
+    res["max_w_rel_vs_fp64_truth"] = float(abs(mw - mws) / abs(mws))
+    if "ref_x" in chk:
+        wr = chk["ref_x"][0::3]
+        mwr = wr[np.argmax(np.abs(wr))]
+        res["max_w_rel_vs_reference_cpu"] = float(abs(mw - mwr) / abs(mwr))
+    return res
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+
+def run_reference(args, world, rank):
+    """The reference CPU algorithm (oracle port, reference precision)."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle as O
+    from plategpu import workloads
+
+    wl = workloads.WORKLOADS[args.workload]()
+    m, mat = wl.mesh, wl.material
+    npe = m.nodesPerElement
+    F = wl.F.astype(np.float64)
+    offs, flat = wl.coloring.flat()
+
+    def solve(maxit, tol):
+        ke = O.all_ke(m.nodes, m.elements, npe, mat.E, mat.nu, mat.t, elem_t=mat.elem_t,
+                      mode=O.REF)
+        bd = O.invert_block_diag(O.block_diag(m.nodeCount, m.elements, npe, ke, O.REF),
+                                 wl.cons_mask, O.REF)
+        return O.solve_pcg(m.nodeCount, m.elements, npe, ke, offs, flat, wl.cons_mask, bd, F,
+                           tol, maxit, O.REF)
+
+    # warm-up: one full solve gives the iteration count of a complete solve
+    _x, full_iters, _r, conv = solve(20000, 1e-6)
+    for _ in range(max(0, args.warmup - 1)):
+        solve(20, 0.0)
+    sample_iters = 150
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        solve(sample_iters, 0.0)
+        times.append((time.perf_counter() - t0) * 1e3)
+    step_ms = statistics.mean(times)
+    value = step_ms * full_iters / sample_iters
+    sample = (f"set-up + {sample_iters} PCG iterations per step, scaled by the "
+              f"{full_iters} iterations a full reference-precision solve of {args.workload} "
+              f"takes at tolerance 1e-6 (converged={conv}); single thread")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "ms",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": step_ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 storage / f64 arithmetic",
+            "data": "synthetic (seeded workload)",
+            "config": {"workload": args.workload, "dof": wl.n_dof, "parallelism": "replicas"},
+            "cpu_baseline": {"value": value, "unit": "ms", "cores": 1, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_plategpu(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    from plategpu import _lib, workloads
+
+    torch.cuda.set_device(local)
+    wl = workloads.WORKLOADS[args.workload]()
+    n = wl.n_dof
+    ctx = _lib.Context(local)
+    stream = torch.cuda.Stream(device=local)
+    ctx.set_stream(stream.cuda_stream)
+    prob = _lib.Problem(wl.mesh, wl.material, wl.coloring, wl.F, wl.cons_mask)
+    prec = _lib.PG_PREC_FP64 if args.precision == "fp64" else _lib.PG_PREC_MIXED
+    opts = _lib.make_options(tolerance=args.tol, max_iterations=20000, precision=prec,
+                             stop_rule=_lib.PG_STOP_RELATIVE, ctas=args.ctas,
+                             threads=args.threads)
+    plan = ctx.plan(prob, opts)
+    F_dev = torch.from_numpy(wl.F).to(f"cuda:{local}")
+    x_dev = torch.zeros(n, dtype=torch.float64, device=f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            plan.solve_device(opts, F_dev.data_ptr(), x_dev.data_ptr())
+        sampler = ClockSampler(local) if rank == 0 else None
+        if sampler:
+            sampler.start()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        infos = []
+        barrier(world)
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            starts[k].record(stream)
+            infos.append(plan.solve_device(opts, F_dev.data_ptr(), x_dev.data_ptr()))
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        clocks = sampler.stop() if sampler else None
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = max_over_ranks(world, sum(step_ms), local)
+    value = total_ms / (world * args.steps)
+    kernel_ms = statistics.mean(i.solve_ms for i in infos)
+    setup_ms = statistics.mean(i.setup_ms for i in infos)
+    iters = infos[-1].iterations
+    x_last = x_dev.cpu().numpy()
+
+    # e2e through the C ABI from host buffers (pg_solve)
+    e2e_steps = args.e2e_steps or args.steps
+    rng = np.random.default_rng(1234)
+    loads = [(wl.F * np.float32(1.0 + 0.1 * rng.random())).astype(np.float32)
+             for _ in range(min(e2e_steps, 16))]
+    for k in range(2):
+        prob.set_F(loads[k % len(loads)])
+        ctx.solve(prob, opts)
+    barrier(world)
+    e2e = []
+    for k in range(e2e_steps):
+        prob.set_F(loads[k % len(loads)])
+        t0 = time.perf_counter()
+        ctx.solve(prob, opts)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    barrier(world)
+    e2e_total = max_over_ranks(world, sum(e2e), local)
+    e2e_value = e2e_total / (world * e2e_steps)
+
+    if rank != 0:
+        plan.close()
+        ctx.close()
+        return
+    # roofline of the dominant kernel: algorithmic bytes per launch
+    # (16 vector words per DOF per iteration, 8 bytes each in FP64)
+    word = 8 if args.precision == "fp64" else 4
+    alg_bytes = 16.0 * n * word * iters
+    peak, peak_src = hbm_peak()
+    achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
+    kernel_tag = "pcg_fp64" if args.precision == "fp64" else "pcg_mixed"
+    traffic = ncu_traffic(kernel_tag, args.workload)
+    line = {
+        "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(step_ms),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32 inner / f64 refinement",
+        "data": "synthetic (seeded plate_q4_141: 5 kPa + 32 point loads, 16 columns)",
+        "config": {"workload": args.workload, "dof": n, "elements": wl.mesh.elementCount,
+                   "precision": args.precision, "preconditioner": "block-jacobi",
+                   "stop": f"||r||/||b|| < {args.tol:g}", "ctas": infos[-1].ctas,
+                   "threads": infos[-1].threads, "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}"},
+        "iterations": iters,
+        "kernel_ms": kernel_ms, "setup_ms": setup_ms,
+        "us_per_iteration": kernel_ms * 1e3 / max(iters, 1),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": f"{kernel_tag}_kernel", "peak_source": peak_src,
+                     "algorithmic_bytes_per_launch": alg_bytes},
+        "e2e": {"value": e2e_value, "unit": "ms", "h2d_bytes_per_step": 4 * n,
+                "d2h_bytes_per_step": 8 * n + 64},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        chk = oracle_checks(wl, want_baseline=True)
+        line["accuracy"] = accuracy(x_last, chk)
+        line["cpu_baseline"] = {
+            "value": chk["ref_ms"], "unit": "ms", "cores": 1, "kind": "port",
+            "sample": (f"one full reference-precision solve of {args.workload} "
+                       f"({chk['ref_iters']} iterations, tol 1e-6) by the C restatement "
+                       "of solvePCG/applyGlobalK, single thread")}
+    else:
+        line["accuracy"] = None
+        line["cpu_baseline"] = None
+    print(json.dumps(line), flush=True)
+    plan.close()
+    ctx.close()
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_plategpu(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

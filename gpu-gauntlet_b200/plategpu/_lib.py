@@ -1,0 +1,313 @@
+"""ctypes binding of libplategpu.so (the C ABI declared in include/plategpu.h).
+
+The library is built in-tree by ``plategpu.build.build_library()`` (nvcc,
+sm_100a).  Loading fails loudly when it is missing: there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libplategpu.so")
+
+PG_OK, PG_EINVAL, PG_ENOMEM, PG_ECUDA, PG_ETIMEOUT, PG_ENONFINITE, PG_EUNSUPPORTED = range(7)
+STATUS_NAMES = {0: "PG_OK", 1: "PG_EINVAL", 2: "PG_ENOMEM", 3: "PG_ECUDA", 4: "PG_ETIMEOUT",
+                5: "PG_ENONFINITE", 6: "PG_EUNSUPPORTED"}
+PG_PREC_FP64, PG_PREC_MIXED = 0, 1
+PG_STOP_REFERENCE, PG_STOP_RELATIVE = 0, 1
+STOP_REASONS = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "zero_rhs"}
+
+# every symbol include/plategpu.h declares
+EXPORTED = ("pg_options_default", "pg_is_available", "pg_create", "pg_destroy", "pg_last_error",
+            "pg_clear_cache", "pg_set_stream", "pg_solve", "pg_plan_create", "pg_plan_solve_device",
+            "pg_plan_destroy", "pg_apply_k",
+            "pg_block_jacobi", "pg_element_stiffness", "pg_plan_inspect")
+
+
+class PgProblem(C.Structure):
+    _fields_ = [
+        ("node_count", C.c_uint32),
+        ("element_count", C.c_uint32),
+        ("nodes_per_element", C.c_uint32),
+        ("nodes", C.c_void_p),
+        ("elements", C.c_void_p),
+        ("color_count", C.c_uint32),
+        ("color_offsets", C.c_void_p),
+        ("elements_by_color", C.c_void_p),
+        ("E", C.c_double),
+        ("nu", C.c_double),
+        ("t", C.c_double),
+        ("elem_t", C.c_void_p),
+        ("F", C.c_void_p),
+        ("constrained", C.c_void_p),
+    ]
+
+
+class PgOptions(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("tolerance", C.c_double),
+        ("max_iterations", C.c_int32),
+        ("precision", C.c_int32),
+        ("stop_rule", C.c_int32),
+        ("ctas", C.c_int32),
+        ("threads", C.c_int32),
+        ("wait_timeout_ms", C.c_double),
+        ("reliable_interval", C.c_int32),
+        ("reliable_delta", C.c_double),
+    ]
+
+
+class PgInfo(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("iterations", C.c_int32),
+        ("converged", C.c_int32),
+        ("stop_reason", C.c_int32),
+        ("final_residual", C.c_double),
+        ("true_rel_residual", C.c_double),
+        ("b_norm", C.c_double),
+        ("setup_ms", C.c_double),
+        ("solve_ms", C.c_double),
+        ("total_ms", C.c_double),
+        ("ctas", C.c_int32),
+        ("threads", C.c_int32),
+        ("reliable_updates", C.c_int32),
+        ("plan_cached", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["stop_reason"] = STOP_REASONS.get(d["stop_reason"], d["stop_reason"])
+        return d
+
+
+class PlateGPUError(RuntimeError):
+    """A non-OK pg_status; ``status`` holds the code name."""
+
+    def __init__(self, status: int, message: str):
+        self.status = STATUS_NAMES.get(status, str(status))
+        self.code = status
+        super().__init__(f"{self.status}: {message}")
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run plategpu.build.build_library() "
+                          "(nvcc, sm_100a). There is no CPU fallback.")
+    L = C.CDLL(LIB_PATH)
+    P, I = C.c_void_p, C.c_int
+    L.pg_options_default.argtypes = [C.POINTER(PgOptions)]
+    L.pg_options_default.restype = None
+    L.pg_is_available.argtypes = []
+    L.pg_is_available.restype = I
+    L.pg_create.argtypes = [I, C.POINTER(P)]
+    L.pg_create.restype = I
+    L.pg_destroy.argtypes = [P]
+    L.pg_destroy.restype = None
+    L.pg_last_error.argtypes = [P]
+    L.pg_last_error.restype = C.c_char_p
+    L.pg_clear_cache.argtypes = [P]
+    L.pg_clear_cache.restype = I
+    L.pg_set_stream.argtypes = [P, P]
+    L.pg_set_stream.restype = I
+    L.pg_solve.argtypes = [P, C.POINTER(PgProblem), C.POINTER(PgOptions), P, C.POINTER(PgInfo)]
+    L.pg_solve.restype = I
+    L.pg_plan_create.argtypes = [P, C.POINTER(PgProblem), C.POINTER(PgOptions), C.POINTER(P)]
+    L.pg_plan_create.restype = I
+    L.pg_plan_solve_device.argtypes = [P, C.POINTER(PgOptions), P, P, C.POINTER(PgInfo)]
+    L.pg_plan_solve_device.restype = I
+    L.pg_plan_destroy.argtypes = [P]
+    L.pg_plan_destroy.restype = None
+    L.pg_apply_k.argtypes = [P, C.POINTER(PgProblem), P, P]
+    L.pg_apply_k.restype = I
+    L.pg_block_jacobi.argtypes = [P, C.POINTER(PgProblem), P]
+    L.pg_block_jacobi.restype = I
+    L.pg_element_stiffness.argtypes = [P, C.POINTER(PgProblem), P]
+    L.pg_element_stiffness.restype = I
+    L.pg_plan_inspect.argtypes = [C.POINTER(PgProblem), I, P, C.c_char_p, C.c_size_t]
+    L.pg_plan_inspect.restype = I
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class Problem:
+    """Owns contiguous copies of the arrays a PgProblem points at."""
+
+    def __init__(self, mesh, material, coloring, F=None, constrained=None):
+        self.nodes = np.array(mesh.nodes, np.float32, order="C")
+        self.elements = np.array(mesh.elements, np.uint32, order="C")
+        if coloring is not None:
+            offs, flat = coloring.flat()
+            self.color_offsets = np.array(offs, np.uint32, order="C")
+            self.elements_by_color = np.array(flat, np.uint32, order="C")
+            ncol = int(coloring.colorCount)
+        else:
+            self.color_offsets = self.elements_by_color = None
+            ncol = 0
+        self.elem_t = (None if getattr(material, "elem_t", None) is None
+                       else np.array(material.elem_t, np.float32, order="C"))
+        n = 3 * int(mesh.nodeCount)
+        self.F = np.zeros(n, np.float32) if F is None else np.array(F, np.float32, order="C")
+        if self.F.size != n:
+            raise ValueError(f"F has {self.F.size} entries, expected {n}")
+        self.cons = (np.zeros(n, np.uint8) if constrained is None
+                     else np.array(constrained, np.uint8, order="C"))
+        if self.cons.size != n:
+            raise ValueError(f"constrained mask has {self.cons.size} entries, expected {n}")
+        s = PgProblem()
+        s.node_count = int(mesh.nodeCount)
+        s.element_count = int(mesh.elementCount)
+        s.nodes_per_element = int(mesh.nodesPerElement)
+        s.nodes = _ptr(self.nodes)
+        s.elements = _ptr(self.elements)
+        s.color_count = ncol
+        s.color_offsets = _ptr(self.color_offsets)
+        s.elements_by_color = _ptr(self.elements_by_color)
+        s.E, s.nu, s.t = float(material.E), float(material.nu), float(material.t)
+        s.elem_t = _ptr(self.elem_t)
+        s.F = _ptr(self.F)
+        s.constrained = _ptr(self.cons)
+        self.struct = s
+
+    def set_F(self, F):
+        F = np.ascontiguousarray(F, np.float32)
+        if F.size != self.F.size:
+            raise ValueError("F size mismatch")
+        self.F = F
+        self.struct.F = _ptr(F)
+
+
+PLAN_STATS = ("parts", "colors", "recolored", "max_local_nodes", "max_owned_nodes",
+              "max_part_elements", "ghost_nodes", "violations")
+
+
+def plan_inspect(prob: "Problem", ctas: int) -> dict:
+    """pg_plan_inspect: host-only partition statistics and invariant check."""
+    stats = np.zeros(8, np.int32)
+    msg = C.create_string_buffer(256)
+    st = load().pg_plan_inspect(C.byref(prob.struct), int(ctas), _ptr(stats), msg, 256)
+    if st != PG_OK:
+        raise PlateGPUError(st, msg.value.decode())
+    return dict(zip(PLAN_STATS, stats.tolist()))
+
+
+def make_options(tolerance=1e-6, max_iterations=1000, precision=PG_PREC_FP64,
+                 stop_rule=PG_STOP_REFERENCE, ctas=0, threads=0, wait_timeout_ms=None,
+                 reliable_interval=0, reliable_delta=0.0) -> PgOptions:
+    o = PgOptions()
+    load().pg_options_default(C.byref(o))
+    o.tolerance = float(tolerance)
+    o.max_iterations = int(max_iterations)
+    o.precision = int(precision)
+    o.stop_rule = int(stop_rule)
+    o.ctas = int(ctas)
+    o.threads = int(threads)
+    if wait_timeout_ms is not None:
+        o.wait_timeout_ms = float(wait_timeout_ms)
+    o.reliable_interval = int(reliable_interval)
+    o.reliable_delta = float(reliable_delta)
+    return o
+
+
+class Context:
+    """A pg_ctx on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        h = C.c_void_p()
+        st = self.L.pg_create(int(device), C.byref(h))
+        if st != PG_OK:
+            raise PlateGPUError(st, self.L.pg_last_error(None).decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != PG_OK:
+            raise PlateGPUError(st, self.L.pg_last_error(self.h).decode())
+
+    def solve(self, prob: Problem, opts: PgOptions):
+        x = np.zeros(prob.F.size, np.float64)
+        info = PgInfo()
+        st = self.L.pg_solve(self.h, C.byref(prob.struct), C.byref(opts), _ptr(x), C.byref(info))
+        self._check(st)
+        return x, info
+
+    def plan(self, prob: Problem, opts: PgOptions) -> "DevicePlan":
+        return DevicePlan(self, prob, opts)
+
+    def apply_k(self, prob: Problem, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros_like(x)
+        self._check(self.L.pg_apply_k(self.h, C.byref(prob.struct), _ptr(x), _ptr(y)))
+        return y
+
+    def block_jacobi(self, prob: Problem):
+        out = np.zeros(9 * prob.struct.node_count, np.float64)
+        self._check(self.L.pg_block_jacobi(self.h, C.byref(prob.struct), _ptr(out)))
+        return out
+
+    def element_stiffness(self, prob: Problem):
+        npe = prob.struct.nodes_per_element
+        out = np.zeros(prob.struct.element_count * 9 * npe * npe, np.float64)
+        self._check(self.L.pg_element_stiffness(self.h, C.byref(prob.struct), _ptr(out)))
+        return out.reshape(prob.struct.element_count, 3 * npe, 3 * npe)
+
+    def set_stream(self, stream_ptr: int):
+        self._check(self.L.pg_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def clear_cache(self):
+        self._check(self.L.pg_clear_cache(self.h))
+
+
+class DevicePlan:
+    """A pg_plan: the partition and device copies of one mesh, for repeated
+    device-resident solves with new loads."""
+
+    def __init__(self, ctx: Context, prob: Problem, opts: PgOptions):
+        self.ctx = ctx
+        self.prob = prob  # keeps the host arrays alive while the plan is built
+        h = C.c_void_p()
+        ctx._check(ctx.L.pg_plan_create(ctx.h, C.byref(prob.struct), C.byref(opts), C.byref(h)))
+        self.h = h
+
+    def solve_device(self, opts: PgOptions, F_dev_ptr: int, x_dev_ptr: int) -> PgInfo:
+        info = PgInfo()
+        st = self.ctx.L.pg_plan_solve_device(self.h, C.byref(opts), C.c_void_p(F_dev_ptr),
+                                             C.c_void_p(x_dev_ptr), C.byref(info))
+        self.ctx._check(st)
+        return info
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.pg_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,156 @@
+"""Seeded synthetic plate workloads.
+
+Every workload is a 10 m x 10 m plate, E = 2.1e11 Pa, nu = 0.3, shear
+correction 5/6 (fixed in the element, element.ts:235), built through the
+host mirrors of the reference's mesher / colouring / support / load
+functions.  Loads are a uniform pressure (as nodal equivalent loads) plus
+point loads at seeded nodes, rounded once to the float32 F of the solver
+interface, with the constrained entries zeroed (applyBCsToRHS).
+
+  plate_q4_32      32x32 Q4 (3,267 DOF), all edges clamped, 1 kPa + 4 point
+                   loads U(1,10) kN at seeded interior nodes.
+  plate_q4_141     141x141 Q4 (60,492 DOF), edges simply supported (w = 0)
+                   plus w = 0 at a seeded 4x4 grid of interior column nodes,
+                   5 kPa + 32 point loads U(1,10) kN at seeded nodes.
+  plate_dkt_200    200x200 quads split into 80,000 DKT triangles along
+                   alternating diagonals (121,203 DOF), interior nodes
+                   jittered U(-0.2h, 0.2h), thickness 0.1(1 + 0.3 g) clipped
+                   to [0.05, 0.15] with g a squared-exponential Gaussian
+                   random field (length-scale 2 m), clamped edges, 3 kPa.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import coloring as _col
+from . import mesher as _mesh
+from . import problem as _prob
+from .types import ElementColoring, PlateMaterial, PlateMesh, PlateSupport
+
+WIDTH = 10.0
+E_STEEL = 2.1e11
+NU = 0.3
+T_PLATE = 0.1
+
+
+@dataclass
+class Workload:
+    name: str
+    mesh: PlateMesh
+    material: PlateMaterial
+    coloring: ElementColoring
+    supports: List[PlateSupport]
+    constrainedDOFs: set
+    F: np.ndarray  # float32, BCs applied
+    point_loads: list = field(default_factory=list)
+    description: str = ""
+
+    @property
+    def n_dof(self) -> int:
+        return self.mesh.nodeCount * 3
+
+    @property
+    def cons_mask(self) -> np.ndarray:
+        return _prob.constrained_mask(self.n_dof, self.constrainedDOFs)
+
+
+def _finish_loads(mesh, pressure, point_nodes, point_mags, constrainedDOFs):
+    F = _prob.pressure_load_vector(mesh, pressure)
+    xy = mesh.nodes.reshape(-1, 2)
+    loads = []
+    for n, m in zip(point_nodes, point_mags):
+        F[3 * int(n)] += float(m)
+        loads.append(((float(xy[n, 0]), float(xy[n, 1])), float(m)))
+    F32 = F.astype(np.float32)
+    _prob.applyBCsToRHS(F32, constrainedDOFs)
+    return F32, loads
+
+
+def _interior_nodes(nx, ny):
+    jj, ii = np.meshgrid(np.arange(1, ny), np.arange(1, nx), indexing="ij")
+    return (jj * (nx + 1) + ii).reshape(-1)
+
+
+def plate_q4(nx: int, seed: int, edges: str = "fixed", pressure: float = 1e3,
+             n_point_loads: int = 4, column_grid: int = 0, t: float = T_PLATE,
+             E: float = E_STEEL, nu: float = NU, name: Optional[str] = None) -> Workload:
+    """Structured nx x nx Q4 Mindlin plate with seeded loads and columns."""
+    rng = np.random.default_rng(seed)
+    mesh = _mesh.rectangular_mesh_nxny(WIDTH, WIDTH, nx, nx)
+    supports = [PlateSupport(edges, "all_edges")]
+    if column_grid:
+        # a k x k grid of interior column nodes, each grid line shifted by a
+        # seeded offset of up to 2 elements
+        base = [round((a + 1) * nx / (column_grid + 1)) for a in range(column_grid)]
+        off_i = rng.integers(-2, 3, size=column_grid)
+        off_j = rng.integers(-2, 3, size=column_grid)
+        for a in range(column_grid):
+            for b in range(column_grid):
+                i = int(np.clip(base[a] + off_i[a], 1, nx - 1))
+                j = int(np.clip(base[b] + off_j[b], 1, nx - 1))
+                supports.append(PlateSupport("pinned", j * (nx + 1) + i))
+    cons = _prob.identifyConstrainedDOFs(mesh, supports)
+    interior = _interior_nodes(nx, nx)
+    free_w = np.array([n for n in interior if 3 * int(n) not in cons])
+    nodes = rng.choice(free_w, size=n_point_loads, replace=False)
+    mags = rng.uniform(1e3, 1e4, size=n_point_loads)
+    F, loads = _finish_loads(mesh, pressure, nodes, mags, cons)
+    return Workload(name=name or f"plate_q4_{nx}", mesh=mesh,
+                    material=PlateMaterial(E=E, nu=nu, t=t),
+                    coloring=_col.computeElementColoring(mesh), supports=supports,
+                    constrainedDOFs=cons, F=F, point_loads=loads)
+
+
+def plate_q4_32(seed: int = 1) -> Workload:
+    return plate_q4(32, seed, edges="fixed", pressure=1e3, n_point_loads=4,
+                    name="plate_q4_32")
+
+
+def plate_q4_141(seed: int = 2) -> Workload:
+    return plate_q4(141, seed, edges="pinned", pressure=5e3, n_point_loads=32, column_grid=4,
+                    name="plate_q4_141")
+
+
+def grf_squared_exponential(nx: int, ny: int, h: float, length: float,
+                            rng: np.random.Generator) -> np.ndarray:
+    """Zero-mean, unit-variance Gaussian random field with squared-
+    exponential covariance exp(-d^2 / (2 l^2)) on an (ny+1) x (nx+1) node
+    grid of spacing h, sampled spectrally on a periodic grid padded by
+    4 l so that the wrap-around correlation is negligible."""
+    pad = int(np.ceil(4 * length / h))
+    Mx, My = nx + 1 + pad, ny + 1 + pad
+    kx = 2 * np.pi * np.fft.fftfreq(Mx, d=h)
+    ky = 2 * np.pi * np.fft.fftfreq(My, d=h)
+    K2 = ky[:, None] ** 2 + kx[None, :] ** 2
+    spec = np.exp(-0.5 * length ** 2 * K2)
+    noise = rng.standard_normal((My, Mx))
+    field = np.real(np.fft.ifft2(np.fft.fft2(noise) * np.sqrt(spec)))
+    field = field[: ny + 1, : nx + 1]
+    return (field - field.mean()) / field.std()
+
+
+def plate_dkt_200(seed: int = 3, n: int = 200) -> Workload:
+    rng = np.random.default_rng(seed)
+    mesh = _mesh.split_triangle_mesh(WIDTH, WIDTH, n, n, jitter=0.2,
+                                     seed=int(rng.integers(1 << 31)))
+    g_nodes = grf_squared_exponential(n, n, WIDTH / n, 2.0, rng).reshape(-1)
+    el = mesh.elements.astype(np.int64).reshape(-1, 3)
+    g_elem = g_nodes[el].mean(axis=1)
+    elem_t = np.clip(T_PLATE * (1 + 0.3 * g_elem), 0.05, 0.15).astype(np.float32)
+    supports = [PlateSupport("fixed", "all_edges")]
+    cons = _prob.identifyConstrainedDOFs(mesh, supports)
+    F, loads = _finish_loads(mesh, 3e3, [], [], cons)
+    return Workload(name=f"plate_dkt_{n}", mesh=mesh,
+                    material=PlateMaterial(E=E_STEEL, nu=NU, t=T_PLATE, elem_t=elem_t),
+                    coloring=_col.computeElementColoringGreedy(mesh), supports=supports,
+                    constrainedDOFs=cons, F=F, point_loads=loads)
+
+
+WORKLOADS = {
+    "plate_q4_32": plate_q4_32,
+    "plate_q4_141": plate_q4_141,
+    "plate_dkt_200": plate_dkt_200,
+}

@@ -1,0 +1,197 @@
+/*
+ * plategpu.h -- C ABI of the B200 (sm_100a) matrix-free plate-bending PCG
+ * solver.
+ *
+ * This is the drop-in boundary for the GPU plate solve of
+ * cseifert512/gpu-gauntlet: the entry points below are what the
+ * reference's GPU-solver module would bind through an N-API addon.  Every
+ * argument is a plain pointer or a size; no C++ or torch type crosses this
+ * boundary; no exception, exit or abort either: every call returns a
+ * pg_status and pg_last_error() describes the last failure.  There is no CPU
+ * fallback: without a usable CUDA device every solve fails with PG_ECUDA.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   pg_solve         solveGPU(mesh, material, coloring, F, constrainedDOFs,
+ *                    options) -> GPUSolveResult   src/lib/plate/gpu/solver.ts:80-104
+ *                    (with solveGPUInternal :109-185 and runGPUPCG :190-553)
+ *   pg_problem       PlateMesh, PlateMaterial, ElementColoring
+ *                    src/lib/plate/types.ts:14-102; F and constrainedDOFs as
+ *                    solveGPU receives them
+ *   pg_options       GPUSolverOptions  src/lib/plate/gpu/solver.ts:35-42
+ *   pg_info          GPUSolveResult    src/lib/plate/gpu/solver.ts:47-60
+ *   pg_apply_k       gpuApplyK + apply_k_q4 / apply_k_dkt
+ *                    src/lib/plate/gpu/solver.ts:413-461 (single-colour K.x
+ *                    test pattern of src/lib/plate/gpu/single_color_test.ts)
+ *   pg_block_jacobi  computeBlockDiagonal + invertBlockDiagonal
+ *                    src/lib/plate/solver.ts:188-304 as solveGPUInternal calls
+ *                    them (gpu/solver.ts:130-131)
+ *   pg_is_available  isWebGPUAvailable  src/lib/plate/gpu/context.ts:19
+ *   pg_clear_cache   clearPipelineCache src/lib/plate/gpu/solver.ts:601-603
+ *
+ * Semantics kept from the reference: F arrives with the boundary conditions
+ * applied (applyBCsToRHS); constrained DOFs are identity rows, (K p)_c = p_c,
+ * so the solution is 0 there; the block-Jacobi preconditioner is built
+ * inside the solve from mesh and material; defaults tolerance 1e-6,
+ * max_iterations 1000; the reference stop rule is ||r|| < tol or
+ * ||r|| / ||b|| < tol on the recursive residual; |p.Ap| < 1e-30 is a
+ * breakdown that returns converged = 0.
+ */
+#ifndef PLATEGPU_H
+#define PLATEGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PG_ABI_VERSION 1
+
+typedef enum pg_status {
+    PG_OK = 0,
+    PG_EINVAL = 1,        /* malformed problem or options */
+    PG_ENOMEM = 2,        /* device or host allocation failed */
+    PG_ECUDA = 3,         /* CUDA runtime error / no device */
+    PG_ETIMEOUT = 4,      /* a grid-wide wait ran past its time limit */
+    PG_ENONFINITE = 5,    /* NaN or Inf in the inputs or the iteration */
+    PG_EUNSUPPORTED = 6   /* a request this build does not serve */
+} pg_status;
+
+typedef enum pg_precision {
+    PG_PREC_FP64 = 0,  /* plain FP64 block-Jacobi PCG */
+    PG_PREC_MIXED = 1  /* FP32 inner iterations, FP64 solution and
+                          FP64 true-residual replacement */
+} pg_precision;
+
+typedef enum pg_stop_rule {
+    PG_STOP_REFERENCE = 0, /* ||r|| < tol  or  ||r||/||b|| < tol  (gpu/solver.ts:516) */
+    PG_STOP_RELATIVE = 1   /* ||r||/||b|| < tol only */
+} pg_stop_rule;
+
+typedef enum pg_stop_reason {
+    PG_STOP_CONVERGED = 0,
+    PG_STOP_MAX_ITER = 1,
+    PG_STOP_BREAKDOWN = 2, /* |p.Ap| < 1e-30 (pcg.ts:154, gpu/solver.ts:496) */
+    PG_STOP_ZERO_RHS = 3   /* ||b|| < 1e-30: x = 0, 0 iterations */
+} pg_stop_reason;
+
+/* One plate problem, in the reference's host layout. */
+typedef struct pg_problem {
+    uint32_t node_count;
+    uint32_t element_count;
+    uint32_t nodes_per_element;        /* 4 = Q4 Mindlin quad, 3 = DKT triangle */
+    const float* nodes;                /* [2*node_count] x0,y0,x1,y1,...      */
+    const uint32_t* elements;          /* [nodes_per_element*element_count]   */
+    uint32_t color_count;
+    const uint32_t* color_offsets;     /* [color_count+1], offsets into:      */
+    const uint32_t* elements_by_color; /* [element_count] element ids by colour */
+    double E, nu, t;                   /* PlateMaterial                        */
+    const float* elem_t;               /* optional [element_count] thickness,
+                                          overrides t (NULL = uniform t)       */
+    const float* F;                    /* [3*node_count] load vector           */
+    const uint8_t* constrained;        /* [3*node_count] 1 = constrained DOF   */
+} pg_problem;
+
+typedef struct pg_options {
+    uint32_t struct_size;         /* sizeof(pg_options); set by pg_options_default */
+    double tolerance;             /* default 1e-6 */
+    int32_t max_iterations;       /* default 1000 */
+    int32_t precision;            /* pg_precision, default PG_PREC_FP64 */
+    int32_t stop_rule;            /* pg_stop_rule, default PG_STOP_REFERENCE */
+    int32_t ctas;                 /* persistent grid size; 0 = automatic */
+    int32_t threads;              /* threads per CTA; 0 = automatic */
+    double wait_timeout_ms;       /* limit on each grid-wide wait; default 1000 */
+    int32_t reliable_interval;    /* mixed: max inner iterations between FP64
+                                     residual replacements; 0 = automatic */
+    double reliable_delta;        /* mixed: replace when the FP32 residual fell
+                                     by this factor; 0 = automatic (0.1) */
+} pg_options;
+
+/* Per-solve result (GPUSolveResult plus extended statistics). */
+typedef struct pg_info {
+    int32_t status;               /* pg_status of the call */
+    int32_t iterations;
+    int32_t converged;
+    int32_t stop_reason;          /* pg_stop_reason */
+    double final_residual;        /* ||r|| of the recursive residual (reference meaning) */
+    double true_rel_residual;     /* ||F - K x|| / ||F||, recomputed in FP64 on the GPU */
+    double b_norm;                /* ||F|| */
+    double setup_ms;              /* device: element stiffness + block-Jacobi setup */
+    double solve_ms;              /* device: persistent PCG launch */
+    double total_ms;              /* host wall clock of the whole call (gpuTimeMs) */
+    int32_t ctas;
+    int32_t threads;
+    int32_t reliable_updates;     /* mixed precision: FP64 residual replacements */
+    int32_t plan_cached;          /* 1 when the partition plan was reused */
+} pg_info;
+
+typedef struct pg_ctx pg_ctx;
+
+/* pg_options filled with the reference defaults. */
+void pg_options_default(pg_options* opt);
+
+/* 1 when a CUDA device of compute capability 10.x can be used. */
+int pg_is_available(void);
+
+/* Context on CUDA device `device`: owns a stream, device buffers and the
+ * cache of partition plans.  One context per host thread (calls on one
+ * context are serialised by an internal mutex). */
+int pg_create(int device, pg_ctx** out);
+void pg_destroy(pg_ctx* ctx);
+
+/* Message of the last failing call on ctx (or of pg_create when ctx is NULL). */
+const char* pg_last_error(const pg_ctx* ctx);
+
+/* Drops every cached partition plan and device buffer of ctx. */
+int pg_clear_cache(pg_ctx* ctx);
+
+/* Runs all work of ctx on `stream` (a cudaStream_t; NULL = the context's
+ * own stream). */
+int pg_set_stream(pg_ctx* ctx, void* stream);
+
+/* Solves K x = F.  x_out: [3*node_count] FP64 (the TypeScript wrapper
+ * narrows it to the reference's Float32Array).  info may be NULL. */
+int pg_solve(pg_ctx* ctx, const pg_problem* prob, const pg_options* opt, double* x_out,
+             pg_info* info);
+
+/* Device-resident solves.  A plan holds the partition of one mesh and its
+ * device copies (nodes, elements, colouring, constraints, material); each
+ * pg_plan_solve_device recomputes the element stiffness and block-Jacobi
+ * set-up on the device and runs the persistent PCG for a new load.  F_dev is
+ * a device float [3*node_count], x_dev a device double [3*node_count]; work
+ * runs on the context stream and the call returns after its one readback
+ * of the result record.  A plan must not outlive its context. */
+typedef struct pg_plan pg_plan;
+int pg_plan_create(pg_ctx* ctx, const pg_problem* prob, const pg_options* opt, pg_plan** out);
+int pg_plan_solve_device(pg_plan* plan, const pg_options* opt, const float* F_dev,
+                         double* x_dev, pg_info* info);
+void pg_plan_destroy(pg_plan* plan);
+
+/* Test hook: y = K x in FP64 with the reference BC rule (y_c = x_c). */
+int pg_apply_k(pg_ctx* ctx, const pg_problem* prob, const double* x, double* y);
+
+/* Test hook: inverted 3x3 block diagonal (9 doubles per node, row-major),
+ * constrained rows/columns replaced by identity before inversion and
+ * |det| < 1e-30 blocks replaced by identity (solver.ts:231-304). */
+int pg_block_jacobi(pg_ctx* ctx, const pg_problem* prob, double* binv_out);
+
+/* Test hook: element stiffness matrices, [element_count * (3*npe)^2] FP64. */
+int pg_element_stiffness(pg_ctx* ctx, const pg_problem* prob, double* ke_out);
+
+/* Host-only test hook (no device needed): builds the partition plan the
+ * solver would use with `ctas` blocks and checks its invariants (every
+ * node owned by exactly one part, every element touching an owned node
+ * present in that part, ghosts = the other nodes of those elements, no two
+ * elements of one colour sharing a node).  stats_out[8]: parts, colours,
+ * recoloured (0/1), max local nodes, max owned nodes, max elements per
+ * part, total ghost nodes, invariant violations (0 when valid).
+ * msg/msg_len (optional) receive the failure reason. */
+int pg_plan_inspect(const pg_problem* prob, int ctas, int32_t* stats_out, char* msg,
+                    size_t msg_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PLATEGPU_H */

@@ -1,0 +1,98 @@
+"""Host-side mirrors (mesher, colouring, supports, loads, workloads) vs the oracle."""
+import numpy as np
+import pytest
+
+from plategpu import coloring as col
+from plategpu import mesher, problem, workloads
+from plategpu.types import PlateLoad, PlateSupport
+
+
+@pytest.mark.parametrize("w,h,target", [(10, 10, 2.0), (10, 10, 0.28), (7.5, 3.0, 0.4),
+                                         (10, 10, 10 / 141)])
+def test_rectangular_mesh_matches_oracle(oracle, w, h, target):
+    m = mesher.generateRectangularMesh(w, h, target)
+    nx, ny = oracle.rect_dims(w, h, target)
+    assert (m.gridNx, m.gridNy) == (nx, ny)
+    nodes, el, bnd = oracle.rect_mesh(w, h, nx, ny)
+    np.testing.assert_array_equal(m.nodes, nodes)
+    np.testing.assert_array_equal(m.elements, el)
+    np.testing.assert_array_equal(m.boundaryNodes, bnd)
+
+
+def test_dof_counts_of_workload_meshes():
+    assert 3 * mesher.rectangular_mesh_nxny(10, 10, 32, 32).nodeCount == 3267
+    assert 3 * mesher.rectangular_mesh_nxny(10, 10, 141, 141).nodeCount == 60492
+    t = mesher.split_triangle_mesh(10, 10, 200, 200, jitter=0.2, seed=1)
+    assert 3 * t.nodeCount == 121203 and t.elementCount == 80000
+
+
+def test_structured_coloring_matches_oracle(oracle):
+    m = mesher.rectangular_mesh_nxny(10, 10, 9, 6)
+    c = col.computeElementColoring(m)
+    ec, flat, counts = oracle.color_structured(m.elementCount, m.gridNx)
+    np.testing.assert_array_equal(c.elementColors, ec)
+    np.testing.assert_array_equal(np.concatenate(c.colors), flat)
+    assert col.verifyColoring(m, c)
+
+
+def test_greedy_coloring_matches_oracle(oracle):
+    m = mesher.split_triangle_mesh(10, 10, 11, 9, jitter=0.2, seed=3)
+    c = col.computeElementColoringGreedy(m)
+    ec, flat, counts = oracle.color_greedy(m.nodeCount, m.elementCount, 3, m.elements)
+    np.testing.assert_array_equal(c.elementColors, ec)
+    np.testing.assert_array_equal(np.concatenate(c.colors), flat)
+    assert col.verifyColoring(m, c)
+
+
+def test_constrained_dofs_match_oracle(oracle):
+    m = mesher.rectangular_mesh_nxny(10, 10, 8, 8)
+    sups = [PlateSupport("pinned", "all_edges"), PlateSupport("fixed", 40),
+            PlateSupport("roller", 12)]
+    got = problem.constrained_mask(3 * m.nodeCount, problem.identifyConstrainedDOFs(m, sups))
+    ref = oracle.constrained(m.nodeCount, [(s.type, s.location) for s in sups], m.boundaryNodes)
+    np.testing.assert_array_equal(got, ref)
+
+
+def test_load_vector_matches_oracle(oracle):
+    m = mesher.rectangular_mesh_nxny(10, 10, 16, 16)
+    rng = np.random.default_rng(0)
+    loads = [PlateLoad((float(a), float(b)), float(c)) for a, b, c in
+             zip(rng.uniform(0, 10, 9), rng.uniform(0, 10, 9), rng.uniform(1e3, 1e4, 9))]
+    loads.append(PlateLoad((5.0, 5.0), 1234.5))
+    loads.append(PlateLoad((5.0, 5.0), 0.1))  # accumulates in float32 at the same node
+    F = problem.buildLoadVector(m, loads)
+    Fo = oracle.load_vector(m.nodes, [(l.position, l.magnitude) for l in loads], 0)
+    np.testing.assert_array_equal(F.astype(np.float64), Fo)
+
+
+def test_pressure_load_total():
+    m = mesher.split_triangle_mesh(10, 10, 20, 20, jitter=0.2, seed=7)
+    F = problem.pressure_load_vector(m, 3e3)
+    assert abs(F.sum() - 3e3 * 100.0) < 1e-6 * 3e5
+
+
+@pytest.mark.parametrize("name,ndof", [("plate_q4_32", 3267), ("plate_q4_141", 60492)])
+def test_workload_shapes(name, ndof):
+    wl = workloads.WORKLOADS[name]()
+    assert wl.n_dof == ndof
+    assert wl.F.dtype == np.float32 and np.all(wl.F[wl.cons_mask != 0] == 0)
+    assert col.verifyColoring(wl.mesh, wl.coloring)
+    wl2 = workloads.WORKLOADS[name]()
+    np.testing.assert_array_equal(wl.F, wl2.F)  # seeded
+
+
+def test_q4_141_columns_and_loads():
+    wl = workloads.plate_q4_141()
+    cols = [s for s in wl.supports if s.location != "all_edges"]
+    assert len(cols) == 16
+    assert len(wl.point_loads) == 32
+    assert all(1e3 <= m <= 1e4 for _p, m in wl.point_loads)
+
+
+def test_dkt_workload_thickness_field():
+    wl = workloads.plate_dkt_200()
+    t = wl.material.elem_t
+    assert t.size == 80000 and t.min() >= 0.05 and t.max() <= 0.15
+    assert 0.08 < float(t.mean()) < 0.12 and t.std() > 0.005
+    assert wl.n_dof == 121203
+    assert col.verifyColoring(wl.mesh, wl.coloring)
