@@ -20,41 +20,44 @@ __host__ __device__ inline double flexural_rigidity(double E, double nu, double 
     return (E * t * t * t) / (12.0 * (1.0 - nu * nu));
 }
 
+// Physical shape-function derivatives of the Q4 element at (xi, eta);
+// returns det J.  (element.ts:80-184)
+__device__ __forceinline__ double q4_derivs(const double* __restrict__ c, double xi, double eta,
+                                            double* __restrict__ dNdx, double* __restrict__ dNdy) {
+    const double xm = 1 - xi, xp = 1 + xi, em = 1 - eta, ep = 1 + eta;
+    const double dxi[4] = {-em * 0.25, em * 0.25, ep * 0.25, -ep * 0.25};
+    const double deta[4] = {-xm * 0.25, -xp * 0.25, xp * 0.25, xm * 0.25};
+    double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        J11 += dxi[k] * c[2 * k];
+        J12 += dxi[k] * c[2 * k + 1];
+        J21 += deta[k] * c[2 * k];
+        J22 += deta[k] * c[2 * k + 1];
+    }
+    const double det = J11 * J22 - J12 * J21;
+    const double inv = 1.0 / det;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        dNdx[k] = inv * (J22 * dxi[k] - J12 * deta[k]);
+        dNdy[k] = inv * (-J21 * dxi[k] + J11 * deta[k]);
+    }
+    return det;
+}
+
 // coords: x0,y0,x1,y1,... (the mesh's float32 values, widened)
-__device__ inline void q4_ke(const double c[8], double E, double nu, double t, double* Ke) {
+__device__ inline void q4_ke(const double* __restrict__ c, double E, double nu, double t,
+                             double* __restrict__ Ke) {
     const double gp = 0.5773502691896257;
     const double D = flexural_rigidity(E, nu, t);
     const double D11 = D, D12 = D * nu, D22 = D, D33 = D * (1.0 - nu) * 0.5;
     const double Dsc = (5.0 / 6.0) * (E / (2.0 * (1.0 + nu))) * t;
     for (int i = 0; i < 144; i++) Ke[i] = 0.0;
 
-    // natural-coordinate derivative table for a point (xi, eta)
-    auto derivs = [&](double xi, double eta, double dNdx[4], double dNdy[4]) -> double {
-        const double xm = 1 - xi, xp = 1 + xi, em = 1 - eta, ep = 1 + eta;
-        const double dxi[4] = {-em * 0.25, em * 0.25, ep * 0.25, -ep * 0.25};
-        const double deta[4] = {-xm * 0.25, -xp * 0.25, xp * 0.25, xm * 0.25};
-        double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            J11 += dxi[k] * c[2 * k];
-            J12 += dxi[k] * c[2 * k + 1];
-            J21 += deta[k] * c[2 * k];
-            J22 += deta[k] * c[2 * k + 1];
-        }
-        const double det = J11 * J22 - J12 * J21;
-        const double inv = 1.0 / det;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            dNdx[k] = inv * (J22 * dxi[k] - J12 * deta[k]);
-            dNdy[k] = inv * (-J21 * dxi[k] + J11 * deta[k]);
-        }
-        return det;
-    };
-
     const double sx[4] = {-1, 1, 1, -1}, sy[4] = {-1, -1, 1, 1};
     for (int g = 0; g < 4; g++) {
         double dNdx[4], dNdy[4];
-        const double f = fabs(derivs(sx[g] * gp, sy[g] * gp, dNdx, dNdy));
+        const double f = fabs(q4_derivs(c, sx[g] * gp, sy[g] * gp, dNdx, dNdy));
         for (int i = 0; i < 4; i++) {
             for (int j = 0; j < 4; j++) {
                 const int tx_i = 3 * i + 1, ty_i = 3 * i + 2, tx_j = 3 * j + 1, ty_j = 3 * j + 2;
@@ -67,7 +70,7 @@ __device__ inline void q4_ke(const double c[8], double E, double nu, double t, d
     }
     {
         double dNdx[4], dNdy[4];
-        const double f = 4.0 * fabs(derivs(0.0, 0.0, dNdx, dNdy));
+        const double f = 4.0 * fabs(q4_derivs(c, 0.0, 0.0, dNdx, dNdy));
         const double N = 0.25;  // every Q4 shape function at the centre
         for (int i = 0; i < 4; i++) {
             for (int j = 0; j < 4; j++) {
@@ -85,7 +88,8 @@ __device__ inline void q4_ke(const double c[8], double E, double nu, double t, d
     }
 }
 
-__device__ inline void dkt_ke(const double c[6], double E, double nu, double t, double* Ke) {
+__device__ inline void dkt_ke(const double* __restrict__ c, double E, double nu, double t,
+                              double* __restrict__ Ke) {
     for (int i = 0; i < 81; i++) Ke[i] = 0.0;
     const double x1 = c[0], y1 = c[1], x2 = c[2], y2 = c[3], x3 = c[4], y3 = c[5];
     const double x12 = x1 - x2, y12 = y1 - y2, x23 = x2 - x3, y23 = y2 - y3;

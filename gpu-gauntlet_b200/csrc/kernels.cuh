@@ -36,28 +36,42 @@ struct PcgResult {
     double b_norm;
     int reliable_updates;
     int wait_failures;
+    int nonfinite_it;          // reduction index where a non-finite value appeared
+    int reductions;            // grid-wide reductions performed
+    double nonfinite_vals[3];  // gamma, delta, rho at that reduction
+    unsigned long long phase_cycles[4];  // block 0: K.u; gather, dots, publish; exchange; update
+};
+
+// Byte offsets of the shared-memory arrays of one block (computed on the
+// host from the plan's maxima; T is the inner vector type).
+struct SmemLayout {
+    int r, u, p, s, w, B, yt, kt;  // T
+    int x, xl, ytd, red, scal, sp;  // double
+    int gid, tptr;                 // int
+    int tnode;                     // uint16
+    int cm;                        // uint8
+    int total;
 };
 
 struct PcgArgs {
-    int G, npe, C, Nn;
+    int G, NT, Nn;
     const int* node_off;
     const int* nown;
     const int* nodes;
-    const int* elem_off;
-    const int* color_off;
-    const int* elems;
-    const int* lnode;
-    const double* ke64;   // [Ne][nd*nd]
-    const float* ke32;    // [Ne][nd*nd]
-    const double* binv64; // [Nn][9]
-    const float* binv32;  // [Nn][9]
-    const uint8_t* cons;  // [3Nn]
-    const float* F;       // [3Nn]
-    double* x;            // [3Nn]
-    double* xch64;        // [2][3Nn]
-    float* xch32;         // [2][3Nn]
-    double* partials;     // [2][G][4]
-    unsigned int* bar;
+    const int* task_off;
+    const int* tp_off;
+    const int* tptr;
+    const uint16_t* task_nodes;  // [NT][npe] -> staged [npe][ntask]
+    const double* kt64;          // [3*nd][NT] task blocks, FP64
+    const float* kt32;           // [3*nd][NT] task blocks, FP32
+    const double* binv64;        // [Nn][9]
+    const float* binv32;         // [Nn][9]
+    const uint8_t* cons;         // [3Nn]
+    const float* F;              // [3Nn]
+    double* x;                   // [3Nn]
+    unsigned long long* llv;     // [2][3Nn][2] tagged w / r values of the owners
+    unsigned long long* llx;     // [3Nn][2] tagged x values (FP64 residual rounds)
+    unsigned long long* llp;     // [2][G][8] tagged partial sums
     int* abort_flag;
     PcgResult* res;
     double tol;
@@ -65,37 +79,41 @@ struct PcgArgs {
     int stop_rule;
     unsigned long long timeout_ns;
     int ke_smem;
-    int sm_nloc, sm_nown, sm_nel;  // shared-memory strides (max over parts)
+    int timing;
+    int test_stall;  // test hook: block 0 waits once for a tag nobody writes
     int reliable_interval;
     double reliable_delta;
+    SmemLayout L;
 };
 
 // ---------------------------------------------------------------------------
 // setup kernels
 // ---------------------------------------------------------------------------
 
-__global__ void ke_kernel(int Ne, int npe, const float* __restrict__ nodes,
+template <int NPE>
+__global__ void ke_kernel(int Ne, const float* __restrict__ nodes,
                           const uint32_t* __restrict__ elements, double E, double nu, double t,
                           const float* __restrict__ elem_t, double* __restrict__ ke64,
                           float* __restrict__ ke32) {
+    constexpr int KK = 9 * NPE * NPE;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= Ne) return;
-    double c[8];
-    for (int k = 0; k < npe; k++) {
-        const uint32_t n = elements[(size_t)e * npe + k];
+    double c[2 * NPE];
+#pragma unroll
+    for (int k = 0; k < NPE; k++) {
+        const uint32_t n = elements[(size_t)e * NPE + k];
         c[2 * k] = nodes[2 * n];
         c[2 * k + 1] = nodes[2 * n + 1];
     }
     const double te = elem_t ? (double)elem_t[e] : t;
-    double Ke[144];
-    const int kk = npe == 4 ? 144 : 81;
-    if (npe == 4)
+    double Ke[KK];
+    if constexpr (NPE == 4)
         q4_ke(c, E, nu, te, Ke);
     else
         dkt_ke(c, E, nu, te, Ke);
-    for (int i = 0; i < kk; i++) {
-        ke64[(size_t)e * kk + i] = Ke[i];
-        if (ke32) ke32[(size_t)e * kk + i] = (float)Ke[i];
+    for (int i = 0; i < KK; i++) {
+        ke64[(size_t)e * KK + i] = Ke[i];
+        if (ke32) ke32[(size_t)e * KK + i] = (float)Ke[i];
     }
 }
 
@@ -178,18 +196,16 @@ __global__ void bc_copy_kernel(int n, const uint8_t* __restrict__ cons,
 }
 
 // ---------------------------------------------------------------------------
-// grid-wide wait with a time limit
+// tagged exchange between blocks (no grid barrier)
 // ---------------------------------------------------------------------------
-
-__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
-    unsigned int v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void red_release_add(unsigned int* p, unsigned int v) {
-    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
+// A value a block publishes for other blocks is stored as 64-bit words
+// {32-bit payload, 32-bit round tag}; an aligned 64-bit store is
+// single-copy atomic, so a reader that sees the current round's tag also
+// sees that round's payload -- no fence, no arrival counter, no second
+// load.  FP64 values take two words (low and high halves).  Each block
+// waits only for the words it needs: every block's partial sums, and its
+// own ghosts' values.  Every wait has a time limit: past it the block
+// raises the abort flag and the kernel ends with PG_ETIMEOUT.
 
 __device__ __forceinline__ unsigned long long gtimer() {
     unsigned long long t;
@@ -197,31 +213,85 @@ __device__ __forceinline__ unsigned long long gtimer() {
     return t;
 }
 
-// Every block arrives once per wait; the wait ends when the arrival count
-// reaches target = waits_so_far * G.  A block that sees the abort flag, or
-// waits longer than timeout_ns, returns false (and raises the flag), so a
-// lost block ends the kernel with PG_ETIMEOUT instead of a hang.
-__device__ bool grid_wait(const PcgArgs& a, unsigned int target, int* s_flag) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        red_release_add(a.bar, 1u);
-        int ok = 1;
-        const unsigned long long t0 = gtimer();
-        while (ld_acquire(a.bar) < target) {
-            if (*(volatile int*)a.abort_flag) { ok = 0; break; }
-            if (gtimer() - t0 >= a.timeout_ns) {
-                atomicExch(a.abort_flag, 1);
-                atomicAdd(&a.res->wait_failures, 1);
-                ok = 0;
-                break;
-            }
-        }
-        __threadfence();
-        *s_flag = ok;
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+template <typename T>
+struct Tag;
+
+template <>
+struct Tag<float> {
+    static constexpr int W = 1;
+    __device__ static __forceinline__ void put(unsigned long long* p, float v, unsigned f) {
+        st_relaxed(p, ((unsigned long long)f << 32) | __float_as_uint(v));
     }
-    __syncthreads();
-    return *s_flag != 0;
+    __device__ static __forceinline__ bool get(const unsigned long long* p, unsigned f, float& v) {
+        const unsigned long long a = ld_relaxed(p);
+        if ((unsigned)(a >> 32) != f) return false;
+        v = __uint_as_float((unsigned)a);
+        return true;
+    }
+};
+
+template <>
+struct Tag<double> {
+    static constexpr int W = 2;
+    __device__ static __forceinline__ void put(unsigned long long* p, double v, unsigned f) {
+        const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+        st_relaxed(p, ((unsigned long long)f << 32) | (b & 0xffffffffull));
+        st_relaxed(p + 1, ((unsigned long long)f << 32) | (b >> 32));
+    }
+    __device__ static __forceinline__ bool get(const unsigned long long* p, unsigned f, double& v) {
+        const unsigned long long a = ld_relaxed(p), b = ld_relaxed(p + 1);
+        if ((unsigned)(a >> 32) != f || (unsigned)(b >> 32) != f) return false;
+        v = __longlong_as_double((long long)((b << 32) | (a & 0xffffffffull)));
+        return true;
+    }
+};
+
+// Time limit of one wait (a spin loop of one thread).  The clock starts at
+// the wait's first time check (after 32 failed reads), so a wait that is
+// already satisfied costs no timer read.
+struct Waiter {
+    unsigned long long t0, limit;
+    int* abort_flag;
+    int* failures;
+    unsigned spins;
+    __device__ __forceinline__ void start(unsigned long long lim, int* ab, int* fails) {
+        limit = lim;
+        abort_flag = ab;
+        failures = fails;
+        spins = 0;
+        t0 = 0;
+    }
+    // false when the wait must give up (time limit, or another block gave up)
+    __device__ __forceinline__ bool keep_going() {
+        if ((++spins & 31u) != 0) return true;
+        const unsigned long long now = gtimer();
+        if (spins == 32u) t0 = now;
+        if (*(volatile int*)abort_flag) return false;
+        if (now - t0 >= limit) {
+            atomicExch(abort_flag, 1);
+            atomicAdd(failures, 1);
+            return false;
+        }
+        return true;
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ bool poll(const unsigned long long* p, unsigned f, T& v, Waiter& wt) {
+    wt.spins = 0;
+    while (!Tag<T>::get(p, f, v))
+        if (!wt.keep_going()) return false;
+    return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -248,252 +318,517 @@ __device__ void block_sum(double (&v)[K], double* red) {
     __syncthreads();
 }
 
-// Sums slot values k < K over all G blocks; result in out[k] (shared).
-template <int K>
-__device__ void grid_sum(const double* __restrict__ slots, int G, double* out) {
-    if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        double v[K];
+// One exchange round, all threads of the block: waits for the K tagged
+// FP64 partial sums of every block (staged to sp[G * K]) and for the tagged
+// values of this block's ghost DOFs in vector buffer vb (written to
+// dst[3 * no .. 3 * nloc)).  Each thread keeps up to 4 loads in flight, so a
+// round costs about one L2 round trip.  Returns false if a wait gave up.
+template <typename T>
+__device__ bool exchange_round(const unsigned long long* __restrict__ pb, int G, int K,
+                               const unsigned long long* __restrict__ vb, T* dst, int no, int nloc,
+                               const int* __restrict__ gid, unsigned f, double* sp, Waiter& wt) {
+    constexpr int TW = Tag<T>::W;
+    const int np = G * K, n = np + 3 * (nloc - no);
+    for (int i0 = threadIdx.x; i0 < n; i0 += 4 * blockDim.x) {
+        const unsigned long long* ptr[4];
+        bool done[4];
 #pragma unroll
-        for (int k = 0; k < K; k++) v[k] = 0.0;
-        for (int b = lane; b < G; b += 32)
-#pragma unroll
-            for (int k = 0; k < K; k++) v[k] += __ldcg(slots + (size_t)b * 4 + k);
-#pragma unroll
-        for (int k = 0; k < K; k++)
-            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-        if (lane == 0)
-#pragma unroll
-            for (int k = 0; k < K; k++) out[k] = v[k];
-    }
-    __syncthreads();
-}
-
-// ---------------------------------------------------------------------------
-// element-by-element K.u for the owned rows of a block
-// ---------------------------------------------------------------------------
-
-__device__ __forceinline__ int sym_index(int i, int j, int nd) {
-    if (i > j) { const int t = i; i = j; j = t; }
-    return i * nd - (i * (i - 1)) / 2 + (j - i);
-}
-
-// y[owned dofs] += sum over part elements of Ke u_e, colour by colour; one
-// thread per (element, row); rows of ghost nodes are skipped.
-template <typename T, int NPE>
-__device__ void matvec_owned(const T* __restrict__ u, T* __restrict__ y, int no, int nel, int C,
-                             const int* __restrict__ coff, const int* __restrict__ ln,
-                             const T* __restrict__ kes, const T* __restrict__ keg,
-                             const int* __restrict__ elems, bool ks) {
-    constexpr int ND = 3 * NPE, KK = ND * ND;
-    for (int c = 0; c < C; c++) {
-        const int cs = coff[c], cnt = coff[c + 1] - cs;
-        for (int t = threadIdx.x; t < cnt * ND; t += blockDim.x) {
-            const int row = t / cnt, el = cs + (t - row * cnt);
-            const int rn = ln[el * NPE + row / 3];
-            if (rn >= no) continue;
-            int nn[NPE];
-#pragma unroll
-            for (int k = 0; k < NPE; k++) nn[k] = ln[el * NPE + k] * 3;
-            T acc = T(0);
-            if (ks) {
-#pragma unroll
-                for (int col = 0; col < ND; col++)
-                    acc += kes[sym_index(row, col, ND) * nel + el] * u[nn[col / 3] + col % 3];
+        for (int j = 0; j < 4; j++) {
+            const int i = i0 + j * (int)blockDim.x;
+            done[j] = i >= n;
+            if (done[j]) {
+                ptr[j] = nullptr;
+            } else if (i < np) {
+                ptr[j] = pb + (size_t)(i / K) * 8 + 2 * (i % K);
             } else {
-                const T* K = keg + (size_t)elems[el] * KK + row * ND;
-#pragma unroll
-                for (int col = 0; col < ND; col++) acc += __ldg(K + col) * u[nn[col / 3] + col % 3];
+                const int k = 3 * no + i - np;
+                ptr[j] = vb + (size_t)(3 * gid[k / 3] + k % 3) * TW;
             }
-            y[rn * 3 + row % 3] += acc;
         }
-        __syncthreads();
+        wt.spins = 0;
+        for (;;) {
+            unsigned long long lo[4], hi[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (done[j]) continue;
+                const int i = i0 + j * (int)blockDim.x;
+                lo[j] = ld_relaxed(ptr[j]);
+                hi[j] = (i < np || TW == 2) ? ld_relaxed(ptr[j] + 1) : lo[j];
+            }
+            bool all = true;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (done[j]) continue;
+                const int i = i0 + j * (int)blockDim.x;
+                if ((unsigned)(lo[j] >> 32) != f || (unsigned)(hi[j] >> 32) != f) {
+                    all = false;
+                    continue;
+                }
+                done[j] = true;
+                const double dv =
+                    __longlong_as_double((long long)((hi[j] << 32) | (lo[j] & 0xffffffffull)));
+                if (i < np) {
+                    sp[i] = dv;
+                } else {
+                    const int k = 3 * no + i - np;
+                    if constexpr (TW == 2)
+                        dst[k] = (T)dv;
+                    else
+                        dst[k] = (T)__uint_as_float((unsigned)lo[j]);
+                }
+            }
+            if (all) break;
+            if (!wt.keep_going()) return false;
+        }
     }
+    return true;
+}
+
+// Warp 0: adds the staged partials sp[G][K] in block order (the same bits
+// in every block) into out[K].
+template <int K>
+__device__ __forceinline__ void sum_partials(const double* __restrict__ sp, int G, double* out) {
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = 0.0;
+    for (int b = lane; b < G; b += 32)
+#pragma unroll
+        for (int k = 0; k < K; k++) v[k] += sp[b * K + k];
+#pragma unroll
+    for (int k = 0; k < K; k++)
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; k++) out[k] = v[k];
 }
 
 // ---------------------------------------------------------------------------
-// persistent PCG (FP64)
+// task matvec: the owned rows of K u, one (element, owned node) per thread
+// ---------------------------------------------------------------------------
+
+// Task block layout: entry (row r of the node, column c of the rotated
+// element) of task t sits at kt[(r * ND + c) * stride + t], so consecutive
+// threads read consecutive words.  Task node ids sit at tn[j * ntask + t].
+template <int NPE, typename T, typename KT>
+__device__ __forceinline__ void task_matvec(const T* __restrict__ u, T* __restrict__ yt, int ntask,
+                                            const uint16_t* __restrict__ tn,
+                                            const KT* __restrict__ kt, size_t stride) {
+    constexpr int ND = 3 * NPE;
+    for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
+        T a0 = T(0), a1 = T(0), a2 = T(0);
+#pragma unroll
+        for (int j = 0; j < NPE; j++) {
+            const int b = 3 * (int)tn[j * ntask + t];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const T v = u[b + d];
+                const int c = 3 * j + d;
+                a0 += (T)kt[(size_t)(0 * ND + c) * stride + t] * v;
+                a1 += (T)kt[(size_t)(1 * ND + c) * stride + t] * v;
+                a2 += (T)kt[(size_t)(2 * ND + c) * stride + t] * v;
+            }
+        }
+        yt[t] = a0;
+        yt[ntask + t] = a1;
+        yt[2 * ntask + t] = a2;
+    }
+}
+
+// Task blocks of every task from the element matrices (setup, per solve):
+// the owned node's 3 rows, columns rotated to start at the owned node.
+template <int NPE>
+__global__ void task_ke_kernel(int NT, const int* __restrict__ task_elem,
+                               const uint8_t* __restrict__ task_pos,
+                               const double* __restrict__ ke64, double* __restrict__ kt64,
+                               float* __restrict__ kt32) {
+    constexpr int ND = 3 * NPE, KK = ND * ND;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= NT) return;
+    const int e = task_elem[t], k = task_pos[t];
+    const double* K = ke64 + (size_t)e * KK;
+    for (int r = 0; r < 3; r++)
+        for (int j = 0; j < NPE; j++)
+            for (int d = 0; d < 3; d++) {
+                const double v = K[(3 * k + r) * ND + 3 * ((k + j) % NPE) + d];
+                const size_t o = (size_t)(r * ND + 3 * j + d) * NT + t;
+                kt64[o] = v;
+                if (kt32) kt32[o] = (float)v;
+            }
+}
+
+// ---------------------------------------------------------------------------
+// persistent PCG
 // ---------------------------------------------------------------------------
 
 enum { STOP_CONVERGED = 0, STOP_MAX_ITER = 1, STOP_BREAKDOWN = 2, STOP_ZERO_RHS = 3 };
 enum { ST_OK = 0, ST_TIMEOUT = 4, ST_NONFINITE = 5 };
 
-template <int NPE>
-__global__ void __launch_bounds__(512, 1) pcg_fp64_kernel(PcgArgs a) {
-    constexpr int ND = 3 * NPE;
-    extern __shared__ __align__(16) unsigned char smem[];
+constexpr int kMaxThreads = 640;
+
+// Per-phase SM cycles of block 0, when timing is requested.
+struct PhaseClock {
+    bool on;
+    long long last, t0, t1, t2, t3;
+    __device__ __forceinline__ void start(bool enable) {
+        on = enable;
+        t0 = t1 = t2 = t3 = 0;
+        last = on ? clock64() : 0;
+    }
+    __device__ __forceinline__ void lap(int k) {
+        if (!on) return;
+        const long long now = clock64();
+        const long long d = now - last;
+        last = now;
+        if (k == 0) t0 += d;
+        else if (k == 1) t1 += d;
+        else if (k == 2) t2 += d;
+        else t3 += d;
+    }
+};
+
+// Owned-node gather of task results: w_n = sum of the node's task rows.
+template <typename T>
+__device__ __forceinline__ void gather3(const T* __restrict__ yt, int ntask, int ta, int tb,
+                                        T& w0, T& w1, T& w2) {
+    w0 = T(0);
+    w1 = T(0);
+    w2 = T(0);
+    for (int t = ta; t < tb; t++) {
+        w0 += yt[t];
+        w1 += yt[ntask + t];
+        w2 += yt[2 * ntask + t];
+    }
+}
+
+__device__ __forceinline__ void block_jacobi3(const float* Bn, const float* rv, float* u) {
+    u[0] = Bn[0] * rv[0] + Bn[1] * rv[1] + Bn[2] * rv[2];
+    u[1] = Bn[3] * rv[0] + Bn[4] * rv[1] + Bn[5] * rv[2];
+    u[2] = Bn[6] * rv[0] + Bn[7] * rv[1] + Bn[8] * rv[2];
+}
+__device__ __forceinline__ void block_jacobi3(const double* Bn, const double* rv, double* u) {
+    u[0] = Bn[0] * rv[0] + Bn[1] * rv[1] + Bn[2] * rv[2];
+    u[1] = Bn[3] * rv[0] + Bn[4] * rv[1] + Bn[5] * rv[2];
+    u[2] = Bn[6] * rv[0] + Bn[7] * rv[1] + Bn[8] * rv[2];
+}
+
+// The whole PCG solve.  T = double: plain FP64.  T = float (MIXED): inner
+// iterations in FP32 with FP64 dot products, FP64 solution x, and FP64
+// true-residual replacement r = F - K x ("reliable update") whenever the
+// recursive residual has fallen by reliable_delta, after reliable_interval
+// updates, or when it meets the tolerance (convergence is then decided on
+// the true residual).
+//
+// Exchange rounds: round e (e = 1, 2, ...) carries every block's partial
+// sums and the owners' values of one vector (w, or the replaced r), in
+// buffers [e & 1]; x rounds (for the FP64 residual) use their own tags.
+// A block overwrites buffer [e & 1] only after it has seen every block's
+// round e - 1 partials, and every block reads round e - 2 before it
+// publishes round e - 1, so no reader can still need the old values.
+template <int NPE, typename T, bool MIXED>
+__global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
+    constexpr int ND = 3 * NPE, TW = Tag<T>::W;
+    extern __shared__ __align__(16) unsigned char sm[];
+    const SmemLayout& L = a.L;
     const int g = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
     const int n0 = a.node_off[g], nloc = a.node_off[g + 1] - n0, no = a.nown[g];
-    const int e0 = a.elem_off[g], nel = a.elem_off[g + 1] - e0;
-    const int C = a.C;
-    const int* __restrict__ gnodes = a.nodes + n0;
-    const int* __restrict__ gelems = a.elems + e0;
+    const int t0 = a.task_off[g], ntask = a.task_off[g + 1] - t0;
+    const size_t N3 = 3 * (size_t)a.Nn;
 
-    // shared-memory carve-up (doubles first, then ints and bytes)
-    double* r = (double*)smem;
-    double* u = r + 3 * a.sm_nloc;
-    double* p = u + 3 * a.sm_nloc;
-    double* s = p + 3 * a.sm_nloc;
-    double* w = s + 3 * a.sm_nloc;
-    double* x = w + 3 * a.sm_nloc;
-    double* bi = x + 3 * a.sm_nown;
-    double* red = bi + 9 * a.sm_nloc;
-    double* scal = red + 32 * 4;
-    double* kes = scal + 8;
-    int* ln = (int*)(kes + (a.ke_smem ? (size_t)a.sm_nel * (ND * (ND + 1) / 2) : 0));
-    int* coff = ln + NPE * a.sm_nel;
-    int* iflag = coff + (C + 1);
-    unsigned char* cm = (unsigned char*)(iflag + 4);
+    T* r = (T*)(sm + L.r);
+    T* u = (T*)(sm + L.u);
+    T* p = (T*)(sm + L.p);
+    T* s = (T*)(sm + L.s);
+    T* w = (T*)(sm + L.w);
+    T* B = (T*)(sm + L.B);
+    T* yt = (T*)(sm + L.yt);
+    T* kts = (T*)(sm + L.kt);
+    double* x = (double*)(sm + L.x);
+    double* red = (double*)(sm + L.red);
+    double* scal = (double*)(sm + L.scal);
+    double* sp = (double*)(sm + L.sp);
+    int* gid = (int*)(sm + L.gid);
+    int* tptr = (int*)(sm + L.tptr);
+    uint16_t* tn = (uint16_t*)(sm + L.tnode);
+    unsigned char* cm = (unsigned char*)(sm + L.cm);
+    // FP64 views for the true residual: dedicated arrays in MIXED mode,
+    // the (then dead) p / yt arrays in FP64 mode
+    double* xl = MIXED ? (double*)(sm + L.xl) : (double*)p;
+    double* ytd = MIXED ? (double*)(sm + L.ytd) : (double*)yt;
+    const T* ktg = MIXED ? (const T*)a.kt32 : (const T*)a.kt64;
+    const T* Bg = MIXED ? (const T*)a.binv32 : (const T*)a.binv64;
 
     // ---- load the part ----
-    for (int k = tid; k < 3 * nloc; k += nt) {
-        const int gd = gnodes[k / 3] * 3 + k % 3;
-        const unsigned char c = a.cons[gd];
-        cm[k] = c;
-        r[k] = c ? 0.0 : (double)a.F[gd];
-        p[k] = 0.0;
-        s[k] = 0.0;
-        if (k < 3 * no) x[k] = 0.0;
+    for (int i = tid; i < nloc; i += nt) gid[i] = a.nodes[n0 + i];
+    for (int i = tid; i <= no; i += nt) tptr[i] = a.tptr[a.tp_off[g] + i];
+    for (int i = tid; i < NPE * ntask; i += nt) {
+        const int t = i % ntask, j = i / ntask;
+        tn[i] = a.task_nodes[(size_t)(t0 + t) * NPE + j];
     }
-    for (int k = tid; k < 9 * nloc; k += nt) bi[k] = a.binv64[(size_t)gnodes[k / 9] * 9 + k % 9];
-    for (int k = tid; k < NPE * nel; k += nt) ln[k] = a.lnode[(size_t)e0 * NPE + k];
-    for (int k = tid; k <= C; k += nt) coff[k] = a.color_off[(size_t)g * (C + 1) + k] - e0;
-    if (a.ke_smem) {
-        constexpr int NS = ND * (ND + 1) / 2;
-        for (int k = tid; k < NS * nel; k += nt) {
-            const int el = k % nel, q = k / nel;
-            int i = 0, rem = q;
-            while (rem >= ND - i) { rem -= ND - i; i++; }
-            kes[k] = a.ke64[(size_t)gelems[el] * ND * ND + i * ND + i + rem];
+    if (a.ke_smem)
+        for (int i = tid; i < 3 * ND * ntask; i += nt) {
+            const int t = i % ntask, q = i / ntask;
+            kts[i] = ktg[(size_t)q * a.NT + t0 + t];
         }
-    }
     __syncthreads();
-    for (int nd = tid; nd < nloc; nd += nt) {
-        const double* B = bi + 9 * nd;
-        const double r0 = r[3 * nd], r1 = r[3 * nd + 1], r2 = r[3 * nd + 2];
-        u[3 * nd] = B[0] * r0 + B[1] * r1 + B[2] * r2;
-        u[3 * nd + 1] = B[3] * r0 + B[4] * r1 + B[5] * r2;
-        u[3 * nd + 2] = B[6] * r0 + B[7] * r1 + B[8] * r2;
+    for (int n = tid; n < nloc; n += nt) {
+        const int G3 = 3 * gid[n];
+        T rv[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const unsigned char c = a.cons[G3 + d];
+            cm[3 * n + d] = c;
+            rv[d] = c ? T(0) : (T)a.F[G3 + d];
+            r[3 * n + d] = rv[d];
+            p[3 * n + d] = T(0);
+            s[3 * n + d] = T(0);
+            if (n < no) x[3 * n + d] = 0.0;
+        }
+        T* Bn = B + 9 * n;
+#pragma unroll
+        for (int q = 0; q < 9; q++) Bn[q] = Bg[(size_t)gid[n] * 9 + q];
+        block_jacobi3(Bn, rv, u + 3 * n);
     }
     __syncthreads();
 
-    double gamma_prev = 1.0, alpha_prev = 1.0, bnorm = 0.0;
-    unsigned int waits = 0;
-    int it = 0, par = 0, stop = -1, status = ST_OK, iters = 0;
-    double final_res = 0.0;
+    const T* kt = a.ke_smem ? kts : ktg + t0;
+    const size_t kstride = a.ke_smem ? (size_t)ntask : (size_t)a.NT;
+    PhaseClock clk;
+    clk.start(a.timing && g == 0 && tid == 0);
+    Waiter wt;
+    wt.start(a.timeout_ns, a.abort_flag, &a.res->wait_failures);
+
+    double gamma_prev = 1.0, alpha_prev = 1.0, bnorm = 0.0, rn_ref = 0.0;
+    unsigned e = 1, xe = 1;  // round tags
+    int it = 0, stop = -1, status = ST_OK, xupd = 0, xupd_ref = 0, nru = 0;
+    double final_res = 0.0, true_rel = -1.0;
+    bool first = true;
 
     for (;; it++) {
         // ---- w = A u on owned rows ----
-        for (int k = tid; k < 3 * no; k += nt) w[k] = 0.0;
+        task_matvec<NPE, T, T>(u, yt, ntask, tn, kt, kstride);
         __syncthreads();
-        matvec_owned<double, NPE>(u, w, no, nel, C, coff, ln, kes, a.ke64, gelems, a.ke_smem != 0);
+        clk.lap(0);
+        // ---- gather, BC rows, dot products, publish w ----
         double v[3] = {0.0, 0.0, 0.0};
-        double* xo = a.xch64 + (size_t)par * 3 * a.Nn;
-        for (int k = tid; k < 3 * no; k += nt) {
-            if (cm[k]) w[k] = u[k];
-            v[0] += r[k] * u[k];
-            v[1] += w[k] * u[k];
-            v[2] += r[k] * r[k];
-            __stcg(xo + gnodes[k / 3] * 3 + k % 3, w[k]);
+        unsigned long long* vb = a.llv + (size_t)(e & 1) * N3 * 2;
+        unsigned long long* pb = a.llp + (size_t)(e & 1) * a.G * 8;
+        for (int n = tid; n < no; n += nt) {
+            T wv[3];
+            gather3(yt, ntask, tptr[n], tptr[n + 1], wv[0], wv[1], wv[2]);
+            const int G3 = 3 * gid[n];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const int k = 3 * n + d;
+                if (cm[k]) wv[d] = u[k];
+                w[k] = wv[d];
+                v[0] += (double)r[k] * (double)u[k];
+                v[1] += (double)wv[d] * (double)u[k];
+                v[2] += (double)r[k] * (double)r[k];
+                Tag<T>::put(vb + (size_t)(G3 + d) * TW, wv[d], e);
+            }
         }
         block_sum<3>(v, red);
-        if (tid == 0) {
-            double* slot = a.partials + ((size_t)par * a.G + g) * 4;
-            __stcg(slot, v[0]);
-            __stcg(slot + 1, v[1]);
-            __stcg(slot + 2, v[2]);
+        if (tid == 0)
+#pragma unroll
+            for (int k = 0; k < 3; k++) Tag<double>::put(pb + (size_t)g * 8 + 2 * k, v[k], e);
+        clk.lap(1);
+        // ---- exchange: every block's partials and this block's ghost w ----
+        {
+            bool ok = exchange_round<T>(pb, a.G, 3, vb, w, no, nloc, gid, e, sp, wt);
+            if (a.test_stall && it == 0 && tid == 0) {
+                double never;  // a tag no block writes: the wait must run out
+                ok = ok && poll<double>(a.llp + (size_t)a.G * 16, 0xffffffffu, never, wt);
+            }
+            if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
+            sum_partials<3>(sp, a.G, scal);
+            __syncthreads();
         }
-        if (!grid_wait(a, (++waits) * a.G, iflag)) { status = ST_TIMEOUT; break; }
-        grid_sum<3>(a.partials + (size_t)par * a.G * 4, a.G, scal);
+        e++;
+        clk.lap(2);
         const double gamma = scal[0], delta = scal[1], rho = scal[2];
 
         // ---- decisions (identical in every block) ----
-        const double rn = sqrt(rho);
-        if (!isfinite(gamma) || !isfinite(delta) || !isfinite(rho)) { status = ST_NONFINITE; break; }
-        if (it == 0) {
-            bnorm = rn;
-            if (bnorm < 1e-30) { stop = STOP_ZERO_RHS; iters = 0; final_res = 0.0; break; }
-        } else if ((a.stop_rule == 0 && rn < a.tol) || rn / bnorm < a.tol) {
-            stop = STOP_CONVERGED; iters = it; final_res = rn; break;
+        if (!isfinite(gamma) || !isfinite(delta) || !isfinite(rho)) {
+            if (g == 0 && tid == 0) {
+                a.res->nonfinite_it = it;
+                a.res->nonfinite_vals[0] = gamma;
+                a.res->nonfinite_vals[1] = delta;
+                a.res->nonfinite_vals[2] = rho;
+            }
+            status = ST_NONFINITE;
+            break;
         }
-        if (it >= a.maxit) { stop = STOP_MAX_ITER; iters = it; final_res = rn; break; }
-        const double beta = it == 0 ? 0.0 : gamma / gamma_prev;
-        const double pap = it == 0 ? delta : delta - beta * gamma / alpha_prev;
-        if (fabs(pap) < 1e-30) { stop = STOP_BREAKDOWN; iters = it + 1; final_res = rn; break; }
+        const double rn = sqrt(rho);
+        if (first) {
+            bnorm = rn;
+            rn_ref = rn;
+            if (bnorm < 1e-30) { stop = STOP_ZERO_RHS; final_res = 0.0; true_rel = 0.0; break; }
+        } else {
+            const bool conv = (a.stop_rule == 0 && rn < a.tol) || rn / bnorm < a.tol;
+            if constexpr (MIXED) {
+                const bool want = conv || rn <= a.reliable_delta * rn_ref ||
+                                  xupd - xupd_ref >= a.reliable_interval;
+                if (want) {
+                    // ---- reliable update: r = F - K x in FP64 ----
+                    for (int n = tid; n < no; n += nt)
+#pragma unroll
+                        for (int d = 0; d < 3; d++)
+                            Tag<double>::put(a.llx + (size_t)(3 * gid[n] + d) * 2, x[3 * n + d], xe);
+                    bool ok = true;
+                    for (int k = tid; k < 3 * nloc && ok; k += nt) {
+                        if (k < 3 * no) { xl[k] = x[k]; continue; }
+                        double xv;
+                        ok = poll<double>(a.llx + (size_t)(3 * gid[k / 3] + k % 3) * 2, xe, xv, wt);
+                        xl[k] = xv;
+                    }
+                    if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
+                    xe++;
+                    task_matvec<NPE, double, double>(xl, ytd, ntask, tn, a.kt64 + t0, (size_t)a.NT);
+                    __syncthreads();
+                    double vt[1] = {0.0};
+                    unsigned long long* rb = a.llv + (size_t)(e & 1) * N3 * 2;
+                    unsigned long long* qb = a.llp + (size_t)(e & 1) * a.G * 8;
+                    for (int n = tid; n < no; n += nt) {
+                        double kx[3];
+                        gather3(ytd, ntask, tptr[n], tptr[n + 1], kx[0], kx[1], kx[2]);
+                        const int G3 = 3 * gid[n];
+#pragma unroll
+                        for (int d = 0; d < 3; d++) {
+                            const int k = 3 * n + d;
+                            const double rt = cm[k] ? -xl[k] : (double)a.F[G3 + d] - kx[d];
+                            vt[0] += rt * rt;
+                            r[k] = (T)rt;
+                            Tag<T>::put(rb + (size_t)(G3 + d) * TW, (T)rt, e);
+                        }
+                    }
+                    block_sum<1>(vt, red);
+                    if (tid == 0) Tag<double>::put(qb + (size_t)g * 8, vt[0], e);
+                    ok = exchange_round<T>(qb, a.G, 1, rb, r, no, nloc, gid, e, sp, wt);
+                    if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
+                    sum_partials<1>(sp, a.G, scal);
+                    __syncthreads();
+                    e++;
+                    const double trn = sqrt(scal[0]);
+                    for (int n = tid; n < nloc; n += nt) block_jacobi3(B + 9 * n, r + 3 * n, u + 3 * n);
+                    __syncthreads();
+                    nru++;
+                    rn_ref = trn;
+                    xupd_ref = xupd;
+                    if (!isfinite(trn)) { status = ST_NONFINITE; break; }
+                    if ((a.stop_rule == 0 && trn < a.tol) || trn / bnorm < a.tol) {
+                        stop = STOP_CONVERGED; final_res = trn; true_rel = trn / bnorm; break;
+                    }
+                    if (xupd >= a.maxit) { stop = STOP_MAX_ITER; final_res = trn; true_rel = trn / bnorm; break; }
+                    clk.lap(3);
+                    continue;
+                }
+            } else {
+                if (conv) { stop = STOP_CONVERGED; final_res = rn; break; }
+            }
+        }
+        if (xupd >= a.maxit) { stop = STOP_MAX_ITER; final_res = rn; break; }
+        const double beta = first ? 0.0 : gamma / gamma_prev;
+        const double pap = first ? delta : delta - beta * gamma / alpha_prev;
+        if (fabs(pap) < 1e-30) { stop = STOP_BREAKDOWN; xupd++; final_res = rn; break; }
         const double alpha = gamma / pap;
         gamma_prev = gamma;
         alpha_prev = alpha;
+        first = false;
 
-        // ---- ghost w from their owners ----
-        for (int k = 3 * no + tid; k < 3 * nloc; k += nt) w[k] = __ldcg(xo + gnodes[k / 3] * 3 + k % 3);
-        __syncthreads();
-        // ---- vector updates on owned and ghost DOFs ----
-        for (int k = tid; k < 3 * nloc; k += nt) {
-            const double pk = u[k] + beta * p[k];
-            const double sk = w[k] + beta * s[k];
-            p[k] = pk;
-            s[k] = sk;
-            if (k < 3 * no) x[k] += alpha * pk;
-            r[k] -= alpha * sk;
+        // ---- p, s, x, r updates and u = M^-1 r on owned and ghost nodes ----
+        const T bt = (T)beta, at = (T)alpha;
+        for (int n = tid; n < nloc; n += nt) {
+            T rv[3];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const int k = 3 * n + d;
+                const T pk = u[k] + bt * p[k];
+                const T sk = w[k] + bt * s[k];
+                p[k] = pk;
+                s[k] = sk;
+                if (n < no) x[k] += alpha * (double)pk;
+                rv[d] = r[k] - at * sk;
+                r[k] = rv[d];
+            }
+            block_jacobi3(B + 9 * n, rv, u + 3 * n);
         }
         __syncthreads();
-        for (int nd = tid; nd < nloc; nd += nt) {
-            const double* B = bi + 9 * nd;
-            const double r0 = r[3 * nd], r1 = r[3 * nd + 1], r2 = r[3 * nd + 2];
-            u[3 * nd] = B[0] * r0 + B[1] * r1 + B[2] * r2;
-            u[3 * nd + 1] = B[3] * r0 + B[4] * r1 + B[5] * r2;
-            u[3 * nd + 2] = B[6] * r0 + B[7] * r1 + B[8] * r2;
-        }
-        __syncthreads();
-        par ^= 1;
+        xupd++;
+        clk.lap(3);
     }
 
-    // ---- write x; FP64 true residual F - K x ----
-    for (int k = tid; k < 3 * no; k += nt) a.x[gnodes[k / 3] * 3 + k % 3] = x[k];
-    if (status == ST_OK) {
-        par ^= 1;
-        double* xo = a.xch64 + (size_t)par * 3 * a.Nn;
-        for (int k = tid; k < 3 * no; k += nt) __stcg(xo + gnodes[k / 3] * 3 + k % 3, x[k]);
-        if (!grid_wait(a, (++waits) * a.G, iflag)) {
+    // ---- write x; FP64 true residual ||F - K x|| unless already known ----
+    for (int n = tid; n < no; n += nt)
+#pragma unroll
+        for (int d = 0; d < 3; d++) a.x[3 * gid[n] + d] = x[3 * n + d];
+    if (status == ST_OK && true_rel < 0.0) {
+        for (int n = tid; n < no; n += nt)
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+                Tag<double>::put(a.llx + (size_t)(3 * gid[n] + d) * 2, x[3 * n + d], xe);
+        bool ok = true;
+        for (int k = tid; k < 3 * nloc && ok; k += nt) {
+            if (k < 3 * no) { xl[k] = x[k]; continue; }
+            double xv;
+            ok = poll<double>(a.llx + (size_t)(3 * gid[k / 3] + k % 3) * 2, xe, xv, wt);
+            xl[k] = xv;
+        }
+        if (__syncthreads_or(!ok)) {
             status = ST_TIMEOUT;
         } else {
-            // p <- x on owned and ghost DOFs
-            for (int k = tid; k < 3 * nloc; k += nt)
-                p[k] = k < 3 * no ? x[k] : __ldcg(xo + gnodes[k / 3] * 3 + k % 3);
-            for (int k = tid; k < 3 * no; k += nt) w[k] = 0.0;
+            if (MIXED || !a.ke_smem)
+                task_matvec<NPE, double, double>(xl, ytd, ntask, tn, a.kt64 + t0, (size_t)a.NT);
+            else
+                task_matvec<NPE, double, double>(xl, ytd, ntask, tn, (const double*)kts, (size_t)ntask);
             __syncthreads();
-            matvec_owned<double, NPE>(p, w, no, nel, C, coff, ln, kes, a.ke64, gelems, a.ke_smem != 0);
             double v[2] = {0.0, 0.0};
-            for (int k = tid; k < 3 * no; k += nt) {
-                const double f = cm[k] ? 0.0 : (double)a.F[gnodes[k / 3] * 3 + k % 3];
-                const double kx = cm[k] ? p[k] : w[k];
-                const double d = (cm[k] ? 0.0 : f) - (cm[k] ? kx : w[k]);
-                v[0] += d * d;
-                v[1] += f * f;
+            for (int n = tid; n < no; n += nt) {
+                double kx[3];
+                gather3(ytd, ntask, tptr[n], tptr[n + 1], kx[0], kx[1], kx[2]);
+                const int G3 = 3 * gid[n];
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const int k = 3 * n + d;
+                    const double f = cm[k] ? 0.0 : (double)a.F[G3 + d];
+                    const double rt = cm[k] ? -xl[k] : f - kx[d];
+                    v[0] += rt * rt;
+                    v[1] += f * f;
+                }
             }
             block_sum<2>(v, red);
-            double* slots = a.partials + (size_t)par * a.G * 4;
+            unsigned long long* pb = a.llp + (size_t)(e & 1) * a.G * 8;
             if (tid == 0) {
-                __stcg(slots + (size_t)g * 4, v[0]);
-                __stcg(slots + (size_t)g * 4 + 1, v[1]);
+                Tag<double>::put(pb + (size_t)g * 8, v[0], e);
+                Tag<double>::put(pb + (size_t)g * 8 + 2, v[1], e);
             }
-            if (!grid_wait(a, (++waits) * a.G, iflag)) {
-                status = ST_TIMEOUT;
-            } else if (g == 0) {
-                grid_sum<2>(slots, a.G, scal);
-                if (tid == 0) {
-                    a.res->true_rel_residual = scal[1] > 0 ? sqrt(scal[0] / scal[1]) : 0.0;
+            if (g == 0) {
+                ok = exchange_round<T>(pb, a.G, 2, nullptr, w, no, no, gid, e, sp, wt);
+                if (__syncthreads_or(!ok)) {
+                    status = ST_TIMEOUT;
+                } else {
+                    sum_partials<2>(sp, a.G, scal);
+                    __syncthreads();
+                    if (tid == 0) true_rel = scal[1] > 0 ? sqrt(scal[0] / scal[1]) : 0.0;
                 }
             }
         }
     }
     if (g == 0 && tid == 0) {
         a.res->status = status;
-        a.res->iterations = iters;
+        a.res->iterations = xupd;
         a.res->converged = (stop == STOP_CONVERGED || stop == STOP_ZERO_RHS) ? 1 : 0;
         a.res->stop_reason = stop < 0 ? STOP_MAX_ITER : stop;
         a.res->final_residual = final_res;
+        a.res->true_rel_residual = true_rel < 0.0 ? 0.0 : true_rel;
         a.res->b_norm = bnorm;
+        a.res->reliable_updates = nru;
+        a.res->reductions = (int)e - 1;
+        a.res->phase_cycles[0] = clk.t0;
+        a.res->phase_cycles[1] = clk.t1;
+        a.res->phase_cycles[2] = clk.t2;
+        a.res->phase_cycles[3] = clk.t3;
     }
 }
 

@@ -129,102 +129,121 @@ std::string build_structure(const pg_problem& p, HostPlan& plan) {
 
 namespace {
 
-void rcb(int* ids, int n, int parts, int base, const float* xy, std::vector<int>& part_of) {
-    if (parts <= 1 || n <= 1) {
-        for (int i = 0; i < n; i++) part_of[ids[i]] = base;
-        return;
-    }
+// Near-square partition of a node cloud into G parts (see plan.h).
+void strip_partition(const float* xy, int Nn, int G, std::vector<int>& part_of) {
+    part_of.assign(Nn, 0);
+    if (G <= 1 || Nn == 0) return;
     float lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
-    for (int i = 0; i < n; i++)
+    for (int n = 0; n < Nn; n++)
         for (int d = 0; d < 2; d++) {
-            lo[d] = std::min(lo[d], xy[2 * ids[i] + d]);
-            hi[d] = std::max(hi[d], xy[2 * ids[i] + d]);
+            lo[d] = std::min(lo[d], xy[2 * n + d]);
+            hi[d] = std::max(hi[d], xy[2 * n + d]);
         }
-    const int ax = (hi[0] - lo[0] >= hi[1] - lo[1]) ? 0 : 1;
-    const int p1 = parts / 2;
-    const int n1 = (int)((long long)n * p1 / parts);
-    std::nth_element(ids, ids + n1, ids + n, [&](int a, int b) {
-        float va = xy[2 * a + ax], vb = xy[2 * b + ax];
-        return va < vb || (va == vb && a < b);
-    });
-    rcb(ids, n1, p1, base, xy, part_of);
-    rcb(ids + n1, n - n1, parts - p1, base + p1, xy, part_of);
+    const double W = std::max(1e-30, (double)hi[0] - lo[0]), H = std::max(1e-30, (double)hi[1] - lo[1]);
+    int R = (int)std::lround(std::sqrt((double)G * H / W));
+    R = std::max(1, std::min(R, G));
+    std::vector<int> ids(Nn);
+    std::iota(ids.begin(), ids.end(), 0);
+    auto by = [&](int a, int b) {
+        const float ya = xy[2 * a + 1], yb = xy[2 * b + 1];
+        if (ya != yb) return ya < yb;
+        const float xa = xy[2 * a], xb = xy[2 * b];
+        return xa < xb || (xa == xb && a < b);
+    };
+    auto bx = [&](int a, int b) {
+        const float xa = xy[2 * a], xb = xy[2 * b];
+        if (xa != xb) return xa < xb;
+        const float ya = xy[2 * a + 1], yb = xy[2 * b + 1];
+        return ya < yb || (ya == yb && a < b);
+    };
+    std::sort(ids.begin(), ids.end(), by);
+    int part = 0;
+    long long done_blocks = 0;
+    int start = 0;
+    for (int s = 0; s < R; s++) {
+        const int blocks = G / R + (s < G % R ? 1 : 0);
+        done_blocks += blocks;
+        const int end = (int)((long long)Nn * done_blocks / G);
+        std::sort(ids.begin() + start, ids.begin() + end, bx);
+        const int len = end - start;
+        for (int b = 0; b < blocks; b++) {
+            const int b0 = start + (int)((long long)len * b / blocks);
+            const int b1 = start + (int)((long long)len * (b + 1) / blocks);
+            for (int i = b0; i < b1; i++) part_of[ids[i]] = part;
+            part++;
+        }
+        start = end;
+    }
 }
 
 }  // namespace
 
 std::string build_partition(const pg_problem& p, int G, HostPlan& plan) {
-    const int Nn = plan.Nn, npe = plan.npe, C = plan.colors;
+    const int Nn = plan.Nn, npe = plan.npe;
     if (G < 1) G = 1;
     if (G > std::max(Nn, 1)) G = std::max(Nn, 1);
     plan.G = G;
-    std::vector<int> part_of(Nn, 0), ids(Nn);
-    std::iota(ids.begin(), ids.end(), 0);
-    rcb(ids.data(), Nn, G, 0, p.nodes, part_of);
-
-    std::vector<int> elem_color(plan.Ne, 0);
-    for (int c = 0; c < C; c++)
-        for (uint32_t q = plan.color_offsets[c]; q < plan.color_offsets[c + 1]; q++)
-            elem_color[plan.elements_by_color[q]] = c;
+    std::vector<int> part_of;
+    strip_partition(p.nodes, Nn, G, part_of);
 
     std::vector<std::vector<int>> owned(G);
     for (int n = 0; n < Nn; n++) owned[part_of[n]].push_back(n);
 
     plan.node_off.assign(G + 1, 0);
     plan.nown.assign(G, 0);
-    plan.elem_off.assign(G + 1, 0);
-    plan.color_off.assign((size_t)G * (C + 1), 0);
+    plan.task_off.assign(G + 1, 0);
+    plan.tp_off.assign(G + 1, 0);
     plan.nodes.clear();
-    plan.elems.clear();
-    plan.lnode.clear();
-    plan.max_nloc = plan.max_nown = plan.max_nel = 0;
+    plan.task_elem.clear();
+    plan.task_pos.clear();
+    plan.task_nodes.clear();
+    plan.tptr.clear();
+    plan.max_nloc = plan.max_nown = plan.max_ntask = 0;
 
-    std::vector<int> estamp(plan.Ne, -1), local(Nn, -1);
-    std::vector<int> pel, ghosts;
+    std::vector<int> local(Nn, -1), ghosts;
     for (int g = 0; g < G; g++) {
         const std::vector<int>& own = owned[g];
-        pel.clear();
-        for (int n : own)
-            for (int q = plan.inc_ptr[n]; q < plan.inc_ptr[n + 1]; q++) {
-                int e = plan.inc_idx[q] / 4;
-                if (estamp[e] != g) { estamp[e] = g; pel.push_back(e); }
-            }
-        std::sort(pel.begin(), pel.end(), [&](int a, int b) {
-            return elem_color[a] < elem_color[b] || (elem_color[a] == elem_color[b] && a < b);
-        });
         for (size_t i = 0; i < own.size(); i++) local[own[i]] = (int)i;
         ghosts.clear();
-        for (int e : pel)
-            for (int k = 0; k < npe; k++) {
-                int n = (int)p.elements[(size_t)e * npe + k];
-                if (part_of[n] != g && local[n] < 0) { local[n] = -2; ghosts.push_back(n); }
+        for (int n : own)
+            for (int q = plan.inc_ptr[n]; q < plan.inc_ptr[n + 1]; q++) {
+                const int e = plan.inc_idx[q] / 4;
+                for (int k = 0; k < npe; k++) {
+                    const int m = (int)p.elements[(size_t)e * npe + k];
+                    if (local[m] == -1) { local[m] = -2; ghosts.push_back(m); }
+                }
             }
         std::sort(ghosts.begin(), ghosts.end());
         for (size_t i = 0; i < ghosts.size(); i++) local[ghosts[i]] = (int)(own.size() + i);
+        const int nloc = (int)(own.size() + ghosts.size());
+        if (nloc > 65535) return "a part has more than 65535 local nodes: use more ctas";
 
         plan.nown[g] = (int)own.size();
         plan.nodes.insert(plan.nodes.end(), own.begin(), own.end());
         plan.nodes.insert(plan.nodes.end(), ghosts.begin(), ghosts.end());
         plan.node_off[g + 1] = (int)plan.nodes.size();
-        const int ebase = (int)plan.elems.size();
-        for (int c = 0; c <= C; c++) {
-            // absolute offset of the first element of colour c within this part
-            int cnt = 0;
-            for (int e : pel)
-                if (elem_color[e] < c) cnt++;
-            plan.color_off[(size_t)g * (C + 1) + c] = ebase + cnt;
+        const int t0 = (int)plan.task_elem.size();
+        plan.tp_off[g] = (int)plan.tptr.size();
+        for (int n : own) {
+            plan.tptr.push_back((int)plan.task_elem.size() - t0);
+            for (int q = plan.inc_ptr[n]; q < plan.inc_ptr[n + 1]; q++) {
+                const int e = plan.inc_idx[q] / 4, k = plan.inc_idx[q] % 4;
+                plan.task_elem.push_back(e);
+                plan.task_pos.push_back((uint8_t)k);
+                for (int j = 0; j < npe; j++)
+                    plan.task_nodes.push_back(
+                        (uint16_t)local[p.elements[(size_t)e * npe + (k + j) % npe]]);
+            }
         }
-        for (int e : pel) {
-            plan.elems.push_back(e);
-            for (int k = 0; k < npe; k++) plan.lnode.push_back(local[p.elements[(size_t)e * npe + k]]);
-        }
-        plan.elem_off[g + 1] = (int)plan.elems.size();
-        plan.max_nloc = std::max(plan.max_nloc, (int)(own.size() + ghosts.size()));
+        plan.tptr.push_back((int)plan.task_elem.size() - t0);
+        plan.task_off[g + 1] = (int)plan.task_elem.size();
+        plan.max_nloc = std::max(plan.max_nloc, nloc);
         plan.max_nown = std::max(plan.max_nown, (int)own.size());
-        plan.max_nel = std::max(plan.max_nel, (int)pel.size());
+        plan.max_ntask = std::max(plan.max_ntask, (int)plan.task_elem.size() - t0);
         for (int n : own) local[n] = -1;
         for (int n : ghosts) local[n] = -1;
     }
+    plan.tp_off[G] = (int)plan.tptr.size();
     return "";
 }
 

@@ -1,12 +1,15 @@
 // Host-side partition plan for the persistent PCG kernel.
 //
-// The node set is cut into G parts by recursive coordinate bisection (each
-// cut at the proportional median of the longer bounding-box side), one part
-// per thread block of the persistent launch.  A part owns its nodes; it also
-// holds every element touching an owned node and, as ghosts, the nodes of
-// those elements it does not own.  Within a part, elements are ordered by
-// colour so that one colour's rows can be added into shared memory without
-// atomics; local node numbering is owned nodes first, then ghosts.
+// The node set is cut into G parts, one per thread block of the persistent
+// launch: nodes sorted by y are cut into R strips (R ~ sqrt(G * height /
+// width)), and each strip, sorted by x, into its share of the G blocks, so
+// parts are near-square for any G and any node cloud.  A part owns its
+// nodes.  Its work items ("tasks") are the (element, owned node) incidences:
+// a task computes the node's 3 rows of Ke u_e.  Tasks are ordered node by
+// node, so a node's K u is the sum of a contiguous run of task results (an
+// owner-computes gather: no scatter, no atomics, fixed summation order).
+// Nodes of a part's elements that it does not own are its ghosts; local
+// numbering is owned nodes first, then ghosts.
 #pragma once
 
 #include <cstdint>
@@ -21,16 +24,21 @@ struct HostPlan {
     int Nn = 0, Ne = 0, npe = 4, colors = 0, G = 0;
     // per part: [node_off[g], node_off[g+1]) local nodes (owned first), nown[g] owned
     std::vector<int> node_off, nown, nodes;
-    // per part: [elem_off[g], elem_off[g+1]) elements; color_off[g*(colors+1)+c] absolute
-    std::vector<int> elem_off, color_off, elems;
-    std::vector<int> lnode;  // npe local node indices per part element
+    // per part: [task_off[g], task_off[g+1]) tasks (global task numbering)
+    std::vector<int> task_off;
+    std::vector<int> task_elem;           // element of each task
+    std::vector<uint8_t> task_pos;        // position of the owned node in the element
+    std::vector<uint16_t> task_nodes;     // npe local node ids per task, owned node first,
+                                          // then the element's next nodes cyclically
+    // per part: nown[g]+1 task offsets (relative to the part) at tp_off[g]
+    std::vector<int> tptr, tp_off;
     // node -> (element*4 + position) incidence, for block-diagonal assembly
     std::vector<int> inc_ptr, inc_idx;
     // the colouring actually used (the caller's, or a greedy one when the
     // caller's colouring had node-sharing elements of one colour)
     std::vector<uint32_t> color_offsets, elements_by_color;
     bool recolored = false;
-    int max_nloc = 0, max_nown = 0, max_nel = 0;
+    int max_nloc = 0, max_nown = 0, max_ntask = 0;
 };
 
 // Checks the problem arrays; returns "" when valid, else the reason.

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <list>
 #include <memory>
@@ -61,13 +62,15 @@ struct Plan {
     pg::HostPlan hp;
     double E = 0, nu = 0, t = 0;
     bool has_elem_t = false;
-    DevBuf<int> node_off, nown, nodes, elem_off, color_off, elems, lnode, inc_ptr, inc_idx;
+    DevBuf<int> node_off, nown, nodes, task_off, tp_off, tptr, task_elem, inc_ptr, inc_idx;
+    DevBuf<uint16_t> task_nodes;
+    DevBuf<uint8_t> task_pos;
     DevBuf<float> mesh_nodes, elem_t, F;
     DevBuf<uint32_t> mesh_elements, cob_off, cob_list;
     DevBuf<uint8_t> cons;
-    DevBuf<double> ke64, binv64, x, xch64, partials;
-    DevBuf<float> ke32, binv32, xch32;
-    DevBuf<unsigned int> bar;
+    DevBuf<double> ke64, kt64, binv64, x;
+    DevBuf<float> ke32, kt32, binv32;
+    DevBuf<unsigned long long> llv, llx, llp;
     DevBuf<int> abort_flag;
     DevBuf<pg::PcgResult> res;
 };
@@ -83,6 +86,7 @@ struct pg_ctx {
     int device = 0;
     int sms = 0;
     int max_smem = 0;
+    double clock_khz = 1.0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -115,13 +119,36 @@ int auto_ctas(const pg_ctx* c, int Nn) {
     return std::max(1, std::min(G, c->sms));
 }
 
-size_t smem_bytes(const pg::HostPlan& hp, bool ke_smem) {
-    const int nd = 3 * hp.npe, ns = nd * (nd + 1) / 2;
-    size_t dbl = 15 * (size_t)hp.max_nloc + 3 * (size_t)hp.max_nown + 9 * (size_t)hp.max_nloc + 32 * 4 +
-                 8 + (ke_smem ? (size_t)hp.max_nel * ns : 0);
-    size_t ints = (size_t)hp.npe * hp.max_nel + (hp.colors + 1) + 4;
-    size_t bytes = 3 * (size_t)hp.max_nloc;
-    return dbl * 8 + ints * 4 + bytes + 16;
+pg::SmemLayout make_layout(const pg::HostPlan& hp, bool mixed, bool ke_smem) {
+    const size_t T = mixed ? 4 : 8, nd = 3 * hp.npe;
+    const size_t nloc = hp.max_nloc, nown = hp.max_nown, ntask = hp.max_ntask;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const int o = (int)off;
+        off = (off + bytes + 15) & ~(size_t)15;
+        return o;
+    };
+    pg::SmemLayout L{};
+    L.x = take(3 * nown * 8);
+    L.xl = take(mixed ? 3 * nloc * 8 : 0);
+    L.ytd = take(mixed ? 3 * ntask * 8 : 0);
+    L.red = take(128 * 8);
+    L.scal = take(8 * 8);
+    L.sp = take((size_t)3 * hp.G * 8);
+    L.r = take(3 * nloc * T);
+    L.u = take(3 * nloc * T);
+    L.p = take(3 * nloc * T);
+    L.s = take(3 * nloc * T);
+    L.w = take(3 * nloc * T);
+    L.B = take(9 * nloc * T);
+    L.yt = take(3 * ntask * T);
+    L.kt = take(ke_smem ? 3 * nd * ntask * T : 0);
+    L.gid = take(nloc * 4);
+    L.tptr = take((nown + 1) * 4);
+    L.tnode = take(hp.npe * ntask * 2);
+    L.cm = take(3 * nloc);
+    L.total = (int)off;
+    return L;
 }
 
 std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G) {
@@ -140,10 +167,12 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G) {
     pl->node_off.upload(hp.node_off.data(), hp.node_off.size(), st);
     pl->nown.upload(hp.nown.data(), hp.nown.size(), st);
     pl->nodes.upload(hp.nodes.data(), hp.nodes.size(), st);
-    pl->elem_off.upload(hp.elem_off.data(), hp.elem_off.size(), st);
-    pl->color_off.upload(hp.color_off.data(), hp.color_off.size(), st);
-    pl->elems.upload(hp.elems.data(), hp.elems.size(), st);
-    pl->lnode.upload(hp.lnode.data(), hp.lnode.size(), st);
+    pl->task_off.upload(hp.task_off.data(), hp.task_off.size(), st);
+    pl->tp_off.upload(hp.tp_off.data(), hp.tp_off.size(), st);
+    pl->tptr.upload(hp.tptr.data(), hp.tptr.size(), st);
+    pl->task_elem.upload(hp.task_elem.data(), hp.task_elem.size(), st);
+    pl->task_pos.upload(hp.task_pos.data(), hp.task_pos.size(), st);
+    pl->task_nodes.upload(hp.task_nodes.data(), hp.task_nodes.size(), st);
     pl->inc_ptr.upload(hp.inc_ptr.data(), hp.inc_ptr.size(), st);
     pl->inc_idx.upload(hp.inc_idx.data(), hp.inc_idx.size(), st);
     pl->mesh_nodes.upload(p.nodes, 2 * Nn, st);
@@ -154,15 +183,17 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G) {
     pl->has_elem_t = p.elem_t != nullptr;
     if (p.elem_t) pl->elem_t.upload(p.elem_t, Ne, st);
     pl->F.alloc(3 * Nn);
+    const size_t NT = hp.task_elem.size();
     pl->ke64.alloc(std::max<size_t>(1, Ne * kk));
     pl->ke32.alloc(std::max<size_t>(1, Ne * kk));
+    pl->kt64.alloc(std::max<size_t>(1, NT * 9 * npe));
+    pl->kt32.alloc(std::max<size_t>(1, NT * 9 * npe));
     pl->binv64.alloc(9 * Nn);
     pl->binv32.alloc(9 * Nn);
     pl->x.alloc(3 * Nn);
-    pl->xch64.alloc(6 * Nn);
-    pl->xch32.alloc(6 * Nn);
-    pl->partials.alloc(8 * (size_t)pl->G);
-    pl->bar.alloc(1);
+    pl->llv.alloc(12 * Nn);
+    pl->llx.alloc(6 * Nn);
+    pl->llp.alloc(16 * (size_t)pl->G + 2);
     pl->abort_flag.alloc(1);
     pl->res.alloc(1);
     // synchronous: uploads read the host plan arrays
@@ -190,15 +221,26 @@ Plan* get_plan(pg_ctx* c, const pg_problem& p, int G, bool* cached) {
 void run_setup(pg_ctx* c, Plan* pl) {
     const pg::HostPlan& hp = pl->hp;
     const int Ne = hp.Ne, Nn = hp.Nn;
-    if (Ne > 0)
-        pg::ke_kernel<<<(Ne + 127) / 128, 128, 0, c->stream>>>(
-            Ne, hp.npe, pl->mesh_nodes.p, pl->mesh_elements.p, pl->E, pl->nu, pl->t,
-            pl->has_elem_t ? pl->elem_t.p : nullptr, pl->ke64.p, pl->ke32.p);
+    const float* et = pl->has_elem_t ? pl->elem_t.p : nullptr;
+    if (Ne > 0 && hp.npe == 4)
+        pg::ke_kernel<4><<<(Ne + 127) / 128, 128, 0, c->stream>>>(
+            Ne, pl->mesh_nodes.p, pl->mesh_elements.p, pl->E, pl->nu, pl->t, et, pl->ke64.p, pl->ke32.p);
+    else if (Ne > 0)
+        pg::ke_kernel<3><<<(Ne + 127) / 128, 128, 0, c->stream>>>(
+            Ne, pl->mesh_nodes.p, pl->mesh_elements.p, pl->E, pl->nu, pl->t, et, pl->ke64.p, pl->ke32.p);
     CK(cudaGetLastError());
     if (Nn > 0)
         pg::binv_kernel<<<(Nn + 127) / 128, 128, 0, c->stream>>>(
             Nn, hp.npe, pl->inc_ptr.p, pl->inc_idx.p, pl->ke64.p, pl->cons.p, pl->binv64.p,
             pl->binv32.p);
+    CK(cudaGetLastError());
+    const int NT = (int)hp.task_elem.size();
+    if (NT > 0 && hp.npe == 4)
+        pg::task_ke_kernel<4><<<(NT + 127) / 128, 128, 0, c->stream>>>(
+            NT, pl->task_elem.p, pl->task_pos.p, pl->ke64.p, pl->kt64.p, pl->kt32.p);
+    else if (NT > 0)
+        pg::task_ke_kernel<3><<<(NT + 127) / 128, 128, 0, c->stream>>>(
+            NT, pl->task_elem.p, pl->task_pos.p, pl->ke64.p, pl->kt64.p, pl->kt32.p);
     CK(cudaGetLastError());
 }
 
@@ -224,48 +266,49 @@ void fill_options(const pg_options* in, pg_options* o) {
 // result record (one small readback).  F must already be in pl->F.
 void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info) {
     const pg::HostPlan& hp = pl->hp;
-    if (o.precision == PG_PREC_MIXED) throw Fail{PG_EUNSUPPORTED, "mixed precision is not built yet"};
-    const int threads = o.threads ? o.threads : 512;
+    const bool mixed = o.precision == PG_PREC_MIXED;
+    int threads = o.threads;
+    if (!threads) threads = std::min(pg::kMaxThreads, std::max(128, (hp.max_ntask + 31) / 32 * 32));
     bool ke_smem = true;
-    size_t sm = smem_bytes(hp, true);
-    if (sm > (size_t)c->max_smem) {
+    pg::SmemLayout L = make_layout(hp, mixed, true);
+    if (L.total > c->max_smem) {
         ke_smem = false;
-        sm = smem_bytes(hp, false);
+        L = make_layout(hp, mixed, false);
     }
-    if (sm > (size_t)c->max_smem)
+    if (L.total > c->max_smem)
         throw Fail{PG_EUNSUPPORTED, "partition too large for shared memory: use more ctas"};
-    if (pl->G > c->sms) throw Fail{PG_EINVAL, "ctas exceeds the number of SMs"};
 
     CK(cudaEventRecord(c->ev[0], c->stream));
     run_setup(c, pl);
     CK(cudaEventRecord(c->ev[1], c->stream));
-    CK(cudaMemsetAsync(pl->bar.p, 0, sizeof(unsigned int), c->stream));
+    // round tags start at 1 in every launch: clear the tagged buffers
+    CK(cudaMemsetAsync(pl->llv.p, 0, pl->llv.n * sizeof(unsigned long long), c->stream));
+    CK(cudaMemsetAsync(pl->llx.p, 0, pl->llx.n * sizeof(unsigned long long), c->stream));
+    CK(cudaMemsetAsync(pl->llp.p, 0, pl->llp.n * sizeof(unsigned long long), c->stream));
     CK(cudaMemsetAsync(pl->abort_flag.p, 0, sizeof(int), c->stream));
     CK(cudaMemsetAsync(pl->res.p, 0, sizeof(pg::PcgResult), c->stream));
 
     pg::PcgArgs a{};
     a.G = pl->G;
-    a.npe = hp.npe;
-    a.C = hp.colors;
+    a.NT = (int)hp.task_elem.size();
     a.Nn = hp.Nn;
     a.node_off = pl->node_off.p;
     a.nown = pl->nown.p;
     a.nodes = pl->nodes.p;
-    a.elem_off = pl->elem_off.p;
-    a.color_off = pl->color_off.p;
-    a.elems = pl->elems.p;
-    a.lnode = pl->lnode.p;
-    a.ke64 = pl->ke64.p;
-    a.ke32 = pl->ke32.p;
+    a.task_off = pl->task_off.p;
+    a.tp_off = pl->tp_off.p;
+    a.tptr = pl->tptr.p;
+    a.task_nodes = pl->task_nodes.p;
+    a.kt64 = pl->kt64.p;
+    a.kt32 = pl->kt32.p;
     a.binv64 = pl->binv64.p;
     a.binv32 = pl->binv32.p;
     a.cons = pl->cons.p;
     a.F = pl->F.p;
     a.x = pl->x.p;
-    a.xch64 = pl->xch64.p;
-    a.xch32 = pl->xch32.p;
-    a.partials = pl->partials.p;
-    a.bar = pl->bar.p;
+    a.llv = pl->llv.p;
+    a.llx = pl->llx.p;
+    a.llp = pl->llp.p;
     a.abort_flag = pl->abort_flag.p;
     a.res = pl->res.p;
     a.tol = o.tolerance;
@@ -273,20 +316,24 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info) {
     a.stop_rule = o.stop_rule;
     a.timeout_ns = (unsigned long long)(o.wait_timeout_ms * 1e6);
     a.ke_smem = ke_smem ? 1 : 0;
-    a.sm_nloc = hp.max_nloc;
-    a.sm_nown = hp.max_nown;
-    a.sm_nel = hp.max_nel;
-    a.reliable_interval = o.reliable_interval;
-    a.reliable_delta = o.reliable_delta;
+    a.timing = o.phase_timing ? 1 : 0;
+    a.test_stall = o.test_stall ? 1 : 0;
+    a.reliable_interval = o.reliable_interval > 0 ? o.reliable_interval : 1 << 30;
+    a.reliable_delta = o.reliable_delta > 0 ? o.reliable_delta : 0.1;
+    a.L = L;
 
-    const void* fn = hp.npe == 4 ? (const void*)pg::pcg_fp64_kernel<4> : (const void*)pg::pcg_fp64_kernel<3>;
-    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const void* fn;
+    if (hp.npe == 4)
+        fn = mixed ? (const void*)pg::pcg_kernel<4, float, true> : (const void*)pg::pcg_kernel<4, double, false>;
+    else
+        fn = mixed ? (const void*)pg::pcg_kernel<3, float, true> : (const void*)pg::pcg_kernel<3, double, false>;
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total));
     int nb = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, sm));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, L.total));
     if (nb < 1 || nb * c->sms < pl->G)
         throw Fail{PG_EUNSUPPORTED, "persistent grid does not fit on the device"};
     void* args[] = {&a};
-    CK(cudaLaunchCooperativeKernel(fn, dim3(pl->G), dim3(threads), args, sm, c->stream));
+    CK(cudaLaunchCooperativeKernel(fn, dim3(pl->G), dim3(threads), args, L.total, c->stream));
     CK(cudaEventRecord(c->ev[2], c->stream));
     pg::PcgResult r{};
     CK(cudaMemcpyAsync(&r, pl->res.p, sizeof(r), cudaMemcpyDeviceToHost, c->stream));
@@ -306,10 +353,19 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info) {
         info->ctas = pl->G;
         info->threads = threads;
         info->reliable_updates = r.reliable_updates;
+        info->reductions = r.reductions;
+        info->shared_bytes = L.total;
+        for (int k = 0; k < 4; k++) info->phase_us[k] = r.phase_cycles[k] / (c->clock_khz * 1e-3);
     }
     if (r.wait_failures > 0 || r.status == PG_ETIMEOUT)
-        throw Fail{PG_ETIMEOUT, "a grid-wide wait exceeded wait_timeout_ms"};
-    if (r.status == PG_ENONFINITE) throw Fail{PG_ENONFINITE, "non-finite value in the PCG iteration"};
+        throw Fail{PG_ETIMEOUT, "a wait for another block exceeded wait_timeout_ms"};
+    if (r.status == PG_ENONFINITE) {
+        char buf[256];
+        std::snprintf(buf, sizeof buf,
+                      "non-finite value in the PCG iteration (reduction %d: gamma=%g delta=%g rho=%g)",
+                      r.nonfinite_it, r.nonfinite_vals[0], r.nonfinite_vals[1], r.nonfinite_vals[2]);
+        throw Fail{PG_ENONFINITE, buf};
+    }
 }
 
 template <typename F>
@@ -395,6 +451,9 @@ int pg_create(int device, pg_ctx** out) {
         if (!pr.cooperativeLaunch) throw Fail{PG_ECUDA, "device lacks cooperative launch"};
         c->sms = pr.multiProcessorCount;
         c->max_smem = (int)pr.sharedMemPerBlockOptin;
+        int khz = 0;
+        CK(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, device));
+        c->clock_khz = khz > 0 ? khz : 1.0;
         CK(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
         c->stream = c->own_stream;
         for (auto& e : c->ev) CK(cudaEventCreate(&e));
@@ -598,33 +657,39 @@ int pg_plan_inspect(const pg_problem* p, int ctas, int32_t* stats, char* msg, si
                 if (owner[hp.nodes[n0 + k]] >= 0) bad++;
                 owner[hp.nodes[n0 + k]] = g;
             }
-            // elements: exactly those touching an owned node, colour-sorted
-            std::vector<char> in_part(hp.Ne, 0);
-            for (int q = hp.elem_off[g]; q < hp.elem_off[g + 1]; q++) in_part[hp.elems[q]] = 1;
+            // tasks of owned node k: exactly its incidences, in order, owned node first
+            const int t0 = hp.task_off[g];
+            const int* tp = hp.tptr.data() + hp.tp_off[g];
+            if (hp.tp_off[g + 1] - hp.tp_off[g] != no + 1 || tp[0] != 0 ||
+                tp[no] != hp.task_off[g + 1] - t0)
+                bad++;
+            std::vector<char> used(nl, 0);
             for (int k = 0; k < no; k++) {
                 const int n = hp.nodes[n0 + k];
-                for (int q = hp.inc_ptr[n]; q < hp.inc_ptr[n + 1]; q++)
-                    if (!in_part[hp.inc_idx[q] / 4]) bad++;
-            }
-            for (int c = 0; c < C; c++) {
-                for (int q = hp.color_off[(size_t)g * (C + 1) + c]; q < hp.color_off[(size_t)g * (C + 1) + c + 1]; q++) {
-                    const int e = hp.elems[q];
-                    bool touches = false;
-                    for (int k = 0; k < npe; k++) {
-                        const int ln = hp.lnode[(size_t)q * npe + k];
-                        if (ln < 0 || ln >= nl || hp.nodes[n0 + ln] != (int)p->elements[(size_t)e * npe + k]) bad++;
-                        if (ln >= 0 && ln < no) touches = true;
+                used[k] = 1;
+                if (tp[k + 1] - tp[k] != hp.inc_ptr[n + 1] - hp.inc_ptr[n]) { bad++; continue; }
+                for (int i = 0; i < tp[k + 1] - tp[k]; i++) {
+                    const int t = t0 + tp[k] + i, inc = hp.inc_idx[hp.inc_ptr[n] + i];
+                    const int e = inc / 4, pos = inc % 4;
+                    if (hp.task_elem[t] != e || hp.task_pos[t] != pos) bad++;
+                    for (int j = 0; j < npe; j++) {
+                        const int ln = hp.task_nodes[(size_t)t * npe + j];
+                        if (ln >= nl || hp.nodes[n0 + ln] != (int)p->elements[(size_t)e * npe + (pos + j) % npe])
+                            bad++;
+                        else
+                            used[ln] = 1;
                     }
-                    if (!touches) bad++;
-                    bool found = false;
-                    for (uint32_t q2 = hp.color_offsets[c]; q2 < hp.color_offsets[c + 1] && !found; q2++)
-                        found = hp.elements_by_color[q2] == (uint32_t)e;
-                    if (!found) bad++;
+                    if (hp.task_nodes[(size_t)t * npe] != k) bad++;
                 }
             }
+            for (int k = no; k < nl; k++)  // ghosts: referenced, and not owned here
+                if (!used[k]) bad++;
         }
         for (int n = 0; n < Nn; n++)
             if (owner[n] < 0) bad++;
+        for (int g = 0; g < hp.G; g++)
+            for (int k = hp.nown[g]; k < hp.node_off[g + 1] - hp.node_off[g]; k++)
+                if (owner[hp.nodes[hp.node_off[g] + k]] == g) bad++;
         // colour validity of the colouring in use
         std::vector<int> col(hp.Ne, -1), stamp(C, -1);
         for (int c = 0; c < C; c++)
@@ -640,7 +705,7 @@ int pg_plan_inspect(const pg_problem* p, int ctas, int32_t* stats, char* msg, si
         stats[2] = hp.recolored ? 1 : 0;
         stats[3] = hp.max_nloc;
         stats[4] = hp.max_nown;
-        stats[5] = hp.max_nel;
+        stats[5] = hp.max_ntask;
         stats[6] = (int32_t)ghosts;
         stats[7] = bad;
         put(bad ? "plan invariants violated" : "");

@@ -58,6 +58,8 @@ class PgOptions(C.Structure):
         ("wait_timeout_ms", C.c_double),
         ("reliable_interval", C.c_int32),
         ("reliable_delta", C.c_double),
+        ("phase_timing", C.c_int32),
+        ("test_stall", C.c_int32),
     ]
 
 
@@ -77,10 +79,14 @@ class PgInfo(C.Structure):
         ("threads", C.c_int32),
         ("reliable_updates", C.c_int32),
         ("plan_cached", C.c_int32),
+        ("reductions", C.c_int32),
+        ("shared_bytes", C.c_int32),
+        ("phase_us", C.c_double * 4),
     ]
 
     def as_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["phase_us"] = list(self.phase_us)
         d["stop_reason"] = STOP_REASONS.get(d["stop_reason"], d["stop_reason"])
         return d
 
@@ -192,7 +198,7 @@ class Problem:
 
 
 PLAN_STATS = ("parts", "colors", "recolored", "max_local_nodes", "max_owned_nodes",
-              "max_part_elements", "ghost_nodes", "violations")
+              "max_part_tasks", "ghost_nodes", "violations")
 
 
 def plan_inspect(prob: "Problem", ctas: int) -> dict:
@@ -207,7 +213,8 @@ def plan_inspect(prob: "Problem", ctas: int) -> dict:
 
 def make_options(tolerance=1e-6, max_iterations=1000, precision=PG_PREC_FP64,
                  stop_rule=PG_STOP_REFERENCE, ctas=0, threads=0, wait_timeout_ms=None,
-                 reliable_interval=0, reliable_delta=0.0) -> PgOptions:
+                 reliable_interval=0, reliable_delta=0.0, phase_timing=False,
+                 test_stall=False) -> PgOptions:
     o = PgOptions()
     load().pg_options_default(C.byref(o))
     o.tolerance = float(tolerance)
@@ -220,6 +227,8 @@ def make_options(tolerance=1e-6, max_iterations=1000, precision=PG_PREC_FP64,
         o.wait_timeout_ms = float(wait_timeout_ms)
     o.reliable_interval = int(reliable_interval)
     o.reliable_delta = float(reliable_delta)
+    o.phase_timing = 1 if phase_timing else 0
+    o.test_stall = 1 if test_stall else 0
     return o
 
 

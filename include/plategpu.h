@@ -53,7 +53,7 @@ typedef enum pg_status {
     PG_EINVAL = 1,        /* malformed problem or options */
     PG_ENOMEM = 2,        /* device or host allocation failed */
     PG_ECUDA = 3,         /* CUDA runtime error / no device */
-    PG_ETIMEOUT = 4,      /* a grid-wide wait ran past its time limit */
+    PG_ETIMEOUT = 4,      /* a wait for another block's data ran past its time limit */
     PG_ENONFINITE = 5,    /* NaN or Inf in the inputs or the iteration */
     PG_EUNSUPPORTED = 6   /* a request this build does not serve */
 } pg_status;
@@ -101,11 +101,15 @@ typedef struct pg_options {
     int32_t stop_rule;            /* pg_stop_rule, default PG_STOP_REFERENCE */
     int32_t ctas;                 /* persistent grid size; 0 = automatic */
     int32_t threads;              /* threads per CTA; 0 = automatic */
-    double wait_timeout_ms;       /* limit on each grid-wide wait; default 1000 */
+    double wait_timeout_ms;       /* limit on each wait for another block's data; default 1000 */
     int32_t reliable_interval;    /* mixed: max inner iterations between FP64
                                      residual replacements; 0 = automatic */
     double reliable_delta;        /* mixed: replace when the FP32 residual fell
                                      by this factor; 0 = automatic (0.1) */
+    int32_t phase_timing;         /* 1: record per-phase device time (pg_info.phase_us) */
+    int32_t test_stall;           /* test hook: 1 makes block 0 wait once for a value no
+                                     block ever writes, so the call must end with
+                                     PG_ETIMEOUT after wait_timeout_ms */
 } pg_options;
 
 /* Per-solve result (GPUSolveResult plus extended statistics). */
@@ -124,6 +128,13 @@ typedef struct pg_info {
     int32_t threads;
     int32_t reliable_updates;     /* mixed precision: FP64 residual replacements */
     int32_t plan_cached;          /* 1 when the partition plan was reused */
+    int32_t reductions;           /* grid-wide reductions (one per iteration, plus
+                                     one per residual replacement) */
+    int32_t shared_bytes;         /* dynamic shared memory per block */
+    double phase_us[4];           /* with phase_timing, block 0's time (SM cycles at
+                                     the nominal clock) in: K.u; gather, dot products
+                                     and publishing; the exchange wait; decisions and
+                                     vector updates */
 } pg_info;
 
 typedef struct pg_ctx pg_ctx;
@@ -181,11 +192,11 @@ int pg_element_stiffness(pg_ctx* ctx, const pg_problem* prob, double* ke_out);
 
 /* Host-only test hook (no device needed): builds the partition plan the
  * solver would use with `ctas` blocks and checks its invariants (every
- * node owned by exactly one part, every element touching an owned node
- * present in that part, ghosts = the other nodes of those elements, no two
- * elements of one colour sharing a node).  stats_out[8]: parts, colours,
- * recoloured (0/1), max local nodes, max owned nodes, max elements per
- * part, total ghost nodes, invariant violations (0 when valid).
+ * node owned by exactly one part, ghosts = the other nodes of the owned
+ * nodes' elements, no two elements of one colour sharing a node, every (element, owned node)
+ * incidence present once as a task of the owning part).  stats_out[8]:
+ * parts, colours, recoloured (0/1), max local nodes, max owned nodes, max
+ * tasks per part, total ghost nodes, invariant violations (0 when valid).
  * msg/msg_len (optional) receive the failure reason. */
 int pg_plan_inspect(const pg_problem* prob, int ctas, int32_t* stats_out, char* msg,
                     size_t msg_len);

@@ -35,8 +35,9 @@ def test_struct_layout_matches_header():
 #include <stddef.h>
 #include "plategpu.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(pg_problem), sizeof(pg_options), sizeof(pg_info),
-         offsetof(pg_problem, F), offsetof(pg_options, reliable_delta), offsetof(pg_info, plan_cached));
+  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(pg_problem), sizeof(pg_options), sizeof(pg_info),
+         offsetof(pg_problem, F), offsetof(pg_options, phase_timing), offsetof(pg_info, plan_cached),
+         offsetof(pg_info, phase_us));
   return 0;
 }
 """
@@ -49,8 +50,8 @@ int main(void) {
         vals = [int(v) for v in subprocess.run([exe], capture_output=True, text=True,
                                                check=True).stdout.split()]
     assert vals == [C.sizeof(_lib.PgProblem), C.sizeof(_lib.PgOptions), C.sizeof(_lib.PgInfo),
-                    _lib.PgProblem.F.offset, _lib.PgOptions.reliable_delta.offset,
-                    _lib.PgInfo.plan_cached.offset]
+                    _lib.PgProblem.F.offset, _lib.PgOptions.phase_timing.offset,
+                    _lib.PgInfo.plan_cached.offset, _lib.PgInfo.phase_us.offset]
 
 
 def test_defaults_match_reference():

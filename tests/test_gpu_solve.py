@@ -173,7 +173,14 @@ def test_dkt_thickness_field(gpu_ctx, oracle):
     assert conv and abs(max_w(x) - max_w(xr)) / abs(max_w(xr)) < 1e-4
 
 
-@pytest.mark.parametrize("ctas", [1, 13, 64, 148])
+def test_too_few_blocks_is_unsupported(gpu_ctx, c1):
+    """The whole part of a block must fit in shared memory; one block cannot
+    hold 3,267 DOF and says so instead of running out of bounds."""
+    with pytest.raises(PlateGPUError, match="PG_EUNSUPPORTED"):
+        gsolve(gpu_ctx, c1, ctas=1)
+
+
+@pytest.mark.parametrize("ctas", [3, 13, 64, 148])
 def test_grid_sizes_agree(gpu_ctx, c1, ctas):
     x0, i0 = gsolve(gpu_ctx, c1, tolerance=1e-8, max_iterations=5000,
                     stop_rule=_lib.PG_STOP_RELATIVE, ctas=9)
@@ -209,12 +216,13 @@ def test_nonfinite_rhs_rejected(gpu_ctx, c1):
 
 
 def test_wait_timeout_reports_and_context_survives(gpu_ctx, c1):
-    """A zero wait limit makes every grid-wide wait give up at once: the
-    kernel returns PG_ETIMEOUT (no trap, no hang) and the context stays
-    usable."""
+    """Block 0 waits for a value no block ever writes: the wait runs out
+    after its 20 ms limit, every block leaves, the call returns
+    PG_ETIMEOUT (no trap, no hang) and the context stays usable."""
     with pytest.raises(PlateGPUError, match="PG_ETIMEOUT"):
-        gsolve(gpu_ctx, c1, wait_timeout_ms=0.0, ctas=16)
-    x, info = gsolve(gpu_ctx, c1, tolerance=1e-8, stop_rule=_lib.PG_STOP_RELATIVE)
+        gsolve(gpu_ctx, c1, wait_timeout_ms=20.0, ctas=16, test_stall=True)
+    x, info = gsolve(gpu_ctx, c1, tolerance=1e-8, max_iterations=5000,
+                     stop_rule=_lib.PG_STOP_RELATIVE)
     assert info.converged
 
 
