@@ -23,7 +23,7 @@ STOP_REASONS = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "zero_rh
 # every symbol include/plategpu.h declares
 EXPORTED = ("pg_options_default", "pg_is_available", "pg_create", "pg_destroy", "pg_last_error",
             "pg_clear_cache", "pg_set_stream", "pg_solve", "pg_plan_create", "pg_plan_solve_device",
-            "pg_plan_destroy", "pg_apply_k",
+            "pg_plan_destroy", "pg_apply_k", "pg_apply_k_static",
             "pg_block_jacobi", "pg_element_stiffness", "pg_plan_inspect")
 
 
@@ -140,6 +140,8 @@ def load() -> C.CDLL:
     L.pg_block_jacobi.restype = I
     L.pg_element_stiffness.argtypes = [P, C.POINTER(PgProblem), P]
     L.pg_element_stiffness.restype = I
+    L.pg_apply_k_static.argtypes = [C.POINTER(PgProblem), P, P, P, C.c_char_p, C.c_size_t]
+    L.pg_apply_k_static.restype = I
     L.pg_plan_inspect.argtypes = [C.POINTER(PgProblem), I, P, C.c_char_p, C.c_size_t]
     L.pg_plan_inspect.restype = I
     _lib = L

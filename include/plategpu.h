@@ -187,6 +187,32 @@ int pg_apply_k(pg_ctx* ctx, const pg_problem* prob, const double* x, double* y);
  * |det| < 1e-30 blocks replaced by identity (solver.ts:231-304). */
 int pg_block_jacobi(pg_ctx* ctx, const pg_problem* prob, double* binv_out);
 
+/* y = K x (same operator and BC rule as pg_apply_k) without allocating
+ * anything.  No counterpart in the reference: it is for callers that may
+ * not call cudaMalloc -- code whose device memory belongs to another
+ * allocator with no untracked blocks to spare (a framework's caching
+ * allocator, a fixed memory budget), or code that must not allocate once it
+ * is running (a real-time loop, a driver callback).
+ *   - prob's nodes, elements, elements_by_color, elem_t (optional) and
+ *     constrained, and x and y ([3*node_count] doubles), are DEVICE pointers
+ *     on the calling thread's current device; color_offsets is a HOST
+ *     pointer; F is not used.  The colouring must be valid (no two elements
+ *     of one colour share a node); it is not checked.
+ *   - The element matrices go to a static device array of 8 MiB that the
+ *     library holds on every GPU it is loaded on until the process exits:
+ *     at most 7,281 Q4 or 12,945 DKT elements; larger problems fail with
+ *     PG_EINVAL before any work is queued.
+ *   - The first call on a device looks up that array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream
+ *     capture.
+ *   - Work is queued on `stream` (a cudaStream_t; NULL = legacy default
+ *     stream) and the call returns without waiting.  All calls share the
+ *     one array, so calls whose work overlaps on the GPU (other streams,
+ *     other host threads) race; serialise them.
+ *   - msg/msg_len (optional) receive the reason for a failure. */
+int pg_apply_k_static(const pg_problem* prob, const double* x, double* y, void* stream, char* msg,
+                      size_t msg_len);
+
 /* Test hook: element stiffness matrices, [element_count * (3*npe)^2] FP64. */
 int pg_element_stiffness(pg_ctx* ctx, const pg_problem* prob, double* ke_out);
 
