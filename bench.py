@@ -43,7 +43,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["plategpu", "reference"], default="plategpu")
     ap.add_argument("--workload", default="plate_q4_141")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--tol", type=float, default=7e-7,
                     help="relative recursive-residual tolerance (||r||/||b||)")
     ap.add_argument("--ctas", type=int, default=0)
@@ -273,6 +273,45 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def time_variant(args, world, local, ctx, prob, precision, stream, F_dev, x_dev, flush):
+    """Warm-up + timed device-resident solves of one precision variant."""
+    import torch
+
+    from plategpu import _lib
+
+    prec = _lib.PG_PREC_FP64 if precision == "fp64" else _lib.PG_PREC_MIXED
+    opts = _lib.make_options(tolerance=args.tol, max_iterations=20000, precision=prec,
+                             stop_rule=_lib.PG_STOP_RELATIVE, ctas=args.ctas,
+                             threads=args.threads)
+    plan = ctx.plan(prob, opts)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            plan.solve_device(opts, F_dev.data_ptr(), x_dev.data_ptr())
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        infos = []
+        barrier(world)
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            starts[k].record(stream)
+            infos.append(plan.solve_device(opts, F_dev.data_ptr(), x_dev.data_ptr()))
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    step_ms = [s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)]
+    total = max_over_ranks(world, sum(step_ms), local)
+    plan.close()
+    return {"opts": opts, "value": total / (world * args.steps), "step_ms": step_ms,
+            "kernel_ms": statistics.mean(i.solve_ms for i in infos),
+            "setup_ms": statistics.mean(i.setup_ms for i in infos),
+            "iterations": infos[-1].iterations, "reductions": infos[-1].reductions,
+            "reliable_updates": infos[-1].reliable_updates,
+            "true_rel_residual": infos[-1].true_rel_residual,
+            "ctas": infos[-1].ctas, "threads": infos[-1].threads,
+            "x": x_dev.cpu().numpy().copy()}
+
+
 def run_plategpu(args, world, rank, local):
     import numpy as np
     import torch
@@ -286,109 +325,103 @@ def run_plategpu(args, world, rank, local):
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
     prob = _lib.Problem(wl.mesh, wl.material, wl.coloring, wl.F, wl.cons_mask)
-    prec = _lib.PG_PREC_FP64 if args.precision == "fp64" else _lib.PG_PREC_MIXED
-    opts = _lib.make_options(tolerance=args.tol, max_iterations=20000, precision=prec,
-                             stop_rule=_lib.PG_STOP_RELATIVE, ctas=args.ctas,
-                             threads=args.threads)
-    plan = ctx.plan(prob, opts)
     F_dev = torch.from_numpy(wl.F).to(f"cuda:{local}")
     x_dev = torch.zeros(n, dtype=torch.float64, device=f"cuda:{local}")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    variants = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
 
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            plan.solve_device(opts, F_dev.data_ptr(), x_dev.data_ptr())
-        sampler = ClockSampler(local) if rank == 0 else None
-        if sampler:
-            sampler.start()
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        infos = []
-        barrier(world)
-        torch.cuda.synchronize()
-        for k in range(args.steps):
-            flush.fill_(k & 0xFF)
-            starts[k].record(stream)
-            infos.append(plan.solve_device(opts, F_dev.data_ptr(), x_dev.data_ptr()))
-            ends[k].record(stream)
-        torch.cuda.synchronize()
-        barrier(world)
-        clocks = sampler.stop() if sampler else None
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = max_over_ranks(world, sum(step_ms), local)
-    value = total_ms / (world * args.steps)
-    kernel_ms = statistics.mean(i.solve_ms for i in infos)
-    setup_ms = statistics.mean(i.setup_ms for i in infos)
-    iters = infos[-1].iterations
-    x_last = x_dev.cpu().numpy()
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    res = {v: time_variant(args, world, local, ctx, prob, v, stream, F_dev, x_dev, flush)
+           for v in variants}
+    clocks = sampler.stop() if sampler else None
 
-    # e2e through the C ABI from host buffers (pg_solve)
+    chk = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        chk = oracle_checks(wl, want_baseline=True)
+        for v in variants:
+            res[v]["accuracy"] = accuracy(res[v]["x"], chk)
+    # headline: the fastest variant whose FP64-checked error meets 1e-6
+    # (without the checker, the fastest variant whose true residual met the
+    # tolerance)
+    def meets(v):
+        acc = res[v].get("accuracy")
+        if acc is not None:
+            return acc["rel_l2_vs_fp64_truth"] <= 1e-6
+        return res[v]["true_rel_residual"] <= args.tol
+    ok = [v for v in variants if meets(v)] or variants
+    head = min(ok, key=lambda v: res[v]["value"])
+    H = res[head]
+
+    # e2e through the C ABI from host buffers (pg_solve), headline variant
     e2e_steps = args.e2e_steps or args.steps
     rng = np.random.default_rng(1234)
     loads = [(wl.F * np.float32(1.0 + 0.1 * rng.random())).astype(np.float32)
              for _ in range(min(e2e_steps, 16))]
     for k in range(2):
         prob.set_F(loads[k % len(loads)])
-        ctx.solve(prob, opts)
+        ctx.solve(prob, H["opts"])
     barrier(world)
     e2e = []
     for k in range(e2e_steps):
         prob.set_F(loads[k % len(loads)])
         t0 = time.perf_counter()
-        ctx.solve(prob, opts)
+        ctx.solve(prob, H["opts"])
         e2e.append((time.perf_counter() - t0) * 1e3)
     barrier(world)
-    e2e_total = max_over_ranks(world, sum(e2e), local)
-    e2e_value = e2e_total / (world * e2e_steps)
+    e2e_value = max_over_ranks(world, sum(e2e), local) / (world * e2e_steps)
 
     if rank != 0:
-        plan.close()
         ctx.close()
         return
     # roofline of the dominant kernel: algorithmic bytes per launch
-    # (16 vector words per DOF per iteration, 8 bytes each in FP64)
-    word = 8 if args.precision == "fp64" else 4
+    # (16 vector words per DOF per iteration; 8-byte words in FP64, 4-byte
+    # words for the FP32 inner iterations)
+    word = 8 if head == "fp64" else 4
+    iters = H["iterations"]
     alg_bytes = 16.0 * n * word * iters
     peak, peak_src = hbm_peak()
-    achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
-    kernel_tag = "pcg_fp64" if args.precision == "fp64" else "pcg_mixed"
-    traffic = ncu_traffic(kernel_tag, args.workload)
+    achieved = alg_bytes / (H["kernel_ms"] * 1e-3) / 1e9
+    kernel_tag = "pcg_fp64" if head == "fp64" else "pcg_mixed"
     line = {
-        "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(step_ms),
+        "metric": METRIC, "value": H["value"], "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": statistics.mean(H["step_ms"]),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32 inner / f64 refinement",
+        "dtype": "f64" if head == "fp64" else "f32 inner / f64 refinement",
         "data": "synthetic (seeded plate_q4_141: 5 kPa + 32 point loads, 16 columns)",
         "config": {"workload": args.workload, "dof": n, "elements": wl.mesh.elementCount,
-                   "precision": args.precision, "preconditioner": "block-jacobi",
-                   "stop": f"||r||/||b|| < {args.tol:g}", "ctas": infos[-1].ctas,
-                   "threads": infos[-1].threads, "l2": "flushed between steps (256 MiB write)",
+                   "method": head, "preconditioner": "block-jacobi",
+                   "stop": f"||r||/||b|| < {args.tol:g}", "ctas": H["ctas"],
+                   "threads": H["threads"], "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas x{world}"},
         "iterations": iters,
-        "kernel_ms": kernel_ms, "setup_ms": setup_ms,
-        "us_per_iteration": kernel_ms * 1e3 / max(iters, 1),
+        "kernel_ms": H["kernel_ms"], "setup_ms": H["setup_ms"],
+        "us_per_iteration": H["kernel_ms"] * 1e3 / max(iters, 1),
+        "variants": {v: {k: res[v][k] for k in ("value", "kernel_ms", "setup_ms", "iterations",
+                                               "reductions", "reliable_updates",
+                                               "true_rel_residual")}
+                     | {"accuracy": res[v].get("accuracy")} for v in variants},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
+                     "frac": achieved / peak, "traffic": ncu_traffic(kernel_tag, args.workload),
                      "kernel": f"{kernel_tag}_kernel", "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": alg_bytes},
         "e2e": {"value": e2e_value, "unit": "ms", "h2d_bytes_per_step": 4 * n,
                 "d2h_bytes_per_step": 8 * n + 64},
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": 4 * args.steps,
         "clocks": clocks,
+        "accuracy": H.get("accuracy"),
     }
-    if world == 1 and not args.no_cpu_baseline:
-        chk = oracle_checks(wl, want_baseline=True)
-        line["accuracy"] = accuracy(x_last, chk)
+    if chk is not None:
         line["cpu_baseline"] = {
             "value": chk["ref_ms"], "unit": "ms", "cores": 1, "kind": "port",
             "sample": (f"one full reference-precision solve of {args.workload} "
                        f"({chk['ref_iters']} iterations, tol 1e-6) by the C restatement "
                        "of solvePCG/applyGlobalK, single thread")}
     else:
-        line["accuracy"] = None
         line["cpu_baseline"] = None
     print(json.dumps(line), flush=True)
-    plan.close()
     ctx.close()
 
 
