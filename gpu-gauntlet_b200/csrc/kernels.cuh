@@ -39,7 +39,7 @@ struct PcgResult {
     int nonfinite_it;          // reduction index where a non-finite value appeared
     int reductions;            // grid-wide reductions performed
     double nonfinite_vals[3];  // gamma, delta, rho at that reduction
-    unsigned long long phase_cycles[4];  // block 0: K.u; gather, dots, publish; exchange; update
+    long long phase_cycles[8];  // block 0, see PhaseClock
 };
 
 // Byte offsets of the shared-memory arrays of one block (computed on the
@@ -47,6 +47,13 @@ struct PcgResult {
 struct SmemLayout {
     int r, u, p, s, w, B, yt, kt;  // T
     int x, xl, ytd, red, scal, sp;  // double
+    int Pr, Ps, cv, cpart;          // double: coarse residual, coarse s, coarse solution rows,
+                                    // per-thread partial dots of the coarse solve
+    int prc;                        // T: contiguous coarse residual
+    int ctl;                        // int[4]: decision broadcast
+    int clk;                        // long long[8]: phase timers
+    int nb, ainv;                   // T: per-node basis data, A_c^-1 rows
+    int nslot;                      // int
     int gid, tptr;                 // int
     int tnode;                     // uint16
     int cm;                        // uint8
@@ -81,8 +88,20 @@ struct PcgArgs {
     int ke_smem;
     int timing;
     int test_stall;  // test hook: block 0 waits once for a tag nobody writes
+    // two-level preconditioner (coarse = 1): u = M_bj r + P A_c^-1 P^T r
+    int coarse;
+    int C;                      // coarse DOFs, 3 per part
+    const int* cagg_off;        // [G+1] aggregates touching each part's nodes
+    const int* node_slot;       // per part-local node: slot in its part's aggregate list
+    const double* node_basis;   // per part-local node: dx, dy, 1/h
+    const int* ainv_off;        // [G+1] first A_c^-1 row of each part
+    const double* ainv64;       // [rows][C]
+    const float* ainv32;        // [rows][C]
+    int ainv_smem;
     int reliable_interval;
     double reliable_delta;
+    int trace_it;                   // iteration traced (-1: none)
+    unsigned long long* trace;      // [G][4] globaltimer: start, published, exchanged, end
     SmemLayout L;
 };
 
@@ -298,8 +317,11 @@ __device__ __forceinline__ bool poll(const unsigned long long* p, unsigned f, T&
 // block / grid reductions (fixed order: identical bits in every block)
 // ---------------------------------------------------------------------------
 
-template <int K>
-__device__ void block_sum(double (&v)[K], double* red) {
+// Block-wide sums of K values; thread 0 ends with the totals.  With
+// trailing = false the other warps may leave before warp 0 has finished
+// (the caller must not touch `red` again before a later barrier).
+template <int K, bool trailing = true>
+__device__ void block_sum(double* v, double* red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
     for (int k = 0; k < K; k++)
@@ -315,31 +337,32 @@ __device__ void block_sum(double (&v)[K], double* red) {
             for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
         }
     }
-    __syncthreads();
+    if (trailing) __syncthreads();
 }
 
 // One exchange round, all threads of the block: waits for the K tagged
-// FP64 partial sums of every block (staged to sp[G * K]) and for the tagged
+// FP64 partial sums of every block (slots of 16 words; staged to
+// sp[G * K]) and for the tagged
 // values of this block's ghost DOFs in vector buffer vb (written to
-// dst[3 * no .. 3 * nloc)).  Each thread keeps up to 4 loads in flight, so a
-// round costs about one L2 round trip.  Returns false if a wait gave up.
-template <typename T>
+// dst[3 * no .. 3 * nloc)).  Each thread keeps up to IF items in flight, so
+// a round costs about one L2 round trip.  Returns false if a wait gave up.
+template <typename T, int IF = 2>
 __device__ bool exchange_round(const unsigned long long* __restrict__ pb, int G, int K,
                                const unsigned long long* __restrict__ vb, T* dst, int no, int nloc,
                                const int* __restrict__ gid, unsigned f, double* sp, Waiter& wt) {
     constexpr int TW = Tag<T>::W;
     const int np = G * K, n = np + 3 * (nloc - no);
-    for (int i0 = threadIdx.x; i0 < n; i0 += 4 * blockDim.x) {
-        const unsigned long long* ptr[4];
-        bool done[4];
+    for (int i0 = threadIdx.x; i0 < n; i0 += IF * blockDim.x) {
+        const unsigned long long* ptr[IF];
+        bool done[IF];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
+        for (int j = 0; j < IF; j++) {
             const int i = i0 + j * (int)blockDim.x;
             done[j] = i >= n;
             if (done[j]) {
                 ptr[j] = nullptr;
             } else if (i < np) {
-                ptr[j] = pb + (size_t)(i / K) * 8 + 2 * (i % K);
+                ptr[j] = pb + (size_t)(i / K) * 16 + 2 * (i % K);
             } else {
                 const int k = 3 * no + i - np;
                 ptr[j] = vb + (size_t)(3 * gid[k / 3] + k % 3) * TW;
@@ -347,9 +370,9 @@ __device__ bool exchange_round(const unsigned long long* __restrict__ pb, int G,
         }
         wt.spins = 0;
         for (;;) {
-            unsigned long long lo[4], hi[4];
+            unsigned long long lo[IF], hi[IF];
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
+            for (int j = 0; j < IF; j++) {
                 if (done[j]) continue;
                 const int i = i0 + j * (int)blockDim.x;
                 lo[j] = ld_relaxed(ptr[j]);
@@ -357,7 +380,7 @@ __device__ bool exchange_round(const unsigned long long* __restrict__ pb, int G,
             }
             bool all = true;
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
+            for (int j = 0; j < IF; j++) {
                 if (done[j]) continue;
                 const int i = i0 + j * (int)blockDim.x;
                 if ((unsigned)(lo[j] >> 32) != f || (unsigned)(hi[j] >> 32) != f) {
@@ -384,10 +407,11 @@ __device__ bool exchange_round(const unsigned long long* __restrict__ pb, int G,
     return true;
 }
 
-// Warp 0: adds the staged partials sp[G][K] in block order (the same bits
-// in every block) into out[K].
+// Warp 0: adds the first K of each block's `stride` staged partials
+// (sp[G][stride]) in block order (the same bits in every block) into out[K].
 template <int K>
-__device__ __forceinline__ void sum_partials(const double* __restrict__ sp, int G, double* out) {
+__device__ __forceinline__ void sum_partials(const double* __restrict__ sp, int G, int stride,
+                                             double* out) {
     if (threadIdx.x >= 32) return;
     const int lane = threadIdx.x;
     double v[K];
@@ -395,7 +419,7 @@ __device__ __forceinline__ void sum_partials(const double* __restrict__ sp, int 
     for (int k = 0; k < K; k++) v[k] = 0.0;
     for (int b = lane; b < G; b += 32)
 #pragma unroll
-        for (int k = 0; k < K; k++) v[k] += sp[b * K + k];
+        for (int k = 0; k < K; k++) v[k] += sp[b * stride + k];
 #pragma unroll
     for (int k = 0; k < K; k++)
         for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
@@ -463,28 +487,31 @@ __global__ void task_ke_kernel(int NT, const int* __restrict__ task_elem,
 // ---------------------------------------------------------------------------
 
 enum { STOP_CONVERGED = 0, STOP_MAX_ITER = 1, STOP_BREAKDOWN = 2, STOP_ZERO_RHS = 3 };
+enum { ACT_UPDATE = 0, ACT_STOP = 1, ACT_RU = 2, ACT_NONFINITE = 3 };
 enum { ST_OK = 0, ST_TIMEOUT = 4, ST_NONFINITE = 5 };
 
-constexpr int kMaxThreads = 640;
+constexpr int kMaxThreads = 576;
 
-// Per-phase SM cycles of block 0, when timing is requested.
+// Per-phase SM cycles of thread 0 of block 0, when timing is requested:
+// 0 K.u, 1 gather + dots + publish w, 2 block reduction, 3 publish partials,
+// 4 exchange wait, 5 decisions, 6 coarse solve, 7 vector update (and the
+// residual replacement rounds of the mixed mode).
 struct PhaseClock {
     bool on;
-    long long last, t0, t1, t2, t3;
-    __device__ __forceinline__ void start(bool enable) {
+    long long last;
+    long long* t;  // 8 accumulators in shared memory
+    __device__ __forceinline__ void start(bool enable, long long* acc) {
         on = enable;
-        t0 = t1 = t2 = t3 = 0;
+        t = acc;
+        if (on)
+            for (int k = 0; k < 8; k++) t[k] = 0;
         last = on ? clock64() : 0;
     }
     __device__ __forceinline__ void lap(int k) {
         if (!on) return;
         const long long now = clock64();
-        const long long d = now - last;
+        t[k] += now - last;
         last = now;
-        if (k == 0) t0 += d;
-        else if (k == 1) t1 += d;
-        else if (k == 2) t2 += d;
-        else t3 += d;
     }
 };
 
@@ -511,6 +538,56 @@ __device__ __forceinline__ void block_jacobi3(const double* Bn, const double* rv
     u[0] = Bn[0] * rv[0] + Bn[1] * rv[1] + Bn[2] * rv[2];
     u[1] = Bn[3] * rv[0] + Bn[4] * rv[1] + Bn[5] * rv[2];
     u[2] = Bn[6] * rv[0] + Bn[7] * rv[1] + Bn[8] * rv[2];
+}
+
+// Restriction of a nodal 3-vector to the node's aggregate modes (P^T v):
+// mode 0 w = 1; mode 1 w = dy, thx = 1/h; mode 2 w = dx, thy = -1/h,
+// constrained DOFs excluded.
+template <typename V, typename T>
+__device__ __forceinline__ void restrict3(const V* v, const unsigned char* c, const T* bas,
+                                          double* acc) {
+    const double w = c[0] ? 0.0 : (double)v[0], tx = c[1] ? 0.0 : (double)v[1];
+    const double ty = c[2] ? 0.0 : (double)v[2];
+    acc[0] += w;
+    acc[1] += (double)bas[1] * w + (double)bas[2] * tx;
+    acc[2] += (double)bas[0] * w - (double)bas[2] * ty;
+}
+
+// u += P c for one node (c = the 3 coarse values of its aggregate).
+template <typename T>
+__device__ __forceinline__ void prolong3(const double* cvn, const unsigned char* c, const T* bas,
+                                         T* u) {
+    if (!c[0]) u[0] += (T)(cvn[0] + (double)bas[1] * cvn[1] + (double)bas[0] * cvn[2]);
+    if (!c[1]) u[1] += (T)((double)bas[2] * cvn[1]);
+    if (!c[2]) u[2] -= (T)((double)bas[2] * cvn[2]);
+}
+
+// Coarse solve cv[q] = (A_c^-1 P^T r)_q for the part's rows q < rows, from
+// the contiguous coarse residual pr (type T): 16 lanes per row reading
+// consecutive columns, two accumulators each, then a 16-lane shuffle
+// reduction (fixed order, the same bits on every run).
+template <typename T>
+__device__ __forceinline__ void coarse_solve(const T* __restrict__ Ai, int C, int rows,
+                                             const T* __restrict__ pr, double* cv) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int half = lane >> 4, hl = lane & 15;
+    for (int q0 = 2 * warp; q0 < rows; q0 += 2 * nw) {
+        const int q = q0 + half;
+        T acc0 = T(0), acc1 = T(0);
+        if (q < rows) {
+            const T* row = Ai + (size_t)q * C;
+            int j = hl;
+            for (; j + 16 < C; j += 32) {
+                acc0 += row[j] * pr[j];
+                acc1 += row[j + 16] * pr[j + 16];
+            }
+            if (j < C) acc0 += row[j] * pr[j];
+        }
+        double acc = (double)acc0 + (double)acc1;
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (hl == 0 && q < rows) cv[q] = acc;
+    }
 }
 
 // The whole PCG solve.  T = double: plain FP64.  T = float (MIXED): inner
@@ -552,6 +629,19 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
     int* tptr = (int*)(sm + L.tptr);
     uint16_t* tn = (uint16_t*)(sm + L.tnode);
     unsigned char* cm = (unsigned char*)(sm + L.cm);
+    double* Pr = (double*)(sm + L.Pr);
+    double* Ps = (double*)(sm + L.Ps);
+    double* cv = (double*)(sm + L.cv);
+    T* prc = (T*)(sm + L.prc);  // contiguous copy of the current coarse residual
+    int* ctl = (int*)(sm + L.ctl);  // [0] action, [1] final residual needed
+    T* nb = (T*)(sm + L.nb);
+    int* nslot = (int*)(sm + L.nslot);
+    const int rows = a.coarse ? 3 * (a.cagg_off[g + 1] - a.cagg_off[g]) : 0;
+    const T* aig = a.coarse ? (MIXED ? (const T*)a.ainv32 : (const T*)a.ainv64) + (size_t)a.ainv_off[g] * a.C
+                            : nullptr;
+    T* ais = (T*)(sm + L.ainv);
+    const T* Ai = a.ainv_smem ? (const T*)ais : aig;
+    const int KP = a.coarse ? 6 : 3;  // partial sums per block in a main round
     // FP64 views for the true residual: dedicated arrays in MIXED mode,
     // the (then dead) p / yt arrays in FP64 mode
     double* xl = MIXED ? (double*)(sm + L.xl) : (double*)p;
@@ -571,6 +661,19 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             const int t = i % ntask, q = i / ntask;
             kts[i] = ktg[(size_t)q * a.NT + t0 + t];
         }
+    if (a.coarse) {
+        for (int i = tid; i < nloc; i += nt) {
+            nslot[i] = a.node_slot[n0 + i];
+#pragma unroll
+            for (int q = 0; q < 3; q++) nb[3 * i + q] = (T)a.node_basis[3 * (size_t)(n0 + i) + q];
+        }
+        for (int j = tid; j < a.C; j += nt) {
+            Pr[j] = 0.0;
+            Ps[j] = 0.0;
+        }
+        if (a.ainv_smem)
+            for (int i = tid; i < rows * a.C; i += nt) ais[i] = aig[i];
+    }
     __syncthreads();
     for (int n = tid; n < nloc; n += nt) {
         const int G3 = 3 * gid[n];
@@ -595,175 +698,311 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
     const T* kt = a.ke_smem ? kts : ktg + t0;
     const size_t kstride = a.ke_smem ? (size_t)ntask : (size_t)a.NT;
     PhaseClock clk;
-    clk.start(a.timing && g == 0 && tid == 0);
+    clk.start(a.timing && g == 0 && tid == 0, (long long*)(sm + L.clk));
     Waiter wt;
     wt.start(a.timeout_ns, a.abort_flag, &a.res->wait_failures);
+    unsigned e = 1, xe = 1;  // round tags
+    int status = ST_OK;
+
+    // ---- two-level: u0 = M_bj r0 + P A_c^-1 P^T r0 (one exchange round) ----
+    if (a.coarse) {
+        double v0[3] = {0.0, 0.0, 0.0};
+        for (int n = tid; n < no; n += nt) restrict3(r + 3 * n, cm + 3 * n, nb + 3 * n, v0);
+        block_sum<3>(v0, red);
+        unsigned long long* pb0 = a.llp + (size_t)(e & 1) * a.G * 16;
+        if (tid == 0)
+#pragma unroll
+            for (int k = 0; k < 3; k++) Tag<double>::put(pb0 + (size_t)g * 16 + 2 * k, v0[k], e);
+        const bool ok = exchange_round<T>(pb0, a.G, 3, nullptr, w, no, no, gid, e, sp, wt);
+        if (__syncthreads_or(!ok)) {
+            status = ST_TIMEOUT;
+        } else {
+            for (int j = tid; j < a.C; j += nt) {
+                Pr[j] = sp[j];
+                prc[j] = (T)sp[j];
+            }
+            __syncthreads();
+            coarse_solve<T>(Ai, a.C, rows, prc, cv);
+            __syncthreads();
+            for (int n = tid; n < nloc; n += nt) prolong3(cv + 3 * nslot[n], cm + 3 * n, nb + 3 * n, u + 3 * n);
+            __syncthreads();
+        }
+        e++;
+    }
 
     double gamma_prev = 1.0, alpha_prev = 1.0, bnorm = 0.0, rn_ref = 0.0;
-    unsigned e = 1, xe = 1;  // round tags
-    int it = 0, stop = -1, status = ST_OK, xupd = 0, xupd_ref = 0, nru = 0;
+    int it = 0, stop = -1, xupd = 0, xupd_ref = 0, nru = 0;
     double final_res = 0.0, true_rel = -1.0;
     bool first = true;
 
-    for (;; it++) {
+    for (; status == ST_OK; it++) {
+        const bool tr = it == a.trace_it && tid == 0;
+        if (tr) a.trace[4 * g] = gtimer();
         // ---- w = A u on owned rows ----
         task_matvec<NPE, T, T>(u, yt, ntask, tn, kt, kstride);
         __syncthreads();
         clk.lap(0);
         // ---- gather, BC rows, dot products, publish w ----
-        double v[3] = {0.0, 0.0, 0.0};
+        double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         unsigned long long* vb = a.llv + (size_t)(e & 1) * N3 * 2;
-        unsigned long long* pb = a.llp + (size_t)(e & 1) * a.G * 8;
-        for (int n = tid; n < no; n += nt) {
-            T wv[3];
-            gather3(yt, ntask, tptr[n], tptr[n + 1], wv[0], wv[1], wv[2]);
-            const int G3 = 3 * gid[n];
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-                const int k = 3 * n + d;
-                if (cm[k]) wv[d] = u[k];
-                w[k] = wv[d];
-                v[0] += (double)r[k] * (double)u[k];
-                v[1] += (double)wv[d] * (double)u[k];
-                v[2] += (double)r[k] * (double)r[k];
-                Tag<T>::put(vb + (size_t)(G3 + d) * TW, wv[d], e);
+        unsigned long long* pb = a.llp + (size_t)(e & 1) * a.G * 16;
+        for (int k = tid; k < 3 * no; k += nt) {
+            const int n = k / 3, d = k - 3 * n;
+            const int tb = tptr[n + 1];
+            T wk = T(0);
+            for (int t = tptr[n]; t < tb; t++) wk += yt[d * ntask + t];
+            const bool c = cm[k] != 0;
+            const T uk = u[k], rk = r[k];
+            if (c) wk = uk;
+            w[k] = wk;
+            v[0] += (double)rk * (double)uk;
+            v[1] += (double)wk * (double)uk;
+            v[2] += (double)rk * (double)rk;
+            Tag<T>::put(vb + (size_t)(3 * gid[n] + d) * TW, wk, e);
+            if (a.coarse && !c) {
+                const T* bs = nb + 3 * n;  // dx, dy, 1/h
+                const double wd = (double)wk;
+                if (d == 0) {
+                    v[3] += wd;
+                    v[4] += (double)bs[1] * wd;
+                    v[5] += (double)bs[0] * wd;
+                } else if (d == 1) {
+                    v[4] += (double)bs[2] * wd;
+                } else {
+                    v[5] -= (double)bs[2] * wd;
+                }
             }
         }
-        block_sum<3>(v, red);
-        if (tid == 0)
-#pragma unroll
-            for (int k = 0; k < 3; k++) Tag<double>::put(pb + (size_t)g * 8 + 2 * k, v[k], e);
         clk.lap(1);
+        if (a.coarse)
+            block_sum<6, false>(v, red);
+        else
+            block_sum<3, false>(v, red);
+        clk.lap(2);
+        if (tid == 0)
+            for (int k = 0; k < KP; k++) Tag<double>::put(pb + (size_t)g * 16 + 2 * k, v[k], e);
+        if (tr) a.trace[4 * g + 1] = gtimer();
+        clk.lap(3);
         // ---- exchange: every block's partials and this block's ghost w ----
         {
-            bool ok = exchange_round<T>(pb, a.G, 3, vb, w, no, nloc, gid, e, sp, wt);
+            bool ok = exchange_round<T>(pb, a.G, KP, vb, w, no, nloc, gid, e, sp, wt);
             if (a.test_stall && it == 0 && tid == 0) {
                 double never;  // a tag no block writes: the wait must run out
-                ok = ok && poll<double>(a.llp + (size_t)a.G * 16, 0xffffffffu, never, wt);
+                ok = ok && poll<double>(a.llp + (size_t)a.G * 32, 0xffffffffu, never, wt);
             }
             if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
-            sum_partials<3>(sp, a.G, scal);
-            __syncthreads();
+            sum_partials<3>(sp, a.G, KP, scal);
         }
         e++;
-        clk.lap(2);
-        const double gamma = scal[0], delta = scal[1], rho = scal[2];
-
-        // ---- decisions (identical in every block) ----
-        if (!isfinite(gamma) || !isfinite(delta) || !isfinite(rho)) {
-            if (g == 0 && tid == 0) {
-                a.res->nonfinite_it = it;
-                a.res->nonfinite_vals[0] = gamma;
-                a.res->nonfinite_vals[1] = delta;
-                a.res->nonfinite_vals[2] = rho;
-            }
-            status = ST_NONFINITE;
-            break;
-        }
-        const double rn = sqrt(rho);
-        if (first) {
-            bnorm = rn;
-            rn_ref = rn;
-            if (bnorm < 1e-30) { stop = STOP_ZERO_RHS; final_res = 0.0; true_rel = 0.0; break; }
-        } else {
-            const bool conv = (a.stop_rule == 0 && rn < a.tol) || rn / bnorm < a.tol;
-            if constexpr (MIXED) {
-                const bool want = conv || rn <= a.reliable_delta * rn_ref ||
-                                  xupd - xupd_ref >= a.reliable_interval;
-                if (want) {
-                    // ---- reliable update: r = F - K x in FP64 ----
-                    for (int n = tid; n < no; n += nt)
-#pragma unroll
-                        for (int d = 0; d < 3; d++)
-                            Tag<double>::put(a.llx + (size_t)(3 * gid[n] + d) * 2, x[3 * n + d], xe);
-                    bool ok = true;
-                    for (int k = tid; k < 3 * nloc && ok; k += nt) {
-                        if (k < 3 * no) { xl[k] = x[k]; continue; }
-                        double xv;
-                        ok = poll<double>(a.llx + (size_t)(3 * gid[k / 3] + k % 3) * 2, xe, xv, wt);
-                        xl[k] = xv;
-                    }
-                    if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
-                    xe++;
-                    task_matvec<NPE, double, double>(xl, ytd, ntask, tn, a.kt64 + t0, (size_t)a.NT);
-                    __syncthreads();
-                    double vt[1] = {0.0};
-                    unsigned long long* rb = a.llv + (size_t)(e & 1) * N3 * 2;
-                    unsigned long long* qb = a.llp + (size_t)(e & 1) * a.G * 8;
-                    for (int n = tid; n < no; n += nt) {
-                        double kx[3];
-                        gather3(ytd, ntask, tptr[n], tptr[n + 1], kx[0], kx[1], kx[2]);
-                        const int G3 = 3 * gid[n];
-#pragma unroll
-                        for (int d = 0; d < 3; d++) {
-                            const int k = 3 * n + d;
-                            const double rt = cm[k] ? -xl[k] : (double)a.F[G3 + d] - kx[d];
-                            vt[0] += rt * rt;
-                            r[k] = (T)rt;
-                            Tag<T>::put(rb + (size_t)(G3 + d) * TW, (T)rt, e);
-                        }
-                    }
-                    block_sum<1>(vt, red);
-                    if (tid == 0) Tag<double>::put(qb + (size_t)g * 8, vt[0], e);
-                    ok = exchange_round<T>(qb, a.G, 1, rb, r, no, nloc, gid, e, sp, wt);
-                    if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
-                    sum_partials<1>(sp, a.G, scal);
-                    __syncthreads();
-                    e++;
-                    const double trn = sqrt(scal[0]);
-                    for (int n = tid; n < nloc; n += nt) block_jacobi3(B + 9 * n, r + 3 * n, u + 3 * n);
-                    __syncthreads();
-                    nru++;
-                    rn_ref = trn;
-                    xupd_ref = xupd;
-                    if (!isfinite(trn)) { status = ST_NONFINITE; break; }
-                    if ((a.stop_rule == 0 && trn < a.tol) || trn / bnorm < a.tol) {
-                        stop = STOP_CONVERGED; final_res = trn; true_rel = trn / bnorm; break;
-                    }
-                    if (xupd >= a.maxit) { stop = STOP_MAX_ITER; final_res = trn; true_rel = trn / bnorm; break; }
-                    clk.lap(3);
-                    continue;
+        clk.lap(4);
+        // ---- decisions: thread 0 decides (warp 0 just summed the partials),
+        //      the block follows after one barrier ----
+        __syncwarp();
+        if (tid == 0) {
+            const double gamma = scal[0], delta = scal[1], rho = scal[2];
+            int act = ACT_UPDATE;
+            const double rn = sqrt(rho);
+            if (!isfinite(gamma) || !isfinite(delta) || !isfinite(rho)) {
+                if (g == 0) {
+                    a.res->nonfinite_it = it;
+                    a.res->nonfinite_vals[0] = gamma;
+                    a.res->nonfinite_vals[1] = delta;
+                    a.res->nonfinite_vals[2] = rho;
                 }
+                act = ACT_NONFINITE;
+            } else if (first && rn < 1e-30) {
+                bnorm = rn;
+                stop = STOP_ZERO_RHS; final_res = 0.0; true_rel = 0.0; act = ACT_STOP;
             } else {
-                if (conv) { stop = STOP_CONVERGED; final_res = rn; break; }
+                if (first) {
+                    bnorm = rn;
+                    rn_ref = rn;
+                } else {
+                    const bool conv = (a.stop_rule == 0 && rn < a.tol) || rn / bnorm < a.tol;
+                    if (MIXED && (conv || rn <= a.reliable_delta * rn_ref ||
+                                  xupd - xupd_ref >= a.reliable_interval))
+                        act = ACT_RU;
+                    else if (!MIXED && conv) {
+                        stop = STOP_CONVERGED; final_res = rn; act = ACT_STOP;
+                    }
+                }
+                if (act == ACT_UPDATE && xupd >= a.maxit) {
+                    stop = STOP_MAX_ITER; final_res = rn; act = ACT_STOP;
+                }
+                if (act == ACT_UPDATE) {
+                    const double beta = first ? 0.0 : gamma / gamma_prev;
+                    const double pap = first ? delta : delta - beta * gamma / alpha_prev;
+                    if (fabs(pap) < 1e-30) {
+                        stop = STOP_BREAKDOWN; xupd++; final_res = rn; act = ACT_STOP;
+                    } else {
+                        const double alpha = gamma / pap;
+                        gamma_prev = gamma;
+                        alpha_prev = alpha;
+                        first = false;
+                        xupd++;
+                        scal[3] = alpha;
+                        scal[4] = beta;
+                    }
+                }
             }
+            ctl[0] = act;
+            ctl[1] = (act == ACT_STOP && true_rel < 0.0) ? 1 : 0;
         }
-        if (xupd >= a.maxit) { stop = STOP_MAX_ITER; final_res = rn; break; }
-        const double beta = first ? 0.0 : gamma / gamma_prev;
-        const double pap = first ? delta : delta - beta * gamma / alpha_prev;
-        if (fabs(pap) < 1e-30) { stop = STOP_BREAKDOWN; xupd++; final_res = rn; break; }
-        const double alpha = gamma / pap;
-        gamma_prev = gamma;
-        alpha_prev = alpha;
-        first = false;
+        __syncthreads();
+        const int act = ctl[0];
+        if (tr) a.trace[4 * g + 2] = gtimer();
+        if (act == ACT_NONFINITE) { status = ST_NONFINITE; break; }
+        if (act == ACT_STOP) break;
+        clk.lap(5);
 
-        // ---- p, s, x, r updates and u = M^-1 r on owned and ghost nodes ----
-        const T bt = (T)beta, at = (T)alpha;
-        for (int n = tid; n < nloc; n += nt) {
-            T rv[3];
+        if (MIXED && act == ACT_RU) {
+            // ---- reliable update: r = F - K x in FP64 ----
+            for (int n = tid; n < no; n += nt)
 #pragma unroll
-            for (int d = 0; d < 3; d++) {
-                const int k = 3 * n + d;
+                for (int d = 0; d < 3; d++)
+                    Tag<double>::put(a.llx + (size_t)(3 * gid[n] + d) * 2, x[3 * n + d], xe);
+            bool ok = true;
+            for (int k = tid; k < 3 * nloc && ok; k += nt) {
+                if (k < 3 * no) { xl[k] = x[k]; continue; }
+                double xv;
+                ok = poll<double>(a.llx + (size_t)(3 * gid[k / 3] + k % 3) * 2, xe, xv, wt);
+                xl[k] = xv;
+            }
+            if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
+            xe++;
+            task_matvec<NPE, double, double>(xl, ytd, ntask, tn, a.kt64 + t0, (size_t)a.NT);
+            __syncthreads();
+            double vt[4] = {0.0, 0.0, 0.0, 0.0};
+            const int KR = a.coarse ? 4 : 1;
+            unsigned long long* rb = a.llv + (size_t)(e & 1) * N3 * 2;
+            unsigned long long* qb = a.llp + (size_t)(e & 1) * a.G * 16;
+            for (int n = tid; n < no; n += nt) {
+                double kx[3], rtv[3];
+                gather3(ytd, ntask, tptr[n], tptr[n + 1], kx[0], kx[1], kx[2]);
+                const int G3 = 3 * gid[n];
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const int k = 3 * n + d;
+                    const double rt = cm[k] ? -xl[k] : (double)a.F[G3 + d] - kx[d];
+                    vt[0] += rt * rt;
+                    rtv[d] = rt;
+                    r[k] = (T)rt;
+                    Tag<T>::put(rb + (size_t)(G3 + d) * TW, (T)rt, e);
+                }
+                if (a.coarse) restrict3(rtv, cm + 3 * n, nb + 3 * n, vt + 1);
+            }
+            if (a.coarse)
+                block_sum<4>(vt, red);
+            else
+                block_sum<1>(vt, red);
+            if (tid == 0)
+                for (int k = 0; k < KR; k++) Tag<double>::put(qb + (size_t)g * 16 + 2 * k, vt[k], e);
+            ok = exchange_round<T>(qb, a.G, KR, rb, r, no, nloc, gid, e, sp, wt);
+            if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
+            sum_partials<1>(sp, a.G, KR, scal);
+            if (a.coarse)
+                for (int j = tid; j < a.C; j += nt) {
+                    Pr[j] = sp[(j / 3) * 4 + 1 + j % 3];
+                    prc[j] = (T)Pr[j];
+                }
+            __syncthreads();
+            e++;
+            if (a.coarse) {
+                coarse_solve<T>(Ai, a.C, rows, prc, cv);
+                __syncthreads();
+            }
+            for (int n = tid; n < nloc; n += nt) {
+                block_jacobi3(B + 9 * n, r + 3 * n, u + 3 * n);
+                if (a.coarse) prolong3(cv + 3 * nslot[n], cm + 3 * n, nb + 3 * n, u + 3 * n);
+            }
+            if (tid == 0) {
+                const double trn = sqrt(scal[0]);
+                int act2 = ACT_UPDATE;
+                nru++;
+                rn_ref = trn;
+                xupd_ref = xupd;
+                if (!isfinite(trn)) {
+                    act2 = ACT_NONFINITE;
+                } else if ((a.stop_rule == 0 && trn < a.tol) || trn / bnorm < a.tol) {
+                    stop = STOP_CONVERGED; final_res = trn; true_rel = trn / bnorm; act2 = ACT_STOP;
+                } else if (xupd >= a.maxit) {
+                    stop = STOP_MAX_ITER; final_res = trn; true_rel = trn / bnorm; act2 = ACT_STOP;
+                }
+                ctl[0] = act2;
+                ctl[1] = 0;
+            }
+            __syncthreads();
+            if (ctl[0] == ACT_NONFINITE) { status = ST_NONFINITE; break; }
+            if (ctl[0] == ACT_STOP) break;
+            clk.lap(7);
+            // the next round runs on buffers [e & 1]; the other pair may still be read
+            continue;
+        }
+
+        // ---- coarse correction: c = A_c^-1 P^T r_new, with
+        //      P^T s = P^T w + beta P^T s and P^T r_new = P^T r - alpha P^T s ----
+        const double alpha = scal[3], beta = scal[4];
+        const T bt = (T)beta, at = (T)alpha;
+        if (a.coarse) {
+            // P^T s = P^T w + beta P^T s;  P^T r -= alpha P^T s  (every block, all C)
+            const double* Pw = sp + 3;  // stride 6: this round's P^T w of every block
+            for (int j = tid; j < a.C; j += nt) {
+                const double ps = Pw[(j / 3) * 6 + j % 3] + beta * Ps[j];
+                const double prn = Pr[j] - alpha * ps;
+                Ps[j] = ps;
+                Pr[j] = prn;
+                prc[j] = (T)prn;
+            }
+            // p, s, x, r on owned and ghost nodes
+            for (int k = tid; k < 3 * nloc; k += nt) {
                 const T pk = u[k] + bt * p[k];
                 const T sk = w[k] + bt * s[k];
                 p[k] = pk;
                 s[k] = sk;
-                if (n < no) x[k] += alpha * (double)pk;
-                rv[d] = r[k] - at * sk;
-                r[k] = rv[d];
+                if (k < 3 * no) x[k] += alpha * (double)pk;
+                r[k] -= at * sk;
             }
-            block_jacobi3(B + 9 * n, rv, u + 3 * n);
+            __syncthreads();
+            clk.lap(7);
+            coarse_solve<T>(Ai, a.C, rows, prc, cv);
+            __syncthreads();
+            clk.lap(6);
+            // u = M_bj r + P c
+            for (int n = tid; n < nloc; n += nt) {
+                block_jacobi3(B + 9 * n, r + 3 * n, u + 3 * n);
+                prolong3(cv + 3 * nslot[n], cm + 3 * n, nb + 3 * n, u + 3 * n);
+            }
+            __syncthreads();
+            clk.lap(7);
+            if (tr) a.trace[4 * g + 3] = gtimer();
+        } else {
+            // p, s, x, r updates and u = M_bj r on owned and ghost nodes
+            for (int n = tid; n < nloc; n += nt) {
+                T rv[3];
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const int k = 3 * n + d;
+                    const T pk = u[k] + bt * p[k];
+                    const T sk = w[k] + bt * s[k];
+                    p[k] = pk;
+                    s[k] = sk;
+                    if (n < no) x[k] += alpha * (double)pk;
+                    rv[d] = r[k] - at * sk;
+                    r[k] = rv[d];
+                }
+                block_jacobi3(B + 9 * n, rv, u + 3 * n);
+            }
+            __syncthreads();
+            clk.lap(7);
+            if (tr) a.trace[4 * g + 3] = gtimer();
         }
-        __syncthreads();
-        xupd++;
-        clk.lap(3);
     }
 
     // ---- write x; FP64 true residual ||F - K x|| unless already known ----
     for (int n = tid; n < no; n += nt)
 #pragma unroll
         for (int d = 0; d < 3; d++) a.x[3 * gid[n] + d] = x[3 * n + d];
-    if (status == ST_OK && true_rel < 0.0) {
+    if (status == ST_OK && ctl[1]) {
         for (int n = tid; n < no; n += nt)
 #pragma unroll
             for (int d = 0; d < 3; d++)
@@ -798,17 +1037,17 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
                 }
             }
             block_sum<2>(v, red);
-            unsigned long long* pb = a.llp + (size_t)(e & 1) * a.G * 8;
+            unsigned long long* pb = a.llp + (size_t)(e & 1) * a.G * 16;
             if (tid == 0) {
-                Tag<double>::put(pb + (size_t)g * 8, v[0], e);
-                Tag<double>::put(pb + (size_t)g * 8 + 2, v[1], e);
+                Tag<double>::put(pb + (size_t)g * 16, v[0], e);
+                Tag<double>::put(pb + (size_t)g * 16 + 2, v[1], e);
             }
             if (g == 0) {
                 ok = exchange_round<T>(pb, a.G, 2, nullptr, w, no, no, gid, e, sp, wt);
                 if (__syncthreads_or(!ok)) {
                     status = ST_TIMEOUT;
                 } else {
-                    sum_partials<2>(sp, a.G, scal);
+                    sum_partials<2>(sp, a.G, 2, scal);
                     __syncthreads();
                     if (tid == 0) true_rel = scal[1] > 0 ? sqrt(scal[0] / scal[1]) : 0.0;
                 }
@@ -825,10 +1064,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
         a.res->b_norm = bnorm;
         a.res->reliable_updates = nru;
         a.res->reductions = (int)e - 1;
-        a.res->phase_cycles[0] = clk.t0;
-        a.res->phase_cycles[1] = clk.t1;
-        a.res->phase_cycles[2] = clk.t2;
-        a.res->phase_cycles[3] = clk.t3;
+        for (int k = 0; k < 8; k++) a.res->phase_cycles[k] = clk.on ? clk.t[k] : 0;
     }
 }
 

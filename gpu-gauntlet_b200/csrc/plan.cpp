@@ -247,6 +247,149 @@ std::string build_partition(const pg_problem& p, int G, HostPlan& plan) {
     return "";
 }
 
+std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, HostPlan& plan) {
+    const int G = plan.G, Nn = plan.Nn, npe = plan.npe, nd = 3 * npe;
+    const int C = 3 * G;
+    plan.C = C;
+    std::vector<int> owner(Nn, 0);
+    std::vector<double> cx(G, 0.0), cy(G, 0.0), ih(G, 1.0);
+    for (int g = 0; g < G; g++) {
+        const int n0 = plan.node_off[g], no = plan.nown[g];
+        double sx = 0, sy = 0, lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
+        for (int k = 0; k < no; k++) {
+            const int n = plan.nodes[n0 + k];
+            owner[n] = g;
+            const double x = p.nodes[2 * n], y = p.nodes[2 * n + 1];
+            sx += x;
+            sy += y;
+            lo[0] = std::min(lo[0], x); hi[0] = std::max(hi[0], x);
+            lo[1] = std::min(lo[1], y); hi[1] = std::max(hi[1], y);
+        }
+        if (no > 0) {
+            cx[g] = sx / no;
+            cy[g] = sy / no;
+            const double h = std::max(hi[0] - lo[0], hi[1] - lo[1]);
+            ih[g] = h > 0 ? 1.0 / h : 1.0;
+        }
+    }
+    // basis of node n in mode m, DOF d (masked by constraints); Phi[d][m]
+    auto phi = [&](int n, double Phi[3][3]) {
+        const int a = owner[n];
+        const double dx = (p.nodes[2 * n] - cx[a]) * ih[a], dy = (p.nodes[2 * n + 1] - cy[a]) * ih[a];
+        const double v[3][3] = {{1.0, dy, dx}, {0.0, ih[a], 0.0}, {0.0, 0.0, -ih[a]}};
+        for (int d = 0; d < 3; d++)
+            for (int m = 0; m < 3; m++) Phi[d][m] = p.constrained[3 * n + d] ? 0.0 : v[d][m];
+    };
+    // A_c = P^T K P, element by element
+    std::vector<double> Ac((size_t)C * C, 0.0);
+    const size_t kk = (size_t)nd * nd;
+    for (int e = 0; e < plan.Ne; e++) {
+        const double* K = ke64.data() + (size_t)e * kk;
+        double Ph[4][3][3];
+        int ag[4];
+        for (int i = 0; i < npe; i++) {
+            const int n = (int)p.elements[(size_t)e * npe + i];
+            phi(n, Ph[i]);
+            ag[i] = owner[n];
+        }
+        for (int i = 0; i < npe; i++)
+            for (int j = 0; j < npe; j++) {
+                double T[3][3];  // K_ij Phi_j
+                for (int d = 0; d < 3; d++)
+                    for (int m = 0; m < 3; m++) {
+                        double acc = 0;
+                        for (int f = 0; f < 3; f++) acc += K[(3 * i + d) * nd + 3 * j + f] * Ph[j][f][m];
+                        T[d][m] = acc;
+                    }
+                for (int mi = 0; mi < 3; mi++)
+                    for (int mj = 0; mj < 3; mj++) {
+                        double acc = 0;
+                        for (int d = 0; d < 3; d++) acc += Ph[i][d][mi] * T[d][mj];
+                        Ac[(size_t)(3 * ag[i] + mi) * C + 3 * ag[j] + mj] += acc;
+                    }
+            }
+    }
+    // Cholesky with dependent modes dropped, then the explicit inverse
+    std::vector<double> Lm((size_t)C * C, 0.0);
+    std::vector<char> keep(C, 1);
+    double dmax = 0;
+    for (int i = 0; i < C; i++) dmax = std::max(dmax, Ac[(size_t)i * C + i]);
+    plan.dropped_modes = 0;
+    for (int j = 0; j < C; j++) {
+        double d = Ac[(size_t)j * C + j];
+        for (int k = 0; k < j; k++) d -= Lm[(size_t)j * C + k] * Lm[(size_t)j * C + k];
+        if (!(d > 1e-13 * dmax)) {
+            keep[j] = 0;
+            plan.dropped_modes++;
+            continue;
+        }
+        const double ljj = std::sqrt(d);
+        Lm[(size_t)j * C + j] = ljj;
+        for (int i = j + 1; i < C; i++) {
+            double s = Ac[(size_t)i * C + j];
+            for (int k = 0; k < j; k++) s -= Lm[(size_t)i * C + k] * Lm[(size_t)j * C + k];
+            Lm[(size_t)i * C + j] = s / ljj;
+        }
+    }
+    // inverse of L (lower), dropped columns stay zero
+    std::vector<double> Li((size_t)C * C, 0.0);
+    for (int j = 0; j < C; j++) {
+        if (!keep[j]) continue;
+        Li[(size_t)j * C + j] = 1.0 / Lm[(size_t)j * C + j];
+        for (int i = j + 1; i < C; i++) {
+            if (!keep[i]) continue;
+            double s = 0;
+            for (int k = j; k < i; k++) s += Lm[(size_t)i * C + k] * Li[(size_t)k * C + j];
+            Li[(size_t)i * C + j] = -s / Lm[(size_t)i * C + i];
+        }
+    }
+    std::vector<double> Ainv((size_t)C * C, 0.0);  // L^-T L^-1
+    for (int i = 0; i < C; i++)
+        for (int j = 0; j <= i; j++) {
+            double s = 0;
+            for (int k = i; k < C; k++) s += Li[(size_t)k * C + i] * Li[(size_t)k * C + j];
+            Ainv[(size_t)i * C + j] = s;
+            Ainv[(size_t)j * C + i] = s;
+        }
+    // per part: aggregates of its local nodes, node slots and basis data
+    plan.node_basis.assign(3 * plan.nodes.size(), 0.0);
+    plan.node_slot.assign(plan.nodes.size(), 0);
+    plan.cagg_off.assign(G + 1, 0);
+    plan.cagg.clear();
+    plan.ainv_off.assign(G + 1, 0);
+    plan.ainv.clear();
+    plan.max_kagg = 0;
+    std::vector<int> slot_of(G, -1);
+    for (int g = 0; g < G; g++) {
+        const int n0 = plan.node_off[g], nl = plan.node_off[g + 1] - n0;
+        std::vector<int> list = {g};
+        slot_of[g] = 0;
+        for (int k = 0; k < nl; k++) {
+            const int a = owner[plan.nodes[n0 + k]];
+            if (slot_of[a] < 0) { slot_of[a] = (int)list.size(); list.push_back(a); }
+        }
+        for (int k = 0; k < nl; k++) {
+            const int n = plan.nodes[n0 + k], a = owner[n];
+            plan.node_slot[n0 + k] = slot_of[a];
+            plan.node_basis[3 * (n0 + k)] = (p.nodes[2 * n] - cx[a]) * ih[a];
+            plan.node_basis[3 * (n0 + k) + 1] = (p.nodes[2 * n + 1] - cy[a]) * ih[a];
+            plan.node_basis[3 * (n0 + k) + 2] = ih[a];
+        }
+        plan.ainv_off[g] = (int)(plan.ainv.size() / C);
+        for (int a : list)
+            for (int m = 0; m < 3; m++)
+                plan.ainv.insert(plan.ainv.end(), Ainv.begin() + (size_t)(3 * a + m) * C,
+                                 Ainv.begin() + (size_t)(3 * a + m + 1) * C);
+        plan.cagg.insert(plan.cagg.end(), list.begin(), list.end());
+        plan.cagg_off[g + 1] = (int)plan.cagg.size();
+        plan.max_kagg = std::max(plan.max_kagg, (int)list.size());
+        for (int a : list) slot_of[a] = -1;
+    }
+    plan.ainv_off[G] = (int)(plan.ainv.size() / C);
+    plan.coarse = true;
+    return "";
+}
+
 uint64_t problem_hash(const pg_problem& p) {
     uint64_t h = 0x9e3779b97f4a7c15ull;
     auto mix = [&](uint64_t v) {

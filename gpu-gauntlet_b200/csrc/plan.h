@@ -39,6 +39,19 @@ struct HostPlan {
     std::vector<uint32_t> color_offsets, elements_by_color;
     bool recolored = false;
     int max_nloc = 0, max_nown = 0, max_ntask = 0;
+
+    // Two-level coarse space: one aggregate per part (its owned nodes), 3
+    // modes each (the plate's rigid-body motions: w = 1; w = y, thx = 1;
+    // w = x, thy = -1, in coordinates about the aggregate centre scaled by
+    // its size h).  C = 3 G coarse DOFs.
+    bool coarse = false;
+    int C = 0, max_kagg = 0;
+    std::vector<double> node_basis;  // per part-local node: dx, dy, 1/h of its aggregate
+    std::vector<int> node_slot;      // per part-local node: index in the part's aggregate list
+    std::vector<int> cagg_off, cagg; // per part: aggregates touching its local nodes (own first)
+    std::vector<int> ainv_off;       // per part: first row of its A_c^-1 rows (3 per aggregate)
+    std::vector<double> ainv;        // rows of A_c^-1, [rows][C]
+    int dropped_modes = 0;           // coarse modes dropped as numerically dependent
 };
 
 // Checks the problem arrays; returns "" when valid, else the reason.
@@ -49,6 +62,11 @@ std::string build_structure(const pg_problem& p, HostPlan& plan);
 
 // Partitions into G parts (G <= node_count) and fills the part arrays.
 std::string build_partition(const pg_problem& p, int G, HostPlan& plan);
+
+// Coarse space of the two-level preconditioner from the element matrices
+// ke64 ([Ne][(3 npe)^2], FP64): per-node basis data, per-part aggregate
+// lists, and the rows of A_c^-1 = (P^T A P)^-1 each part needs.
+std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, HostPlan& plan);
 
 // 64-bit FNV-1a over the problem's mesh, colouring, material and
 // constraint arrays (not F): the key of the plan cache.

@@ -60,6 +60,11 @@ struct Plan {
     uint64_t key = 0;
     int G = 0;
     pg::HostPlan hp;
+    // host copies of the mesh arrays the coarse-space set-up reads later
+    std::vector<float> h_nodes;
+    std::vector<uint32_t> h_elements;
+    std::vector<uint8_t> h_cons;
+    pg_problem prob_view{};
     double E = 0, nu = 0, t = 0;
     bool has_elem_t = false;
     DevBuf<int> node_off, nown, nodes, task_off, tp_off, tptr, task_elem, inc_ptr, inc_idx;
@@ -71,7 +76,11 @@ struct Plan {
     DevBuf<double> ke64, kt64, binv64, x;
     DevBuf<float> ke32, kt32, binv32;
     DevBuf<unsigned long long> llv, llx, llp;
+    DevBuf<int> cagg_off, node_slot, ainv_off;
+    DevBuf<double> node_basis, ainv64;
+    DevBuf<float> ainv32;
     DevBuf<int> abort_flag;
+    DevBuf<unsigned long long> trace;
     DevBuf<pg::PcgResult> res;
 };
 
@@ -119,7 +128,8 @@ int auto_ctas(const pg_ctx* c, int Nn) {
     return std::max(1, std::min(G, c->sms));
 }
 
-pg::SmemLayout make_layout(const pg::HostPlan& hp, bool mixed, bool ke_smem) {
+pg::SmemLayout make_layout(const pg::HostPlan& hp, bool mixed, bool ke_smem, bool coarse,
+                           bool ainv_smem) {
     const size_t T = mixed ? 4 : 8, nd = 3 * hp.npe;
     const size_t nloc = hp.max_nloc, nown = hp.max_nown, ntask = hp.max_ntask;
     size_t off = 0;
@@ -134,7 +144,14 @@ pg::SmemLayout make_layout(const pg::HostPlan& hp, bool mixed, bool ke_smem) {
     L.ytd = take(mixed ? 3 * ntask * 8 : 0);
     L.red = take(128 * 8);
     L.scal = take(8 * 8);
-    L.sp = take((size_t)3 * hp.G * 8);
+    L.sp = take((size_t)6 * hp.G * 8);
+    L.Pr = take(coarse ? (size_t)hp.C * 8 : 0);
+    L.Ps = take(coarse ? (size_t)hp.C * 8 : 0);
+    L.cv = take(coarse ? (size_t)3 * hp.max_kagg * 8 : 0);
+    L.cpart = take(0);
+    L.prc = take(coarse ? (size_t)hp.C * T : 0);
+    L.ctl = take(4 * 4);
+    L.clk = take(8 * 8);
     L.r = take(3 * nloc * T);
     L.u = take(3 * nloc * T);
     L.p = take(3 * nloc * T);
@@ -143,6 +160,9 @@ pg::SmemLayout make_layout(const pg::HostPlan& hp, bool mixed, bool ke_smem) {
     L.B = take(9 * nloc * T);
     L.yt = take(3 * ntask * T);
     L.kt = take(ke_smem ? 3 * nd * ntask * T : 0);
+    L.nb = take(coarse ? 3 * nloc * T : 0);
+    L.ainv = take(coarse && ainv_smem ? (size_t)3 * hp.max_kagg * hp.C * T : 0);
+    L.nslot = take(coarse ? nloc * 4 : 0);
     L.gid = take(nloc * 4);
     L.tptr = take((nown + 1) * 4);
     L.tnode = take(hp.npe * ntask * 2);
@@ -157,6 +177,17 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G) {
     if (e.empty()) e = pg::build_partition(p, G, pl->hp);
     if (!e.empty()) throw Fail{PG_EINVAL, e};
     pl->G = pl->hp.G;
+    pl->h_nodes.assign(p.nodes, p.nodes + 2 * (size_t)p.node_count);
+    pl->h_elements.assign(p.elements, p.elements + (size_t)p.nodes_per_element * p.element_count);
+    pl->h_cons.assign(p.constrained, p.constrained + 3 * (size_t)p.node_count);
+    pl->prob_view = p;
+    pl->prob_view.nodes = pl->h_nodes.data();
+    pl->prob_view.elements = pl->h_elements.data();
+    pl->prob_view.constrained = pl->h_cons.data();
+    pl->prob_view.F = nullptr;
+    pl->prob_view.color_offsets = nullptr;
+    pl->prob_view.elements_by_color = nullptr;
+    pl->prob_view.elem_t = nullptr;
     pl->E = p.E;
     pl->nu = p.nu;
     pl->t = p.t;
@@ -193,8 +224,9 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G) {
     pl->x.alloc(3 * Nn);
     pl->llv.alloc(12 * Nn);
     pl->llx.alloc(6 * Nn);
-    pl->llp.alloc(16 * (size_t)pl->G + 2);
+    pl->llp.alloc(32 * (size_t)pl->G + 2);
     pl->abort_flag.alloc(1);
+    pl->trace.alloc(4 * (size_t)pl->G);
     pl->res.alloc(1);
     // synchronous: uploads read the host plan arrays
     CK(cudaStreamSynchronize(st));
@@ -256,10 +288,36 @@ void fill_options(const pg_options* in, pg_options* o) {
         throw Fail{PG_EINVAL, "unknown precision"};
     if (o->stop_rule != PG_STOP_REFERENCE && o->stop_rule != PG_STOP_RELATIVE)
         throw Fail{PG_EINVAL, "unknown stop_rule"};
-    if (o->threads < 0 || o->threads > 512 || (o->threads % 32) != 0)
-        throw Fail{PG_EINVAL, "threads must be a multiple of 32 in [32, 512] (0 = automatic)"};
+    if (o->threads < 0 || o->threads > pg::kMaxThreads || (o->threads % 32) != 0)
+        throw Fail{PG_EINVAL, "threads must be a multiple of 32 in [32, 576] (0 = automatic)"};
     if (o->ctas < 0) throw Fail{PG_EINVAL, "ctas must be >= 0"};
     if (!(o->wait_timeout_ms >= 0)) throw Fail{PG_EINVAL, "wait_timeout_ms must be >= 0"};
+}
+
+// Coarse data of the two-level preconditioner, built once per plan: the
+// element matrices come from the device, A_c = P^T K P and its inverse are
+// formed on the host, and each part's A_c^-1 rows go back to the device.
+void ensure_coarse(pg_ctx* c, Plan* pl) {
+    pg::HostPlan& hp = pl->hp;
+    if (hp.coarse) return;
+    run_setup(c, pl);
+    const size_t kk = 9 * (size_t)hp.npe * hp.npe;
+    std::vector<double> ke(std::max<size_t>(1, (size_t)hp.Ne * kk));
+    if (hp.Ne > 0)
+        CK(cudaMemcpyAsync(ke.data(), pl->ke64.p, (size_t)hp.Ne * kk * sizeof(double),
+                           cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::string e = pg::build_coarse(pl->prob_view, ke, hp);
+    if (!e.empty()) throw Fail{PG_EINVAL, e};
+    cudaStream_t st = c->stream;
+    pl->cagg_off.upload(hp.cagg_off.data(), hp.cagg_off.size(), st);
+    pl->node_slot.upload(hp.node_slot.data(), hp.node_slot.size(), st);
+    pl->node_basis.upload(hp.node_basis.data(), hp.node_basis.size(), st);
+    pl->ainv_off.upload(hp.ainv_off.data(), hp.ainv_off.size(), st);
+    pl->ainv64.upload(hp.ainv.data(), hp.ainv.size(), st);
+    std::vector<float> a32(hp.ainv.begin(), hp.ainv.end());
+    pl->ainv32.upload(a32.data(), a32.size(), st);
+    CK(cudaStreamSynchronize(st));
 }
 
 // Queues setup + persistent PCG on the context stream, then waits for the
@@ -269,11 +327,24 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info) {
     const bool mixed = o.precision == PG_PREC_MIXED;
     int threads = o.threads;
     if (!threads) threads = std::min(pg::kMaxThreads, std::max(128, (hp.max_ntask + 31) / 32 * 32));
-    bool ke_smem = true;
-    pg::SmemLayout L = make_layout(hp, mixed, true);
-    if (L.total > c->max_smem) {
+    const bool coarse = o.preconditioner == PG_PRECOND_TWO_LEVEL;
+    if (coarse) ensure_coarse(c, pl);
+    // keep in shared memory what fits: both the Ke blocks and the A_c^-1
+    // rows, else the larger of the two, else neither (read from L2)
+    bool ke_smem = true, ainv_smem = coarse;
+    pg::SmemLayout L = make_layout(hp, mixed, true, coarse, ainv_smem);
+    if (L.total > c->max_smem && coarse) {
+        const bool ke_first = 3 * 3 * hp.npe * (size_t)hp.max_ntask >= (size_t)3 * hp.max_kagg * hp.C;
+        const bool opts[2][2] = {{ke_first, !ke_first}, {false, false}};
+        for (auto& op : opts) {
+            ke_smem = op[0];
+            ainv_smem = op[1];
+            L = make_layout(hp, mixed, ke_smem, coarse, ainv_smem);
+            if (L.total <= c->max_smem) break;
+        }
+    } else if (L.total > c->max_smem) {
         ke_smem = false;
-        L = make_layout(hp, mixed, false);
+        L = make_layout(hp, mixed, false, false, false);
     }
     if (L.total > c->max_smem)
         throw Fail{PG_EUNSUPPORTED, "partition too large for shared memory: use more ctas"};
@@ -318,6 +389,19 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info) {
     a.ke_smem = ke_smem ? 1 : 0;
     a.timing = o.phase_timing ? 1 : 0;
     a.test_stall = o.test_stall ? 1 : 0;
+    a.coarse = coarse ? 1 : 0;
+    a.C = coarse ? hp.C : 0;
+    a.cagg_off = pl->cagg_off.p;
+    a.node_slot = pl->node_slot.p;
+    a.node_basis = pl->node_basis.p;
+    a.ainv_off = pl->ainv_off.p;
+    a.ainv64 = pl->ainv64.p;
+    a.ainv32 = pl->ainv32.p;
+    a.ainv_smem = ainv_smem ? 1 : 0;
+    a.trace_it = o.trace_iteration > 0 ? o.trace_iteration : -1;
+    a.trace = pl->trace.p;
+    if (a.trace_it > 0)
+        CK(cudaMemsetAsync(pl->trace.p, 0, pl->trace.n * sizeof(unsigned long long), c->stream));
     a.reliable_interval = o.reliable_interval > 0 ? o.reliable_interval : 1 << 30;
     a.reliable_delta = o.reliable_delta > 0 ? o.reliable_delta : 0.1;
     a.L = L;
@@ -355,7 +439,28 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info) {
         info->reliable_updates = r.reliable_updates;
         info->reductions = r.reductions;
         info->shared_bytes = L.total;
-        for (int k = 0; k < 4; k++) info->phase_us[k] = r.phase_cycles[k] / (c->clock_khz * 1e-3);
+        info->coarse_dim = coarse ? hp.C - hp.dropped_modes : 0;
+        for (int k = 0; k < 8; k++) info->phase_us[k] = r.phase_cycles[k] / (c->clock_khz * 1e-3);
+        if (a.trace_it > 0) {
+            std::vector<unsigned long long> tr(pl->trace.n);
+            CK(cudaMemcpy(tr.data(), pl->trace.p, tr.size() * sizeof(unsigned long long),
+                          cudaMemcpyDeviceToHost));
+            unsigned long long s0 = ~0ull, s1 = 0, p0 = ~0ull, p1 = 0, x0 = ~0ull, x1 = 0, e1 = 0;
+            for (int g = 0; g < pl->G; g++) {
+                s0 = std::min(s0, tr[4 * g]); s1 = std::max(s1, tr[4 * g]);
+                p0 = std::min(p0, tr[4 * g + 1]); p1 = std::max(p1, tr[4 * g + 1]);
+                x0 = std::min(x0, tr[4 * g + 2]); x1 = std::max(x1, tr[4 * g + 2]);
+                e1 = std::max(e1, tr[4 * g + 3]);
+            }
+            if (s0 > 0) {
+                info->trace_ns[0] = (double)(s1 - s0);  // start spread
+                info->trace_ns[1] = (double)(p1 - p0);  // publish spread
+                info->trace_ns[2] = (double)(p1 - s0);  // first start -> last publish
+                info->trace_ns[3] = (double)(x0 - p1);  // last publish -> first block done
+                info->trace_ns[4] = (double)(x1 - x0);  // exchange-done spread
+                info->trace_ns[5] = (double)(e1 - s0);  // whole iteration (first start -> last end)
+            }
+        }
     }
     if (r.wait_failures > 0 || r.status == PG_ETIMEOUT)
         throw Fail{PG_ETIMEOUT, "a wait for another block exceeded wait_timeout_ms"};

@@ -18,6 +18,7 @@ STATUS_NAMES = {0: "PG_OK", 1: "PG_EINVAL", 2: "PG_ENOMEM", 3: "PG_ECUDA", 4: "P
                 5: "PG_ENONFINITE", 6: "PG_EUNSUPPORTED"}
 PG_PREC_FP64, PG_PREC_MIXED = 0, 1
 PG_STOP_REFERENCE, PG_STOP_RELATIVE = 0, 1
+PG_PRECOND_BLOCK_JACOBI, PG_PRECOND_TWO_LEVEL = 0, 1
 STOP_REASONS = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "zero_rhs"}
 
 # every symbol include/plategpu.h declares
@@ -60,6 +61,8 @@ class PgOptions(C.Structure):
         ("reliable_delta", C.c_double),
         ("phase_timing", C.c_int32),
         ("test_stall", C.c_int32),
+        ("preconditioner", C.c_int32),
+        ("trace_iteration", C.c_int32),
     ]
 
 
@@ -81,12 +84,16 @@ class PgInfo(C.Structure):
         ("plan_cached", C.c_int32),
         ("reductions", C.c_int32),
         ("shared_bytes", C.c_int32),
-        ("phase_us", C.c_double * 4),
+        ("coarse_dim", C.c_int32),
+        ("pad_", C.c_int32),
+        ("phase_us", C.c_double * 8),
+        ("trace_ns", C.c_double * 6),
     ]
 
     def as_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_}
         d["phase_us"] = list(self.phase_us)
+        d["trace_ns"] = list(self.trace_ns)
         d["stop_reason"] = STOP_REASONS.get(d["stop_reason"], d["stop_reason"])
         return d
 
@@ -216,7 +223,8 @@ def plan_inspect(prob: "Problem", ctas: int) -> dict:
 def make_options(tolerance=1e-6, max_iterations=1000, precision=PG_PREC_FP64,
                  stop_rule=PG_STOP_REFERENCE, ctas=0, threads=0, wait_timeout_ms=None,
                  reliable_interval=0, reliable_delta=0.0, phase_timing=False,
-                 test_stall=False) -> PgOptions:
+                 test_stall=False, preconditioner=PG_PRECOND_BLOCK_JACOBI,
+                 trace_iteration=0) -> PgOptions:
     o = PgOptions()
     load().pg_options_default(C.byref(o))
     o.tolerance = float(tolerance)
@@ -231,6 +239,8 @@ def make_options(tolerance=1e-6, max_iterations=1000, precision=PG_PREC_FP64,
     o.reliable_delta = float(reliable_delta)
     o.phase_timing = 1 if phase_timing else 0
     o.test_stall = 1 if test_stall else 0
+    o.preconditioner = int(preconditioner)
+    o.trace_iteration = int(trace_iteration)
     return o
 
 

@@ -64,6 +64,12 @@ typedef enum pg_precision {
                           FP64 true-residual replacement */
 } pg_precision;
 
+typedef enum pg_preconditioner {
+    PG_PRECOND_BLOCK_JACOBI = 0, /* 3x3 block Jacobi, as the reference (solver.ts:188-339) */
+    PG_PRECOND_TWO_LEVEL = 1     /* block Jacobi + Galerkin coarse correction on one
+                                    aggregate per thread block (3 rigid-body modes each) */
+} pg_preconditioner;
+
 typedef enum pg_stop_rule {
     PG_STOP_REFERENCE = 0, /* ||r|| < tol  or  ||r||/||b|| < tol  (gpu/solver.ts:516) */
     PG_STOP_RELATIVE = 1   /* ||r||/||b|| < tol only */
@@ -110,6 +116,9 @@ typedef struct pg_options {
     int32_t test_stall;           /* test hook: 1 makes block 0 wait once for a value no
                                      block ever writes, so the call must end with
                                      PG_ETIMEOUT after wait_timeout_ms */
+    int32_t preconditioner;       /* pg_preconditioner, default PG_PRECOND_BLOCK_JACOBI */
+    int32_t trace_iteration;      /* > 0: time-stamp that iteration in every block
+                                     (pg_info.trace_ns) */
 } pg_options;
 
 /* Per-solve result (GPUSolveResult plus extended statistics). */
@@ -131,10 +140,18 @@ typedef struct pg_info {
     int32_t reductions;           /* grid-wide reductions (one per iteration, plus
                                      one per residual replacement) */
     int32_t shared_bytes;         /* dynamic shared memory per block */
-    double phase_us[4];           /* with phase_timing, block 0's time (SM cycles at
-                                     the nominal clock) in: K.u; gather, dot products
-                                     and publishing; the exchange wait; decisions and
-                                     vector updates */
+    int32_t coarse_dim;           /* two-level: coarse DOFs kept (0 otherwise) */
+    int32_t pad_;
+    double phase_us[8];           /* with phase_timing, block 0's time (SM cycles at
+                                     the nominal clock) in: K.u; gather, dots and
+                                     publishing w; block reduction; publishing the
+                                     partials; the exchange wait; decisions; the
+                                     coarse solve; the vector updates */
+    double trace_ns[6];           /* with trace_iteration, over all blocks: spread of
+                                     iteration starts; spread of partial publication;
+                                     first start to last publication; last publication
+                                     to the first block holding every partial; spread
+                                     of exchange completion; whole iteration */
 } pg_info;
 
 typedef struct pg_ctx pg_ctx;
