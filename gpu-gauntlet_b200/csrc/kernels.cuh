@@ -60,6 +60,10 @@ struct SmemLayout {
     int total;
 };
 
+// Copies of every block's partial sums in the exchange buffer: each block
+// reads one copy, which spreads the pollers of a slot line over kRep lines.
+constexpr int kRep = 8;
+
 struct PcgArgs {
     int G, NT, Nn;
     const int* node_off;
@@ -78,7 +82,7 @@ struct PcgArgs {
     double* x;                   // [3Nn]
     unsigned long long* llv;     // [2][3Nn][2] tagged w / r values of the owners
     unsigned long long* llx;     // [3Nn][2] tagged x values (FP64 residual rounds)
-    unsigned long long* llp;     // [2][G][8] tagged partial sums
+    unsigned long long* llp;     // [2][kRep][G][16] tagged partial sums (kRep copies)
     int* abort_flag;
     PcgResult* res;
     double tol;
@@ -242,6 +246,19 @@ __device__ __forceinline__ void st_relaxed(unsigned long long* p, unsigned long 
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// 128-bit forms (p 16-byte aligned).  Each 64-bit half carries its own tag,
+// so a reader that sees the two halves from different rounds rejects the
+// pair: the pair needs no 128-bit single-copy atomicity.
+__device__ __forceinline__ void ld_relaxed2(const unsigned long long* p, unsigned long long& a,
+                                            unsigned long long& b) {
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
+}
+
+__device__ __forceinline__ void st_relaxed2(unsigned long long* p, unsigned long long a,
+                                            unsigned long long b) {
+    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b) : "memory");
+}
+
 template <typename T>
 struct Tag;
 
@@ -264,11 +281,12 @@ struct Tag<double> {
     static constexpr int W = 2;
     __device__ static __forceinline__ void put(unsigned long long* p, double v, unsigned f) {
         const unsigned long long b = (unsigned long long)__double_as_longlong(v);
-        st_relaxed(p, ((unsigned long long)f << 32) | (b & 0xffffffffull));
-        st_relaxed(p + 1, ((unsigned long long)f << 32) | (b >> 32));
+        st_relaxed2(p, ((unsigned long long)f << 32) | (b & 0xffffffffull),
+                    ((unsigned long long)f << 32) | (b >> 32));
     }
     __device__ static __forceinline__ bool get(const unsigned long long* p, unsigned f, double& v) {
-        const unsigned long long a = ld_relaxed(p), b = ld_relaxed(p + 1);
+        unsigned long long a, b;
+        ld_relaxed2(p, a, b);
         if ((unsigned)(a >> 32) != f || (unsigned)(b >> 32) != f) return false;
         v = __longlong_as_double((long long)((b << 32) | (a & 0xffffffffull)));
         return true;
@@ -340,6 +358,26 @@ __device__ void block_sum(double* v, double* red) {
     if (trailing) __syncthreads();
 }
 
+// Warp 0, after block_sum: copy r < kRep of this block's K totals goes to
+// slots pb[r][g][2k, 2k+1] (lane r writes copy r).  Every block reads the
+// copy blockIdx % kRep, so each slot line has about G / kRep readers instead
+// of G.
+template <int KMAX>
+__device__ __forceinline__ void publish_partials(unsigned long long* pb, int G, int g,
+                                                 const double* v, int K, unsigned f) {
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    double t[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; k++) t[k] = __shfl_sync(0xffffffffu, v[k], 0);
+    if (lane < kRep) {
+        unsigned long long* q = pb + ((size_t)lane * G + g) * 16;
+#pragma unroll
+        for (int k = 0; k < KMAX; k++)
+            if (k < K) Tag<double>::put(q + 2 * k, t[k], f);
+    }
+}
+
 // One exchange round, all threads of the block: waits for the K tagged
 // FP64 partial sums of every block (slots of 16 words; staged to
 // sp[G * K]) and for the tagged
@@ -352,6 +390,7 @@ __device__ bool exchange_round(const unsigned long long* __restrict__ pb, int G,
                                const int* __restrict__ gid, unsigned f, double* sp, Waiter& wt) {
     constexpr int TW = Tag<T>::W;
     const int np = G * K, n = np + 3 * (nloc - no);
+    pb += (size_t)(blockIdx.x % kRep) * G * 16;  // the copy of the partials this block reads
     for (int i0 = threadIdx.x; i0 < n; i0 += IF * blockDim.x) {
         const unsigned long long* ptr[IF];
         bool done[IF];
@@ -375,8 +414,12 @@ __device__ bool exchange_round(const unsigned long long* __restrict__ pb, int G,
             for (int j = 0; j < IF; j++) {
                 if (done[j]) continue;
                 const int i = i0 + j * (int)blockDim.x;
-                lo[j] = ld_relaxed(ptr[j]);
-                hi[j] = (i < np || TW == 2) ? ld_relaxed(ptr[j] + 1) : lo[j];
+                if (i < np || TW == 2) {
+                    ld_relaxed2(ptr[j], lo[j], hi[j]);
+                } else {
+                    lo[j] = ld_relaxed(ptr[j]);
+                    hi[j] = lo[j];
+                }
             }
             bool all = true;
 #pragma unroll
@@ -709,10 +752,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
         double v0[3] = {0.0, 0.0, 0.0};
         for (int n = tid; n < no; n += nt) restrict3(r + 3 * n, cm + 3 * n, nb + 3 * n, v0);
         block_sum<3>(v0, red);
-        unsigned long long* pb0 = a.llp + (size_t)(e & 1) * a.G * 16;
-        if (tid == 0)
-#pragma unroll
-            for (int k = 0; k < 3; k++) Tag<double>::put(pb0 + (size_t)g * 16 + 2 * k, v0[k], e);
+        unsigned long long* pb0 = a.llp + (size_t)(e & 1) * kRep * a.G * 16;
+        publish_partials<3>(pb0, a.G, g, v0, 3, e);
         const bool ok = exchange_round<T>(pb0, a.G, 3, nullptr, w, no, no, gid, e, sp, wt);
         if (__syncthreads_or(!ok)) {
             status = ST_TIMEOUT;
@@ -745,7 +786,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
         // ---- gather, BC rows, dot products, publish w ----
         double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         unsigned long long* vb = a.llv + (size_t)(e & 1) * N3 * 2;
-        unsigned long long* pb = a.llp + (size_t)(e & 1) * a.G * 16;
+        unsigned long long* pb = a.llp + (size_t)(e & 1) * kRep * a.G * 16;
         for (int k = tid; k < 3 * no; k += nt) {
             const int n = k / 3, d = k - 3 * n;
             const int tb = tptr[n + 1];
@@ -779,8 +820,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
         else
             block_sum<3, false>(v, red);
         clk.lap(2);
-        if (tid == 0)
-            for (int k = 0; k < KP; k++) Tag<double>::put(pb + (size_t)g * 16 + 2 * k, v[k], e);
+        publish_partials<6>(pb, a.G, g, v, KP, e);
         if (tr) a.trace[4 * g + 1] = gtimer();
         clk.lap(3);
         // ---- exchange: every block's partials and this block's ghost w ----
@@ -788,7 +828,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             bool ok = exchange_round<T>(pb, a.G, KP, vb, w, no, nloc, gid, e, sp, wt);
             if (a.test_stall && it == 0 && tid == 0) {
                 double never;  // a tag no block writes: the wait must run out
-                ok = ok && poll<double>(a.llp + (size_t)a.G * 32, 0xffffffffu, never, wt);
+                ok = ok && poll<double>(a.llp + (size_t)kRep * a.G * 32, 0xffffffffu, never, wt);
             }
             if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
             sum_partials<3>(sp, a.G, KP, scal);
@@ -875,7 +915,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             double vt[4] = {0.0, 0.0, 0.0, 0.0};
             const int KR = a.coarse ? 4 : 1;
             unsigned long long* rb = a.llv + (size_t)(e & 1) * N3 * 2;
-            unsigned long long* qb = a.llp + (size_t)(e & 1) * a.G * 16;
+            unsigned long long* qb = a.llp + (size_t)(e & 1) * kRep * a.G * 16;
             for (int n = tid; n < no; n += nt) {
                 double kx[3], rtv[3];
                 gather3(ytd, ntask, tptr[n], tptr[n + 1], kx[0], kx[1], kx[2]);
@@ -895,8 +935,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
                 block_sum<4>(vt, red);
             else
                 block_sum<1>(vt, red);
-            if (tid == 0)
-                for (int k = 0; k < KR; k++) Tag<double>::put(qb + (size_t)g * 16 + 2 * k, vt[k], e);
+            publish_partials<4>(qb, a.G, g, vt, KR, e);
             ok = exchange_round<T>(qb, a.G, KR, rb, r, no, nloc, gid, e, sp, wt);
             if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
             sum_partials<1>(sp, a.G, KR, scal);
@@ -1037,11 +1076,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
                 }
             }
             block_sum<2>(v, red);
-            unsigned long long* pb = a.llp + (size_t)(e & 1) * a.G * 16;
-            if (tid == 0) {
-                Tag<double>::put(pb + (size_t)g * 16, v[0], e);
-                Tag<double>::put(pb + (size_t)g * 16 + 2, v[1], e);
-            }
+            unsigned long long* pb = a.llp + (size_t)(e & 1) * kRep * a.G * 16;
+            publish_partials<2>(pb, a.G, g, v, 2, e);
             if (g == 0) {
                 ok = exchange_round<T>(pb, a.G, 2, nullptr, w, no, no, gid, e, sp, wt);
                 if (__syncthreads_or(!ok)) {

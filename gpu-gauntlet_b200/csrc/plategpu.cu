@@ -224,7 +224,7 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G) {
     pl->x.alloc(3 * Nn);
     pl->llv.alloc(12 * Nn);
     pl->llx.alloc(6 * Nn);
-    pl->llp.alloc(32 * (size_t)pl->G + 2);
+    pl->llp.alloc(32 * (size_t)pg::kRep * pl->G + 2);
     pl->abort_flag.alloc(1);
     pl->trace.alloc(4 * (size_t)pl->G);
     pl->res.alloc(1);
