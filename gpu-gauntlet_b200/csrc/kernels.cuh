@@ -47,9 +47,8 @@ struct PcgResult {
 struct SmemLayout {
     int r, u, p, s, w, B, yt, kt;  // T
     int x, xl, ytd, red, scal, sp;  // double
-    int Pr, Ps, cv, cpart;          // double: coarse residual, coarse s, coarse solution rows,
-                                    // per-thread partial dots of the coarse solve
-    int prc;                        // T: contiguous coarse residual
+    int qw, cs, cv;                 // double, per coarse row of the part: A_c^-1 P^T w,
+                                    // A_c^-1 P^T s and c = A_c^-1 P^T r (two copies of cs, cv)
     int ctl;                        // int[4]: decision broadcast
     int clk;                        // long long[8]: phase timers
     int nb, ainv;                   // T: per-node basis data, A_c^-1 rows
@@ -293,6 +292,22 @@ struct Tag<double> {
     }
 };
 
+// 1/x for the PCG scalars: the hardware's approximate reciprocal
+// (rcp.approx.ftz.f64) refined by three Newton-Raphson steps
+// r <- r + r (1 - x r), each of which about doubles the number of correct
+// bits, so the result is within a few ulp of 1/x for normal x.  Shorter than
+// a correctly rounded division on the thread-0 path every block waits on.
+__device__ __forceinline__ double recip(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const double e = __fma_rn(-x, r, 1.0);
+        r = __fma_rn(r, e, r);
+    }
+    return r;
+}
+
 // Time limit of one wait (a spin loop of one thread).  The clock starts at
 // the wait's first time check (after 32 failed reads), so a wait that is
 // already satisfied costs no timer read.
@@ -335,46 +350,59 @@ __device__ __forceinline__ bool poll(const unsigned long long* p, unsigned f, T&
 // block / grid reductions (fixed order: identical bits in every block)
 // ---------------------------------------------------------------------------
 
-// Block-wide sums of K values; thread 0 ends with the totals.  With
-// trailing = false the other warps may leave before warp 0 has finished
-// (the caller must not touch `red` again before a later barrier).
-template <int K, bool trailing = true>
-__device__ void block_sum(double* v, double* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+// Sums KM values (KM a power of two <= 32) over the 32 lanes of a warp by
+// recursive halving: at each of the first log2(KM) steps a lane keeps half
+// of its values and adds the partner's copy of that half (one shuffle per
+// kept value), then the single remaining value is summed over the lanes
+// that share it.  Lane l ends with the warp total of value l / (32 / KM):
+// KM - 1 + 5 - log2(KM) shuffles instead of 5 KM.  Fixed order.
+template <int KM>
+__device__ __forceinline__ double warp_reduce_scatter(double (&v)[KM]) {
+    const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int k = 0; k < K; k++)
-        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
-    if (lane == 0)
+    for (int lv = 0; (KM >> (lv + 1)) >= 1; lv++) {
+        const int h = KM >> (lv + 1), o = 16 >> lv;
+        const bool up = (lane & o) != 0;
 #pragma unroll
-        for (int k = 0; k < K; k++) red[warp * K + k] = v[k];
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-            v[k] = lane < nw ? red[lane * K + k] : 0.0;
-            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+        for (int i = 0; i < h; i++) {
+            const double keep = up ? v[h + i] : v[i];
+            const double send = up ? v[i] : v[h + i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
         }
     }
-    if (trailing) __syncthreads();
+    double t = v[0];
+#pragma unroll
+    for (int o = 16 / KM; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    return t;
 }
 
-// Warp 0, after block_sum: copy r < kRep of this block's K totals goes to
-// slots pb[r][g][2k, 2k+1] (lane r writes copy r).  Every block reads the
-// copy blockIdx % kRep, so each slot line has about G / kRep readers instead
-// of G.
-template <int KMAX>
-__device__ __forceinline__ void publish_partials(unsigned long long* pb, int G, int g,
-                                                 const double* v, int K, unsigned f) {
-    if (threadIdx.x >= 32) return;
-    const int lane = threadIdx.x;
-    double t[KMAX];
+// Block-wide totals of the first K (<= KM) of the KM values v, published
+// as this block's partial sums: copy r < kRep goes to slots
+// pb[r][g][2k, 2k+1] (lane r of warp 0 writes copy r).  Every block reads
+// the copy blockIdx % kRep, so each slot line has about G / kRep readers
+// instead of G.  All threads call it; it has one barrier, and warp 0 alone
+// works after it, so `red` must not be written again before a later barrier.
+template <int KM>
+__device__ void block_publish(double (&v)[KM], double* red, unsigned long long* pb, int G, int g,
+                              int K, unsigned f) {
+    constexpr int SH = 32 / KM;  // lanes that share one value after the reduce-scatter
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const double t = warp_reduce_scatter<KM>(v);
+    if (lane % SH == 0) red[warp * KM + lane / SH] = t;
+    __syncthreads();
+    if (warp != 0) return;
+    double q[KM];
 #pragma unroll
-    for (int k = 0; k < KMAX; k++) t[k] = __shfl_sync(0xffffffffu, v[k], 0);
+    for (int k = 0; k < KM; k++) q[k] = lane < nw ? red[lane * KM + k] : 0.0;
+    const double tt = warp_reduce_scatter<KM>(q);
+    double tk[KM];
+#pragma unroll
+    for (int k = 0; k < KM; k++) tk[k] = __shfl_sync(0xffffffffu, tt, k * SH);
     if (lane < kRep) {
-        unsigned long long* q = pb + ((size_t)lane * G + g) * 16;
+        unsigned long long* dst = pb + ((size_t)lane * G + g) * 16;
 #pragma unroll
-        for (int k = 0; k < KMAX; k++)
-            if (k < K) Tag<double>::put(q + 2 * k, t[k], f);
+        for (int k = 0; k < KM; k++)
+            if (k < K) Tag<double>::put(dst + 2 * k, tk[k], f);
     }
 }
 
@@ -605,31 +633,36 @@ __device__ __forceinline__ void prolong3(const double* cvn, const unsigned char*
     if (!c[2]) u[2] -= (T)((double)bas[2] * cvn[2]);
 }
 
-// Coarse solve cv[q] = (A_c^-1 P^T r)_q for the part's rows q < rows, from
-// the contiguous coarse residual pr (type T): 16 lanes per row reading
-// consecutive columns, two accumulators each, then a 16-lane shuffle
-// reduction (fixed order, the same bits on every run).
+// out[q] = sum_j Ai[q][j] y_j for the part's coarse rows q < rows, where
+// y_{3b+m} = (T) sp[b * stride + off + m] is the restriction of block b's
+// aggregate staged by the exchange (no contiguous copy needed).  Warps
+// w0.. take two rows each (16 lanes per row, lane l reading the 3 columns
+// of blocks l, l + 16, ...), then a 16-lane shuffle reduction: fixed order,
+// so every block computes the same bits for the same row.
 template <typename T>
-__device__ __forceinline__ void coarse_solve(const T* __restrict__ Ai, int C, int rows,
-                                             const T* __restrict__ pr, double* cv) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int half = lane >> 4, hl = lane & 15;
+__device__ __forceinline__ void coarse_apply(const T* __restrict__ Ai, int G, int rows,
+                                             const double* __restrict__ sp, int stride, int off,
+                                             double* __restrict__ out, int w0) {
+    const int lane = threadIdx.x & 31, warp = (int)(threadIdx.x >> 5) - w0;
+    const int nw = (int)(blockDim.x >> 5) - w0;
+    if (warp < 0) return;
+    const int half = lane >> 4, hl = lane & 15, C = 3 * G;
     for (int q0 = 2 * warp; q0 < rows; q0 += 2 * nw) {
         const int q = q0 + half;
-        T acc0 = T(0), acc1 = T(0);
+        T acc0 = T(0), acc1 = T(0), acc2 = T(0);
         if (q < rows) {
             const T* row = Ai + (size_t)q * C;
-            int j = hl;
-            for (; j + 16 < C; j += 32) {
-                acc0 += row[j] * pr[j];
-                acc1 += row[j + 16] * pr[j + 16];
+            for (int b = hl; b < G; b += 16) {
+                const double* y = sp + b * stride + off;
+                acc0 += row[3 * b] * (T)y[0];
+                acc1 += row[3 * b + 1] * (T)y[1];
+                acc2 += row[3 * b + 2] * (T)y[2];
             }
-            if (j < C) acc0 += row[j] * pr[j];
         }
-        double acc = (double)acc0 + (double)acc1;
+        double acc = (double)acc0 + (double)acc1 + (double)acc2;
 #pragma unroll
         for (int o = 8; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (hl == 0 && q < rows) cv[q] = acc;
+        if (hl == 0 && q < rows) out[q] = acc;
     }
 }
 
@@ -672,10 +705,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
     int* tptr = (int*)(sm + L.tptr);
     uint16_t* tn = (uint16_t*)(sm + L.tnode);
     unsigned char* cm = (unsigned char*)(sm + L.cm);
-    double* Pr = (double*)(sm + L.Pr);
-    double* Ps = (double*)(sm + L.Ps);
-    double* cv = (double*)(sm + L.cv);
-    T* prc = (T*)(sm + L.prc);  // contiguous copy of the current coarse residual
+    // coarse state per row of this part: c = A_c^-1 P^T r and cs = A_c^-1 P^T s
+    // in two copies (copy cb is current; an update writes copy cb ^ 1, so
+    // nodes can read the current copy while the new one is written), and
+    // qw = A_c^-1 P^T w of the current round
+    double* qw = (double*)(sm + L.qw);
+    double* csb = (double*)(sm + L.cs);
+    double* cvb = (double*)(sm + L.cv);
     int* ctl = (int*)(sm + L.ctl);  // [0] action, [1] final residual needed
     T* nb = (T*)(sm + L.nb);
     int* nslot = (int*)(sm + L.nslot);
@@ -710,10 +746,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
 #pragma unroll
             for (int q = 0; q < 3; q++) nb[3 * i + q] = (T)a.node_basis[3 * (size_t)(n0 + i) + q];
         }
-        for (int j = tid; j < a.C; j += nt) {
-            Pr[j] = 0.0;
-            Ps[j] = 0.0;
-        }
+        for (int j = tid; j < rows; j += nt) csb[j] = 0.0;
         if (a.ainv_smem)
             for (int i = tid; i < rows * a.C; i += nt) ais[i] = aig[i];
     }
@@ -749,29 +782,29 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
 
     // ---- two-level: u0 = M_bj r0 + P A_c^-1 P^T r0 (one exchange round) ----
     if (a.coarse) {
-        double v0[3] = {0.0, 0.0, 0.0};
+        double v0[4] = {0.0, 0.0, 0.0, 0.0};
         for (int n = tid; n < no; n += nt) restrict3(r + 3 * n, cm + 3 * n, nb + 3 * n, v0);
-        block_sum<3>(v0, red);
         unsigned long long* pb0 = a.llp + (size_t)(e & 1) * kRep * a.G * 16;
-        publish_partials<3>(pb0, a.G, g, v0, 3, e);
+        block_publish<4>(v0, red, pb0, a.G, g, 3, e);
         const bool ok = exchange_round<T>(pb0, a.G, 3, nullptr, w, no, no, gid, e, sp, wt);
         if (__syncthreads_or(!ok)) {
             status = ST_TIMEOUT;
         } else {
-            for (int j = tid; j < a.C; j += nt) {
-                Pr[j] = sp[j];
-                prc[j] = (T)sp[j];
-            }
+            coarse_apply<T>(Ai, a.G, rows, sp, 3, 0, cvb, 0);
             __syncthreads();
-            coarse_solve<T>(Ai, a.C, rows, prc, cv);
-            __syncthreads();
-            for (int n = tid; n < nloc; n += nt) prolong3(cv + 3 * nslot[n], cm + 3 * n, nb + 3 * n, u + 3 * n);
+            for (int n = tid; n < nloc; n += nt) prolong3(cvb + 3 * nslot[n], cm + 3 * n, nb + 3 * n, u + 3 * n);
             __syncthreads();
         }
         e++;
     }
 
-    double gamma_prev = 1.0, alpha_prev = 1.0, bnorm = 0.0, rn_ref = 0.0;
+    // decision state (thread 0): reciprocals of the previous gamma and
+    // alpha, and squared thresholds, so the step to the barrier has one
+    // division and no square root
+    double inv_gamma = 1.0, inv_alpha = 1.0, bnorm = 0.0, rn_ref = 0.0;
+    const double thr_abs = a.tol * a.tol;
+    double thr_rel = 0.0, thr_ru = 0.0;
+    int cb = 0;  // current copy of the coarse state
     int it = 0, stop = -1, xupd = 0, xupd_ref = 0, nru = 0;
     double final_res = 0.0, true_rel = -1.0;
     bool first = true;
@@ -784,7 +817,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
         __syncthreads();
         clk.lap(0);
         // ---- gather, BC rows, dot products, publish w ----
-        double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        double v[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         unsigned long long* vb = a.llv + (size_t)(e & 1) * N3 * 2;
         unsigned long long* pb = a.llp + (size_t)(e & 1) * kRep * a.G * 16;
         for (int k = tid; k < 3 * no; k += nt) {
@@ -815,12 +848,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             }
         }
         clk.lap(1);
-        if (a.coarse)
-            block_sum<6, false>(v, red);
-        else
-            block_sum<3, false>(v, red);
+        if (a.coarse) {
+            block_publish<8>(v, red, pb, a.G, g, 6, e);
+        } else {
+            double v4[4] = {v[0], v[1], v[2], 0.0};
+            block_publish<4>(v4, red, pb, a.G, g, 3, e);
+        }
         clk.lap(2);
-        publish_partials<6>(pb, a.G, g, v, KP, e);
         if (tr) a.trace[4 * g + 1] = gtimer();
         clk.lap(3);
         // ---- exchange: every block's partials and this block's ghost w ----
@@ -841,7 +875,6 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
         if (tid == 0) {
             const double gamma = scal[0], delta = scal[1], rho = scal[2];
             int act = ACT_UPDATE;
-            const double rn = sqrt(rho);
             if (!isfinite(gamma) || !isfinite(delta) || !isfinite(rho)) {
                 if (g == 0) {
                     a.res->nonfinite_it = it;
@@ -850,34 +883,37 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
                     a.res->nonfinite_vals[2] = rho;
                 }
                 act = ACT_NONFINITE;
-            } else if (first && rn < 1e-30) {
-                bnorm = rn;
+            } else if (first && rho < 1e-60) {
+                bnorm = sqrt(rho);
                 stop = STOP_ZERO_RHS; final_res = 0.0; true_rel = 0.0; act = ACT_STOP;
             } else {
+                // ||r|| < tol  <=>  rho < tol^2, and so on for the other tests
                 if (first) {
-                    bnorm = rn;
-                    rn_ref = rn;
+                    bnorm = sqrt(rho);
+                    rn_ref = bnorm;
+                    thr_rel = a.tol * bnorm * (a.tol * bnorm);
+                    thr_ru = a.reliable_delta * rn_ref * (a.reliable_delta * rn_ref);
                 } else {
-                    const bool conv = (a.stop_rule == 0 && rn < a.tol) || rn / bnorm < a.tol;
-                    if (MIXED && (conv || rn <= a.reliable_delta * rn_ref ||
-                                  xupd - xupd_ref >= a.reliable_interval))
+                    const bool conv = (a.stop_rule == 0 && rho < thr_abs) || rho < thr_rel;
+                    if (MIXED && (conv || rho <= thr_ru || xupd - xupd_ref >= a.reliable_interval))
                         act = ACT_RU;
                     else if (!MIXED && conv) {
-                        stop = STOP_CONVERGED; final_res = rn; act = ACT_STOP;
+                        stop = STOP_CONVERGED; final_res = sqrt(rho); act = ACT_STOP;
                     }
                 }
                 if (act == ACT_UPDATE && xupd >= a.maxit) {
-                    stop = STOP_MAX_ITER; final_res = rn; act = ACT_STOP;
+                    stop = STOP_MAX_ITER; final_res = sqrt(rho); act = ACT_STOP;
                 }
                 if (act == ACT_UPDATE) {
-                    const double beta = first ? 0.0 : gamma / gamma_prev;
-                    const double pap = first ? delta : delta - beta * gamma / alpha_prev;
+                    const double beta = first ? 0.0 : gamma * inv_gamma;
+                    const double pap = first ? delta : delta - beta * gamma * inv_alpha;
                     if (fabs(pap) < 1e-30) {
-                        stop = STOP_BREAKDOWN; xupd++; final_res = rn; act = ACT_STOP;
+                        stop = STOP_BREAKDOWN; xupd++; final_res = sqrt(rho); act = ACT_STOP;
                     } else {
-                        const double alpha = gamma / pap;
-                        gamma_prev = gamma;
-                        alpha_prev = alpha;
+                        // two independent reciprocals; only alpha gates the barrier
+                        const double alpha = gamma * recip(pap);
+                        inv_gamma = recip(gamma);
+                        inv_alpha = pap * inv_gamma;
                         first = false;
                         xupd++;
                         scal[3] = alpha;
@@ -887,7 +923,10 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             }
             ctl[0] = act;
             ctl[1] = (act == ACT_STOP && true_rel < 0.0) ? 1 : 0;
+            clk.lap(6);
         }
+        // meanwhile warps 1.. apply A_c^-1 to this round's P^T w
+        if (a.coarse) coarse_apply<T>(Ai, a.G, rows, sp, 6, 3, qw, 1);
         __syncthreads();
         const int act = ctl[0];
         if (tr) a.trace[4 * g + 2] = gtimer();
@@ -931,34 +970,24 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
                 }
                 if (a.coarse) restrict3(rtv, cm + 3 * n, nb + 3 * n, vt + 1);
             }
-            if (a.coarse)
-                block_sum<4>(vt, red);
-            else
-                block_sum<1>(vt, red);
-            publish_partials<4>(qb, a.G, g, vt, KR, e);
+            block_publish<4>(vt, red, qb, a.G, g, KR, e);
             ok = exchange_round<T>(qb, a.G, KR, rb, r, no, nloc, gid, e, sp, wt);
             if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
             sum_partials<1>(sp, a.G, KR, scal);
-            if (a.coarse)
-                for (int j = tid; j < a.C; j += nt) {
-                    Pr[j] = sp[(j / 3) * 4 + 1 + j % 3];
-                    prc[j] = (T)Pr[j];
-                }
+            // c = A_c^-1 P^T r from the true residual (cs is unchanged)
+            if (a.coarse) coarse_apply<T>(Ai, a.G, rows, sp, 4, 1, cvb + cb * rows, 0);
             __syncthreads();
             e++;
-            if (a.coarse) {
-                coarse_solve<T>(Ai, a.C, rows, prc, cv);
-                __syncthreads();
-            }
             for (int n = tid; n < nloc; n += nt) {
                 block_jacobi3(B + 9 * n, r + 3 * n, u + 3 * n);
-                if (a.coarse) prolong3(cv + 3 * nslot[n], cm + 3 * n, nb + 3 * n, u + 3 * n);
+                if (a.coarse) prolong3(cvb + cb * rows + 3 * nslot[n], cm + 3 * n, nb + 3 * n, u + 3 * n);
             }
             if (tid == 0) {
                 const double trn = sqrt(scal[0]);
                 int act2 = ACT_UPDATE;
                 nru++;
                 rn_ref = trn;
+                thr_ru = a.reliable_delta * rn_ref * (a.reliable_delta * rn_ref);
                 xupd_ref = xupd;
                 if (!isfinite(trn)) {
                     act2 = ACT_NONFINITE;
@@ -978,39 +1007,43 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             continue;
         }
 
-        // ---- coarse correction: c = A_c^-1 P^T r_new, with
-        //      P^T s = P^T w + beta P^T s and P^T r_new = P^T r - alpha P^T s ----
+        // ---- vector updates; two-level: with cs = A_c^-1 P^T s and
+        //      c = A_c^-1 P^T r, P^T s = P^T w + beta P^T s and
+        //      P^T r_new = P^T r - alpha P^T s give cs = qw + beta cs and
+        //      c_new = c - alpha cs, so u = M_bj r_new + P c_new needs no
+        //      coarse solve after the decision ----
         const double alpha = scal[3], beta = scal[4];
         const T bt = (T)beta, at = (T)alpha;
         if (a.coarse) {
-            // P^T s = P^T w + beta P^T s;  P^T r -= alpha P^T s  (every block, all C)
-            const double* Pw = sp + 3;  // stride 6: this round's P^T w of every block
-            for (int j = tid; j < a.C; j += nt) {
-                const double ps = Pw[(j / 3) * 6 + j % 3] + beta * Ps[j];
-                const double prn = Pr[j] - alpha * ps;
-                Ps[j] = ps;
-                Pr[j] = prn;
-                prc[j] = (T)prn;
+            const double* cso = csb + cb * rows;
+            const double* cvo = cvb + cb * rows;
+            if (tid < rows) {
+                const double c1 = __fma_rn(beta, cso[tid], qw[tid]);
+                csb[(cb ^ 1) * rows + tid] = c1;
+                cvb[(cb ^ 1) * rows + tid] = __fma_rn(-alpha, c1, cvo[tid]);
             }
-            // p, s, x, r on owned and ghost nodes
-            for (int k = tid; k < 3 * nloc; k += nt) {
-                const T pk = u[k] + bt * p[k];
-                const T sk = w[k] + bt * s[k];
-                p[k] = pk;
-                s[k] = sk;
-                if (k < 3 * no) x[k] += alpha * (double)pk;
-                r[k] -= at * sk;
-            }
-            __syncthreads();
-            clk.lap(7);
-            coarse_solve<T>(Ai, a.C, rows, prc, cv);
-            __syncthreads();
-            clk.lap(6);
-            // u = M_bj r + P c
             for (int n = tid; n < nloc; n += nt) {
-                block_jacobi3(B + 9 * n, r + 3 * n, u + 3 * n);
-                prolong3(cv + 3 * nslot[n], cm + 3 * n, nb + 3 * n, u + 3 * n);
+                T rv[3];
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const int k = 3 * n + d;
+                    const T pk = u[k] + bt * p[k];
+                    const T sk = w[k] + bt * s[k];
+                    p[k] = pk;
+                    s[k] = sk;
+                    if (n < no) x[k] += alpha * (double)pk;
+                    rv[d] = r[k] - at * sk;
+                    r[k] = rv[d];
+                }
+                block_jacobi3(B + 9 * n, rv, u + 3 * n);
+                const int sl = 3 * nslot[n];
+                double c3[3];
+#pragma unroll
+                for (int m = 0; m < 3; m++)
+                    c3[m] = __fma_rn(-alpha, __fma_rn(beta, cso[sl + m], qw[sl + m]), cvo[sl + m]);
+                prolong3(c3, cm + 3 * n, nb + 3 * n, u + 3 * n);
             }
+            cb ^= 1;
             __syncthreads();
             clk.lap(7);
             if (tr) a.trace[4 * g + 3] = gtimer();
@@ -1075,9 +1108,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
                     v[1] += f * f;
                 }
             }
-            block_sum<2>(v, red);
             unsigned long long* pb = a.llp + (size_t)(e & 1) * kRep * a.G * 16;
-            publish_partials<2>(pb, a.G, g, v, 2, e);
+            block_publish<2>(v, red, pb, a.G, g, 2, e);
             if (g == 0) {
                 ok = exchange_round<T>(pb, a.G, 2, nullptr, w, no, no, gid, e, sp, wt);
                 if (__syncthreads_or(!ok)) {

@@ -142,14 +142,12 @@ pg::SmemLayout make_layout(const pg::HostPlan& hp, bool mixed, bool ke_smem, boo
     L.x = take(3 * nown * 8);
     L.xl = take(mixed ? 3 * nloc * 8 : 0);
     L.ytd = take(mixed ? 3 * ntask * 8 : 0);
-    L.red = take(128 * 8);
+    L.red = take(32 * 8 * 8);  // [warps][8]
     L.scal = take(8 * 8);
     L.sp = take((size_t)6 * hp.G * 8);
-    L.Pr = take(coarse ? (size_t)hp.C * 8 : 0);
-    L.Ps = take(coarse ? (size_t)hp.C * 8 : 0);
-    L.cv = take(coarse ? (size_t)3 * hp.max_kagg * 8 : 0);
-    L.cpart = take(0);
-    L.prc = take(coarse ? (size_t)hp.C * T : 0);
+    L.qw = take(coarse ? (size_t)3 * hp.max_kagg * 8 : 0);
+    L.cs = take(coarse ? (size_t)2 * 3 * hp.max_kagg * 8 : 0);
+    L.cv = take(coarse ? (size_t)2 * 3 * hp.max_kagg * 8 : 0);
     L.ctl = take(4 * 4);
     L.clk = take(8 * 8);
     L.r = take(3 * nloc * T);
