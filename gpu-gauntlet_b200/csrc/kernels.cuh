@@ -71,7 +71,7 @@ struct PcgArgs {
     const int* task_off;
     const int* tp_off;
     const int* tptr;
-    const uint16_t* task_nodes;  // [NT][npe] -> staged [npe][ntask]
+    const uint16_t* task_nodes;  // [NT][npe] -> staged [npe][part tasks]
     const double* kt64;          // [3*nd][NT] task blocks, FP64
     const float* kt32;           // [3*nd][NT] task blocks, FP32
     const double* binv64;        // [Nn][9]
@@ -88,7 +88,7 @@ struct PcgArgs {
     int maxit;
     int stop_rule;
     unsigned long long timeout_ns;
-    int ke_smem;
+    int ke_smem;                 // Ke blocks in shared memory: 0 none, 1 owned tasks, 2 all
     int timing;
     int test_stall;  // test hook: block 0 waits once for a tag nobody writes
     // two-level preconditioner (coarse = 1): u = M_bj r + P A_c^-1 P^T r
@@ -103,6 +103,12 @@ struct PcgArgs {
     int ainv_smem;
     int reliable_interval;
     double reliable_delta;
+    // polynomial smoother (smoother = 1; needs a plan with a 2-ring halo):
+    // u = a D^-1 r - b D^-1 K D^-1 r (the degree-2 Chebyshev step for
+    // D^-1 K) in place of u = D^-1 r
+    int smoother;
+    const int* n1;                  // [G] owned + ring-1 nodes of each part
+    double cheb_a, cheb_b;
     int trace_it;                   // iteration traced (-1: none)
     unsigned long long* trace;      // [G][4] globaltimer: start, published, exchanged, end
     SmemLayout L;
@@ -505,29 +511,37 @@ __device__ __forceinline__ void sum_partials(const double* __restrict__ sp, int 
 
 // Task block layout: entry (row r of the node, column c of the rotated
 // element) of task t sits at kt[(r * ND + c) * stride + t], so consecutive
-// threads read consecutive words.  Task node ids sit at tn[j * ntask + t].
+// threads read consecutive words.  Task node ids sit at tn[j * ts + t];
+// results go to yt[r * ys + t].  Tasks t >= ksplit read their blocks from
+// kt2 (stride2) instead of kt (stride): the ring-1 tasks of a 2-ring plan
+// when only the owned tasks' blocks are staged in shared memory.
 template <int NPE, typename T, typename KT>
-__device__ __forceinline__ void task_matvec(const T* __restrict__ u, T* __restrict__ yt, int ntask,
-                                            const uint16_t* __restrict__ tn,
-                                            const KT* __restrict__ kt, size_t stride) {
+__device__ __forceinline__ void task_matvec(const T* __restrict__ u, T* __restrict__ yt, int ys,
+                                            int count, const uint16_t* __restrict__ tn, int ts,
+                                            const KT* __restrict__ kt, size_t stride,
+                                            int ksplit = 1 << 30,
+                                            const KT* __restrict__ kt2 = nullptr,
+                                            size_t stride2 = 0) {
     constexpr int ND = 3 * NPE;
-    for (int t = threadIdx.x; t < ntask; t += blockDim.x) {
+    for (int t = threadIdx.x; t < count; t += blockDim.x) {
+        const KT* kb = t < ksplit ? kt + t : kt2 + t;
+        const size_t ks = t < ksplit ? stride : stride2;
         T a0 = T(0), a1 = T(0), a2 = T(0);
 #pragma unroll
         for (int j = 0; j < NPE; j++) {
-            const int b = 3 * (int)tn[j * ntask + t];
+            const int b = 3 * (int)tn[j * ts + t];
 #pragma unroll
             for (int d = 0; d < 3; d++) {
                 const T v = u[b + d];
                 const int c = 3 * j + d;
-                a0 += (T)kt[(size_t)(0 * ND + c) * stride + t] * v;
-                a1 += (T)kt[(size_t)(1 * ND + c) * stride + t] * v;
-                a2 += (T)kt[(size_t)(2 * ND + c) * stride + t] * v;
+                a0 += (T)kb[(size_t)(0 * ND + c) * ks] * v;
+                a1 += (T)kb[(size_t)(1 * ND + c) * ks] * v;
+                a2 += (T)kb[(size_t)(2 * ND + c) * ks] * v;
             }
         }
         yt[t] = a0;
-        yt[ntask + t] = a1;
-        yt[2 * ntask + t] = a2;
+        yt[ys + t] = a1;
+        yt[2 * ys + t] = a2;
     }
 }
 
@@ -611,6 +625,23 @@ __device__ __forceinline__ void block_jacobi3(const double* Bn, const double* rv
     u[2] = Bn[6] * rv[0] + Bn[7] * rv[1] + Bn[8] * rv[2];
 }
 
+// Polynomial smoother at one node: with t = D^-1 r in un and the node's
+// task results K t in yt[ta, tb), un = ca t - cb D_n^-1 (K t); constrained
+// rows of K are the identity.
+template <typename T>
+__device__ __forceinline__ void smooth_node(T* un, const T* __restrict__ yt, int ys, int ta, int tb,
+                                            const T* Bn, const unsigned char* cn, T ca, T cb) {
+    T k3[3];
+    gather3(yt, ys, ta, tb, k3[0], k3[1], k3[2]);
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        if (cn[d]) k3[d] = un[d];
+    T v[3];
+    block_jacobi3(Bn, k3, v);
+#pragma unroll
+    for (int d = 0; d < 3; d++) un[d] = ca * un[d] - cb * v[d];
+}
+
 // Restriction of a nodal 3-vector to the node's aggregate modes (P^T v):
 // mode 0 w = 1; mode 1 w = dy, thx = 1/h; mode 2 w = dx, thy = -1/h,
 // constrained DOFs excluded.
@@ -686,7 +717,12 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
     const SmemLayout& L = a.L;
     const int g = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
     const int n0 = a.node_off[g], nloc = a.node_off[g + 1] - n0, no = a.nown[g];
-    const int t0 = a.task_off[g], ntask = a.task_off[g + 1] - t0;
+    // tasks [0, nta) of the part; the owned nodes' are [0, ntm) (all of them
+    // unless the plan has a 2-ring halo: then ring-1 nodes' tasks follow)
+    const int t0 = a.task_off[g], nta = a.task_off[g + 1] - t0;
+    const int nn1 = a.n1[g], ntm = a.tptr[a.tp_off[g] + no];
+    const bool cheb = a.smoother == 1;
+    const T ca = (T)a.cheb_a, cbc = (T)a.cheb_b;
     const size_t N3 = 3 * (size_t)a.Nn;
 
     T* r = (T*)(sm + L.r);
@@ -721,7 +757,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
     T* ais = (T*)(sm + L.ainv);
     const T* Ai = a.ainv_smem ? (const T*)ais : aig;
     const int KP = a.coarse ? 6 : 3;  // partial sums per block in a main round
-    // FP64 views for the true residual: dedicated arrays in MIXED mode,
+    // FP64 views for the true residual: own arrays in MIXED mode (ytd may
+    // share the dead yt / w / u space),
     // the (then dead) p / yt arrays in FP64 mode
     double* xl = MIXED ? (double*)(sm + L.xl) : (double*)p;
     double* ytd = MIXED ? (double*)(sm + L.ytd) : (double*)yt;
@@ -730,14 +767,17 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
 
     // ---- load the part ----
     for (int i = tid; i < nloc; i += nt) gid[i] = a.nodes[n0 + i];
-    for (int i = tid; i <= no; i += nt) tptr[i] = a.tptr[a.tp_off[g] + i];
-    for (int i = tid; i < NPE * ntask; i += nt) {
-        const int t = i % ntask, j = i / ntask;
+    for (int i = tid; i <= nn1; i += nt) tptr[i] = a.tptr[a.tp_off[g] + i];
+    for (int i = tid; i < NPE * nta; i += nt) {
+        const int t = i % nta, j = i / nta;
         tn[i] = a.task_nodes[(size_t)(t0 + t) * NPE + j];
     }
+    // Ke blocks staged in shared memory: none, the owned tasks' (ke_smem 1)
+    // or every task's (2)
+    const int nk = a.ke_smem == 2 ? nta : ntm;
     if (a.ke_smem)
-        for (int i = tid; i < 3 * ND * ntask; i += nt) {
-            const int t = i % ntask, q = i / ntask;
+        for (int i = tid; i < 3 * ND * nk; i += nt) {
+            const int t = i % nk, q = i / nk;
             kts[i] = ktg[(size_t)q * a.NT + t0 + t];
         }
     if (a.coarse) {
@@ -772,7 +812,17 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
     __syncthreads();
 
     const T* kt = a.ke_smem ? kts : ktg + t0;
-    const size_t kstride = a.ke_smem ? (size_t)ntask : (size_t)a.NT;
+    const size_t kstride = a.ke_smem ? (size_t)nk : (size_t)a.NT;
+    // the smoother's K t also runs ring-1 tasks, whose blocks may stay in global memory
+    const int ksplit = a.ke_smem == 1 ? ntm : (1 << 30);
+    if (cheb) {
+        // u0 = a t - b D^-1 K t, t = D^-1 r0 (u holds t on every local node)
+        task_matvec<NPE, T, T>(u, yt, nta, nta, tn, nta, kt, kstride, ksplit, ktg + t0, (size_t)a.NT);
+        __syncthreads();
+        for (int n = tid; n < nn1; n += nt)
+            smooth_node(u + 3 * n, yt, nta, tptr[n], tptr[n + 1], B + 9 * n, cm + 3 * n, ca, cbc);
+        __syncthreads();
+    }
     PhaseClock clk;
     clk.start(a.timing && g == 0 && tid == 0, (long long*)(sm + L.clk));
     Waiter wt;
@@ -813,7 +863,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
         const bool tr = it == a.trace_it && tid == 0;
         if (tr) a.trace[4 * g] = gtimer();
         // ---- w = A u on owned rows ----
-        task_matvec<NPE, T, T>(u, yt, ntask, tn, kt, kstride);
+        task_matvec<NPE, T, T>(u, yt, nta, ntm, tn, nta, kt, kstride);
         __syncthreads();
         clk.lap(0);
         // ---- gather, BC rows, dot products, publish w ----
@@ -824,7 +874,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             const int n = k / 3, d = k - 3 * n;
             const int tb = tptr[n + 1];
             T wk = T(0);
-            for (int t = tptr[n]; t < tb; t++) wk += yt[d * ntask + t];
+            for (int t = tptr[n]; t < tb; t++) wk += yt[d * nta + t];
             const bool c = cm[k] != 0;
             const T uk = u[k], rk = r[k];
             if (c) wk = uk;
@@ -854,9 +904,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             double v4[4] = {v[0], v[1], v[2], 0.0};
             block_publish<4>(v4, red, pb, a.G, g, 3, e);
         }
-        clk.lap(2);
         if (tr) a.trace[4 * g + 1] = gtimer();
-        clk.lap(3);
+        clk.lap(2);
         // ---- exchange: every block's partials and this block's ghost w ----
         {
             bool ok = exchange_round<T>(pb, a.G, KP, vb, w, no, nloc, gid, e, sp, wt);
@@ -949,7 +998,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             }
             if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
             xe++;
-            task_matvec<NPE, double, double>(xl, ytd, ntask, tn, a.kt64 + t0, (size_t)a.NT);
+            task_matvec<NPE, double, double>(xl, ytd, ntm, ntm, tn, nta, a.kt64 + t0, (size_t)a.NT);
             __syncthreads();
             double vt[4] = {0.0, 0.0, 0.0, 0.0};
             const int KR = a.coarse ? 4 : 1;
@@ -957,7 +1006,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             unsigned long long* qb = a.llp + (size_t)(e & 1) * kRep * a.G * 16;
             for (int n = tid; n < no; n += nt) {
                 double kx[3], rtv[3];
-                gather3(ytd, ntask, tptr[n], tptr[n + 1], kx[0], kx[1], kx[2]);
+                gather3(ytd, ntm, tptr[n], tptr[n + 1], kx[0], kx[1], kx[2]);
                 const int G3 = 3 * gid[n];
 #pragma unroll
                 for (int d = 0; d < 3; d++) {
@@ -980,7 +1029,18 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             e++;
             for (int n = tid; n < nloc; n += nt) {
                 block_jacobi3(B + 9 * n, r + 3 * n, u + 3 * n);
-                if (a.coarse) prolong3(cvb + cb * rows + 3 * nslot[n], cm + 3 * n, nb + 3 * n, u + 3 * n);
+                if (a.coarse && !cheb)
+                    prolong3(cvb + cb * rows + 3 * nslot[n], cm + 3 * n, nb + 3 * n, u + 3 * n);
+            }
+            if (cheb) {
+                __syncthreads();
+                task_matvec<NPE, T, T>(u, yt, nta, nta, tn, nta, kt, kstride, ksplit, ktg + t0, (size_t)a.NT);
+                __syncthreads();
+                for (int n = tid; n < nn1; n += nt) {
+                    smooth_node(u + 3 * n, yt, nta, tptr[n], tptr[n + 1], B + 9 * n, cm + 3 * n, ca, cbc);
+                    if (a.coarse)
+                        prolong3(cvb + cb * rows + 3 * nslot[n], cm + 3 * n, nb + 3 * n, u + 3 * n);
+                }
             }
             if (tid == 0) {
                 const double trn = sqrt(scal[0]);
@@ -1014,7 +1074,55 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
         //      coarse solve after the decision ----
         const double alpha = scal[3], beta = scal[4];
         const T bt = (T)beta, at = (T)alpha;
-        if (a.coarse) {
+        if (cheb) {
+            // s, r on every local node, p and x on owned nodes, t = D^-1 r
+            // into u; then K t on owned and ring-1 rows and
+            // u = a t - b D^-1 K t (+ P c_new, c by the recurrences below)
+            const double* cso = csb + cb * rows;
+            const double* cvo = cvb + cb * rows;
+            if (a.coarse && tid < rows) {
+                const double c1 = __fma_rn(beta, cso[tid], qw[tid]);
+                csb[(cb ^ 1) * rows + tid] = c1;
+                cvb[(cb ^ 1) * rows + tid] = __fma_rn(-alpha, c1, cvo[tid]);
+            }
+            for (int n = tid; n < nloc; n += nt) {
+                T rv[3];
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const int k = 3 * n + d;
+                    const T sk = w[k] + bt * s[k];
+                    s[k] = sk;
+                    if (n < no) {
+                        const T pk = u[k] + bt * p[k];
+                        p[k] = pk;
+                        x[k] += alpha * (double)pk;
+                    }
+                    rv[d] = r[k] - at * sk;
+                    r[k] = rv[d];
+                }
+                block_jacobi3(B + 9 * n, rv, u + 3 * n);
+            }
+            __syncthreads();
+            clk.lap(7);
+            task_matvec<NPE, T, T>(u, yt, nta, nta, tn, nta, kt, kstride, ksplit, ktg + t0, (size_t)a.NT);
+            __syncthreads();
+            clk.lap(3);
+            for (int n = tid; n < nn1; n += nt) {
+                smooth_node(u + 3 * n, yt, nta, tptr[n], tptr[n + 1], B + 9 * n, cm + 3 * n, ca, cbc);
+                if (a.coarse) {
+                    const int sl = 3 * nslot[n];
+                    double c3[3];
+#pragma unroll
+                    for (int m = 0; m < 3; m++)
+                        c3[m] = __fma_rn(-alpha, __fma_rn(beta, cso[sl + m], qw[sl + m]), cvo[sl + m]);
+                    prolong3(c3, cm + 3 * n, nb + 3 * n, u + 3 * n);
+                }
+            }
+            if (a.coarse) cb ^= 1;
+            __syncthreads();
+            clk.lap(7);
+            if (tr) a.trace[4 * g + 3] = gtimer();
+        } else if (a.coarse) {
             const double* cso = csb + cb * rows;
             const double* cvo = cvb + cb * rows;
             if (tid < rows) {
@@ -1090,14 +1198,14 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             status = ST_TIMEOUT;
         } else {
             if (MIXED || !a.ke_smem)
-                task_matvec<NPE, double, double>(xl, ytd, ntask, tn, a.kt64 + t0, (size_t)a.NT);
+                task_matvec<NPE, double, double>(xl, ytd, ntm, ntm, tn, nta, a.kt64 + t0, (size_t)a.NT);
             else
-                task_matvec<NPE, double, double>(xl, ytd, ntask, tn, (const double*)kts, (size_t)ntask);
+                task_matvec<NPE, double, double>(xl, ytd, ntm, ntm, tn, nta, (const double*)kts, kstride);
             __syncthreads();
             double v[2] = {0.0, 0.0};
             for (int n = tid; n < no; n += nt) {
                 double kx[3];
-                gather3(ytd, ntask, tptr[n], tptr[n + 1], kx[0], kx[1], kx[2]);
+                gather3(ytd, ntm, tptr[n], tptr[n + 1], kx[0], kx[1], kx[2]);
                 const int G3 = 3 * gid[n];
 #pragma unroll
                 for (int d = 0; d < 3; d++) {

@@ -178,11 +178,12 @@ void strip_partition(const float* xy, int Nn, int G, std::vector<int>& part_of) 
 
 }  // namespace
 
-std::string build_partition(const pg_problem& p, int G, HostPlan& plan) {
+std::string build_partition(const pg_problem& p, int G, int rings, HostPlan& plan) {
     const int Nn = plan.Nn, npe = plan.npe;
     if (G < 1) G = 1;
     if (G > std::max(Nn, 1)) G = std::max(Nn, 1);
     plan.G = G;
+    plan.rings = rings == 2 ? 2 : 1;
     std::vector<int> part_of;
     strip_partition(p.nodes, Nn, G, part_of);
 
@@ -198,33 +199,51 @@ std::string build_partition(const pg_problem& p, int G, HostPlan& plan) {
     plan.task_pos.clear();
     plan.task_nodes.clear();
     plan.tptr.clear();
-    plan.max_nloc = plan.max_nown = plan.max_ntask = 0;
+    plan.n1.assign(G, 0);
+    plan.max_nloc = plan.max_nown = plan.max_ntask = plan.max_ntask_own = plan.max_n1 = 0;
 
-    std::vector<int> local(Nn, -1), ghosts;
-    for (int g = 0; g < G; g++) {
-        const std::vector<int>& own = owned[g];
-        for (size_t i = 0; i < own.size(); i++) local[own[i]] = (int)i;
-        ghosts.clear();
-        for (int n : own)
+    std::vector<int> local(Nn, -1), ghosts, ring2;
+    // fills `out` (sorted) with the nodes of elements around `from` not yet numbered
+    auto next_ring = [&](const std::vector<int>& from, std::vector<int>& out) {
+        out.clear();
+        for (int n : from)
             for (int q = plan.inc_ptr[n]; q < plan.inc_ptr[n + 1]; q++) {
                 const int e = plan.inc_idx[q] / 4;
                 for (int k = 0; k < npe; k++) {
                     const int m = (int)p.elements[(size_t)e * npe + k];
-                    if (local[m] == -1) { local[m] = -2; ghosts.push_back(m); }
+                    if (local[m] == -1) { local[m] = -2; out.push_back(m); }
                 }
             }
-        std::sort(ghosts.begin(), ghosts.end());
+        std::sort(out.begin(), out.end());
+    };
+    for (int g = 0; g < G; g++) {
+        const std::vector<int>& own = owned[g];
+        for (size_t i = 0; i < own.size(); i++) local[own[i]] = (int)i;
+        next_ring(own, ghosts);
         for (size_t i = 0; i < ghosts.size(); i++) local[ghosts[i]] = (int)(own.size() + i);
-        const int nloc = (int)(own.size() + ghosts.size());
+        ring2.clear();
+        if (plan.rings == 2) {
+            next_ring(ghosts, ring2);
+            for (size_t i = 0; i < ring2.size(); i++)
+                local[ring2[i]] = (int)(own.size() + ghosts.size() + i);
+        }
+        const int nloc = (int)(own.size() + ghosts.size() + ring2.size());
         if (nloc > 65535) return "a part has more than 65535 local nodes: use more ctas";
 
         plan.nown[g] = (int)own.size();
+        plan.n1[g] = plan.rings == 2 ? (int)(own.size() + ghosts.size()) : (int)own.size();
         plan.nodes.insert(plan.nodes.end(), own.begin(), own.end());
         plan.nodes.insert(plan.nodes.end(), ghosts.begin(), ghosts.end());
+        plan.nodes.insert(plan.nodes.end(), ring2.begin(), ring2.end());
         plan.node_off[g + 1] = (int)plan.nodes.size();
         const int t0 = (int)plan.task_elem.size();
         plan.tp_off[g] = (int)plan.tptr.size();
-        for (int n : own) {
+        std::vector<int> task_nodes_of(own);
+        if (plan.rings == 2) task_nodes_of.insert(task_nodes_of.end(), ghosts.begin(), ghosts.end());
+        int ntask_own = 0;
+        for (size_t i = 0; i < task_nodes_of.size(); i++) {
+            const int n = task_nodes_of[i];
+            if (i == own.size()) ntask_own = (int)plan.task_elem.size() - t0;
             plan.tptr.push_back((int)plan.task_elem.size() - t0);
             for (int q = plan.inc_ptr[n]; q < plan.inc_ptr[n + 1]; q++) {
                 const int e = plan.inc_idx[q] / 4, k = plan.inc_idx[q] % 4;
@@ -235,13 +254,17 @@ std::string build_partition(const pg_problem& p, int G, HostPlan& plan) {
                         (uint16_t)local[p.elements[(size_t)e * npe + (k + j) % npe]]);
             }
         }
+        if (task_nodes_of.size() == own.size()) ntask_own = (int)plan.task_elem.size() - t0;
         plan.tptr.push_back((int)plan.task_elem.size() - t0);
         plan.task_off[g + 1] = (int)plan.task_elem.size();
         plan.max_nloc = std::max(plan.max_nloc, nloc);
         plan.max_nown = std::max(plan.max_nown, (int)own.size());
+        plan.max_n1 = std::max(plan.max_n1, plan.n1[g]);
         plan.max_ntask = std::max(plan.max_ntask, (int)plan.task_elem.size() - t0);
+        plan.max_ntask_own = std::max(plan.max_ntask_own, ntask_own);
         for (int n : own) local[n] = -1;
         for (int n : ghosts) local[n] = -1;
+        for (int n : ring2) local[n] = -1;
     }
     plan.tp_off[G] = (int)plan.tptr.size();
     return "";
@@ -361,16 +384,19 @@ std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, H
     plan.max_kagg = 0;
     std::vector<int> slot_of(G, -1);
     for (int g = 0; g < G; g++) {
+        // aggregates of the nodes where the part forms u: owned and ring 1
+        // (ring-2 nodes, rings = 2, carry only r, s and w: slot 0, unused)
         const int n0 = plan.node_off[g], nl = plan.node_off[g + 1] - n0;
+        const int nu = plan.rings == 2 ? plan.n1[g] : nl;
         std::vector<int> list = {g};
         slot_of[g] = 0;
-        for (int k = 0; k < nl; k++) {
+        for (int k = 0; k < nu; k++) {
             const int a = owner[plan.nodes[n0 + k]];
             if (slot_of[a] < 0) { slot_of[a] = (int)list.size(); list.push_back(a); }
         }
         for (int k = 0; k < nl; k++) {
             const int n = plan.nodes[n0 + k], a = owner[n];
-            plan.node_slot[n0 + k] = slot_of[a];
+            plan.node_slot[n0 + k] = k < nu ? slot_of[a] : 0;
             plan.node_basis[3 * (n0 + k)] = (p.nodes[2 * n] - cx[a]) * ih[a];
             plan.node_basis[3 * (n0 + k) + 1] = (p.nodes[2 * n + 1] - cy[a]) * ih[a];
             plan.node_basis[3 * (n0 + k) + 2] = ih[a];
@@ -388,6 +414,50 @@ std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, H
     plan.ainv_off[G] = (int)(plan.ainv.size() / C);
     plan.coarse = true;
     return "";
+}
+
+double estimate_lambda_max(const pg_problem& p, const std::vector<double>& ke64,
+                           const std::vector<double>& binv64, int iters) {
+    const int Nn = (int)p.node_count, Ne = (int)p.element_count, npe = (int)p.nodes_per_element;
+    const int nd = 3 * npe, n = 3 * Nn;
+    if (n == 0) return 1.0;
+    std::vector<double> x(n), y(n);
+    for (int i = 0; i < n; i++) x[i] = p.constrained[i] ? 0.0 : 1.0 + 0.5 * std::sin(0.7 * i);
+    double lam = 1.0;
+    for (int it = 0; it < iters; it++) {
+        // y = A x with A = K_ff (+) I_cc
+        std::fill(y.begin(), y.end(), 0.0);
+        for (int e = 0; e < Ne; e++) {
+            const double* K = ke64.data() + (size_t)e * nd * nd;
+            const uint32_t* en = p.elements + (size_t)e * npe;
+            for (int i = 0; i < nd; i++) {
+                const int gi = 3 * (int)en[i / 3] + i % 3;
+                if (p.constrained[gi]) continue;
+                double acc = 0;
+                for (int j = 0; j < nd; j++) {
+                    const int gj = 3 * (int)en[j / 3] + j % 3;
+                    if (!p.constrained[gj]) acc += K[i * nd + j] * x[gj];
+                }
+                y[gi] += acc;
+            }
+        }
+        for (int i = 0; i < n; i++)
+            if (p.constrained[i]) y[i] = x[i];
+        // x = D^-1 y, normalised; |D^-1 A x| -> lambda_max for |x| = 1
+        double nrm = 0;
+        for (int k = 0; k < Nn; k++)
+            for (int d = 0; d < 3; d++) {
+                const double* Bk = binv64.data() + 9 * (size_t)k + 3 * d;
+                const double v = Bk[0] * y[3 * k] + Bk[1] * y[3 * k + 1] + Bk[2] * y[3 * k + 2];
+                x[3 * k + d] = v;
+                nrm += v * v;
+            }
+        nrm = std::sqrt(nrm);
+        if (!(nrm > 0) || !std::isfinite(nrm)) return (double)npe;
+        for (int i = 0; i < n; i++) x[i] /= nrm;
+        lam = nrm;
+    }
+    return lam;
 }
 
 uint64_t problem_hash(const pg_problem& p) {

@@ -8,8 +8,12 @@
 // a task computes the node's 3 rows of Ke u_e.  Tasks are ordered node by
 // node, so a node's K u is the sum of a contiguous run of task results (an
 // owner-computes gather: no scatter, no atomics, fixed summation order).
-// Nodes of a part's elements that it does not own are its ghosts; local
-// numbering is owned nodes first, then ghosts.
+// Nodes of a part's elements that it does not own are its ghosts (ring 1);
+// with rings = 2 the nodes of the elements around ring-1 nodes that are in
+// neither set form ring 2, and ring-1 nodes get tasks too (the polynomial
+// smoother needs K t on owned and ring-1 rows).  Local numbering: owned
+// nodes, then ring 1, then ring 2; tasks: owned nodes' tasks, then ring-1
+// nodes' tasks.
 #pragma once
 
 #include <cstdint>
@@ -21,7 +25,7 @@
 namespace pg {
 
 struct HostPlan {
-    int Nn = 0, Ne = 0, npe = 4, colors = 0, G = 0;
+    int Nn = 0, Ne = 0, npe = 4, colors = 0, G = 0, rings = 1;
     // per part: [node_off[g], node_off[g+1]) local nodes (owned first), nown[g] owned
     std::vector<int> node_off, nown, nodes;
     // per part: [task_off[g], task_off[g+1]) tasks (global task numbering)
@@ -30,15 +34,17 @@ struct HostPlan {
     std::vector<uint8_t> task_pos;        // position of the owned node in the element
     std::vector<uint16_t> task_nodes;     // npe local node ids per task, owned node first,
                                           // then the element's next nodes cyclically
-    // per part: nown[g]+1 task offsets (relative to the part) at tp_off[g]
-    std::vector<int> tptr, tp_off;
+    // per part: n1[g] = owned + ring-1 nodes (the nodes with tasks when
+    // rings = 2, else nown[g]); n1[g]+1 task offsets (relative to the part)
+    // at tp_off[g]; the owned nodes' tasks are the first tptr[nown] of them
+    std::vector<int> tptr, tp_off, n1;
     // node -> (element*4 + position) incidence, for block-diagonal assembly
     std::vector<int> inc_ptr, inc_idx;
     // the colouring actually used (the caller's, or a greedy one when the
     // caller's colouring had node-sharing elements of one colour)
     std::vector<uint32_t> color_offsets, elements_by_color;
     bool recolored = false;
-    int max_nloc = 0, max_nown = 0, max_ntask = 0;
+    int max_nloc = 0, max_nown = 0, max_ntask = 0, max_ntask_own = 0, max_n1 = 0;
 
     // Two-level coarse space: one aggregate per part (its owned nodes), 3
     // modes each (the plate's rigid-body motions: w = 1; w = y, thx = 1;
@@ -60,13 +66,21 @@ std::string validate_problem(const pg_problem& p, bool need_rhs);
 // Builds the colouring (caller's or greedy) and node incidence.
 std::string build_structure(const pg_problem& p, HostPlan& plan);
 
-// Partitions into G parts (G <= node_count) and fills the part arrays.
-std::string build_partition(const pg_problem& p, int G, HostPlan& plan);
+// Partitions into G parts (G <= node_count) and fills the part arrays, with
+// a ghost halo of `rings` (1 or 2) element layers.
+std::string build_partition(const pg_problem& p, int G, int rings, HostPlan& plan);
 
 // Coarse space of the two-level preconditioner from the element matrices
 // ke64 ([Ne][(3 npe)^2], FP64): per-node basis data, per-part aggregate
 // lists, and the rows of A_c^-1 = (P^T A P)^-1 each part needs.
 std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, HostPlan& plan);
+
+// Largest eigenvalue of D^-1 A (D the 3x3 nodal block diagonal, A = K_ff
+// (+) I_cc) by `iters` power iterations from a fixed start vector, with
+// D^-1 given as binv64 ([Nn][9]) and A element by element from ke64.
+// Underestimates slightly; block Jacobi bounds it by nodes_per_element.
+double estimate_lambda_max(const pg_problem& p, const std::vector<double>& ke64,
+                           const std::vector<double>& binv64, int iters);
 
 // 64-bit FNV-1a over the problem's mesh, colouring, material and
 // constraint arrays (not F): the key of the plan cache.

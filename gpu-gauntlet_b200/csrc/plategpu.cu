@@ -67,7 +67,8 @@ struct Plan {
     pg_problem prob_view{};
     double E = 0, nu = 0, t = 0;
     bool has_elem_t = false;
-    DevBuf<int> node_off, nown, nodes, task_off, tp_off, tptr, task_elem, inc_ptr, inc_idx;
+    DevBuf<int> node_off, nown, nodes, task_off, tp_off, tptr, task_elem, inc_ptr, inc_idx, n1;
+    double lambda_max = 0;  // of D^-1 K, for the polynomial smoother (0 = not estimated)
     DevBuf<uint16_t> task_nodes;
     DevBuf<uint8_t> task_pos;
     DevBuf<float> mesh_nodes, elem_t, F;
@@ -128,10 +129,13 @@ int auto_ctas(const pg_ctx* c, int Nn) {
     return std::max(1, std::min(G, c->sms));
 }
 
-pg::SmemLayout make_layout(const pg::HostPlan& hp, bool mixed, bool ke_smem, bool coarse,
+// ke_mode: Ke task blocks in shared memory for 0 = no task, 1 = the owned
+// nodes' tasks, 2 = every task (ring-1 tasks too, with a 2-ring halo).
+pg::SmemLayout make_layout(const pg::HostPlan& hp, bool mixed, int ke_mode, bool coarse,
                            bool ainv_smem) {
     const size_t T = mixed ? 4 : 8, nd = 3 * hp.npe;
     const size_t nloc = hp.max_nloc, nown = hp.max_nown, ntask = hp.max_ntask;
+    const size_t ntask_own = hp.max_ntask_own, n1 = std::max(hp.max_n1, hp.max_nown);
     size_t off = 0;
     auto take = [&](size_t bytes) {
         const int o = (int)off;
@@ -141,7 +145,6 @@ pg::SmemLayout make_layout(const pg::HostPlan& hp, bool mixed, bool ke_smem, boo
     pg::SmemLayout L{};
     L.x = take(3 * nown * 8);
     L.xl = take(mixed ? 3 * nloc * 8 : 0);
-    L.ytd = take(mixed ? 3 * ntask * 8 : 0);
     L.red = take(32 * 8 * 8);  // [warps][8]
     L.scal = take(8 * 8);
     L.sp = take((size_t)6 * hp.G * 8);
@@ -151,28 +154,33 @@ pg::SmemLayout make_layout(const pg::HostPlan& hp, bool mixed, bool ke_smem, boo
     L.ctl = take(4 * 4);
     L.clk = take(8 * 8);
     L.r = take(3 * nloc * T);
-    L.u = take(3 * nloc * T);
     L.p = take(3 * nloc * T);
     L.s = take(3 * nloc * T);
-    L.w = take(3 * nloc * T);
     L.B = take(9 * nloc * T);
+    // yt, w, u back to back: the mixed-precision FP64 residual's task
+    // results (ytd) reuse them when they fit, since none of the three is
+    // live during a residual replacement or the final residual
     L.yt = take(3 * ntask * T);
-    L.kt = take(ke_smem ? 3 * nd * ntask * T : 0);
+    L.w = take(3 * nloc * T);
+    L.u = take(3 * nloc * T);
+    if (mixed)
+        L.ytd = 3 * ntask_own * 8 <= off - (size_t)L.yt ? L.yt : take(3 * ntask_own * 8);
+    L.kt = take(ke_mode == 2 ? 3 * nd * ntask * T : ke_mode == 1 ? 3 * nd * ntask_own * T : 0);
     L.nb = take(coarse ? 3 * nloc * T : 0);
     L.ainv = take(coarse && ainv_smem ? (size_t)3 * hp.max_kagg * hp.C * T : 0);
     L.nslot = take(coarse ? nloc * 4 : 0);
     L.gid = take(nloc * 4);
-    L.tptr = take((nown + 1) * 4);
+    L.tptr = take((n1 + 1) * 4);
     L.tnode = take(hp.npe * ntask * 2);
     L.cm = take(3 * nloc);
     L.total = (int)off;
     return L;
 }
 
-std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G) {
+std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G, int rings) {
     auto pl = std::make_unique<Plan>();
     std::string e = pg::build_structure(p, pl->hp);
-    if (e.empty()) e = pg::build_partition(p, G, pl->hp);
+    if (e.empty()) e = pg::build_partition(p, G, rings, pl->hp);
     if (!e.empty()) throw Fail{PG_EINVAL, e};
     pl->G = pl->hp.G;
     pl->h_nodes.assign(p.nodes, p.nodes + 2 * (size_t)p.node_count);
@@ -199,6 +207,7 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G) {
     pl->task_off.upload(hp.task_off.data(), hp.task_off.size(), st);
     pl->tp_off.upload(hp.tp_off.data(), hp.tp_off.size(), st);
     pl->tptr.upload(hp.tptr.data(), hp.tptr.size(), st);
+    pl->n1.upload(hp.n1.data(), hp.n1.size(), st);
     pl->task_elem.upload(hp.task_elem.data(), hp.task_elem.size(), st);
     pl->task_pos.upload(hp.task_pos.data(), hp.task_pos.size(), st);
     pl->task_nodes.upload(hp.task_nodes.data(), hp.task_nodes.size(), st);
@@ -231,17 +240,17 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G) {
     return pl;
 }
 
-Plan* get_plan(pg_ctx* c, const pg_problem& p, int G, bool* cached) {
+Plan* get_plan(pg_ctx* c, const pg_problem& p, int G, int rings, bool* cached) {
     const uint64_t key = pg::problem_hash(p);
     for (auto it = c->plans.begin(); it != c->plans.end(); ++it) {
-        if ((*it)->key == key && (*it)->G == G) {
+        if ((*it)->key == key && (*it)->G == G && (*it)->hp.rings == rings) {
             c->plans.splice(c->plans.begin(), c->plans, it);
             *cached = true;
             return c->plans.front().get();
         }
     }
     *cached = false;
-    auto pl = build_plan(c, p, G);
+    auto pl = build_plan(c, p, G, rings);
     pl->key = key;
     c->plans.push_front(std::move(pl));
     while (c->plans.size() > kMaxPlans) c->plans.pop_back();
@@ -290,7 +299,15 @@ void fill_options(const pg_options* in, pg_options* o) {
         throw Fail{PG_EINVAL, "threads must be a multiple of 32 in [32, 576] (0 = automatic)"};
     if (o->ctas < 0) throw Fail{PG_EINVAL, "ctas must be >= 0"};
     if (!(o->wait_timeout_ms >= 0)) throw Fail{PG_EINVAL, "wait_timeout_ms must be >= 0"};
+    if (o->preconditioner != PG_PRECOND_BLOCK_JACOBI && o->preconditioner != PG_PRECOND_TWO_LEVEL)
+        throw Fail{PG_EINVAL, "unknown preconditioner"};
+    if (o->smoother != PG_SMOOTHER_BLOCK_JACOBI && o->smoother != PG_SMOOTHER_CHEBYSHEV)
+        throw Fail{PG_EINVAL, "unknown smoother"};
 }
+
+// Ghost halo a solve with these options needs: 2 element layers for the
+// polynomial smoother, else 1.
+int halo_rings(const pg_options& o) { return o.smoother == PG_SMOOTHER_CHEBYSHEV ? 2 : 1; }
 
 // Coarse data of the two-level preconditioner, built once per plan: the
 // element matrices come from the device, A_c = P^T K P and its inverse are
@@ -318,6 +335,37 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
     CK(cudaStreamSynchronize(st));
 }
 
+// Largest eigenvalue of D^-1 K for the polynomial smoother, estimated once
+// per plan on the host from the device's element matrices and block inverses.
+void ensure_smoother(pg_ctx* c, Plan* pl) {
+    if (pl->lambda_max > 0) return;
+    const pg::HostPlan& hp = pl->hp;
+    run_setup(c, pl);
+    const size_t kk = 9 * (size_t)hp.npe * hp.npe;
+    std::vector<double> ke(std::max<size_t>(1, (size_t)hp.Ne * kk)), binv(9 * (size_t)hp.Nn);
+    if (hp.Ne > 0)
+        CK(cudaMemcpyAsync(ke.data(), pl->ke64.p, (size_t)hp.Ne * kk * sizeof(double),
+                           cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(binv.data(), pl->binv64.p, binv.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const double lam = pg::estimate_lambda_max(pl->prob_view, ke, binv, 30);
+    pl->lambda_max = std::isfinite(lam) && lam > 0 ? lam : (double)hp.npe;
+}
+
+// Coefficients of u = a t - b D^-1 K t (t = D^-1 r): two steps of the
+// Chebyshev iteration for D^-1 K on [lo, hi], hi = 1.1 lambda_max,
+// lo = hi / 20.  The residual polynomial is T2((theta - x) / delta) /
+// T2(theta / delta) with theta, delta the centre and half-width; the
+// preconditioner polynomial a - b x is positive on (0, hi + lo).
+void chebyshev2(double lambda_max, double* a, double* b) {
+    const double hi = 1.1 * lambda_max, lo = hi / 20.0;
+    const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+    const double rho0 = 1.0 / sigma, rho1 = 1.0 / (2.0 * sigma - rho0);
+    *a = (1.0 + rho1 * rho0) / theta + 2.0 * rho1 / delta;
+    *b = 2.0 * rho1 / (delta * theta);
+}
+
 // Queues setup + persistent PCG on the context stream, then waits for the
 // result record (one small readback).  F must already be in pl->F.
 void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info) {
@@ -326,23 +374,27 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info) {
     int threads = o.threads;
     if (!threads) threads = std::min(pg::kMaxThreads, std::max(128, (hp.max_ntask + 31) / 32 * 32));
     const bool coarse = o.preconditioner == PG_PRECOND_TWO_LEVEL;
+    const bool cheb = o.smoother == PG_SMOOTHER_CHEBYSHEV;
+    if (cheb && hp.rings != 2)
+        throw Fail{PG_EINVAL, "the Chebyshev smoother needs a plan made with it (2-ring halo)"};
     if (coarse) ensure_coarse(c, pl);
-    // keep in shared memory what fits: both the Ke blocks and the A_c^-1
-    // rows, else the larger of the two, else neither (read from L2)
-    bool ke_smem = true, ainv_smem = coarse;
-    pg::SmemLayout L = make_layout(hp, mixed, true, coarse, ainv_smem);
-    if (L.total > c->max_smem && coarse) {
-        const bool ke_first = 3 * 3 * hp.npe * (size_t)hp.max_ntask >= (size_t)3 * hp.max_kagg * hp.C;
-        const bool opts[2][2] = {{ke_first, !ke_first}, {false, false}};
-        for (auto& op : opts) {
-            ke_smem = op[0];
-            ainv_smem = op[1];
-            L = make_layout(hp, mixed, ke_smem, coarse, ainv_smem);
-            if (L.total <= c->max_smem) break;
-        }
-    } else if (L.total > c->max_smem) {
-        ke_smem = false;
-        L = make_layout(hp, mixed, false, false, false);
+    if (cheb) ensure_smoother(c, pl);
+    // keep in shared memory what fits, in this order of preference: every
+    // task's Ke blocks (only differs from the owned tasks' with a 2-ring
+    // halo) and the A_c^-1 rows; the owned tasks' blocks and A_c^-1; then
+    // the larger of the owned tasks' blocks and A_c^-1; then neither (L2)
+    const int full = hp.rings == 2 ? 2 : 1;
+    const bool ke_first = 3 * 3 * hp.npe * (size_t)hp.max_ntask_own >= (size_t)3 * hp.max_kagg * hp.C;
+    const int cand[6][2] = {{full, 1}, {1, 1}, {ke_first ? full : 0, ke_first ? 0 : 1},
+                            {ke_first ? 1 : 0, ke_first ? 0 : 1}, {0, 1}, {0, 0}};
+    int ke_mode = 0;
+    bool ainv_smem = false;
+    pg::SmemLayout L{};
+    for (auto& cd : cand) {
+        ke_mode = cd[0];
+        ainv_smem = coarse && cd[1];
+        L = make_layout(hp, mixed, ke_mode, coarse, ainv_smem);
+        if (L.total <= c->max_smem) break;
     }
     if (L.total > c->max_smem)
         throw Fail{PG_EUNSUPPORTED, "partition too large for shared memory: use more ctas"};
@@ -384,7 +436,7 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info) {
     a.maxit = o.max_iterations;
     a.stop_rule = o.stop_rule;
     a.timeout_ns = (unsigned long long)(o.wait_timeout_ms * 1e6);
-    a.ke_smem = ke_smem ? 1 : 0;
+    a.ke_smem = ke_mode;
     a.timing = o.phase_timing ? 1 : 0;
     a.test_stall = o.test_stall ? 1 : 0;
     a.coarse = coarse ? 1 : 0;
@@ -396,6 +448,9 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info) {
     a.ainv64 = pl->ainv64.p;
     a.ainv32 = pl->ainv32.p;
     a.ainv_smem = ainv_smem ? 1 : 0;
+    a.smoother = cheb ? 1 : 0;
+    a.n1 = pl->n1.p;
+    if (cheb) chebyshev2(pl->lambda_max, &a.cheb_a, &a.cheb_b);
     a.trace_it = o.trace_iteration > 0 ? o.trace_iteration : -1;
     a.trace = pl->trace.p;
     if (a.trace_it > 0)
@@ -438,6 +493,7 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info) {
         info->reductions = r.reductions;
         info->shared_bytes = L.total;
         info->coarse_dim = coarse ? hp.C - hp.dropped_modes : 0;
+        info->smoother_lambda_max = cheb ? pl->lambda_max : 0.0;
         for (int k = 0; k < 8; k++) info->phase_us[k] = r.phase_cycles[k] / (c->clock_khz * 1e-3);
         if (a.trace_it > 0) {
             std::vector<unsigned long long> tr(pl->trace.n);
@@ -619,7 +675,7 @@ int pg_solve(pg_ctx* c, const pg_problem* p, const pg_options* opt, double* x_ou
         }
         const int G = o.ctas ? std::min(o.ctas, (int)p->node_count) : auto_ctas(c, (int)p->node_count);
         bool cached = false;
-        Plan* pl = get_plan(c, *p, G, &cached);
+        Plan* pl = get_plan(c, *p, G, halo_rings(o), &cached);
         ensure_staging(c, n);
         std::memcpy(c->hF, p->F, n * sizeof(float));
         CK(cudaMemcpyAsync(pl->F.p, c->hF, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
@@ -642,7 +698,7 @@ int pg_plan_create(pg_ctx* c, const pg_problem* p, const pg_options* opt, pg_pla
         const int G = o.ctas ? std::min(o.ctas, (int)p->node_count) : auto_ctas(c, (int)p->node_count);
         auto h = std::make_unique<pg_plan>();
         h->ctx = c;
-        h->plan = build_plan(c, *p, G);
+        h->plan = build_plan(c, *p, G, halo_rings(o));
         *out = h.release();
     });
 }
@@ -684,7 +740,7 @@ int pg_apply_k(pg_ctx* c, const pg_problem* p, const double* x, double* y) {
         if (n == 0) return;
         if (!x || !y) throw Fail{PG_EINVAL, "x / y is NULL"};
         bool cached = false;
-        Plan* pl = get_plan(c, *p, auto_ctas(c, (int)p->node_count), &cached);
+        Plan* pl = get_plan(c, *p, auto_ctas(c, (int)p->node_count), 1, &cached);
         run_setup(c, pl);
         DevBuf<double> dx, dy;
         dx.upload(x, n, c->stream);
@@ -711,7 +767,7 @@ int pg_block_jacobi(pg_ctx* c, const pg_problem* p, double* binv_out) {
         if (p->node_count == 0) return;
         if (!binv_out) throw Fail{PG_EINVAL, "binv_out is NULL"};
         bool cached = false;
-        Plan* pl = get_plan(c, *p, auto_ctas(c, (int)p->node_count), &cached);
+        Plan* pl = get_plan(c, *p, auto_ctas(c, (int)p->node_count), 1, &cached);
         run_setup(c, pl);
         CK(cudaMemcpyAsync(binv_out, pl->binv64.p, 9 * sizeof(double) * p->node_count,
                            cudaMemcpyDeviceToHost, c->stream));
@@ -725,7 +781,7 @@ int pg_element_stiffness(pg_ctx* c, const pg_problem* p, double* ke_out) {
         if (p->element_count == 0 || p->node_count == 0) return;
         if (!ke_out) throw Fail{PG_EINVAL, "ke_out is NULL"};
         bool cached = false;
-        Plan* pl = get_plan(c, *p, auto_ctas(c, (int)p->node_count), &cached);
+        Plan* pl = get_plan(c, *p, auto_ctas(c, (int)p->node_count), 1, &cached);
         run_setup(c, pl);
         const size_t kk = 9 * (size_t)p->nodes_per_element * p->nodes_per_element;
         CK(cudaMemcpyAsync(ke_out, pl->ke64.p, kk * sizeof(double) * p->element_count,
@@ -735,6 +791,11 @@ int pg_element_stiffness(pg_ctx* c, const pg_problem* p, double* ke_out) {
 }
 
 int pg_plan_inspect(const pg_problem* p, int ctas, int32_t* stats, char* msg, size_t msg_len) {
+    return pg_plan_inspect_halo(p, ctas, 1, stats, msg, msg_len);
+}
+
+int pg_plan_inspect_halo(const pg_problem* p, int ctas, int rings, int32_t* stats, char* msg,
+                         size_t msg_len) {
     auto put = [&](const std::string& m) {
         if (msg && msg_len) {
             std::strncpy(msg, m.c_str(), msg_len - 1);
@@ -747,7 +808,8 @@ int pg_plan_inspect(const pg_problem* p, int ctas, int32_t* stats, char* msg, si
         if (!e.empty()) { put(e); return PG_EINVAL; }
         pg::HostPlan hp;
         e = pg::build_structure(*p, hp);
-        if (e.empty()) e = pg::build_partition(*p, ctas > 0 ? ctas : 1, hp);
+        if (rings != 1 && rings != 2) e = "rings must be 1 or 2";
+        if (e.empty()) e = pg::build_partition(*p, ctas > 0 ? ctas : 1, rings, hp);
         if (!e.empty()) { put(e); return PG_EINVAL; }
         const int Nn = hp.Nn, npe = hp.npe, C = hp.colors;
         int bad = 0;
@@ -760,14 +822,16 @@ int pg_plan_inspect(const pg_problem* p, int ctas, int32_t* stats, char* msg, si
                 if (owner[hp.nodes[n0 + k]] >= 0) bad++;
                 owner[hp.nodes[n0 + k]] = g;
             }
-            // tasks of owned node k: exactly its incidences, in order, owned node first
-            const int t0 = hp.task_off[g];
+            // tasks of node k < n1 (owned, and ring 1 with rings = 2): exactly
+            // its incidences, in order, the node itself first
+            const int t0 = hp.task_off[g], m1 = hp.n1[g];
             const int* tp = hp.tptr.data() + hp.tp_off[g];
-            if (hp.tp_off[g + 1] - hp.tp_off[g] != no + 1 || tp[0] != 0 ||
-                tp[no] != hp.task_off[g + 1] - t0)
+            if (m1 < no || m1 > nl || (rings == 1 && m1 != no)) bad++;
+            if (hp.tp_off[g + 1] - hp.tp_off[g] != m1 + 1 || tp[0] != 0 ||
+                tp[m1] != hp.task_off[g + 1] - t0)
                 bad++;
             std::vector<char> used(nl, 0);
-            for (int k = 0; k < no; k++) {
+            for (int k = 0; k < m1; k++) {
                 const int n = hp.nodes[n0 + k];
                 used[k] = 1;
                 if (tp[k + 1] - tp[k] != hp.inc_ptr[n + 1] - hp.inc_ptr[n]) { bad++; continue; }

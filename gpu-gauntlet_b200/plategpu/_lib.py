@@ -19,13 +19,15 @@ STATUS_NAMES = {0: "PG_OK", 1: "PG_EINVAL", 2: "PG_ENOMEM", 3: "PG_ECUDA", 4: "P
 PG_PREC_FP64, PG_PREC_MIXED = 0, 1
 PG_STOP_REFERENCE, PG_STOP_RELATIVE = 0, 1
 PG_PRECOND_BLOCK_JACOBI, PG_PRECOND_TWO_LEVEL = 0, 1
+PG_SMOOTHER_BLOCK_JACOBI, PG_SMOOTHER_CHEBYSHEV = 0, 1
 STOP_REASONS = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "zero_rhs"}
 
 # every symbol include/plategpu.h declares
 EXPORTED = ("pg_options_default", "pg_is_available", "pg_create", "pg_destroy", "pg_last_error",
             "pg_clear_cache", "pg_set_stream", "pg_solve", "pg_plan_create", "pg_plan_solve_device",
             "pg_plan_destroy", "pg_apply_k", "pg_apply_k_static",
-            "pg_block_jacobi", "pg_element_stiffness", "pg_plan_inspect")
+            "pg_block_jacobi", "pg_element_stiffness", "pg_plan_inspect",
+            "pg_plan_inspect_halo")
 
 
 class PgProblem(C.Structure):
@@ -63,6 +65,7 @@ class PgOptions(C.Structure):
         ("test_stall", C.c_int32),
         ("preconditioner", C.c_int32),
         ("trace_iteration", C.c_int32),
+        ("smoother", C.c_int32),
     ]
 
 
@@ -88,6 +91,7 @@ class PgInfo(C.Structure):
         ("pad_", C.c_int32),
         ("phase_us", C.c_double * 8),
         ("trace_ns", C.c_double * 6),
+        ("smoother_lambda_max", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -151,6 +155,8 @@ def load() -> C.CDLL:
     L.pg_apply_k_static.restype = I
     L.pg_plan_inspect.argtypes = [C.POINTER(PgProblem), I, P, C.c_char_p, C.c_size_t]
     L.pg_plan_inspect.restype = I
+    L.pg_plan_inspect_halo.argtypes = [C.POINTER(PgProblem), I, I, P, C.c_char_p, C.c_size_t]
+    L.pg_plan_inspect_halo.restype = I
     _lib = L
     return L
 
@@ -210,11 +216,12 @@ PLAN_STATS = ("parts", "colors", "recolored", "max_local_nodes", "max_owned_node
               "max_part_tasks", "ghost_nodes", "violations")
 
 
-def plan_inspect(prob: "Problem", ctas: int) -> dict:
-    """pg_plan_inspect: host-only partition statistics and invariant check."""
+def plan_inspect(prob: "Problem", ctas: int, rings: int = 1) -> dict:
+    """pg_plan_inspect(_halo): host-only partition statistics and invariant check."""
     stats = np.zeros(8, np.int32)
     msg = C.create_string_buffer(256)
-    st = load().pg_plan_inspect(C.byref(prob.struct), int(ctas), _ptr(stats), msg, 256)
+    st = load().pg_plan_inspect_halo(C.byref(prob.struct), int(ctas), int(rings), _ptr(stats),
+                                     msg, 256)
     if st != PG_OK:
         raise PlateGPUError(st, msg.value.decode())
     return dict(zip(PLAN_STATS, stats.tolist()))
@@ -224,7 +231,7 @@ def make_options(tolerance=1e-6, max_iterations=1000, precision=PG_PREC_FP64,
                  stop_rule=PG_STOP_REFERENCE, ctas=0, threads=0, wait_timeout_ms=None,
                  reliable_interval=0, reliable_delta=0.0, phase_timing=False,
                  test_stall=False, preconditioner=PG_PRECOND_BLOCK_JACOBI,
-                 trace_iteration=0) -> PgOptions:
+                 trace_iteration=0, smoother=PG_SMOOTHER_BLOCK_JACOBI) -> PgOptions:
     o = PgOptions()
     load().pg_options_default(C.byref(o))
     o.tolerance = float(tolerance)
@@ -241,6 +248,7 @@ def make_options(tolerance=1e-6, max_iterations=1000, precision=PG_PREC_FP64,
     o.test_stall = 1 if test_stall else 0
     o.preconditioner = int(preconditioner)
     o.trace_iteration = int(trace_iteration)
+    o.smoother = int(smoother)
     return o
 
 

@@ -70,6 +70,14 @@ typedef enum pg_preconditioner {
                                     aggregate per thread block (3 rigid-body modes each) */
 } pg_preconditioner;
 
+typedef enum pg_smoother {
+    PG_SMOOTHER_BLOCK_JACOBI = 0, /* u = D^-1 r, D the 3x3 nodal blocks (the reference's) */
+    PG_SMOOTHER_CHEBYSHEV = 1     /* u = a D^-1 r - b D^-1 K D^-1 r: two Chebyshev steps
+                                     for D^-1 K on [hi/20, hi], hi = 1.1 lambda_max
+                                     (power-iteration estimate); one more K product per
+                                     iteration on a 2-ring ghost halo, no extra exchange */
+} pg_smoother;
+
 typedef enum pg_stop_rule {
     PG_STOP_REFERENCE = 0, /* ||r|| < tol  or  ||r||/||b|| < tol  (gpu/solver.ts:516) */
     PG_STOP_RELATIVE = 1   /* ||r||/||b|| < tol only */
@@ -119,6 +127,8 @@ typedef struct pg_options {
     int32_t preconditioner;       /* pg_preconditioner, default PG_PRECOND_BLOCK_JACOBI */
     int32_t trace_iteration;      /* > 0: time-stamp that iteration in every block
                                      (pg_info.trace_ns) */
+    int32_t smoother;             /* pg_smoother, default PG_SMOOTHER_BLOCK_JACOBI (also the
+                                     smoother of the two-level preconditioner) */
 } pg_options;
 
 /* Per-solve result (GPUSolveResult plus extended statistics). */
@@ -144,14 +154,16 @@ typedef struct pg_info {
     int32_t pad_;
     double phase_us[8];           /* with phase_timing, block 0's time (SM cycles at
                                      the nominal clock) in: K.u; gather, dots and
-                                     publishing w; block reduction; publishing the
-                                     partials; the exchange wait; decisions; the
-                                     coarse solve; the vector updates */
+                                     publishing w; block reduction and publishing the
+                                     partials; the Chebyshev smoother's K t; the
+                                     exchange wait; the barrier after the decision;
+                                     thread 0's decision; the other vector updates */
     double trace_ns[6];           /* with trace_iteration, over all blocks: spread of
                                      iteration starts; spread of partial publication;
                                      first start to last publication; last publication
                                      to the first block holding every partial; spread
                                      of exchange completion; whole iteration */
+    double smoother_lambda_max;   /* Chebyshev smoother: the lambda_max(D^-1 K) estimate used */
 } pg_info;
 
 typedef struct pg_ctx pg_ctx;
@@ -243,6 +255,12 @@ int pg_element_stiffness(pg_ctx* ctx, const pg_problem* prob, double* ke_out);
  * msg/msg_len (optional) receive the failure reason. */
 int pg_plan_inspect(const pg_problem* prob, int ctas, int32_t* stats_out, char* msg,
                     size_t msg_len);
+
+/* pg_plan_inspect for a plan with a ghost halo of `rings` element layers
+ * (1, or 2 as the Chebyshev smoother uses: ring-1 nodes then carry tasks
+ * too, and the invariants cover them). */
+int pg_plan_inspect_halo(const pg_problem* prob, int ctas, int rings, int32_t* stats_out,
+                         char* msg, size_t msg_len);
 
 #ifdef __cplusplus
 }
