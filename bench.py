@@ -34,13 +34,20 @@ sys.path.insert(0, os.path.join(ROOT, "gpu-gauntlet_b200"))
 
 METRIC = "ms per 60k-DOF plate solve at 1e-6 FP64-checked error: learned/mixed vs plain PCG"
 FALLBACK_HBM_GBS = 6650.0
-# name -> (precision, preconditioner); "fp64" is the plain method.  Each
-# runs at the residual tolerance that gives about 6e-7 FP64 error on
-# plate_q4_141 (block Jacobi 1e-6, two-level 5e-6; the two-level iterates
-# are closer to the solution at equal residual), and the bench checks the
-# error of every variant against the FP64 truth.
-VARIANTS = {"fp64": ("fp64", "bj"), "mixed": ("mixed", "bj"),
-            "fp64_two_level": ("fp64", "tl"), "mixed_two_level": ("mixed", "tl")}
+# name -> (precision, preconditioner, smoother); "fp64" is the plain
+# method.  Each runs at the residual tolerance that gives 5e-7 to 9e-7 FP64
+# error on plate_q4_141 (block Jacobi 1e-6, two-level 5e-6; the two-level
+# iterates are closer to the solution at equal residual), and the bench
+# checks the error of every variant against the FP64 truth.
+VARIANTS = {"fp64": ("fp64", "bj", "bj"), "mixed": ("mixed", "bj", "bj"),
+            "mixed_cheb": ("mixed", "bj", "cheb"),
+            "fp64_two_level": ("fp64", "tl", "bj"), "mixed_two_level": ("mixed", "tl", "bj"),
+            "fp64_two_level_cheb": ("fp64", "tl", "cheb"),
+            "mixed_two_level_cheb": ("mixed", "tl", "cheb")}
+# algorithmic vector words per DOF and iteration (the minimal fused PCG
+# schedule: K.p 2, x 3, r 3, block Jacobi 5, p 3); the Chebyshev smoother
+# adds its K.t (2) and a second block-Jacobi product (3)
+WORDS = {"bj": 16, "cheb": 21}
 
 
 def parse_args():
@@ -283,16 +290,24 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def describe_preconditioner(v, coarse_dim):
+    sm = ("Chebyshev smoother (degree 2 in D^-1 K, 2-ring halo)" if v[2] == "cheb"
+          else "block Jacobi")
+    return (f"two-level ({sm} + coarse correction, {coarse_dim} coarse DOFs)" if v[1] == "tl"
+            else sm)
+
+
 def variant_options(args, name):
     from plategpu import _lib
 
-    precision, pre = VARIANTS[name]
+    precision, pre, smoother = VARIANTS[name]
     prec = _lib.PG_PREC_FP64 if precision == "fp64" else _lib.PG_PREC_MIXED
     tl = pre == "tl"
     return _lib.make_options(
         tolerance=args.tol_tl if tl else args.tol_bj, max_iterations=20000, precision=prec,
         stop_rule=_lib.PG_STOP_RELATIVE, ctas=args.ctas, threads=args.threads,
-        preconditioner=_lib.PG_PRECOND_TWO_LEVEL if tl else _lib.PG_PRECOND_BLOCK_JACOBI)
+        preconditioner=_lib.PG_PRECOND_TWO_LEVEL if tl else _lib.PG_PRECOND_BLOCK_JACOBI,
+        smoother=_lib.PG_SMOOTHER_CHEBYSHEV if smoother == "cheb" else _lib.PG_SMOOTHER_BLOCK_JACOBI)
 
 
 def time_variant(args, world, local, ctx, prob, name, stream, F_dev, x_dev, flush):
@@ -401,7 +416,7 @@ def run_plategpu(args, world, rank, local):
     # words for the FP32 inner iterations)
     word = 8 if VARIANTS[head][0] == "fp64" else 4
     iters = H["iterations"]
-    alg_bytes = 16.0 * n * word * iters
+    alg_bytes = float(WORDS[VARIANTS[head][2]]) * n * word * iters
     peak, peak_src = hbm_peak()
     achieved = alg_bytes / (H["kernel_ms"] * 1e-3) / 1e9
     kernel_tag = "pcg_" + head
@@ -414,9 +429,7 @@ def run_plategpu(args, world, rank, local):
         "data": "synthetic (seeded plate_q4_141: 5 kPa + 32 point loads, 16 columns)",
         "config": {"workload": args.workload, "dof": n, "elements": wl.mesh.elementCount,
                    "method": head,
-                   "preconditioner": ("two-level (block Jacobi + coarse correction, "
-                                      f"{H['coarse_dim']} coarse DOFs)"
-                                      if VARIANTS[head][1] == "tl" else "block-jacobi"),
+                   "preconditioner": describe_preconditioner(VARIANTS[head], H["coarse_dim"]),
                    "stop": f"||r||/||b|| < {H['tolerance']:g}", "ctas": H["ctas"],
                    "threads": H["threads"], "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas x{world}"},

@@ -125,3 +125,29 @@ def test_dkt_plan_invariants():
     pr = _lib.Problem(m, PlateMaterial(2.1e11, 0.3, 0.1), c)
     st = _lib.plan_inspect(pr, 37)
     assert st["violations"] == 0 and st["parts"] == 37
+
+
+@pytest.mark.parametrize("ctas", [1, 7, 148])
+def test_plan_invariants_two_ring_halo(ctas):
+    wl = workloads.plate_q4_141()
+    pr = _lib.Problem(wl.mesh, wl.material, wl.coloring, wl.F, wl.cons_mask)
+    one = _lib.plan_inspect(pr, ctas, rings=1)
+    two = _lib.plan_inspect(pr, ctas, rings=2)
+    assert two["violations"] == 0 and two["parts"] == one["parts"]
+    if ctas > 1:  # ring-1 nodes carry tasks and a second ghost layer appears
+        assert two["max_part_tasks"] > one["max_part_tasks"]
+        assert two["ghost_nodes"] > one["ghost_nodes"]
+        assert two["max_local_nodes"] > one["max_local_nodes"]
+    else:
+        assert two == one
+
+
+def test_dkt_plan_invariants_two_ring_halo():
+    from plategpu import coloring, mesher
+    from plategpu.types import PlateMaterial
+    m = mesher.split_triangle_mesh(10, 10, 30, 30, jitter=0.2, seed=2)
+    c = coloring.computeElementColoringGreedy(m)
+    pr = _lib.Problem(m, PlateMaterial(2.1e11, 0.3, 0.1), c)
+    assert _lib.plan_inspect(pr, 37, rings=2)["violations"] == 0
+    with pytest.raises(_lib.PlateGPUError, match="rings"):
+        _lib.plan_inspect(pr, 37, rings=3)

@@ -1,11 +1,15 @@
-"""CPU model of the two-level preconditioner (test helper).
+"""CPU model of the two-level preconditioner and the Chebyshev smoother
+(test helper).
 
 Restates, in numpy, the coarse space the library builds: the strip
 partition of the nodes into G parts (one aggregate each), the three
 rigid-body modes per aggregate (w = 1; w = dy, thx = 1/h; w = dx,
 thy = -1/h about the aggregate centre, h its size), P with constrained rows
 removed, A_c = P^T A P, and additive two-level PCG with
-M^-1 = M_bj^-1 + P A_c^-1 P^T, driven by textbook PCG.
+M^-1 = S + P A_c^-1 P^T, driven by textbook PCG.  S is block Jacobi
+(S = D^-1) or the degree-2 Chebyshev smoother S = a D^-1 - b D^-1 A D^-1
+whose coefficients come from a power-iteration estimate of
+lambda_max(D^-1 A) (the library's start vector and iteration count).
 """
 import numpy as np
 import scipy.sparse as sp
@@ -51,16 +55,48 @@ def coarse_basis(xy, cons, part, G):
     return sp.csr_matrix((vals, (rows, cols)), shape=(n, 3 * G))
 
 
-def two_level_pcg(A, b, bd_inv, P, tol, maxit=20000):
-    """Textbook PCG, stop on ||r|| / ||b|| < tol; returns (x, iterations)."""
+def lambda_max_power(A, bd_inv, cons, iters=30):
+    """|D^-1 A x| after `iters` normalised power steps from the library's
+    start vector x_i = 1 + 0.5 sin(0.7 i) (0 on constrained DOFs)."""
     Nn = bd_inv.size // 9
     Bi = bd_inv.reshape(Nn, 3, 3)
-    Ac = (P.T @ A @ P).toarray()
-    Aci = np.linalg.inv(Ac)
+    i = np.arange(3 * Nn)
+    x = np.where(np.asarray(cons) != 0, 0.0, 1.0 + 0.5 * np.sin(0.7 * i))
+    lam = 1.0
+    for _ in range(iters):
+        y = np.einsum("nij,nj->ni", Bi, (A @ x).reshape(Nn, 3)).reshape(-1)
+        lam = np.linalg.norm(y)
+        x = y / lam
+    return lam
+
+
+def chebyshev2(lam):
+    """(a, b) of S = a D^-1 - b D^-1 A D^-1: two Chebyshev steps for D^-1 A
+    on [hi / 20, hi], hi = 1.1 lam."""
+    hi = 1.1 * lam
+    lo = hi / 20.0
+    theta, delta = 0.5 * (hi + lo), 0.5 * (hi - lo)
+    sigma = theta / delta
+    rho0 = 1.0 / sigma
+    rho1 = 1.0 / (2.0 * sigma - rho0)
+    return (1.0 + rho1 * rho0) / theta + 2.0 * rho1 / delta, 2.0 * rho1 / (delta * theta)
+
+
+def two_level_pcg(A, b, bd_inv, P, tol, maxit=20000, cheb=None):
+    """Textbook PCG with M^-1 = S (+ P A_c^-1 P^T when P is given), stop on
+    ||r|| / ||b|| < tol; cheb = (a, b) selects the Chebyshev smoother.
+    Returns (x, iterations)."""
+    Nn = bd_inv.size // 9
+    Bi = bd_inv.reshape(Nn, 3, 3)
+    Aci = None if P is None else np.linalg.inv((P.T @ A @ P).toarray())
+
+    def D(v):
+        return np.einsum("nij,nj->ni", Bi, v.reshape(Nn, 3)).reshape(-1)
 
     def M(r):
-        z = np.einsum("nij,nj->ni", Bi, r.reshape(Nn, 3)).reshape(-1)
-        return z + P @ (Aci @ (P.T @ r))
+        t = D(r)
+        z = t if cheb is None else cheb[0] * t - cheb[1] * D(A @ t)
+        return z if P is None else z + P @ (Aci @ (P.T @ r))
 
     x = np.zeros_like(b)
     r = b.copy()
