@@ -40,6 +40,7 @@ struct PcgResult {
     int reductions;            // grid-wide reductions performed
     double nonfinite_vals[3];  // gamma, delta, rho at that reduction
     long long phase_cycles[8];  // block 0, see PhaseClock
+    unsigned last_tag;         // largest round tag this launch may have written
 };
 
 // Byte offsets of the shared-memory arrays of one block (computed on the
@@ -87,6 +88,9 @@ struct PcgArgs {
     double tol;
     int maxit;
     int stop_rule;
+    // round tags of this launch start at tag0 + 1: the exchange buffers keep
+    // older tags from earlier launches of the plan, which never match
+    unsigned tag0;
     unsigned long long timeout_ns;
     int ke_smem;                 // Ke blocks in shared memory: 0 none, 1 owned tasks, 2 all
     int timing;
@@ -523,7 +527,9 @@ __device__ __forceinline__ void task_matvec(const T* __restrict__ u, T* __restri
                                             const KT* __restrict__ kt2 = nullptr,
                                             size_t stride2 = 0) {
     constexpr int ND = 3 * NPE;
-    for (int t = threadIdx.x; t < count; t += blockDim.x) {
+    const int nt = blockDim.x, full = count <= nt ? count : count - count % nt;
+    // whole tasks while every thread has one
+    for (int t = threadIdx.x; t < full; t += nt) {
         const KT* kb = t < ksplit ? kt + t : kt2 + t;
         const size_t ks = t < ksplit ? stride : stride2;
         T a0 = T(0), a1 = T(0), a2 = T(0);
@@ -542,6 +548,22 @@ __device__ __forceinline__ void task_matvec(const T* __restrict__ u, T* __restri
         yt[t] = a0;
         yt[ys + t] = a1;
         yt[2 * ys + t] = a2;
+    }
+    // the remaining rem < nt tasks one row per thread (3 rem rows), so the
+    // last pass costs about a third of a task instead of a whole one
+    const int rem = count - full;
+    for (int q = threadIdx.x; q < 3 * rem; q += nt) {
+        const int t = full + q % rem, r = q / rem;
+        const KT* kb = t < ksplit ? kt + t : kt2 + t;
+        const size_t ks = t < ksplit ? stride : stride2;
+        T acc = T(0);
+#pragma unroll
+        for (int j = 0; j < NPE; j++) {
+            const int b = 3 * (int)tn[j * ts + t];
+#pragma unroll
+            for (int d = 0; d < 3; d++) acc += (T)kb[(size_t)(r * ND + 3 * j + d) * ks] * u[b + d];
+        }
+        yt[r * ys + t] = acc;
     }
 }
 
@@ -827,7 +849,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
     clk.start(a.timing && g == 0 && tid == 0, (long long*)(sm + L.clk));
     Waiter wt;
     wt.start(a.timeout_ns, a.abort_flag, &a.res->wait_failures);
-    unsigned e = 1, xe = 1;  // round tags
+    unsigned e = a.tag0 + 1, xe = a.tag0 + 1;  // round tags
     int status = ST_OK;
 
     // ---- two-level: u0 = M_bj r0 + P A_c^-1 P^T r0 (one exchange round) ----
@@ -1239,7 +1261,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
         a.res->true_rel_residual = true_rel < 0.0 ? 0.0 : true_rel;
         a.res->b_norm = bnorm;
         a.res->reliable_updates = nru;
-        a.res->reductions = (int)e - 1;
+        a.res->reductions = (int)(e - 1 - a.tag0);
+        a.res->last_tag = e > xe ? e : xe;
         for (int k = 0; k < 8; k++) a.res->phase_cycles[k] = clk.on ? clk.t[k] : 0;
     }
 }

@@ -140,7 +140,8 @@ typedef struct pg_info {
     double final_residual;        /* ||r|| of the recursive residual (reference meaning) */
     double true_rel_residual;     /* ||F - K x|| / ||F||, recomputed in FP64 on the GPU */
     double b_norm;                /* ||F|| */
-    double setup_ms;              /* device: element stiffness + block-Jacobi setup */
+    double setup_ms;              /* device: element stiffness + block-Jacobi setup (about 0
+                                     once the plan's set-up has been done) */
     double solve_ms;              /* device: persistent PCG launch */
     double total_ms;              /* host wall clock of the whole call (gpuTimeMs) */
     int32_t ctas;
@@ -196,12 +197,15 @@ int pg_solve(pg_ctx* ctx, const pg_problem* prob, const pg_options* opt, double*
              pg_info* info);
 
 /* Device-resident solves.  A plan holds the partition of one mesh and its
- * device copies (nodes, elements, colouring, constraints, material); each
- * pg_plan_solve_device recomputes the element stiffness and block-Jacobi
- * set-up on the device and runs the persistent PCG for a new load.  F_dev is
+ * device copies (nodes, elements, colouring, constraints, material).  The
+ * first solve on a plan computes the element stiffness, block-Jacobi and
+ * task set-up on the device (they depend only on the plan's own copies, so
+ * later solves reuse them); every pg_plan_solve_device runs the persistent
+ * PCG for a new load.  F_dev is
  * a device float [3*node_count], x_dev a device double [3*node_count]; work
  * runs on the context stream and the call returns after its one readback
- * of the result record.  A plan must not outlive its context. */
+ * of the result record (x_dev is unspecified when the call fails).  A plan
+ * must not outlive its context. */
 typedef struct pg_plan pg_plan;
 int pg_plan_create(pg_ctx* ctx, const pg_problem* prob, const pg_options* opt, pg_plan** out);
 int pg_plan_solve_device(pg_plan* plan, const pg_options* opt, const float* F_dev,
