@@ -10,8 +10,8 @@
  * Uint32Array, colorOffsets / elementsByColor: Uint32Array, F: Float32Array,
  * constrained: Uint8Array, elemT: Float32Array | undefined) and numbers
  * (nodeCount, elementCount, nodesPerElement, E, nu, t, tolerance,
- * maxIterations, precision).  The inputs are copied before the work is
- * queued, so the caller may reuse its arrays at once; the result's
+ * maxIterations, precision, preconditioner, smoother, stopRule).  The
+ * inputs are copied before the work is queued, so the caller may reuse its arrays at once; the result's
  * `solution` is a fresh Float64Array.  A non-OK pg_status rejects the
  * promise with an Error carrying pg_last_error() and the status name.
  *
@@ -215,14 +215,17 @@ static napi_value js_solve(napi_env env, napi_callback_info info) {
         napi_throw_error(env, "PG_ENOMEM", "out of memory");
         return NULL;
     }
-    double nn, ne, npe, E, nu, t, tol, maxit, prec;
+    double nn, ne, npe, E, nu, t, tol, maxit, prec, pre, smo, stop;
     napi_value o = argv[0];
     int bad = get_number(env, o, "nodeCount", -1, &nn) | get_number(env, o, "elementCount", -1, &ne) |
               get_number(env, o, "nodesPerElement", 4, &npe) | get_number(env, o, "E", 0, &E) |
               get_number(env, o, "nu", 0, &nu) | get_number(env, o, "t", 0, &t) |
               get_number(env, o, "tolerance", 1e-6, &tol) |
               get_number(env, o, "maxIterations", 1000, &maxit) |
-              get_number(env, o, "precision", PG_PREC_FP64, &prec);
+              get_number(env, o, "precision", PG_PREC_FP64, &prec) |
+              get_number(env, o, "preconditioner", PG_PRECOND_BLOCK_JACOBI, &pre) |
+              get_number(env, o, "smoother", PG_SMOOTHER_BLOCK_JACOBI, &smo) |
+              get_number(env, o, "stopRule", PG_STOP_REFERENCE, &stop);
     if (bad || nn < 0 || ne < 0 || nn > 67108864.0 || ne > 67108864.0) {
         job_free(j);
         napi_throw_error(env, "PG_EINVAL", "problem needs nodeCount, elementCount, E, nu, t");
@@ -270,6 +273,9 @@ static napi_value js_solve(napi_env env, napi_callback_info info) {
     j->opt.tolerance = tol;
     j->opt.max_iterations = (int32_t)maxit;
     j->opt.precision = (int32_t)prec;
+    j->opt.preconditioner = (int32_t)pre;
+    j->opt.smoother = (int32_t)smo;
+    j->opt.stop_rule = (int32_t)stop;
     napi_create_promise(env, &j->deferred, &promise);
     napi_create_string_utf8(env, "plategpu.solve", NAPI_AUTO_LENGTH, &name);
     if (napi_create_async_work(env, NULL, name, solve_execute, solve_complete, j, &j->work) != 0 ||

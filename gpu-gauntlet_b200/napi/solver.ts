@@ -23,6 +23,12 @@ export interface GPUSolverOptions {
   forceCPU?: boolean;
   /** 'fp64' (default) or 'mixed' (FP32 inner iterations, FP64 residual checks) */
   precision?: 'fp64' | 'mixed';
+  /** 'block-jacobi' (default, the reference's) or 'two-level' (plus a coarse correction) */
+  preconditioner?: 'block-jacobi' | 'two-level';
+  /** 'block-jacobi' (default) or 'chebyshev' (two Chebyshev steps for D^-1 K) */
+  smoother?: 'block-jacobi' | 'chebyshev';
+  /** 'reference' (default: ||r|| < tol or ||r||/||b|| < tol) or 'relative' (||r||/||b|| < tol) */
+  stopRule?: 'reference' | 'relative';
 }
 
 export interface GPUSolveResult {
@@ -119,6 +125,9 @@ export async function solveGPU(
     tolerance: options.tolerance ?? 1e-6,
     maxIterations: options.maxIterations ?? 1000,
     precision: options.precision === 'mixed' ? 1 : 0,
+    preconditioner: options.preconditioner === 'two-level' ? 1 : 0,
+    smoother: options.smoother === 'chebyshev' ? 1 : 0,
+    stopRule: options.stopRule === 'relative' ? 1 : 0,
   });
   return {
     solution: Float32Array.from(r.solution),

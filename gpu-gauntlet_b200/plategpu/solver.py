@@ -26,6 +26,8 @@ _contexts: Dict[int, _lib.Context] = {}
 
 _PREC = {"fp64": _lib.PG_PREC_FP64, "mixed": _lib.PG_PREC_MIXED}
 _STOP = {"reference": _lib.PG_STOP_REFERENCE, "relative": _lib.PG_STOP_RELATIVE}
+_PRECOND = {"block-jacobi": _lib.PG_PRECOND_BLOCK_JACOBI, "two-level": _lib.PG_PRECOND_TWO_LEVEL}
+_SMOOTHER = {"block-jacobi": _lib.PG_SMOOTHER_BLOCK_JACOBI, "chebyshev": _lib.PG_SMOOTHER_CHEBYSHEV}
 
 
 def get_context(device: int = 0) -> _lib.Context:
@@ -58,6 +60,12 @@ def _mask(mesh: PlateMesh, constrainedDOFs) -> np.ndarray:
     return constrained_mask(n, constrainedDOFs)
 
 
+def _option(table, value, name):
+    if value not in table:
+        raise _lib.PlateGPUError(_lib.PG_EINVAL, f"unknown {name} {value!r}: one of {sorted(table)}")
+    return table[value]
+
+
 def solveGPU(mesh: PlateMesh, material: PlateMaterial, coloring: Optional[ElementColoring],
              F: np.ndarray, constrainedDOFs, options: Optional[GPUSolverOptions] = None,
              device: int = 0) -> GPUSolveResult:
@@ -70,12 +78,15 @@ def solveGPU(mesh: PlateMesh, material: PlateMaterial, coloring: Optional[Elemen
     if F.size != 3 * mesh.nodeCount:
         raise _lib.PlateGPUError(_lib.PG_EINVAL,
                                  f"F has {F.size} entries, expected {3 * mesh.nodeCount}")
-    ctx = get_context(device)
-    prob = _lib.Problem(mesh, material, coloring, F, _mask(mesh, constrainedDOFs))
     opts = _lib.make_options(
         tolerance=1e-6 if options.tolerance is None else options.tolerance,
         max_iterations=1000 if options.maxIterations is None else options.maxIterations,
-        precision=_PREC[options.precision], stop_rule=_STOP[options.stopRule])
+        precision=_option(_PREC, options.precision, "precision"),
+        stop_rule=_option(_STOP, options.stopRule, "stopRule"),
+        preconditioner=_option(_PRECOND, options.preconditioner, "preconditioner"),
+        smoother=_option(_SMOOTHER, options.smoother, "smoother"))
+    ctx = get_context(device)
+    prob = _lib.Problem(mesh, material, coloring, F, _mask(mesh, constrainedDOFs))
     x, info = ctx.solve(prob, opts)
     sol = x if options.returnFloat64 else x.astype(np.float32)
     return GPUSolveResult(solution=sol, iterations=int(info.iterations),

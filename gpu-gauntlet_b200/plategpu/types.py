@@ -104,13 +104,19 @@ class GPUSolverOptions:
     solver has no CPU path.  Extensions: ``precision`` ('fp64' plain FP64
     PCG, 'mixed' FP32 inner iterations with FP64 residual replacement) and
     ``stopRule`` ('reference': ||r|| < tol or ||r||/||b|| < tol on the
-    recursive residual, gpu/solver.ts:516; 'relative': ||r||/||b|| < tol)."""
+    recursive residual, gpu/solver.ts:516; 'relative': ||r||/||b|| < tol),
+    ``preconditioner`` ('block-jacobi', the reference's; 'two-level': plus a
+    coarse correction with the plate's rigid modes on one aggregate per
+    thread block) and ``smoother`` ('block-jacobi'; 'chebyshev': two
+    Chebyshev steps for D^-1 K in place of D^-1)."""
 
     tolerance: Optional[float] = None
     maxIterations: Optional[int] = None
     forceCPU: bool = False
     precision: str = "fp64"
     stopRule: str = "reference"
+    preconditioner: str = "block-jacobi"
+    smoother: str = "block-jacobi"
     returnFloat64: bool = False
 
 

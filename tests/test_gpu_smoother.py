@@ -101,3 +101,19 @@ def test_chebyshev_needs_a_halo_plan(gpu_ctx):
                                                 max_iterations=5000), F.data_ptr(), x.data_ptr())
     assert info.converged and info.smoother_lambda_max > 0
     plan2.close()
+
+
+def test_solvegpu_mirror_with_fast_options(gpu_ctx, oracle):
+    """The reference-shaped entry point with the fastest measured settings."""
+    from plategpu import solveGPU
+    from plategpu.types import GPUSolverOptions
+    wl = workloads.plate_q4_141()
+    ke, A, bd, b = fp64_operator(oracle, wl)
+    import scipy.sparse.linalg as spla
+    xs = spla.spsolve(A.tocsc(), b)
+    res = solveGPU(wl.mesh, wl.material, wl.coloring, wl.F, wl.constrainedDOFs,
+                   GPUSolverOptions(tolerance=5e-6, maxIterations=5000, precision="mixed",
+                                    stopRule="relative", preconditioner="two-level",
+                                    smoother="chebyshev", returnFloat64=True))
+    assert res.converged and res.usedGPU and res.iterations < 250
+    assert rel_err(res.solution, xs) < 1e-6

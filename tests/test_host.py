@@ -96,3 +96,14 @@ def test_dkt_workload_thickness_field():
     assert 0.08 < float(t.mean()) < 0.12 and t.std() > 0.005
     assert wl.n_dof == 121203
     assert col.verifyColoring(wl.mesh, wl.coloring)
+
+
+def test_solver_options_are_checked_before_any_device_work():
+    from plategpu import PlateGPUError, solveGPU
+    from plategpu.types import GPUSolverOptions
+    wl = workloads.plate_q4(4, 0)
+    for bad in (dict(preconditioner="multigrid"), dict(smoother="gauss-seidel"),
+                dict(precision="fp16"), dict(stopRule="absolute")):
+        with pytest.raises(PlateGPUError, match="unknown"):
+            solveGPU(wl.mesh, wl.material, wl.coloring, wl.F, wl.constrainedDOFs,
+                     GPUSolverOptions(**bad))
