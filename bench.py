@@ -44,6 +44,12 @@ VARIANTS = {"fp64": ("fp64", "bj", "bj"), "mixed": ("mixed", "bj", "bj"),
             "fp64_two_level": ("fp64", "tl", "bj"), "mixed_two_level": ("mixed", "tl", "bj"),
             "fp64_two_level_cheb": ("fp64", "tl", "cheb"),
             "mixed_two_level_cheb": ("mixed", "tl", "cheb")}
+WORKLOAD_DATA = {
+    "plate_q4_141": "synthetic (seeded plate_q4_141: 5 kPa + 32 point loads, 16 columns)",
+    "plate_q4_32": "synthetic (seeded plate_q4_32: 1 kPa + 4 point loads, clamped)",
+    "plate_dkt_200": "synthetic (seeded plate_dkt_200: jittered DKT mesh, GRF thickness, "
+                     "3 kPa, clamped)",
+}
 # algorithmic vector words per DOF and iteration (the minimal fused PCG
 # schedule: K.p 2, x 3, r 3, block Jacobi 5, p 3); the Chebyshev smoother
 # adds its K.t (2) and a second block-Jacobi product (3)
@@ -426,7 +432,7 @@ def run_plategpu(args, world, rank, local):
         "ms_per_step": statistics.mean(H["step_ms"]),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if VARIANTS[head][0] == "fp64" else "f32 inner / f64 refinement",
-        "data": "synthetic (seeded plate_q4_141: 5 kPa + 32 point loads, 16 columns)",
+        "data": WORKLOAD_DATA.get(args.workload, "synthetic (seeded workload)"),
         "config": {"workload": args.workload, "dof": n, "elements": wl.mesh.elementCount,
                    "method": head,
                    "preconditioner": describe_preconditioner(VARIANTS[head], H["coarse_dim"]),

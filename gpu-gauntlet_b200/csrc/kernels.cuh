@@ -66,6 +66,7 @@ constexpr int kRep = 8;
 
 struct PcgArgs {
     int G, NT, Nn;
+    int npe;                     // 3 (DKT) or 4 (Q4): the batch kernel's dispatch
     const int* node_off;
     const int* nown;
     const int* nodes;
@@ -389,7 +390,7 @@ __device__ __forceinline__ double warp_reduce_scatter(double (&v)[KM]) {
 // Block-wide totals of the first K (<= KM) of the KM values v, published
 // as this block's partial sums: copy r < kRep goes to slots
 // pb[r][g][2k, 2k+1] (lane r of warp 0 writes copy r).  Every block reads
-// the copy blockIdx % kRep, so each slot line has about G / kRep readers
+// the copy g % kRep, so each slot line has about G / kRep readers
 // instead of G.  All threads call it; it has one barrier, and warp 0 alone
 // works after it, so `red` must not be written again before a later barrier.
 template <int KM>
@@ -425,10 +426,11 @@ __device__ void block_publish(double (&v)[KM], double* red, unsigned long long* 
 template <typename T, int IF = 2>
 __device__ bool exchange_round(const unsigned long long* __restrict__ pb, int G, int K,
                                const unsigned long long* __restrict__ vb, T* dst, int no, int nloc,
-                               const int* __restrict__ gid, unsigned f, double* sp, Waiter& wt) {
+                               const int* __restrict__ gid, int g, unsigned f, double* sp,
+                               Waiter& wt) {
     constexpr int TW = Tag<T>::W;
     const int np = G * K, n = np + 3 * (nloc - no);
-    pb += (size_t)(blockIdx.x % kRep) * G * 16;  // the copy of the partials this block reads
+    pb += (size_t)(g % kRep) * G * 16;  // the copy of the partials part g reads
     for (int i0 = threadIdx.x; i0 < n; i0 += IF * blockDim.x) {
         const unsigned long long* ptr[IF];
         bool done[IF];
@@ -527,7 +529,11 @@ __device__ __forceinline__ void task_matvec(const T* __restrict__ u, T* __restri
                                             const KT* __restrict__ kt2 = nullptr,
                                             size_t stride2 = 0) {
     constexpr int ND = 3 * NPE;
-    const int nt = blockDim.x, full = count <= nt ? count : count - count % nt;
+    // FP64 blocks split the last partial pass into task rows; FP32 blocks do
+    // not (measured on the 60k-DOF plate: the split saves 2% in FP64 and
+    // costs 6% in mixed precision, whose whole-task pass is cheaper)
+    constexpr bool split = sizeof(T) == 8;
+    const int nt = blockDim.x, full = (!split || count <= nt) ? count : count - count % nt;
     // whole tasks while every thread has one
     for (int t = threadIdx.x; t < full; t += nt) {
         const KT* kb = t < ksplit ? kt + t : kt2 + t;
@@ -550,7 +556,7 @@ __device__ __forceinline__ void task_matvec(const T* __restrict__ u, T* __restri
         yt[2 * ys + t] = a2;
     }
     // the remaining rem < nt tasks one row per thread (3 rem rows), so the
-    // last pass costs about a third of a task instead of a whole one
+    // last pass costs about a third of a task instead of a whole one (FP64)
     const int rem = count - full;
     for (int q = threadIdx.x; q < 3 * rem; q += nt) {
         const int t = full + q % rem, r = q / rem;
@@ -593,7 +599,7 @@ __global__ void task_ke_kernel(int NT, const int* __restrict__ task_elem,
 // persistent PCG
 // ---------------------------------------------------------------------------
 
-enum { STOP_CONVERGED = 0, STOP_MAX_ITER = 1, STOP_BREAKDOWN = 2, STOP_ZERO_RHS = 3 };
+enum { STOP_CONVERGED = 0, STOP_MAX_ITER = 1, STOP_BREAKDOWN = 2, STOP_ZERO_RHS = 3, STOP_STAGNATED = 4 };
 enum { ACT_UPDATE = 0, ACT_STOP = 1, ACT_RU = 2, ACT_NONFINITE = 3 };
 enum { ST_OK = 0, ST_TIMEOUT = 4, ST_NONFINITE = 5 };
 
@@ -733,11 +739,10 @@ __device__ __forceinline__ void coarse_apply(const T* __restrict__ Ai, int G, in
 // round e - 1 partials, and every block reads round e - 2 before it
 // publishes round e - 1, so no reader can still need the old values.
 template <int NPE, typename T, bool MIXED>
-__global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
+__device__ __forceinline__ void pcg_body(const PcgArgs& a, const int g, unsigned char* sm) {
     constexpr int ND = 3 * NPE, TW = Tag<T>::W;
-    extern __shared__ __align__(16) unsigned char sm[];
     const SmemLayout& L = a.L;
-    const int g = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x;
     const int n0 = a.node_off[g], nloc = a.node_off[g + 1] - n0, no = a.nown[g];
     // tasks [0, nta) of the part; the owned nodes' are [0, ntm) (all of them
     // unless the plan has a 2-ring halo: then ring-1 nodes' tasks follow)
@@ -858,7 +863,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
         for (int n = tid; n < no; n += nt) restrict3(r + 3 * n, cm + 3 * n, nb + 3 * n, v0);
         unsigned long long* pb0 = a.llp + (size_t)(e & 1) * kRep * a.G * 16;
         block_publish<4>(v0, red, pb0, a.G, g, 3, e);
-        const bool ok = exchange_round<T>(pb0, a.G, 3, nullptr, w, no, no, gid, e, sp, wt);
+        const bool ok = exchange_round<T>(pb0, a.G, 3, nullptr, w, no, no, gid, g, e, sp, wt);
         if (__syncthreads_or(!ok)) {
             status = ST_TIMEOUT;
         } else {
@@ -877,6 +882,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
     const double thr_abs = a.tol * a.tol;
     double thr_rel = 0.0, thr_ru = 0.0;
     int cb = 0;  // current copy of the coarse state
+    double best_trn = INFINITY;  // mixed: smallest FP64 residual seen at a replacement
+    int stall = 0;               // replacements since it last halved
     int it = 0, stop = -1, xupd = 0, xupd_ref = 0, nru = 0;
     double final_res = 0.0, true_rel = -1.0;
     bool first = true;
@@ -930,7 +937,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
         clk.lap(2);
         // ---- exchange: every block's partials and this block's ghost w ----
         {
-            bool ok = exchange_round<T>(pb, a.G, KP, vb, w, no, nloc, gid, e, sp, wt);
+            bool ok = exchange_round<T>(pb, a.G, KP, vb, w, no, nloc, gid, g, e, sp, wt);
             if (a.test_stall && it == 0 && tid == 0) {
                 double never;  // a tag no block writes: the wait must run out
                 ok = ok && poll<double>(a.llp + (size_t)kRep * a.G * 32, 0xffffffffu, never, wt);
@@ -1042,7 +1049,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
                 if (a.coarse) restrict3(rtv, cm + 3 * n, nb + 3 * n, vt + 1);
             }
             block_publish<4>(vt, red, qb, a.G, g, KR, e);
-            ok = exchange_round<T>(qb, a.G, KR, rb, r, no, nloc, gid, e, sp, wt);
+            ok = exchange_round<T>(qb, a.G, KR, rb, r, no, nloc, gid, g, e, sp, wt);
             if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
             sum_partials<1>(sp, a.G, KR, scal);
             // c = A_c^-1 P^T r from the true residual (cs is unchanged)
@@ -1077,6 +1084,14 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
                     stop = STOP_CONVERGED; final_res = trn; true_rel = trn / bnorm; act2 = ACT_STOP;
                 } else if (xupd >= a.maxit) {
                     stop = STOP_MAX_ITER; final_res = trn; true_rel = trn / bnorm; act2 = ACT_STOP;
+                } else if (trn < 0.5 * best_trn) {
+                    best_trn = trn;
+                    stall = 0;
+                } else if (++stall >= 3) {
+                    // three replacements in a row without halving the FP64
+                    // residual: the FP32 inner iterations no longer reduce
+                    // the error (condition number near 1 / FP32 epsilon)
+                    stop = STOP_STAGNATED; final_res = trn; true_rel = trn / bnorm; act2 = ACT_STOP;
                 }
                 ctl[0] = act2;
                 ctl[1] = 0;
@@ -1241,7 +1256,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
             unsigned long long* pb = a.llp + (size_t)(e & 1) * kRep * a.G * 16;
             block_publish<2>(v, red, pb, a.G, g, 2, e);
             if (g == 0) {
-                ok = exchange_round<T>(pb, a.G, 2, nullptr, w, no, no, gid, e, sp, wt);
+                ok = exchange_round<T>(pb, a.G, 2, nullptr, w, no, no, gid, g, e, sp, wt);
                 if (__syncthreads_or(!ok)) {
                     status = ST_TIMEOUT;
                 } else {
@@ -1264,6 +1279,46 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const PcgArgs a) {
         a.res->reductions = (int)(e - 1 - a.tag0);
         a.res->last_tag = e > xe ? e : xe;
         for (int k = 0; k < 8; k++) a.res->phase_cycles[k] = clk.on ? clk.t[k] : 0;
+    }
+}
+
+// One plate on the whole grid: part g = block g.
+template <int NPE, typename T, bool MIXED>
+__global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const __grid_constant__ PcgArgs a) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    pcg_body<NPE, T, MIXED>(a, blockIdx.x, sm);
+}
+
+// Many independent plates in one launch.  The grid is cut into teams of
+// consecutive blocks; a team solves the plates of its queue one after the
+// other, each plate partitioned into as many parts as the team has blocks,
+// with the plate's own exchange buffers (so teams never wait on each other,
+// and a team starts its next plate as soon as its blocks are done).  Team
+// block 0 stamps each plate's start and end (globaltimer).
+struct BatchArgs {
+    const PcgArgs* plates;        // [count], npe 3 or 4, one precision for all
+    const int* block_team;        // [grid] team of each block
+    const int* team_base;         // [teams] first block of each team
+    const int* queue_off;         // [teams + 1] into queue
+    const int* queue;             // plate ids, team by team, in solve order
+    unsigned long long* times;    // [count][2] start / end of each plate
+};
+
+template <typename T, bool MIXED>
+__global__ void __launch_bounds__(kMaxThreads, 1) pcg_batch_kernel(const __grid_constant__ BatchArgs b) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int team = b.block_team[blockIdx.x];
+    const int g = (int)blockIdx.x - b.team_base[team];
+    for (int q = b.queue_off[team]; q < b.queue_off[team + 1]; q++) {
+        const int pi = b.queue[q];
+        const PcgArgs& a = b.plates[pi];
+        if (g == 0 && threadIdx.x == 0) b.times[2 * pi] = gtimer();
+        if (a.npe == 4)
+            pcg_body<4, T, MIXED>(a, g, sm);
+        else
+            pcg_body<3, T, MIXED>(a, g, sm);
+        __syncthreads();  // shared memory is reloaded for the next plate
+        if (g == 0 && threadIdx.x == 0) b.times[2 * pi + 1] = gtimer();
     }
 }
 

@@ -460,6 +460,104 @@ double estimate_lambda_max(const pg_problem& p, const std::vector<double>& ke64,
     return lam;
 }
 
+std::string schedule_batch(const std::vector<int>& nodes, int sms, int cap, BatchSchedule& out) {
+    out = BatchSchedule{};
+    const int count = (int)nodes.size();
+    if (count == 0) return "empty batch";
+    if (sms < 1 || cap < 1) return "no blocks to schedule";
+    int top = 1;  // largest power of two <= sms
+    while (top * 2 <= sms) top *= 2;
+    std::vector<int> d(count);
+    std::vector<double> w(count);
+    for (int i = 0; i < count; i++) {
+        const double n = std::max(1, nodes[i]);
+        int need = 1;
+        while (need < std::ceil(n / cap)) need *= 2;
+        if (need > top) {
+            if ((double)sms * cap < n) return "a plate of the batch needs more blocks than the device has";
+            need = sms;
+        }
+        const int pref = std::max(1, (int)std::lround(std::exp2(std::round(std::log2(std::max(1.0, n / 400.0))))));
+        d[i] = std::max(need, std::min(top, pref));
+        w[i] = std::sqrt(n) * (n + 300.0 * d[i]);
+    }
+    // team sizes, largest first, first-fit into phases (one team of each size fits)
+    std::vector<int> cs;
+    for (int i = 0; i < count; i++)
+        if (std::find(cs.begin(), cs.end(), d[i]) == cs.end()) cs.push_back(d[i]);
+    std::sort(cs.rbegin(), cs.rend());
+    std::vector<std::vector<int>> phase_sizes;
+    std::vector<int> phase_sum;
+    for (int c : cs) {
+        size_t ph = 0;
+        while (ph < phase_sizes.size() && phase_sum[ph] + c > sms) ph++;
+        if (ph == phase_sizes.size()) {
+            phase_sizes.emplace_back();
+            phase_sum.push_back(0);
+        }
+        phase_sizes[ph].push_back(c);
+        phase_sum[ph] += c;
+    }
+    out.plate_phase.assign(count, -1);
+    out.plate_team.assign(count, -1);
+    out.plate_size = d;
+    std::vector<int> order(count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return w[a] > w[b]; });
+    for (size_t ph = 0; ph < phase_sizes.size(); ph++) {
+        const std::vector<int>& pc = phase_sizes[ph];  // descending
+        const int nc = (int)pc.size();
+        std::vector<double> W(nc, 0.0);
+        std::vector<int> teams(nc, 1), nplates(nc, 0);
+        for (int i = 0; i < count; i++) {
+            const auto it = std::find(pc.begin(), pc.end(), d[i]);
+            if (it == pc.end()) continue;
+            W[it - pc.begin()] += w[i];
+            nplates[it - pc.begin()]++;
+        }
+        int used = phase_sum[ph];
+        for (;;) {  // one more team to the size with the most work per block
+            int best = -1;
+            double bw = 0.0;
+            for (int k = 0; k < nc; k++) {
+                if (used + pc[k] > sms || teams[k] >= nplates[k]) continue;
+                const double per = W[k] / ((double)teams[k] * pc[k]);
+                if (per > bw) { bw = per; best = k; }
+            }
+            if (best < 0) break;
+            teams[best]++;
+            used += pc[best];
+        }
+        BatchPhase P;
+        for (int k = 0; k < nc; k++)
+            for (int t = 0; t < teams[k]; t++) {
+                P.team_base.push_back(P.grid);
+                P.team_size.push_back(pc[k]);
+                P.grid += pc[k];
+            }
+        const int T = (int)P.team_size.size();
+        P.team_load.assign(T, 0.0);
+        std::vector<std::vector<int>> q(T);
+        for (int i : order) {
+            if (std::find(pc.begin(), pc.end(), d[i]) == pc.end()) continue;
+            int bt = -1;
+            for (int t = 0; t < T; t++)
+                if (P.team_size[t] == d[i] && (bt < 0 || P.team_load[t] < P.team_load[bt])) bt = t;
+            out.plate_phase[i] = (int)ph;
+            out.plate_team[i] = bt;
+            P.team_load[bt] += w[i];
+            q[bt].push_back(i);
+        }
+        P.queue_off.assign(T + 1, 0);
+        for (int t = 0; t < T; t++) {
+            P.queue_off[t + 1] = P.queue_off[t] + (int)q[t].size();
+            P.queue.insert(P.queue.end(), q[t].begin(), q[t].end());
+        }
+        out.phases.push_back(std::move(P));
+    }
+    return "";
+}
+
 uint64_t problem_hash(const pg_problem& p) {
     uint64_t h = 0x9e3779b97f4a7c15ull;
     auto mix = [&](uint64_t v) {

@@ -82,6 +82,29 @@ std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, H
 double estimate_lambda_max(const pg_problem& p, const std::vector<double>& ke64,
                            const std::vector<double>& binv64, int iters);
 
+// Team schedule of a batch of independent plates.  A plate of n nodes gets
+// a team of d blocks: a power of two, or every block of the device for the
+// largest plates, with at most cap nodes per block (so its parts fit in
+// shared memory) and about n / 400 nodes per block otherwise (fewer blocks
+// per plate cost less block time, since an iteration's latency hardly
+// depends on the part size).  Team sizes that fit side by side form a
+// phase, one persistent launch; inside a phase the blocks are shared out
+// among the team sizes in proportion to their estimated work (sqrt(n)
+// iterations of n + 300 d node-equivalents), one team per size at least,
+// and each size's plates go to its teams longest first to the least-loaded
+// team.
+struct BatchPhase {
+    int grid = 0;                         // blocks of the launch
+    std::vector<int> team_base, team_size;
+    std::vector<int> queue_off, queue;    // per team, plates in solve order
+    std::vector<double> team_load;        // estimated work per team
+};
+struct BatchSchedule {
+    std::vector<BatchPhase> phases;
+    std::vector<int> plate_phase, plate_team, plate_size;  // [count]; team index within its phase
+};
+std::string schedule_batch(const std::vector<int>& nodes, int sms, int cap, BatchSchedule& out);
+
 // 64-bit FNV-1a over the problem's mesh, colouring, material and
 // constraint arrays (not F): the key of the plan cache.
 uint64_t problem_hash(const pg_problem& p);

@@ -64,6 +64,7 @@ struct Plan {
     std::vector<float> h_nodes;
     std::vector<uint32_t> h_elements;
     std::vector<uint8_t> h_cons;
+    std::vector<float> h_elem_t;
     pg_problem prob_view{};
     double E = 0, nu = 0, t = 0;
     bool has_elem_t = false;
@@ -97,6 +98,27 @@ struct Plan {
 struct pg_plan {
     pg_ctx* ctx = nullptr;
     std::unique_ptr<Plan> plan;
+};
+
+// A batch of independent plates: one plan per plate, partitioned for the
+// size of the team of blocks that solves it, and the team schedule (one
+// launch per phase).
+struct BatchPhaseDev {
+    int grid = 0;
+    DevBuf<int> block_team, team_base, queue_off, queue;
+};
+struct pg_batch {
+    pg_ctx* ctx = nullptr;
+    int rings = 1;
+    std::vector<std::unique_ptr<Plan>> plans;
+    pg::BatchSchedule sched;
+    std::vector<std::unique_ptr<BatchPhaseDev>> phases;
+    DevBuf<int> abort_flag;
+    DevBuf<pg::PcgArgs> args;
+    DevBuf<pg::PcgResult> res;
+    DevBuf<unsigned long long> times;
+    int ok_smem = 0;
+    const void* ok_fn = nullptr;
 };
 
 struct pg_ctx {
@@ -199,9 +221,11 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G, int ring
     pl->prob_view.elements = pl->h_elements.data();
     pl->prob_view.constrained = pl->h_cons.data();
     pl->prob_view.F = nullptr;
+    pl->prob_view.color_count = 0;  // a plan rebuilt from the view recolours greedily
     pl->prob_view.color_offsets = nullptr;
     pl->prob_view.elements_by_color = nullptr;
-    pl->prob_view.elem_t = nullptr;
+    if (p.elem_t) pl->h_elem_t.assign(p.elem_t, p.elem_t + (size_t)p.element_count);
+    pl->prob_view.elem_t = p.elem_t ? pl->h_elem_t.data() : nullptr;
     pl->E = p.E;
     pl->nu = p.nu;
     pl->t = p.t;
@@ -382,46 +406,43 @@ void chebyshev2(double lambda_max, double* a, double* b) {
 
 // Queues setup + persistent PCG on the context stream, then waits for the
 // result record (one small readback).  F must already be in pl->F.
-// x_dst (optional) receives the solution by a copy of `kind` queued right
-// behind the kernel, so the call waits for the device once.
-void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_dst = nullptr,
-               cudaMemcpyKind kind = cudaMemcpyDeviceToDevice) {
-    const pg::HostPlan& hp = pl->hp;
-    const bool mixed = o.precision == PG_PREC_MIXED;
-    int threads = o.threads;
-    if (!threads) threads = std::min(pg::kMaxThreads, std::max(128, (hp.max_ntask + 31) / 32 * 32));
-    const bool coarse = o.preconditioner == PG_PRECOND_TWO_LEVEL;
-    const bool cheb = o.smoother == PG_SMOOTHER_CHEBYSHEV;
-    if (cheb && hp.rings != 2)
+// Coarse data and the smoother's eigenvalue, built once per plan on first use.
+void prepare_plan_data(pg_ctx* c, Plan* pl, const pg_options& o) {
+    if (o.smoother == PG_SMOOTHER_CHEBYSHEV && pl->hp.rings != 2)
         throw Fail{PG_EINVAL, "the Chebyshev smoother needs a plan made with it (2-ring halo)"};
-    if (coarse) ensure_coarse(c, pl);
-    if (cheb) ensure_smoother(c, pl);
-    // keep in shared memory what fits, in this order of preference: every
-    // task's Ke blocks (only differs from the owned tasks' with a 2-ring
-    // halo) and the A_c^-1 rows; the owned tasks' blocks and A_c^-1; then
-    // the larger of the owned tasks' blocks and A_c^-1; then neither (L2)
+    if (o.preconditioner == PG_PRECOND_TWO_LEVEL) ensure_coarse(c, pl);
+    if (o.smoother == PG_SMOOTHER_CHEBYSHEV) ensure_smoother(c, pl);
+}
+
+// Shared-memory layout of a launch: keep in shared memory what fits, in this
+// order of preference: every task's Ke blocks (only differs from the owned
+// tasks' with a 2-ring halo) and the A_c^-1 rows; the owned tasks' blocks
+// and A_c^-1; then the larger of the owned tasks' blocks and A_c^-1; then
+// neither (read from L2).
+pg::SmemLayout choose_layout(pg_ctx* c, const pg::HostPlan& hp, const pg_options& o, int* ke_mode,
+                             bool* ainv_smem) {
+    const bool mixed = o.precision == PG_PREC_MIXED, coarse = o.preconditioner == PG_PRECOND_TWO_LEVEL;
     const int full = hp.rings == 2 ? 2 : 1;
     const bool ke_first = 3 * 3 * hp.npe * (size_t)hp.max_ntask_own >= (size_t)3 * hp.max_kagg * hp.C;
     const int cand[6][2] = {{full, 1}, {1, 1}, {ke_first ? full : 0, ke_first ? 0 : 1},
                             {ke_first ? 1 : 0, ke_first ? 0 : 1}, {0, 1}, {0, 0}};
-    int ke_mode = 0;
-    bool ainv_smem = false;
     pg::SmemLayout L{};
     for (auto& cd : cand) {
-        ke_mode = cd[0];
-        ainv_smem = coarse && cd[1];
-        L = make_layout(hp, mixed, ke_mode, coarse, ainv_smem);
+        *ke_mode = cd[0];
+        *ainv_smem = coarse && cd[1];
+        L = make_layout(hp, mixed, *ke_mode, coarse, *ainv_smem);
         if (L.total <= c->max_smem) break;
     }
     if (L.total > c->max_smem)
         throw Fail{PG_EUNSUPPORTED, "partition too large for shared memory: use more ctas"};
+    return L;
+}
 
-    CK(cudaEventRecord(c->ev[0], c->stream));
-    run_setup(c, pl);
-    CK(cudaEventRecord(c->ev[1], c->stream));
-    // round tags continue from the plan's last launch; the tagged buffers
-    // are cleared on the plan's first launch, after a failed one, and before
-    // the 32-bit tags come near 0xffffffff (the test hook's tag)
+// Clears what a launch of pl needs cleared: its result record, and its
+// exchange buffers on the plan's first launch, after a failed one, or when
+// the round tags come near 0xffffffff (the test hook's tag); otherwise the
+// tags simply continue from the last launch.
+void reset_for_launch(pg_ctx* c, Plan* pl, pg::PcgResult* res) {
     if (!pl->ll_ready || pl->tag0 > 0xf0000000u) {
         CK(cudaMemsetAsync(pl->llv.p, 0, pl->llv.n * sizeof(unsigned long long), c->stream));
         CK(cudaMemsetAsync(pl->llx.p, 0, pl->llx.n * sizeof(unsigned long long), c->stream));
@@ -429,13 +450,19 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_
         pl->tag0 = 0;
     }
     pl->ll_ready = false;  // until this launch's result record is back
-    CK(cudaMemsetAsync(pl->abort_flag.p, 0, sizeof(int), c->stream));
-    CK(cudaMemsetAsync(pl->res.p, 0, sizeof(pg::PcgResult), c->stream));
+    CK(cudaMemsetAsync(res, 0, sizeof(pg::PcgResult), c->stream));
+}
 
+pg::PcgArgs fill_args(Plan* pl, const pg_options& o, const pg::SmemLayout& L, int ke_mode,
+                      bool ainv_smem, int* abort_flag, pg::PcgResult* res) {
+    const pg::HostPlan& hp = pl->hp;
+    const bool coarse = o.preconditioner == PG_PRECOND_TWO_LEVEL;
+    const bool cheb = o.smoother == PG_SMOOTHER_CHEBYSHEV;
     pg::PcgArgs a{};
     a.G = pl->G;
     a.NT = (int)hp.task_elem.size();
     a.Nn = hp.Nn;
+    a.npe = hp.npe;
     a.node_off = pl->node_off.p;
     a.nown = pl->nown.p;
     a.nodes = pl->nodes.p;
@@ -453,8 +480,8 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_
     a.llv = pl->llv.p;
     a.llx = pl->llx.p;
     a.llp = pl->llp.p;
-    a.abort_flag = pl->abort_flag.p;
-    a.res = pl->res.p;
+    a.abort_flag = abort_flag;
+    a.res = res;
     a.tol = o.tolerance;
     a.tag0 = pl->tag0;
     a.maxit = o.max_iterations;
@@ -477,21 +504,90 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_
     if (cheb) chebyshev2(pl->lambda_max, &a.cheb_a, &a.cheb_b);
     a.trace_it = o.trace_iteration > 0 ? o.trace_iteration : -1;
     a.trace = pl->trace.p;
-    if (a.trace_it > 0)
-        CK(cudaMemsetAsync(pl->trace.p, 0, pl->trace.n * sizeof(unsigned long long), c->stream));
-    a.reliable_interval = o.reliable_interval > 0 ? o.reliable_interval : 1 << 30;
+    // automatic: a replacement at least every 200 updates, so a mixed solve
+    // whose FP32 residual stalls along with the true one is still checked
+    a.reliable_interval = o.reliable_interval > 0 ? o.reliable_interval : 200;
     a.reliable_delta = o.reliable_delta > 0 ? o.reliable_delta : 0.1;
     a.L = L;
+    return a;
+}
+
+// After the result record is back: tags continue next launch if this one ended cleanly.
+void finish_launch(Plan* pl, const pg::PcgResult& r) {
+    if (r.status == pg::ST_OK && r.wait_failures == 0) {
+        pl->tag0 = r.last_tag;
+        pl->ll_ready = true;
+    }
+}
+
+void fill_info(pg_info* info, const pg::PcgResult& r, const Plan* pl, const pg_options& o, int threads,
+               int shared_bytes) {
+    const pg::HostPlan& hp = pl->hp;
+    info->iterations = r.iterations;
+    info->converged = r.converged;
+    info->stop_reason = r.stop_reason;
+    info->final_residual = r.final_residual;
+    info->true_rel_residual = r.true_rel_residual;
+    info->b_norm = r.b_norm;
+    info->ctas = pl->G;
+    info->threads = threads;
+    info->reliable_updates = r.reliable_updates;
+    info->reductions = r.reductions;
+    info->shared_bytes = shared_bytes;
+    info->coarse_dim = o.preconditioner == PG_PRECOND_TWO_LEVEL ? hp.C - hp.dropped_modes : 0;
+    info->smoother_lambda_max = o.smoother == PG_SMOOTHER_CHEBYSHEV ? pl->lambda_max : 0.0;
+}
+
+void throw_on_failure(const pg::PcgResult& r) {
+    if (r.wait_failures > 0 || r.status == PG_ETIMEOUT)
+        throw Fail{PG_ETIMEOUT, "a wait for another block exceeded wait_timeout_ms"};
+    if (r.status == PG_ENONFINITE) {
+        char buf[256];
+        std::snprintf(buf, sizeof buf,
+                      "non-finite value in the PCG iteration (reduction %d: gamma=%g delta=%g rho=%g)",
+                      r.nonfinite_it, r.nonfinite_vals[0], r.nonfinite_vals[1], r.nonfinite_vals[2]);
+        throw Fail{PG_ENONFINITE, buf};
+    }
+}
+
+// Gives kernel fn the full shared-memory opt-in once per context.
+void opt_in_smem(pg_ctx* c, const void* fn) {
+    if (std::find(c->smem_opt_in.begin(), c->smem_opt_in.end(), fn) == c->smem_opt_in.end()) {
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, c->max_smem));
+        c->smem_opt_in.push_back(fn);
+    }
+}
+
+// Queues set-up (first solve of the plan) and the persistent PCG launch on
+// the context stream, then waits for the result record (one readback).
+// x_dst (optional) receives the solution by a copy of `kind` queued right
+// behind the kernel, so the call waits for the device once.
+void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_dst = nullptr,
+               cudaMemcpyKind kind = cudaMemcpyDeviceToDevice) {
+    const pg::HostPlan& hp = pl->hp;
+    const bool mixed = o.precision == PG_PREC_MIXED;
+    int threads = o.threads;
+    if (!threads) threads = std::min(pg::kMaxThreads, std::max(128, (hp.max_ntask + 31) / 32 * 32));
+    prepare_plan_data(c, pl, o);
+    int ke_mode = 0;
+    bool ainv_smem = false;
+    const pg::SmemLayout L = choose_layout(c, hp, o, &ke_mode, &ainv_smem);
+
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    run_setup(c, pl);
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    reset_for_launch(c, pl, pl->res.p);
+    CK(cudaMemsetAsync(pl->abort_flag.p, 0, sizeof(int), c->stream));
+    pg::PcgArgs a = fill_args(pl, o, L, ke_mode, ainv_smem, pl->abort_flag.p, pl->res.p);
+    if (a.trace_it > 0)
+        CK(cudaMemsetAsync(pl->trace.p, 0, pl->trace.n * sizeof(unsigned long long), c->stream));
 
     const void* fn;
     if (hp.npe == 4)
         fn = mixed ? (const void*)pg::pcg_kernel<4, float, true> : (const void*)pg::pcg_kernel<4, double, false>;
     else
         fn = mixed ? (const void*)pg::pcg_kernel<3, float, true> : (const void*)pg::pcg_kernel<3, double, false>;
-    if (std::find(c->smem_opt_in.begin(), c->smem_opt_in.end(), fn) == c->smem_opt_in.end()) {
-        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, c->max_smem));
-        c->smem_opt_in.push_back(fn);
-    }
+    opt_in_smem(c, fn);
     if (pl->ok_fn != fn || pl->ok_threads != threads || pl->ok_smem != L.total) {
         int nb = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, L.total));
@@ -509,29 +605,14 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_
         CK(cudaMemcpyAsync(x_dst, pl->x.p, 3 * (size_t)hp.Nn * sizeof(double), kind, c->stream));
     CK(cudaMemcpyAsync(&r, pl->res.p, sizeof(r), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    finish_launch(pl, r);
     float ms_setup = 0, ms_solve = 0;
-    if (r.status == pg::ST_OK && r.wait_failures == 0) {
-        pl->tag0 = r.last_tag;
-        pl->ll_ready = true;
-    }
     CK(cudaEventElapsedTime(&ms_setup, c->ev[0], c->ev[1]));
     CK(cudaEventElapsedTime(&ms_solve, c->ev[1], c->ev[2]));
     if (info) {
-        info->iterations = r.iterations;
-        info->converged = r.converged;
-        info->stop_reason = r.stop_reason;
-        info->final_residual = r.final_residual;
-        info->true_rel_residual = r.true_rel_residual;
-        info->b_norm = r.b_norm;
+        fill_info(info, r, pl, o, threads, L.total);
         info->setup_ms = ms_setup;
         info->solve_ms = ms_solve;
-        info->ctas = pl->G;
-        info->threads = threads;
-        info->reliable_updates = r.reliable_updates;
-        info->reductions = r.reductions;
-        info->shared_bytes = L.total;
-        info->coarse_dim = coarse ? hp.C - hp.dropped_modes : 0;
-        info->smoother_lambda_max = cheb ? pl->lambda_max : 0.0;
         for (int k = 0; k < 8; k++) info->phase_us[k] = r.phase_cycles[k] / (c->clock_khz * 1e-3);
         if (a.trace_it > 0) {
             std::vector<unsigned long long> tr(pl->trace.n);
@@ -554,15 +635,24 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_
             }
         }
     }
-    if (r.wait_failures > 0 || r.status == PG_ETIMEOUT)
-        throw Fail{PG_ETIMEOUT, "a wait for another block exceeded wait_timeout_ms"};
-    if (r.status == PG_ENONFINITE) {
-        char buf[256];
-        std::snprintf(buf, sizeof buf,
-                      "non-finite value in the PCG iteration (reduction %d: gamma=%g delta=%g rho=%g)",
-                      r.nonfinite_it, r.nonfinite_vals[0], r.nonfinite_vals[1], r.nonfinite_vals[2]);
-        throw Fail{PG_ENONFINITE, buf};
-    }
+    throw_on_failure(r);
+}
+
+// run_solve, and when a mixed solve stagnated (with o.fallback) the same
+// solve again in FP64 on the same plan; info then describes the FP64 solve,
+// with fallback = 1 and solve_ms covering both.
+void solve_with_fallback(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_dst = nullptr,
+                         cudaMemcpyKind kind = cudaMemcpyDeviceToDevice) {
+    pg_info local{};
+    pg_info* fi = info ? info : &local;
+    run_solve(c, pl, o, fi, x_dst, kind);
+    if (o.precision != PG_PREC_MIXED || !o.fallback || fi->stop_reason != PG_STOP_STAGNATED) return;
+    const double first_ms = fi->setup_ms + fi->solve_ms;
+    pg_options o64 = o;
+    o64.precision = PG_PREC_FP64;
+    run_solve(c, pl, o64, fi, x_dst, kind);
+    fi->fallback = 1;
+    fi->solve_ms += first_ms;
 }
 
 template <typename F>
@@ -604,6 +694,235 @@ void zero_info(pg_info* info) {
 
 }  // namespace
 
+namespace {
+
+// Owned nodes per block that the shared-memory layout holds (vectors, block
+// inverses, task results; the Ke blocks then stay in L2): a first guess,
+// checked against each plate's actual layout by build_batch.
+int batch_capacity(const pg_options& o, int rings) {
+    const bool mixed = o.precision == PG_PREC_MIXED;
+    if (rings == 2) return mixed ? 470 : 250;
+    return mixed ? 560 : 300;
+}
+
+std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int count,
+                                      const pg_options& o) {
+    auto b = std::make_unique<pg_batch>();
+    b->ctx = c;
+    b->rings = halo_rings(o);
+    std::vector<int> nodes(count);
+    for (int i = 0; i < count; i++) {
+        check_problem(&probs[i], true);
+        if (probs[i].node_count == 0) throw Fail{PG_EINVAL, "a plate of the batch has no nodes"};
+        const size_t n = 3 * (size_t)probs[i].node_count;
+        for (size_t k = 0; k < n; k++)
+            if (!std::isfinite(probs[i].F[k])) throw Fail{PG_ENONFINITE, "F contains NaN or Inf"};
+        nodes[i] = (int)probs[i].node_count;
+    }
+    // schedule, then check every plate's layout at its team size; shrink the
+    // capacity and reschedule while some part does not fit
+    int cap = batch_capacity(o, b->rings);
+    for (int attempt = 0;; attempt++) {
+        std::string e = pg::schedule_batch(nodes, c->sms, cap, b->sched);
+        if (!e.empty()) throw Fail{PG_EUNSUPPORTED, e};
+        b->plans.clear();
+        bool fits = true;
+        for (int i = 0; i < count && fits; i++) {
+            const int G = b->sched.plate_size[i];
+            b->plans.push_back(build_plan(c, probs[i], G, b->rings));
+            int ke_mode = 0;
+            bool ainv = false;
+            try {
+                choose_layout(c, b->plans.back()->hp, o, &ke_mode, &ainv);
+            } catch (const Fail&) {
+                fits = false;
+            }
+        }
+        if (fits) break;
+        if (attempt == 4) throw Fail{PG_EUNSUPPORTED, "batch plates too large for shared memory"};
+        cap = cap * 3 / 4;
+    }
+    cudaStream_t st = c->stream;
+    for (const pg::BatchPhase& P : b->sched.phases) {
+        auto d = std::make_unique<BatchPhaseDev>();
+        std::vector<int> bt(P.grid);
+        for (size_t t = 0; t < P.team_size.size(); t++)
+            for (int k = 0; k < P.team_size[t]; k++) bt[P.team_base[t] + k] = (int)t;
+        d->grid = P.grid;
+        d->block_team.upload(bt.data(), bt.size(), st);
+        d->team_base.upload(P.team_base.data(), P.team_base.size(), st);
+        d->queue_off.upload(P.queue_off.data(), P.queue_off.size(), st);
+        d->queue.upload(P.queue.data(), P.queue.size(), st);
+        CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
+        b->phases.push_back(std::move(d));
+    }
+    b->abort_flag.alloc(1);
+    b->args.alloc(count);
+    b->res.alloc(count);
+    b->times.alloc(2 * (size_t)count);
+    for (int i = 0; i < count; i++)
+        CK(cudaMemcpyAsync(b->plans[i]->F.p, probs[i].F, 3 * (size_t)probs[i].node_count * sizeof(float),
+                           cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    return b;
+}
+
+double percentile(std::vector<double> v, double q) {
+    if (v.empty()) return 0.0;
+    std::sort(v.begin(), v.end());
+    const double pos = q * (double)(v.size() - 1);
+    const size_t lo = (size_t)pos, hi = std::min(v.size() - 1, lo + 1);
+    return v[lo] + (pos - (double)lo) * (v[hi] - v[lo]);
+}
+
+void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* const* x_out,
+               pg_info* infos, pg_batch_info* bi) {
+    pg_ctx* c = b->ctx;
+    const int count = (int)b->plans.size();
+    if (halo_rings(o) != b->rings)
+        throw Fail{PG_EINVAL, "the batch was made for another smoother (ghost halo width)"};
+    cudaStream_t st = c->stream;
+    if (F)
+        for (int i = 0; i < count; i++) {
+            if (!F[i]) continue;
+            const size_t n = 3 * (size_t)b->plans[i]->hp.Nn;
+            for (size_t k = 0; k < n; k++)
+                if (!std::isfinite(F[i][k])) throw Fail{PG_ENONFINITE, "F contains NaN or Inf"};
+            CK(cudaMemcpyAsync(b->plans[i]->F.p, F[i], n * sizeof(float), cudaMemcpyHostToDevice, st));
+        }
+    for (auto& pl : b->plans) prepare_plan_data(c, pl.get(), o);
+    CK(cudaEventRecord(c->ev[0], st));
+    for (auto& pl : b->plans) run_setup(c, pl.get());
+    CK(cudaEventRecord(c->ev[1], st));
+    std::vector<pg::PcgArgs> a(count);
+    int smem = 0;
+    for (int i = 0; i < count; i++) {
+        Plan* pl = b->plans[i].get();
+        int ke_mode = 0;
+        bool ainv = false;
+        const pg::SmemLayout L = choose_layout(c, pl->hp, o, &ke_mode, &ainv);
+        reset_for_launch(c, pl, b->res.p + i);
+        pg::PcgArgs ai = fill_args(pl, o, L, ke_mode, ainv, b->abort_flag.p, b->res.p + i);
+        ai.timing = 0;
+        ai.test_stall = 0;
+        ai.trace_it = -1;
+        a[i] = ai;
+        smem = std::max(smem, L.total);
+    }
+    CK(cudaMemcpyAsync(b->args.p, a.data(), count * sizeof(pg::PcgArgs), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(b->abort_flag.p, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(b->times.p, 0, b->times.n * sizeof(unsigned long long), st));
+    const bool mixed = o.precision == PG_PREC_MIXED;
+    const void* fn = mixed ? (const void*)pg::pcg_batch_kernel<float, true>
+                           : (const void*)pg::pcg_batch_kernel<double, false>;
+    opt_in_smem(c, fn);
+    int grid_max = 0;
+    for (auto& ph : b->phases) grid_max = std::max(grid_max, ph->grid);
+    if (b->ok_fn != fn || b->ok_smem != smem) {
+        int nb = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, pg::kMaxThreads, smem));
+        if (nb < 1 || nb * c->sms < grid_max)
+            throw Fail{PG_EUNSUPPORTED, "batch grid does not fit on the device"};
+        b->ok_fn = fn;
+        b->ok_smem = smem;
+    }
+    for (auto& ph : b->phases) {  // one persistent launch per phase, back to back
+        pg::BatchArgs ba{b->args.p, ph->block_team.p, ph->team_base.p, ph->queue_off.p, ph->queue.p,
+                         b->times.p};
+        void* args[] = {&ba};
+        CK(cudaLaunchCooperativeKernel(fn, dim3(ph->grid), dim3(pg::kMaxThreads), args, smem, st));
+    }
+    CK(cudaEventRecord(c->ev[2], st));
+    if (x_out)
+        for (int i = 0; i < count; i++)
+            if (x_out[i])
+                CK(cudaMemcpyAsync(x_out[i], b->plans[i]->x.p, 3 * (size_t)b->plans[i]->hp.Nn * sizeof(double),
+                                   cudaMemcpyDeviceToHost, st));
+    std::vector<pg::PcgResult> r(count);
+    std::vector<unsigned long long> tm(2 * (size_t)count);
+    CK(cudaMemcpyAsync(r.data(), b->res.p, count * sizeof(pg::PcgResult), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(tm.data(), b->times.p, tm.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    float ms_setup = 0, ms_solve = 0;
+    CK(cudaEventElapsedTime(&ms_setup, c->ev[0], c->ev[1]));
+    CK(cudaEventElapsedTime(&ms_solve, c->ev[1], c->ev[2]));
+    std::vector<double> plate_ms(count);
+    int converged = 0;
+    for (int i = 0; i < count; i++) {
+        finish_launch(b->plans[i].get(), r[i]);
+        plate_ms[i] = tm[2 * i + 1] > tm[2 * i] ? (double)(tm[2 * i + 1] - tm[2 * i]) * 1e-6 : 0.0;
+        converged += r[i].converged ? 1 : 0;
+        if (infos) {
+            std::memset(&infos[i], 0, sizeof(pg_info));
+            fill_info(&infos[i], r[i], b->plans[i].get(), o, pg::kMaxThreads, a[i].L.total);
+            infos[i].status = r[i].status;
+            infos[i].solve_ms = plate_ms[i];
+            infos[i].plan_cached = 1;
+        }
+    }
+    if (bi) {
+        bi->count = count;
+        int teams = 0;
+        for (const pg::BatchPhase& P : b->sched.phases) teams += (int)P.team_size.size();
+        bi->teams = teams;
+        bi->grid = grid_max;
+        bi->phases = (int32_t)b->sched.phases.size();
+        bi->converged = converged;
+        bi->setup_ms = ms_setup;
+        bi->solve_ms = ms_solve;
+        bi->plate_ms_p50 = percentile(plate_ms, 0.50);
+        bi->plate_ms_p99 = percentile(plate_ms, 0.99);
+        bi->plate_ms_max = percentile(plate_ms, 1.0);
+        bi->solves_per_s = ms_solve > 0 ? count / (ms_solve * 1e-3) : 0.0;
+        bi->shared_bytes = smem;
+    }
+    for (int i = 0; i < count; i++) throw_on_failure(r[i]);
+    // plates whose mixed solve stagnated: FP64 on their own plan (one launch
+    // each), or on a plan over the whole device when the FP64 parts do not
+    // fit in shared memory at the team's size
+    if (o.precision != PG_PREC_MIXED || !o.fallback) return;
+    pg_options o64 = o;
+    o64.precision = PG_PREC_FP64;
+    double extra_ms = 0.0;
+    int fallbacks = 0;
+    for (int i = 0; i < count; i++) {
+        if (r[i].stop_reason != PG_STOP_STAGNATED) continue;
+        pg_info fi{};
+        void* xd = x_out ? (void*)x_out[i] : nullptr;
+        try {
+            run_solve(c, b->plans[i].get(), o64, &fi, xd, cudaMemcpyDeviceToHost);
+        } catch (const Fail& f) {
+            if (f.status != PG_EUNSUPPORTED) throw;
+            Plan* old = b->plans[i].get();
+            auto np = build_plan(c, old->prob_view, c->sms, b->rings);
+            CK(cudaMemcpyAsync(np->F.p, old->F.p, 3 * (size_t)old->hp.Nn * sizeof(float),
+                               cudaMemcpyDeviceToDevice, st));
+            b->plans[i] = std::move(np);
+            fi = pg_info{};
+            run_solve(c, b->plans[i].get(), o64, &fi, xd, cudaMemcpyDeviceToHost);
+        }
+        extra_ms += fi.setup_ms + fi.solve_ms;
+        fallbacks++;
+        if (infos) {
+            const double mixed_ms = infos[i].solve_ms;
+            infos[i] = fi;
+            infos[i].status = PG_OK;
+            infos[i].fallback = 1;
+            infos[i].solve_ms += mixed_ms;
+            infos[i].plan_cached = 1;
+        }
+        if (fi.converged) converged++;
+    }
+    if (bi) {
+        bi->fallbacks = fallbacks;
+        bi->converged = converged;
+        bi->solve_ms += extra_ms;
+        bi->solves_per_s = bi->solve_ms > 0 ? count / (bi->solve_ms * 1e-3) : 0.0;
+    }
+}
+
+}  // namespace
+
 extern "C" {
 
 void pg_options_default(pg_options* o) {
@@ -615,6 +934,7 @@ void pg_options_default(pg_options* o) {
     o->precision = PG_PREC_FP64;
     o->stop_rule = PG_STOP_REFERENCE;
     o->wait_timeout_ms = 1000.0;
+    o->fallback = 1;
 }
 
 int pg_is_available(void) {
@@ -717,7 +1037,7 @@ int pg_solve(pg_ctx* c, const pg_problem* p, const pg_options* opt, double* x_ou
         ensure_staging(c, n);
         std::memcpy(c->hF, p->F, n * sizeof(float));
         CK(cudaMemcpyAsync(pl->F.p, c->hF, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-        run_solve(c, pl, o, info, c->hx, cudaMemcpyDeviceToHost);
+        solve_with_fallback(c, pl, o, info, c->hx, cudaMemcpyDeviceToHost);
         std::memcpy(x_out, c->hx, n * sizeof(double));
         if (info) info->plan_cached = cached ? 1 : 0;
     });
@@ -751,7 +1071,7 @@ int pg_plan_solve_device(pg_plan* h, const pg_options* opt, const float* F_dev, 
         Plan* pl = h->plan.get();
         const size_t n = 3 * (size_t)pl->hp.Nn;
         CK(cudaMemcpyAsync(pl->F.p, F_dev, n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
-        run_solve(c, pl, o, info, x_dev, cudaMemcpyDeviceToDevice);
+        solve_with_fallback(c, pl, o, info, x_dev, cudaMemcpyDeviceToDevice);
         if (info) info->plan_cached = 1;
     });
 }
@@ -917,6 +1237,90 @@ int pg_plan_inspect_halo(const pg_problem* p, int ctas, int rings, int32_t* stat
     } catch (...) {
         put("internal error");
         return PG_ECUDA;
+    }
+}
+
+int pg_batch_create(pg_ctx* c, const pg_problem* probs, int count, const pg_options* opt,
+                    pg_batch** out) {
+    if (out) *out = nullptr;
+    return guarded(c, nullptr, [&] {
+        if (!out) throw Fail{PG_EINVAL, "out is NULL"};
+        if (!probs || count < 1) throw Fail{PG_EINVAL, "the batch needs at least one problem"};
+        pg_options o;
+        fill_options(opt, &o);
+        *out = build_batch(c, probs, count, o).release();
+    });
+}
+
+int pg_batch_solve(pg_batch* b, const pg_options* opt, const float* const* F, double* const* x_out,
+                   pg_info* infos, pg_batch_info* bi) {
+    if (bi) std::memset(bi, 0, sizeof(*bi));
+    if (!b) return PG_EINVAL;
+    pg_ctx* c = b->ctx;
+    auto t0 = std::chrono::steady_clock::now();
+    const int st = guarded(c, nullptr, [&] {
+        pg_options o;
+        fill_options(opt, &o);
+        run_batch(b, o, F, x_out, infos, bi);
+    });
+    if (bi) {
+        bi->status = st;
+        bi->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return st;
+}
+
+void pg_batch_destroy(pg_batch* b) {
+    if (!b) return;
+    {
+        std::lock_guard<std::mutex> lk(b->ctx->mu);
+        cudaSetDevice(b->ctx->device);
+        cudaStreamSynchronize(b->ctx->stream);
+        b->plans.clear();
+        b->phases.clear();
+        b->abort_flag.release();
+        b->args.release();
+        b->res.release();
+        b->times.release();
+    }
+    delete b;
+}
+
+int pg_solve_batch(pg_ctx* c, const pg_problem* probs, int count, const pg_options* opt,
+                   double* const* x_out, pg_info* infos, pg_batch_info* bi) {
+    if (bi) std::memset(bi, 0, sizeof(*bi));
+    pg_batch* b = nullptr;
+    auto t0 = std::chrono::steady_clock::now();
+    int st = pg_batch_create(c, probs, count, opt, &b);
+    if (st == PG_OK) st = pg_batch_solve(b, opt, nullptr, x_out, infos, bi);
+    pg_batch_destroy(b);
+    if (bi) {
+        bi->status = st;
+        bi->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return st;
+}
+
+int pg_batch_schedule(const uint32_t* node_counts, int count, int sms, int cap, int32_t* plate_phase,
+                      int32_t* plate_size, int32_t* plate_team, int32_t* phase_grid,
+                      int32_t* phases_out) {
+    if (!node_counts || count < 1 || !plate_phase || !plate_size || !plate_team || !phase_grid ||
+        !phases_out)
+        return PG_EINVAL;
+    try {
+        std::vector<int> nodes(node_counts, node_counts + count);
+        pg::BatchSchedule S;
+        if (!pg::schedule_batch(nodes, sms, cap, S).empty()) return PG_EUNSUPPORTED;
+        for (int i = 0; i < count; i++) {
+            plate_phase[i] = S.plate_phase[i];
+            plate_size[i] = S.plate_size[i];
+            plate_team[i] = S.plate_team[i];
+        }
+        for (size_t k = 0; k < S.phases.size(); k++) phase_grid[k] = S.phases[k].grid;
+        *phases_out = (int32_t)S.phases.size();
+        return PG_OK;
+    } catch (...) {
+        return PG_ENOMEM;
     }
 }
 

@@ -20,14 +20,16 @@ PG_PREC_FP64, PG_PREC_MIXED = 0, 1
 PG_STOP_REFERENCE, PG_STOP_RELATIVE = 0, 1
 PG_PRECOND_BLOCK_JACOBI, PG_PRECOND_TWO_LEVEL = 0, 1
 PG_SMOOTHER_BLOCK_JACOBI, PG_SMOOTHER_CHEBYSHEV = 0, 1
-STOP_REASONS = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "zero_rhs"}
+STOP_REASONS = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "zero_rhs",
+                4: "stagnated"}
 
 # every symbol include/plategpu.h declares
 EXPORTED = ("pg_options_default", "pg_is_available", "pg_create", "pg_destroy", "pg_last_error",
             "pg_clear_cache", "pg_set_stream", "pg_solve", "pg_plan_create", "pg_plan_solve_device",
             "pg_plan_destroy", "pg_apply_k", "pg_apply_k_static",
             "pg_block_jacobi", "pg_element_stiffness", "pg_plan_inspect",
-            "pg_plan_inspect_halo")
+            "pg_plan_inspect_halo", "pg_batch_create", "pg_batch_solve", "pg_batch_destroy",
+            "pg_solve_batch", "pg_batch_schedule")
 
 
 class PgProblem(C.Structure):
@@ -66,7 +68,33 @@ class PgOptions(C.Structure):
         ("preconditioner", C.c_int32),
         ("trace_iteration", C.c_int32),
         ("smoother", C.c_int32),
+        ("fallback", C.c_int32),
     ]
+
+
+class PgBatchInfo(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("count", C.c_int32),
+        ("teams", C.c_int32),
+        ("grid", C.c_int32),
+        ("converged", C.c_int32),
+        ("shared_bytes", C.c_int32),
+        ("phases", C.c_int32),
+        ("fallbacks", C.c_int32),
+        ("setup_ms", C.c_double),
+        ("solve_ms", C.c_double),
+        ("total_ms", C.c_double),
+        ("plate_ms_p50", C.c_double),
+        ("plate_ms_p99", C.c_double),
+        ("plate_ms_max", C.c_double),
+        ("solves_per_s", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["status"] = STATUS_NAMES.get(d["status"], d["status"])
+        return d
 
 
 class PgInfo(C.Structure):
@@ -88,7 +116,7 @@ class PgInfo(C.Structure):
         ("reductions", C.c_int32),
         ("shared_bytes", C.c_int32),
         ("coarse_dim", C.c_int32),
-        ("pad_", C.c_int32),
+        ("fallback", C.c_int32),
         ("phase_us", C.c_double * 8),
         ("trace_ns", C.c_double * 6),
         ("smoother_lambda_max", C.c_double),
@@ -157,6 +185,17 @@ def load() -> C.CDLL:
     L.pg_plan_inspect.restype = I
     L.pg_plan_inspect_halo.argtypes = [C.POINTER(PgProblem), I, I, P, C.c_char_p, C.c_size_t]
     L.pg_plan_inspect_halo.restype = I
+    L.pg_batch_create.argtypes = [P, C.POINTER(PgProblem), I, C.POINTER(PgOptions), C.POINTER(P)]
+    L.pg_batch_create.restype = I
+    L.pg_batch_solve.argtypes = [P, C.POINTER(PgOptions), P, P, P, C.POINTER(PgBatchInfo)]
+    L.pg_batch_solve.restype = I
+    L.pg_batch_destroy.argtypes = [P]
+    L.pg_batch_destroy.restype = None
+    L.pg_solve_batch.argtypes = [P, C.POINTER(PgProblem), I, C.POINTER(PgOptions), P, P,
+                                 C.POINTER(PgBatchInfo)]
+    L.pg_solve_batch.restype = I
+    L.pg_batch_schedule.argtypes = [P, I, I, I, P, P, P, P, P]
+    L.pg_batch_schedule.restype = I
     _lib = L
     return L
 
@@ -231,7 +270,8 @@ def make_options(tolerance=1e-6, max_iterations=1000, precision=PG_PREC_FP64,
                  stop_rule=PG_STOP_REFERENCE, ctas=0, threads=0, wait_timeout_ms=None,
                  reliable_interval=0, reliable_delta=0.0, phase_timing=False,
                  test_stall=False, preconditioner=PG_PRECOND_BLOCK_JACOBI,
-                 trace_iteration=0, smoother=PG_SMOOTHER_BLOCK_JACOBI) -> PgOptions:
+                 trace_iteration=0, smoother=PG_SMOOTHER_BLOCK_JACOBI,
+                 fallback=True) -> PgOptions:
     o = PgOptions()
     load().pg_options_default(C.byref(o))
     o.tolerance = float(tolerance)
@@ -249,6 +289,7 @@ def make_options(tolerance=1e-6, max_iterations=1000, precision=PG_PREC_FP64,
     o.preconditioner = int(preconditioner)
     o.trace_iteration = int(trace_iteration)
     o.smoother = int(smoother)
+    o.fallback = 1 if fallback else 0
     return o
 
 
@@ -288,6 +329,21 @@ class Context:
     def plan(self, prob: Problem, opts: PgOptions) -> "DevicePlan":
         return DevicePlan(self, prob, opts)
 
+    def batch(self, probs, opts: PgOptions) -> "Batch":
+        return Batch(self, probs, opts)
+
+    def solve_batch(self, probs, opts: PgOptions):
+        """pg_solve_batch: plan, solve and release in one call."""
+        arr = (PgProblem * len(probs))(*[p.struct for p in probs])
+        xs = [np.zeros(p.F.size, np.float64) for p in probs]
+        xp = (C.c_void_p * len(probs))(*[x.ctypes.data for x in xs])
+        infos = (PgInfo * len(probs))()
+        bi = PgBatchInfo()
+        st = self.L.pg_solve_batch(self.h, arr, len(probs), C.byref(opts), C.cast(xp, C.c_void_p),
+                                   C.cast(infos, C.c_void_p), C.byref(bi))
+        self._check(st)
+        return xs, list(infos), bi
+
     def apply_k(self, prob: Problem, x):
         x = np.ascontiguousarray(x, np.float64)
         y = np.zeros_like(x)
@@ -310,6 +366,66 @@ class Context:
 
     def clear_cache(self):
         self._check(self.L.pg_clear_cache(self.h))
+
+
+class Batch:
+    """A pg_batch: independent plates solved together by one persistent
+    launch (teams of blocks, one queue of plates per team)."""
+
+    def __init__(self, ctx: Context, probs, opts: PgOptions):
+        self.ctx = ctx
+        self.probs = list(probs)  # keeps the host arrays alive while planning
+        arr = (PgProblem * len(self.probs))(*[p.struct for p in self.probs])
+        h = C.c_void_p()
+        ctx._check(ctx.L.pg_batch_create(ctx.h, arr, len(self.probs), C.byref(opts), C.byref(h)))
+        self.h = h
+
+    def solve(self, opts: PgOptions, F=None, want_x: bool = True):
+        """Returns (list of x or None, list of PgInfo, PgBatchInfo); F: optional
+        list of new loads (None entries keep a plate's load)."""
+        n = len(self.probs)
+        fp = None
+        keep = []
+        if F is not None:
+            arrs = [None if f is None else np.ascontiguousarray(f, np.float32) for f in F]
+            keep = arrs
+            fp = (C.c_void_p * n)(*[None if a is None else a.ctypes.data for a in arrs])
+        xs = [np.zeros(p.F.size, np.float64) for p in self.probs] if want_x else None
+        xp = (C.c_void_p * n)(*[x.ctypes.data for x in xs]) if want_x else None
+        infos = (PgInfo * n)()
+        bi = PgBatchInfo()
+        st = self.ctx.L.pg_batch_solve(self.h, C.byref(opts), None if fp is None else C.cast(fp, C.c_void_p),
+                                       None if xp is None else C.cast(xp, C.c_void_p),
+                                       C.cast(infos, C.c_void_p), C.byref(bi))
+        del keep
+        self.ctx._check(st)
+        return xs, list(infos), bi
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.pg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_schedule(node_counts, sms: int, cap: int) -> dict:
+    """pg_batch_schedule (host only): per plate its phase, team size and
+    team within the phase; per phase its grid."""
+    nc = np.ascontiguousarray(node_counts, np.uint32)
+    n = nc.size
+    phase, size, team, grid = (np.zeros(n, np.int32) for _ in range(4))
+    phases = C.c_int32()
+    st = load().pg_batch_schedule(_ptr(nc), n, int(sms), int(cap), _ptr(phase), _ptr(size),
+                                  _ptr(team), _ptr(grid), C.byref(phases))
+    if st != PG_OK:
+        raise PlateGPUError(st, "batch schedule failed")
+    return {"plate_phase": phase, "plate_size": size, "plate_team": team,
+            "phase_grid": grid[:phases.value].copy(), "phases": phases.value}
 
 
 class DevicePlan:

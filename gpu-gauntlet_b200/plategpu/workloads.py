@@ -12,6 +12,9 @@ interface, with the constrained entries zeroed (applyBCsToRHS).
   plate_q4_141     141x141 Q4 (60,492 DOF), edges simply supported (w = 0)
                    plus w = 0 at a seeded 4x4 grid of interior column nodes,
                    5 kPa + 32 point loads U(1,10) kN at seeded nodes.
+  batch_uneven     256 independent plates of uneven size, element type,
+                   material, supports and random-field loads (see its
+                   docstring); a list of workloads for the batched solver.
   plate_dkt_200    200x200 quads split into 80,000 DKT triangles along
                    alternating diagonals (121,203 DOF), interior nodes
                    jittered U(-0.2h, 0.2h), thickness 0.1(1 + 0.3 g) clipped
@@ -147,6 +150,65 @@ def plate_dkt_200(seed: int = 3, n: int = 200) -> Workload:
                     material=PlateMaterial(E=E_STEEL, nu=NU, t=T_PLATE, elem_t=elem_t),
                     coloring=_col.computeElementColoringGreedy(mesh), supports=supports,
                     constrainedDOFs=cons, F=F, point_loads=loads)
+
+
+def _edge_supports(mesh: PlateMesh, kinds) -> List[PlateSupport]:
+    """One support per boundary node: kinds[e] ('fixed' clamped or 'pinned'
+    simply supported) for the left, right, bottom and top edge; a corner
+    takes the stronger of its two edges."""
+    xy = mesh.nodes.reshape(-1, 2)
+    lo, hi = xy.min(axis=0), xy.max(axis=0)
+    tol = 1e-6 * max(1.0, float(np.max(hi - lo)))
+    on = [np.abs(xy[:, 0] - lo[0]) < tol, np.abs(xy[:, 0] - hi[0]) < tol,
+          np.abs(xy[:, 1] - lo[1]) < tol, np.abs(xy[:, 1] - hi[1]) < tol]
+    kind = {}
+    for e in range(4):
+        for n in np.nonzero(on[e])[0].tolist():
+            if kind.get(n) != "fixed":
+                kind[n] = kinds[e]
+    return [PlateSupport(k, str(n)) for n, k in sorted(kind.items())]
+
+
+def batch_uneven(count: int = 256, seed: int = 5, min_side: int = 16,
+                 max_side: int = 256) -> List[Workload]:
+    """Independent 10 m x 10 m plates of uneven sizes: elements per side
+    log-uniform in [min_side, max_side]; 70% Q4 Mindlin, 30% DKT (quads
+    split along alternating diagonals, interior nodes jittered U(-0.2h,
+    0.2h)); thickness U(0.05, 0.3) m, E U(2e10, 2.1e11) Pa, nu U(0.2, 0.3);
+    each edge clamped or simply supported at random; load a Gaussian random
+    field pressure (length-scale U(0.5, 3) m, amplitude U(1, 10) kPa,
+    element values from the nodal field, taken positive downward) plus 0-16
+    point loads U(1, 10) kN at random interior nodes."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(min_side), np.log(max_side)))))
+        dkt = rng.uniform() < 0.3
+        if dkt:
+            mesh = _mesh.split_triangle_mesh(WIDTH, WIDTH, n, n, jitter=0.2,
+                                             seed=int(rng.integers(1 << 31)))
+            coloring = _col.computeElementColoringGreedy(mesh)
+        else:
+            mesh = _mesh.rectangular_mesh_nxny(WIDTH, WIDTH, n, n)
+            coloring = _col.computeElementColoring(mesh)
+        material = PlateMaterial(E=float(rng.uniform(2e10, 2.1e11)), nu=float(rng.uniform(0.2, 0.3)),
+                                 t=float(rng.uniform(0.05, 0.3)))
+        kinds = ["fixed" if rng.uniform() < 0.5 else "pinned" for _ in range(4)]
+        supports = _edge_supports(mesh, kinds)
+        cons = _prob.identifyConstrainedDOFs(mesh, supports)
+        g = grf_squared_exponential(n, n, WIDTH / n, float(rng.uniform(0.5, 3.0)), rng).reshape(-1)
+        amp = float(rng.uniform(1e3, 1e4))
+        npe = mesh.nodesPerElement
+        el = mesh.elements.astype(np.int64).reshape(-1, npe)
+        q = amp * (1.0 + 0.5 * g[el].mean(axis=1))
+        k = int(rng.integers(0, 17))
+        interior = _interior_nodes(n, n)
+        pts = rng.choice(interior, size=k, replace=False) if k else np.zeros(0, np.int64)
+        F, loads = _finish_loads(mesh, q, pts, rng.uniform(1e3, 1e4, size=k), cons)
+        out.append(Workload(name=f"batch{i}_{'dkt' if dkt else 'q4'}_{n}", mesh=mesh,
+                            material=material, coloring=coloring, supports=supports,
+                            constrainedDOFs=cons, F=F, point_loads=loads))
+    return out
 
 
 WORKLOADS = {

@@ -87,7 +87,10 @@ typedef enum pg_stop_reason {
     PG_STOP_CONVERGED = 0,
     PG_STOP_MAX_ITER = 1,
     PG_STOP_BREAKDOWN = 2, /* |p.Ap| < 1e-30 (pcg.ts:154, gpu/solver.ts:496) */
-    PG_STOP_ZERO_RHS = 3   /* ||b|| < 1e-30: x = 0, 0 iterations */
+    PG_STOP_ZERO_RHS = 3,  /* ||b|| < 1e-30: x = 0, 0 iterations */
+    PG_STOP_STAGNATED = 4  /* mixed precision: the FP64 residual did not halve over three
+                              residual replacements (FP32 cannot resolve the problem);
+                              with pg_options.fallback the call re-solves in FP64 */
 } pg_stop_reason;
 
 /* One plate problem, in the reference's host layout. */
@@ -117,7 +120,7 @@ typedef struct pg_options {
     int32_t threads;              /* threads per CTA; 0 = automatic */
     double wait_timeout_ms;       /* limit on each wait for another block's data; default 1000 */
     int32_t reliable_interval;    /* mixed: max inner iterations between FP64
-                                     residual replacements; 0 = automatic */
+                                     residual replacements; 0 = automatic (200) */
     double reliable_delta;        /* mixed: replace when the FP32 residual fell
                                      by this factor; 0 = automatic (0.1) */
     int32_t phase_timing;         /* 1: record per-phase device time (pg_info.phase_us) */
@@ -129,6 +132,9 @@ typedef struct pg_options {
                                      (pg_info.trace_ns) */
     int32_t smoother;             /* pg_smoother, default PG_SMOOTHER_BLOCK_JACOBI (also the
                                      smoother of the two-level preconditioner) */
+    int32_t fallback;             /* mixed precision: 1 (default) re-solves in FP64 when the
+                                     mixed solve stagnates (PG_STOP_STAGNATED); 0 returns
+                                     the stagnated result */
 } pg_options;
 
 /* Per-solve result (GPUSolveResult plus extended statistics). */
@@ -152,7 +158,9 @@ typedef struct pg_info {
                                      one per residual replacement) */
     int32_t shared_bytes;         /* dynamic shared memory per block */
     int32_t coarse_dim;           /* two-level: coarse DOFs kept (0 otherwise) */
-    int32_t pad_;
+    int32_t fallback;             /* 1 when a stagnated mixed solve was redone in FP64 (the
+                                     result fields are then the FP64 solve's; solve_ms
+                                     covers both) */
     double phase_us[8];           /* with phase_timing, block 0's time (SM cycles at
                                      the nominal clock) in: K.u; gather, dots and
                                      publishing w; block reduction and publishing the
@@ -211,6 +219,60 @@ int pg_plan_create(pg_ctx* ctx, const pg_problem* prob, const pg_options* opt, p
 int pg_plan_solve_device(pg_plan* plan, const pg_options* opt, const float* F_dev,
                          double* x_dev, pg_info* info);
 void pg_plan_destroy(pg_plan* plan);
+
+/* Batches of independent plates (no counterpart in the reference, whose
+ * solveGPU takes one plate).  All plates of a batch are solved by one
+ * persistent launch: the grid is cut into teams of blocks, each plate gets a
+ * team sized to it (a power of two; large plates more blocks) and is
+ * partitioned for that team, and every team works through its own queue of
+ * plates, longest first, with no waiting between teams.  Team sizes that
+ * cannot share the device (the largest plates may need every block) run in
+ * separate phases: one launch each, back to back.  Plates may mix Q4
+ * and DKT elements, sizes, materials and supports; the options (precision,
+ * preconditioner, smoother, tolerance, ...) apply to every plate.
+ * pg_batch_create plans the batch and copies each problem's F to the device;
+ * pg_batch_solve solves it, with new loads when F is non-NULL (F[i] NULL
+ * keeps plate i's load); x_out[i] (host, 3*node_count doubles, may be NULL)
+ * and infos[i] (may be NULL) receive each plate's result.  infos[i].solve_ms
+ * is the plate's own start-to-end time inside the launch.  A plate too large
+ * for a batch (more nodes than every block together holds) is rejected with
+ * PG_EUNSUPPORTED: solve it with pg_solve. */
+typedef struct pg_batch_info {
+    int32_t status;
+    int32_t count;                /* plates */
+    int32_t teams;                /* teams of blocks in the launch */
+    int32_t grid;                 /* blocks of the largest launch */
+    int32_t converged;            /* plates that converged */
+    int32_t shared_bytes;         /* dynamic shared memory per block */
+    int32_t phases;               /* launches (team sizes that do not fit side by side
+                                     run in separate phases) */
+    int32_t fallbacks;            /* plates re-solved in FP64 after a stagnated mixed solve
+                                     (one launch each, after the batch; in solve_ms) */
+    double setup_ms;              /* device: element set-up queued by this call (0 once done) */
+    double solve_ms;              /* device: the batch launch (CUDA events) */
+    double total_ms;              /* host wall clock of the call */
+    double plate_ms_p50;          /* per-plate start-to-end time in the launch: median, */
+    double plate_ms_p99;          /*   99th percentile */
+    double plate_ms_max;          /*   and largest */
+    double solves_per_s;          /* count / solve_ms */
+} pg_batch_info;
+
+typedef struct pg_batch pg_batch;
+int pg_batch_create(pg_ctx* ctx, const pg_problem* probs, int count, const pg_options* opt,
+                    pg_batch** out);
+int pg_batch_solve(pg_batch* batch, const pg_options* opt, const float* const* F,
+                   double* const* x_out, pg_info* infos, pg_batch_info* info);
+void pg_batch_destroy(pg_batch* batch);
+/* pg_batch_create + pg_batch_solve + pg_batch_destroy in one call. */
+int pg_solve_batch(pg_ctx* ctx, const pg_problem* probs, int count, const pg_options* opt,
+                   double* const* x_out, pg_info* infos, pg_batch_info* info);
+/* Host-only: the schedule pg_batch_create uses for plates of these node
+ * counts on `sms` blocks with at most `cap` nodes per block: per plate its
+ * phase, team size and team (index within the phase) [count each]; per
+ * phase its grid [count, the first *phases_out entries used]. */
+int pg_batch_schedule(const uint32_t* node_counts, int count, int sms, int cap, int32_t* plate_phase,
+                      int32_t* plate_size, int32_t* plate_team, int32_t* phase_grid,
+                      int32_t* phases_out);
 
 /* Test hook: y = K x in FP64 with the reference BC rule (y_c = x_c). */
 int pg_apply_k(pg_ctx* ctx, const pg_problem* prob, const double* x, double* y);
