@@ -1313,10 +1313,13 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_batch_kernel(const __grid_
         const int pi = b.queue[q];
         const PcgArgs& a = b.plates[pi];
         if (g == 0 && threadIdx.x == 0) b.times[2 * pi] = gtimer();
-        if (a.npe == 4)
-            pcg_body<4, T, MIXED>(a, g, sm);
-        else
-            pcg_body<3, T, MIXED>(a, g, sm);
+        // a plate with fewer parts than the team has blocks leaves the rest idle
+        if (g < a.G) {
+            if (a.npe == 4)
+                pcg_body<4, T, MIXED>(a, g, sm);
+            else
+                pcg_body<3, T, MIXED>(a, g, sm);
+        }
         __syncthreads();  // shared memory is reloaded for the next plate
         if (g == 0 && threadIdx.x == 0) b.times[2 * pi + 1] = gtimer();
     }

@@ -460,17 +460,19 @@ double estimate_lambda_max(const pg_problem& p, const std::vector<double>& ke64,
     return lam;
 }
 
-std::string schedule_batch(const std::vector<int>& nodes, int sms, int cap, BatchSchedule& out) {
+std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>& caps, int sms,
+                           BatchSchedule& out) {
     out = BatchSchedule{};
     const int count = (int)nodes.size();
     if (count == 0) return "empty batch";
-    if (sms < 1 || cap < 1) return "no blocks to schedule";
+    if (sms < 1 || (int)caps.size() != count) return "no blocks to schedule";
     int top = 1;  // largest power of two <= sms
     while (top * 2 <= sms) top *= 2;
     std::vector<int> d(count);
     std::vector<double> w(count);
     for (int i = 0; i < count; i++) {
         const double n = std::max(1, nodes[i]);
+        const int cap = std::max(1, caps[i]);
         int need = 1;
         while (need < std::ceil(n / cap)) need *= 2;
         if (need > top) {

@@ -84,7 +84,7 @@ double estimate_lambda_max(const pg_problem& p, const std::vector<double>& ke64,
 
 // Team schedule of a batch of independent plates.  A plate of n nodes gets
 // a team of d blocks: a power of two, or every block of the device for the
-// largest plates, with at most cap nodes per block (so its parts fit in
+// largest plates, with at most caps[i] nodes per block (so its parts fit in
 // shared memory) and about n / 400 nodes per block otherwise (fewer blocks
 // per plate cost less block time, since an iteration's latency hardly
 // depends on the part size).  Team sizes that fit side by side form a
@@ -103,7 +103,8 @@ struct BatchSchedule {
     std::vector<BatchPhase> phases;
     std::vector<int> plate_phase, plate_team, plate_size;  // [count]; team index within its phase
 };
-std::string schedule_batch(const std::vector<int>& nodes, int sms, int cap, BatchSchedule& out);
+std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>& caps, int sms,
+                           BatchSchedule& out);
 
 // 64-bit FNV-1a over the problem's mesh, colouring, material and
 // constraint arrays (not F): the key of the plan cache.

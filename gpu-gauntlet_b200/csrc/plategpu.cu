@@ -11,7 +11,9 @@
 #include <list>
 #include <memory>
 #include <mutex>
+#include <atomic>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -119,6 +121,9 @@ struct pg_batch {
     DevBuf<unsigned long long> times;
     int ok_smem = 0;
     const void* ok_fn = nullptr;
+    std::vector<std::vector<float>> hF;   // each plate's current load (for the FP64 fallback)
+    std::unique_ptr<pg_batch> fb;         // FP64 batch of the plates whose mixed solve stagnated
+    std::vector<int> fb_ids;              // its plates
 };
 
 struct pg_ctx {
@@ -350,6 +355,8 @@ int halo_rings(const pg_options& o) { return o.smoother == PG_SMOOTHER_CHEBYSHEV
 // Coarse data of the two-level preconditioner, built once per plan: the
 // element matrices come from the device, A_c = P^T K P and its inverse are
 // formed on the host, and each part's A_c^-1 rows go back to the device.
+void upload_coarse(pg_ctx* c, Plan* pl);
+
 void ensure_coarse(pg_ctx* c, Plan* pl) {
     pg::HostPlan& hp = pl->hp;
     if (hp.coarse) return;
@@ -362,6 +369,12 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
     CK(cudaStreamSynchronize(c->stream));
     std::string e = pg::build_coarse(pl->prob_view, ke, hp);
     if (!e.empty()) throw Fail{PG_EINVAL, e};
+    upload_coarse(c, pl);
+}
+
+// Device copies of a plan's coarse data (after build_coarse).
+void upload_coarse(pg_ctx* c, Plan* pl) {
+    const pg::HostPlan& hp = pl->hp;
     cudaStream_t st = c->stream;
     pl->cagg_off.upload(hp.cagg_off.data(), hp.cagg_off.size(), st);
     pl->node_slot.upload(hp.node_slot.data(), hp.node_slot.size(), st);
@@ -412,6 +425,69 @@ void prepare_plan_data(pg_ctx* c, Plan* pl, const pg_options& o) {
         throw Fail{PG_EINVAL, "the Chebyshev smoother needs a plan made with it (2-ring halo)"};
     if (o.preconditioner == PG_PRECOND_TWO_LEVEL) ensure_coarse(c, pl);
     if (o.smoother == PG_SMOOTHER_CHEBYSHEV) ensure_smoother(c, pl);
+}
+
+// prepare_plan_data for many plans (a batch): the element matrices and block
+// inverses come down in chunks of plates, the host work (coarse matrices,
+// eigenvalue estimates) runs on worker threads, and the results go back up.
+void prepare_many(pg_ctx* c, const std::vector<Plan*>& pls, const pg_options& o) {
+    const bool coarse = o.preconditioner == PG_PRECOND_TWO_LEVEL;
+    const bool cheb = o.smoother == PG_SMOOTHER_CHEBYSHEV;
+    std::vector<Plan*> todo;
+    for (Plan* pl : pls) {
+        if (cheb && pl->hp.rings != 2)
+            throw Fail{PG_EINVAL, "the Chebyshev smoother needs a plan made with it (2-ring halo)"};
+        if ((coarse && !pl->hp.coarse) || (cheb && !(pl->lambda_max > 0))) todo.push_back(pl);
+    }
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    for (size_t i = 0; i < todo.size();) {
+        size_t j = i, elems = 0;
+        while (j < todo.size() && (j == i || elems + (size_t)todo[j]->hp.Ne <= 1500000)) elems += todo[j++]->hp.Ne;
+        const size_t m = j - i;
+        std::vector<std::vector<double>> ke(m), binv(m);
+        for (size_t k = 0; k < m; k++) {
+            Plan* pl = todo[i + k];
+            run_setup(c, pl);
+            const size_t kk = 9 * (size_t)pl->hp.npe * pl->hp.npe;
+            ke[k].resize(std::max<size_t>(1, (size_t)pl->hp.Ne * kk));
+            if (pl->hp.Ne > 0)
+                CK(cudaMemcpyAsync(ke[k].data(), pl->ke64.p, (size_t)pl->hp.Ne * kk * sizeof(double),
+                                   cudaMemcpyDeviceToHost, c->stream));
+            if (cheb && !(pl->lambda_max > 0)) {
+                binv[k].resize(9 * (size_t)pl->hp.Nn);
+                CK(cudaMemcpyAsync(binv[k].data(), pl->binv64.p, binv[k].size() * sizeof(double),
+                                   cudaMemcpyDeviceToHost, c->stream));
+            }
+        }
+        CK(cudaStreamSynchronize(c->stream));
+        std::vector<std::string> err(m);
+        std::vector<double> lam(m, 0.0);
+        std::atomic<size_t> next{0};
+        auto work = [&]() {
+            for (size_t k; (k = next.fetch_add(1)) < m;) {
+                Plan* pl = todo[i + k];
+                try {
+                    if (coarse && !pl->hp.coarse) err[k] = pg::build_coarse(pl->prob_view, ke[k], pl->hp);
+                    if (err[k].empty() && cheb && !(pl->lambda_max > 0))
+                        lam[k] = pg::estimate_lambda_max(pl->prob_view, ke[k], binv[k], 30);
+                } catch (...) {
+                    err[k] = "host set-up of the batch failed";
+                }
+            }
+        };
+        std::vector<std::thread> th;
+        for (unsigned t = 1; t < std::min<size_t>(hw, m); t++) th.emplace_back(work);
+        work();
+        for (auto& t : th) t.join();
+        for (size_t k = 0; k < m; k++) {
+            if (!err[k].empty()) throw Fail{PG_EINVAL, err[k]};
+            Plan* pl = todo[i + k];
+            if (coarse && pl->hp.coarse && pl->ainv64.n == 0) upload_coarse(c, pl);
+            if (cheb && !(pl->lambda_max > 0))
+                pl->lambda_max = std::isfinite(lam[k]) && lam[k] > 0 ? lam[k] : (double)pl->hp.npe;
+        }
+        i = j;
+    }
 }
 
 // Shared-memory layout of a launch: keep in shared memory what fits, in this
@@ -698,11 +774,14 @@ namespace {
 
 // Owned nodes per block that the shared-memory layout holds (vectors, block
 // inverses, task results; the Ke blocks then stay in L2): a first guess,
-// checked against each plate's actual layout by build_batch.
-int batch_capacity(const pg_options& o, int rings) {
+// checked against each plate's actual layout by build_batch.  DKT nodes
+// carry about 6 element tasks instead of 4.
+int batch_capacity(const pg_options& o, int rings, int npe) {
     const bool mixed = o.precision == PG_PREC_MIXED;
-    if (rings == 2) return mixed ? 470 : 250;
-    return mixed ? 560 : 300;
+    // about 85% of what the layout holds for a 257 x 257-node plate's parts
+    static const int cap[2][2][2] = {{{450, 300}, {400, 250}},   // FP64: Q4, DKT x rings 1, 2
+                                     {{640, 500}, {560, 380}}};  // mixed
+    return cap[mixed ? 1 : 0][npe == 3 ? 1 : 0][rings == 2 ? 1 : 0];
 }
 
 std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int count,
@@ -719,15 +798,16 @@ std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int co
             if (!std::isfinite(probs[i].F[k])) throw Fail{PG_ENONFINITE, "F contains NaN or Inf"};
         nodes[i] = (int)probs[i].node_count;
     }
-    // schedule, then check every plate's layout at its team size; shrink the
-    // capacity and reschedule while some part does not fit
-    int cap = batch_capacity(o, b->rings);
+    // schedule, then check every plate's layout at its team size; lower the
+    // capacity of the plates whose parts do not fit and reschedule
+    std::vector<int> caps(count);
+    for (int i = 0; i < count; i++) caps[i] = batch_capacity(o, b->rings, (int)probs[i].nodes_per_element);
     for (int attempt = 0;; attempt++) {
-        std::string e = pg::schedule_batch(nodes, c->sms, cap, b->sched);
+        std::string e = pg::schedule_batch(nodes, caps, c->sms, b->sched);
         if (!e.empty()) throw Fail{PG_EUNSUPPORTED, e};
         b->plans.clear();
         bool fits = true;
-        for (int i = 0; i < count && fits; i++) {
+        for (int i = 0; i < count; i++) {
             const int G = b->sched.plate_size[i];
             b->plans.push_back(build_plan(c, probs[i], G, b->rings));
             int ke_mode = 0;
@@ -736,11 +816,11 @@ std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int co
                 choose_layout(c, b->plans.back()->hp, o, &ke_mode, &ainv);
             } catch (const Fail&) {
                 fits = false;
+                caps[i] = caps[i] * 3 / 4;
             }
         }
         if (fits) break;
-        if (attempt == 4) throw Fail{PG_EUNSUPPORTED, "batch plates too large for shared memory"};
-        cap = cap * 3 / 4;
+        if (attempt == 5) throw Fail{PG_EUNSUPPORTED, "batch plates too large for shared memory"};
     }
     cudaStream_t st = c->stream;
     for (const pg::BatchPhase& P : b->sched.phases) {
@@ -760,12 +840,18 @@ std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int co
     b->args.alloc(count);
     b->res.alloc(count);
     b->times.alloc(2 * (size_t)count);
-    for (int i = 0; i < count; i++)
-        CK(cudaMemcpyAsync(b->plans[i]->F.p, probs[i].F, 3 * (size_t)probs[i].node_count * sizeof(float),
+    b->hF.resize(count);
+    for (int i = 0; i < count; i++) {
+        b->hF[i].assign(probs[i].F, probs[i].F + 3 * (size_t)probs[i].node_count);
+        CK(cudaMemcpyAsync(b->plans[i]->F.p, b->hF[i].data(), b->hF[i].size() * sizeof(float),
                            cudaMemcpyHostToDevice, st));
+    }
     CK(cudaStreamSynchronize(st));
     return b;
 }
+
+void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* const* x_out,
+               pg_info* infos, pg_batch_info* bi);
 
 double percentile(std::vector<double> v, double q) {
     if (v.empty()) return 0.0;
@@ -788,9 +874,15 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
             const size_t n = 3 * (size_t)b->plans[i]->hp.Nn;
             for (size_t k = 0; k < n; k++)
                 if (!std::isfinite(F[i][k])) throw Fail{PG_ENONFINITE, "F contains NaN or Inf"};
-            CK(cudaMemcpyAsync(b->plans[i]->F.p, F[i], n * sizeof(float), cudaMemcpyHostToDevice, st));
+            b->hF[i].assign(F[i], F[i] + n);
+            CK(cudaMemcpyAsync(b->plans[i]->F.p, b->hF[i].data(), n * sizeof(float), cudaMemcpyHostToDevice,
+                               st));
         }
-    for (auto& pl : b->plans) prepare_plan_data(c, pl.get(), o);
+    {
+        std::vector<Plan*> pls;
+        for (auto& pl : b->plans) pls.push_back(pl.get());
+        prepare_many(c, pls, o);
+    }
     CK(cudaEventRecord(c->ev[0], st));
     for (auto& pl : b->plans) run_setup(c, pl.get());
     CK(cudaEventRecord(c->ev[1], st));
@@ -877,46 +969,49 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
         bi->shared_bytes = smem;
     }
     for (int i = 0; i < count; i++) throw_on_failure(r[i]);
-    // plates whose mixed solve stagnated: FP64 on their own plan (one launch
-    // each), or on a plan over the whole device when the FP64 parts do not
-    // fit in shared memory at the team's size
+    // plates whose mixed solve stagnated: solved again in FP64 as a batch of
+    // their own (planned for FP64 shared-memory capacity, kept while the same
+    // plates stagnate)
     if (o.precision != PG_PREC_MIXED || !o.fallback) return;
+    std::vector<int> failed;
+    for (int i = 0; i < count; i++)
+        if (r[i].stop_reason == PG_STOP_STAGNATED) failed.push_back(i);
+    if (bi) bi->fallbacks = (int32_t)failed.size();
+    if (failed.empty()) return;
     pg_options o64 = o;
     o64.precision = PG_PREC_FP64;
-    double extra_ms = 0.0;
-    int fallbacks = 0;
-    for (int i = 0; i < count; i++) {
-        if (r[i].stop_reason != PG_STOP_STAGNATED) continue;
-        pg_info fi{};
-        void* xd = x_out ? (void*)x_out[i] : nullptr;
-        try {
-            run_solve(c, b->plans[i].get(), o64, &fi, xd, cudaMemcpyDeviceToHost);
-        } catch (const Fail& f) {
-            if (f.status != PG_EUNSUPPORTED) throw;
-            Plan* old = b->plans[i].get();
-            auto np = build_plan(c, old->prob_view, c->sms, b->rings);
-            CK(cudaMemcpyAsync(np->F.p, old->F.p, 3 * (size_t)old->hp.Nn * sizeof(float),
-                               cudaMemcpyDeviceToDevice, st));
-            b->plans[i] = std::move(np);
-            fi = pg_info{};
-            run_solve(c, b->plans[i].get(), o64, &fi, xd, cudaMemcpyDeviceToHost);
+    const int nf = (int)failed.size();
+    std::vector<const float*> Ff(nf);
+    for (int k = 0; k < nf; k++) Ff[k] = b->hF[failed[k]].data();
+    if (!b->fb || b->fb_ids != failed) {
+        std::vector<pg_problem> fp(nf);
+        for (int k = 0; k < nf; k++) {
+            fp[k] = b->plans[failed[k]]->prob_view;
+            fp[k].F = Ff[k];
         }
-        extra_ms += fi.setup_ms + fi.solve_ms;
-        fallbacks++;
+        b->fb.reset();
+        b->fb = build_batch(c, fp.data(), nf, o64);
+        b->fb_ids = failed;
+    }
+    std::vector<double*> xf(nf, nullptr);
+    if (x_out)
+        for (int k = 0; k < nf; k++) xf[k] = x_out[failed[k]];
+    std::vector<pg_info> inf(nf);
+    pg_batch_info fbi{};
+    run_batch(b->fb.get(), o64, Ff.data(), x_out ? xf.data() : nullptr, inf.data(), &fbi);
+    for (int k = 0; k < nf; k++) {
+        const int i = failed[k];
         if (infos) {
             const double mixed_ms = infos[i].solve_ms;
-            infos[i] = fi;
-            infos[i].status = PG_OK;
+            infos[i] = inf[k];
             infos[i].fallback = 1;
             infos[i].solve_ms += mixed_ms;
-            infos[i].plan_cached = 1;
         }
-        if (fi.converged) converged++;
+        if (inf[k].converged) converged++;
     }
     if (bi) {
-        bi->fallbacks = fallbacks;
         bi->converged = converged;
-        bi->solve_ms += extra_ms;
+        bi->solve_ms += fbi.setup_ms + fbi.solve_ms;
         bi->solves_per_s = bi->solve_ms > 0 ? count / (bi->solve_ms * 1e-3) : 0.0;
     }
 }
@@ -1276,6 +1371,7 @@ void pg_batch_destroy(pg_batch* b) {
         std::lock_guard<std::mutex> lk(b->ctx->mu);
         cudaSetDevice(b->ctx->device);
         cudaStreamSynchronize(b->ctx->stream);
+        b->fb.reset();
         b->plans.clear();
         b->phases.clear();
         b->abort_flag.release();
@@ -1310,7 +1406,7 @@ int pg_batch_schedule(const uint32_t* node_counts, int count, int sms, int cap, 
     try {
         std::vector<int> nodes(node_counts, node_counts + count);
         pg::BatchSchedule S;
-        if (!pg::schedule_batch(nodes, sms, cap, S).empty()) return PG_EUNSUPPORTED;
+        if (!pg::schedule_batch(nodes, std::vector<int>(count, cap), sms, S).empty()) return PG_EUNSUPPORTED;
         for (int i = 0; i < count; i++) {
             plate_phase[i] = S.plate_phase[i];
             plate_size[i] = S.plate_size[i];
