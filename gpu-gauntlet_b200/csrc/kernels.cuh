@@ -573,6 +573,83 @@ __device__ __forceinline__ void task_matvec(const T* __restrict__ u, T* __restri
     }
 }
 
+// Bending moments at each element's centroid (postprocess.ts:59-264):
+// curvatures from the rotations (Q4: shape derivatives at xi = eta = 0
+// through the Jacobian; DKT: linear-triangle derivatives), M = D (k_x +
+// nu k_y, k_y + nu k_x, (1 - nu) k_xy / 2) with the plate's uniform D.
+// em[e] = {Mx, My, Mxy, weight}; weight 0 marks a degenerate triangle
+// (|2A| < 1e-15), which the reference leaves out of the nodal averages.
+template <int NPE>
+__global__ void elem_moments_kernel(int Ne, const float* __restrict__ nodes,
+                                    const uint32_t* __restrict__ el, double D, double nu,
+                                    const double* __restrict__ x, double4* __restrict__ em) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Ne) return;
+    const uint32_t* en = el + (size_t)e * NPE;
+    double dNdx[NPE], dNdy[NPE];
+    if constexpr (NPE == 4) {
+        const double dXi[4] = {-0.25, 0.25, 0.25, -0.25}, dEta[4] = {-0.25, -0.25, 0.25, 0.25};
+        double J11 = 0, J12 = 0, J21 = 0, J22 = 0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const double xi = nodes[2 * en[i]], yi = nodes[2 * en[i] + 1];
+            J11 += dXi[i] * xi;
+            J12 += dXi[i] * yi;
+            J21 += dEta[i] * xi;
+            J22 += dEta[i] * yi;
+        }
+        const double inv = 1.0 / (J11 * J22 - J12 * J21);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            dNdx[i] = inv * (J22 * dXi[i] - J12 * dEta[i]);
+            dNdy[i] = inv * (-J21 * dXi[i] + J11 * dEta[i]);
+        }
+    } else {
+        const double x1 = nodes[2 * en[0]], y1 = nodes[2 * en[0] + 1];
+        const double x2 = nodes[2 * en[1]], y2 = nodes[2 * en[1] + 1];
+        const double x3 = nodes[2 * en[2]], y3 = nodes[2 * en[2] + 1];
+        const double twoA = (x2 - x1) * (y3 - y1) - (x3 - x1) * (y2 - y1);
+        if (fabs(twoA) < 1e-15) {
+            em[e] = make_double4(0.0, 0.0, 0.0, 0.0);
+            return;
+        }
+        const double inv = 1.0 / twoA;
+        dNdx[0] = (y2 - y3) * inv; dNdy[0] = (x3 - x2) * inv;
+        dNdx[1] = (y3 - y1) * inv; dNdy[1] = (x1 - x3) * inv;
+        dNdx[2] = (y1 - y2) * inv; dNdy[2] = (x2 - x1) * inv;
+    }
+    double kx = 0, ky = 0, kxy = 0;
+#pragma unroll
+    for (int i = 0; i < NPE; i++) {
+        const double tx = x[3 * (size_t)en[i] + 1], ty = x[3 * (size_t)en[i] + 2];
+        kx += dNdx[i] * ty;
+        ky += -dNdy[i] * tx;
+        kxy += dNdy[i] * ty - dNdx[i] * tx;
+    }
+    em[e] = make_double4(D * (kx + nu * ky), D * (ky + nu * kx), D * (1 - nu) * kxy / 2, 1.0);
+}
+
+// Nodal averages of the element moments, summed in element order over each
+// node's incidence list (postprocess.ts:132-155).  M: [3][Nn] Mx, My, Mxy.
+__global__ void node_moments_kernel(int Nn, const int* __restrict__ inc_ptr,
+                                    const int* __restrict__ inc_idx, const double4* __restrict__ em,
+                                    double* __restrict__ M) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= Nn) return;
+    double sx = 0, sy = 0, sxy = 0, c = 0;
+    for (int q = inc_ptr[n]; q < inc_ptr[n + 1]; q++) {
+        const double4 m = em[inc_idx[q] / 4];
+        if (m.w == 0.0) continue;
+        sx += m.x;
+        sy += m.y;
+        sxy += m.z;
+        c += 1.0;
+    }
+    M[n] = c > 0 ? sx / c : 0.0;
+    M[Nn + n] = c > 0 ? sy / c : 0.0;
+    M[2 * (size_t)Nn + n] = c > 0 ? sxy / c : 0.0;
+}
+
 // Task blocks of every task from the element matrices (setup, per solve):
 // the owned node's 3 rows, columns rotated to start at the owned node.
 template <int NPE>

@@ -1016,6 +1016,26 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
     }
 }
 
+// Queues the two moment kernels of plan pl: x_dev [3 Nn] -> M_dev [3][Nn].
+void run_moments(pg_ctx* c, Plan* pl, const double* x_dev, double* M_dev) {
+    const pg::HostPlan& hp = pl->hp;
+    if (hp.Ne == 0 || hp.Nn == 0) return;
+    DevBuf<double4> em;
+    em.alloc(hp.Ne);
+    const double D = (pl->E * std::pow(pl->t, 3.0)) / (12.0 * (1.0 - std::pow(pl->nu, 2.0)));
+    if (hp.npe == 4)
+        pg::elem_moments_kernel<4><<<(hp.Ne + 127) / 128, 128, 0, c->stream>>>(
+            hp.Ne, pl->mesh_nodes.p, pl->mesh_elements.p, D, pl->nu, x_dev, em.p);
+    else
+        pg::elem_moments_kernel<3><<<(hp.Ne + 127) / 128, 128, 0, c->stream>>>(
+            hp.Ne, pl->mesh_nodes.p, pl->mesh_elements.p, D, pl->nu, x_dev, em.p);
+    CK(cudaGetLastError());
+    pg::node_moments_kernel<<<(hp.Nn + 127) / 128, 128, 0, c->stream>>>(hp.Nn, pl->inc_ptr.p, pl->inc_idx.p,
+                                                                       em.p, M_dev);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));  // em is released on return
+}
+
 }  // namespace
 
 extern "C" {
@@ -1418,6 +1438,35 @@ int pg_batch_schedule(const uint32_t* node_counts, int count, int sms, int cap, 
     } catch (...) {
         return PG_ENOMEM;
     }
+}
+
+int pg_moments(pg_ctx* c, const pg_problem* p, const double* x, double* Mx, double* My,
+                          double* Mxy) {
+    return guarded(c, nullptr, [&] {
+        check_problem(p, false);
+        const size_t Nn = p->node_count;
+        if (Nn == 0) return;
+        if (!x || !Mx || !My || !Mxy) throw Fail{PG_EINVAL, "x / Mx / My / Mxy is NULL"};
+        bool cached = false;
+        Plan* pl = get_plan(c, *p, auto_ctas(c, (int)Nn), 1, &cached);
+        DevBuf<double> dx, dm;
+        dx.upload(x, 3 * Nn, c->stream);
+        dm.alloc(3 * Nn);
+        run_moments(c, pl, dx.p, dm.p);
+        std::vector<double> h(3 * Nn);
+        CK(cudaMemcpy(h.data(), dm.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        std::memcpy(Mx, h.data(), Nn * sizeof(double));
+        std::memcpy(My, h.data() + Nn, Nn * sizeof(double));
+        std::memcpy(Mxy, h.data() + 2 * Nn, Nn * sizeof(double));
+    });
+}
+
+int pg_plan_moments_device(pg_plan* h, const double* x_dev, double* M_dev) {
+    if (!h) return PG_EINVAL;
+    return guarded(h->ctx, nullptr, [&] {
+        if (!x_dev || !M_dev) throw Fail{PG_EINVAL, "x_dev / M_dev is NULL"};
+        run_moments(h->ctx, h->plan.get(), x_dev, M_dev);
+    });
 }
 
 }  // extern "C"

@@ -14,4 +14,6 @@ from .coloring import (computeElementColoring, computeElementColoringGreedy, get
 from .problem import (applyBCsToRHS, buildLoadVector, constrained_mask, identifyConstrainedDOFs,
                       pressure_load_vector)
 from .solver import clearPipelineCache, isWebGPUAvailable, solveGPU, solveGPUAsync
+from .postprocess import (computeMoments, extractVerticalDisplacements, findMaxDisplacement,
+                          findMaxMoments)
 from ._lib import PlateGPUError

@@ -29,7 +29,7 @@ EXPORTED = ("pg_options_default", "pg_is_available", "pg_create", "pg_destroy", 
             "pg_plan_destroy", "pg_apply_k", "pg_apply_k_static",
             "pg_block_jacobi", "pg_element_stiffness", "pg_plan_inspect",
             "pg_plan_inspect_halo", "pg_batch_create", "pg_batch_solve", "pg_batch_destroy",
-            "pg_solve_batch", "pg_batch_schedule")
+            "pg_solve_batch", "pg_batch_schedule", "pg_moments", "pg_plan_moments_device")
 
 
 class PgProblem(C.Structure):
@@ -196,6 +196,10 @@ def load() -> C.CDLL:
     L.pg_solve_batch.restype = I
     L.pg_batch_schedule.argtypes = [P, I, I, I, P, P, P, P, P]
     L.pg_batch_schedule.restype = I
+    L.pg_moments.argtypes = [P, C.POINTER(PgProblem), P, P, P, P]
+    L.pg_moments.restype = I
+    L.pg_plan_moments_device.argtypes = [P, P, P]
+    L.pg_plan_moments_device.restype = I
     _lib = L
     return L
 
@@ -343,6 +347,14 @@ class Context:
                                    C.cast(infos, C.c_void_p), C.byref(bi))
         self._check(st)
         return xs, list(infos), bi
+
+    def moments(self, prob: Problem, x):
+        """pg_moments: nodal (Mx, My, Mxy) of displacements x (FP64)."""
+        x = np.ascontiguousarray(x, np.float64)
+        n = int(prob.struct.node_count)
+        out = [np.zeros(n, np.float64) for _ in range(3)]
+        self._check(self.L.pg_moments(self.h, C.byref(prob.struct), _ptr(x), *[_ptr(o) for o in out]))
+        return tuple(out)
 
     def apply_k(self, prob: Problem, x):
         x = np.ascontiguousarray(x, np.float64)

@@ -274,6 +274,19 @@ int pg_batch_schedule(const uint32_t* node_counts, int count, int sms, int cap, 
                       int32_t* plate_size, int32_t* plate_team, int32_t* phase_grid,
                       int32_t* phases_out);
 
+/* Nodal bending moments of a solution, as computeMoments
+ * (postprocess.ts:40-264): curvatures at each element's centroid (Q4
+ * shape derivatives at xi = eta = 0, DKT linear-triangle derivatives), Mx =
+ * D (kx + nu ky), My = D (ky + nu kx), Mxy = D (1 - nu) kxy / 2 with the
+ * plate's uniform D (E, nu, t of the problem; like the reference, elem_t is
+ * not used), averaged over the elements around each node; degenerate
+ * triangles are left out.  FP64 on the device.  x: [3*node_count]. */
+int pg_moments(pg_ctx* ctx, const pg_problem* prob, const double* x, double* Mx, double* My,
+               double* Mxy);
+/* The same on a plan's device-resident solution: x_dev [3*node_count] ->
+ * M_dev [3][node_count] (Mx, My, Mxy), on the context stream. */
+int pg_plan_moments_device(pg_plan* plan, const double* x_dev, double* M_dev);
+
 /* Test hook: y = K x in FP64 with the reference BC rule (y_c = x_c). */
 int pg_apply_k(pg_ctx* ctx, const pg_problem* prob, const double* x, double* y);
 

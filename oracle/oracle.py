@@ -57,6 +57,7 @@ def lib():
         L.or_color_structured.argtypes = [_I, _I, _u8p, _up, _ip]
         L.or_color_greedy.argtypes = [_I, _I, _I, _up, _u8p, _up, _ip]
         L.or_color_greedy.restype = _I
+        L.or_moments.argtypes = [_I, _I, _I, _fp, _up, _D, _D, _D, _dp, _I, _dp, _dp, _dp]
         L.or_verify_coloring.argtypes = [_I, _I, _I, _up, _u8p]
         L.or_verify_coloring.restype = _I
         L.or_all_ke.argtypes = [_I, _I, _fp, _up, _D, _D, _D, C.c_void_p, _I, _dp]
@@ -245,6 +246,18 @@ def solve_test_system():
     it, res, conv = C.c_int(), C.c_double(), C.c_int()
     lib().or_solve_test_system(x, C.byref(it), C.byref(res), C.byref(conv))
     return x, it.value, res.value, bool(conv.value)
+
+
+# --- postprocess.ts -------------------------------------------------------------
+
+def moments(nodes, elements, npe, E, nu, t, x, mode=REF):
+    """computeMoments (postprocess.ts:40-264): nodal (Mx, My, Mxy)."""
+    nodes = _f32(nodes)
+    elements = _u32(elements)
+    Nn = nodes.size // 2
+    out = [np.zeros(Nn) for _ in range(3)]
+    lib().or_moments(Nn, elements.size // npe, npe, nodes, elements, E, nu, t, _f64(x), mode, *out)
+    return tuple(out)
 
 
 # --- FP64 truth -----------------------------------------------------------------

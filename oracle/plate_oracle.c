@@ -727,3 +727,67 @@ long or_assemble_coo(int Nn, int Ne, int npe, const uint32_t *el, const double *
     }
     return m;
 }
+
+/* ------------------------------------------------------------------------ */
+/* postprocess.ts: nodal bending moments                                    */
+/* ------------------------------------------------------------------------ */
+
+/* computeMoments (postprocess.ts:40-54) with computeMomentsQuad (:59-157)
+ * and computeMomentsTriangle (:164-264): curvatures at the element centroid
+ * (Q4: shape derivatives at xi = eta = 0 through the Jacobian,
+ * element.ts:80-184; DKT: linear-triangle derivatives, stored in a
+ * Float32Array in the reference), moments with the plate's D and nu, summed
+ * into the element's nodes in element order (Float32Array accumulators) and
+ * averaged.  x: displacements [3 Nn] (a Float32Array in the reference).
+ * Triangles with |2A| < 1e-15 are skipped (:199). */
+void or_moments(int Nn, int Ne, int npe, const float *nodes, const uint32_t *el, double E, double nu,
+                double t, const double *x, int mode, double *Mx, double *My, double *Mxy) {
+    const double D = flexural_rigidity(E, nu, t);
+    double *sx = calloc((size_t)Nn, sizeof(double)), *sy = calloc((size_t)Nn, sizeof(double));
+    double *sxy = calloc((size_t)Nn, sizeof(double)), *cnt = calloc((size_t)Nn, sizeof(double));
+    for (int e = 0; e < Ne; e++) {
+        const uint32_t *en = el + (size_t)e * npe;
+        double dNdx[4], dNdy[4];
+        if (npe == 4) {
+            float c[8];
+            for (int i = 0; i < 4; i++) {
+                c[2 * i] = nodes[2 * en[i]];
+                c[2 * i + 1] = nodes[2 * en[i] + 1];
+            }
+            double dNdXi[4], dNdEta[4];
+            shape_derivs(0.0, 0.0, dNdXi, dNdEta);
+            phys_derivs(c, dNdXi, dNdEta, dNdx, dNdy);
+        } else {
+            const double x1 = nodes[2 * en[0]], y1 = nodes[2 * en[0] + 1];
+            const double x2 = nodes[2 * en[1]], y2 = nodes[2 * en[1] + 1];
+            const double x3 = nodes[2 * en[2]], y3 = nodes[2 * en[2] + 1];
+            const double twoA = (x2 - x1) * (y3 - y1) - (x3 - x1) * (y2 - y1);
+            if (fabs(twoA) < 1e-15) continue;
+            const double inv = 1 / twoA;
+            dNdx[0] = R(mode, (y2 - y3) * inv); dNdy[0] = R(mode, (x3 - x2) * inv);
+            dNdx[1] = R(mode, (y3 - y1) * inv); dNdy[1] = R(mode, (x1 - x3) * inv);
+            dNdx[2] = R(mode, (y1 - y2) * inv); dNdy[2] = R(mode, (x2 - x1) * inv);
+        }
+        double kx = 0, ky = 0, kxy = 0;
+        for (int i = 0; i < npe; i++) {
+            const double tx = R(mode, x[3 * (size_t)en[i] + 1]), ty = R(mode, x[3 * (size_t)en[i] + 2]);
+            kx += dNdx[i] * ty;
+            ky += -dNdy[i] * tx;
+            kxy += dNdy[i] * ty - dNdx[i] * tx;
+        }
+        const double mx = D * (kx + nu * ky), my = D * (ky + nu * kx), mxy = (D * (1 - nu) * kxy) / 2;
+        for (int i = 0; i < npe; i++) {
+            const uint32_t n = en[i];
+            sx[n] = R(mode, sx[n] + mx);
+            sy[n] = R(mode, sy[n] + my);
+            sxy[n] = R(mode, sxy[n] + mxy);
+            cnt[n] = R(mode, cnt[n] + 1);
+        }
+    }
+    for (int n = 0; n < Nn; n++) {
+        Mx[n] = cnt[n] > 0 ? R(mode, sx[n] / cnt[n]) : 0.0;
+        My[n] = cnt[n] > 0 ? R(mode, sy[n] / cnt[n]) : 0.0;
+        Mxy[n] = cnt[n] > 0 ? R(mode, sxy[n] / cnt[n]) : 0.0;
+    }
+    free(sx); free(sy); free(sxy); free(cnt);
+}

@@ -107,3 +107,34 @@ def test_solver_options_are_checked_before_any_device_work():
         with pytest.raises(PlateGPUError, match="unknown"):
             solveGPU(wl.mesh, wl.material, wl.coloring, wl.F, wl.constrainedDOFs,
                      GPUSolverOptions(**bad))
+
+
+def test_postprocess_host_helpers():
+    from plategpu import extractVerticalDisplacements, findMaxDisplacement, findMaxMoments
+    x = np.array([1, 9, 9, -3, 9, 9, 3, 9, 9], np.float32)
+    w = extractVerticalDisplacements(x, 3)
+    assert w.tolist() == [1, -3, 3]
+    nodes = np.array([0, 0, 1, 0, 2, 0], np.float32)
+    m = findMaxDisplacement(w, nodes)
+    assert m == {"maxW": -3.0, "nodeIndex": 1, "x": 1.0, "y": 0.0}  # first of equal magnitudes
+    mm = findMaxMoments([1, -5, 2], [0.5, 0.25, -0.75], [3, 3, -3])
+    assert mm == {"maxMx": -5.0, "maxMy": -0.75, "maxMxy": 3.0}
+
+
+def test_oracle_moments_of_a_pure_bending_field(oracle):
+    """theta_y = c x (so kx = c) and theta_x = -d y (ky = d) on a rectangle:
+    every element carries the same curvatures, so every node gets
+    Mx = D (c + nu d), My = D (d + nu c), Mxy = 0, in both modes."""
+    m = mesher.rectangular_mesh_nxny(4, 3, 8, 6)
+    xy = m.nodes.reshape(-1, 2).astype(np.float64)
+    c, d = 1e-3, -2e-3
+    x = np.zeros(3 * m.nodeCount)
+    x[1::3] = -d * xy[:, 1]
+    x[2::3] = c * xy[:, 0]
+    E, nu, t = 2.1e11, 0.3, 0.1
+    D = E * t ** 3 / (12 * (1 - nu ** 2))
+    for mode in (oracle.FP64, oracle.REF):
+        Mx, My, Mxy = oracle.moments(m.nodes, m.elements, 4, E, nu, t, x, mode)
+        assert np.allclose(Mx, D * (c + nu * d), rtol=1e-6)
+        assert np.allclose(My, D * (d + nu * c), rtol=1e-6)
+        assert np.abs(Mxy).max() < 1e-6 * abs(D * c)
