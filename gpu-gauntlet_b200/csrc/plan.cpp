@@ -567,10 +567,24 @@ uint64_t problem_hash(const pg_problem& p) {
         h *= 0xff51afd7ed558ccdull;
         h ^= h >> 33;
     };
+    // arrays in four independent lanes of multiply-xorshift (32 bytes per
+    // step, so the four multiplications overlap), folded into h at the end:
+    // this runs on every pg_solve, over the whole mesh
     auto bytes = [&](const void* d, size_t n) {
         if (!d) { mix(0xdeadull); return; }
         const unsigned char* b = (const unsigned char*)d;
+        uint64_t l[4] = {0x243f6a8885a308d3ull, 0x13198a2e03707344ull, 0xa4093822299f31d0ull,
+                         0x082efa98ec4e6c89ull};
         size_t i = 0;
+        for (; i + 32 <= n; i += 32) {
+            uint64_t v[4];
+            std::memcpy(v, b + i, 32);
+            for (int k = 0; k < 4; k++) {
+                l[k] = (l[k] ^ v[k]) * 0x9fb21c651e98df25ull;
+                l[k] ^= l[k] >> 29;
+            }
+        }
+        for (int k = 0; k < 4; k++) mix(l[k]);
         for (; i + 8 <= n; i += 8) {
             uint64_t v;
             std::memcpy(&v, b + i, 8);
