@@ -1366,7 +1366,8 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const __grid_consta
     pcg_body<NPE, T, MIXED>(a, blockIdx.x, sm);
 }
 
-// Many independent plates in one launch.  The grid is cut into teams of
+// Many independent plates of one element type (NPE) in one launch.  The
+// grid is cut into teams of
 // consecutive blocks; a team solves the plates of its queue one after the
 // other, each plate partitioned into as many parts as the team has blocks,
 // with the plate's own exchange buffers (so teams never wait on each other,
@@ -1381,7 +1382,7 @@ struct BatchArgs {
     unsigned long long* times;    // [count][2] start / end of each plate
 };
 
-template <typename T, bool MIXED>
+template <int NPE, typename T, bool MIXED>
 __global__ void __launch_bounds__(kMaxThreads, 1) pcg_batch_kernel(const __grid_constant__ BatchArgs b) {
     extern __shared__ __align__(16) unsigned char sm[];
     const int team = b.block_team[blockIdx.x];
@@ -1391,12 +1392,7 @@ __global__ void __launch_bounds__(kMaxThreads, 1) pcg_batch_kernel(const __grid_
         const PcgArgs& a = b.plates[pi];
         if (g == 0 && threadIdx.x == 0) b.times[2 * pi] = gtimer();
         // a plate with fewer parts than the team has blocks leaves the rest idle
-        if (g < a.G) {
-            if (a.npe == 4)
-                pcg_body<4, T, MIXED>(a, g, sm);
-            else
-                pcg_body<3, T, MIXED>(a, g, sm);
-        }
+        if (g < a.G) pcg_body<NPE, T, MIXED>(a, g, sm);
         __syncthreads();  // shared memory is reloaded for the next plate
         if (g == 0 && threadIdx.x == 0) b.times[2 * pi + 1] = gtimer();
     }

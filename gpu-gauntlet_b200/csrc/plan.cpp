@@ -460,12 +460,12 @@ double estimate_lambda_max(const pg_problem& p, const std::vector<double>& ke64,
     return lam;
 }
 
-std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>& caps, int sms,
-                           BatchSchedule& out) {
+std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>& caps,
+                           const std::vector<int>& kinds, int sms, BatchSchedule& out) {
     out = BatchSchedule{};
     const int count = (int)nodes.size();
     if (count == 0) return "empty batch";
-    if (sms < 1 || (int)caps.size() != count) return "no blocks to schedule";
+    if (sms < 1 || (int)caps.size() != count || (int)kinds.size() != count) return "no blocks to schedule";
     int top = 1;  // largest power of two <= sms
     while (top * 2 <= sms) top *= 2;
     std::vector<int> d(count);
@@ -483,10 +483,22 @@ std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>
         d[i] = std::max(need, std::min(top, pref));
         w[i] = std::sqrt(n) * (n + 300.0 * d[i]);
     }
-    // team sizes, largest first, first-fit into phases (one team of each size fits)
+    out.plate_phase.assign(count, -1);
+    out.plate_team.assign(count, -1);
+    out.plate_size = d;
+    std::vector<int> order(count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return w[a] > w[b]; });
+    std::vector<int> ks;
+    for (int i = 0; i < count; i++)
+        if (std::find(ks.begin(), ks.end(), kinds[i]) == ks.end()) ks.push_back(kinds[i]);
+    std::sort(ks.rbegin(), ks.rend());
+    for (int kind : ks) {
+    // team sizes of this kind, largest first, first-fit into phases (one team
+    // of each size fits)
     std::vector<int> cs;
     for (int i = 0; i < count; i++)
-        if (std::find(cs.begin(), cs.end(), d[i]) == cs.end()) cs.push_back(d[i]);
+        if (kinds[i] == kind && std::find(cs.begin(), cs.end(), d[i]) == cs.end()) cs.push_back(d[i]);
     std::sort(cs.rbegin(), cs.rend());
     std::vector<std::vector<int>> phase_sizes;
     std::vector<int> phase_sum;
@@ -500,12 +512,6 @@ std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>
         phase_sizes[ph].push_back(c);
         phase_sum[ph] += c;
     }
-    out.plate_phase.assign(count, -1);
-    out.plate_team.assign(count, -1);
-    out.plate_size = d;
-    std::vector<int> order(count);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return w[a] > w[b]; });
     for (size_t ph = 0; ph < phase_sizes.size(); ph++) {
         const std::vector<int>& pc = phase_sizes[ph];  // descending
         const int nc = (int)pc.size();
@@ -513,7 +519,7 @@ std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>
         std::vector<int> teams(nc, 1), nplates(nc, 0);
         for (int i = 0; i < count; i++) {
             const auto it = std::find(pc.begin(), pc.end(), d[i]);
-            if (it == pc.end()) continue;
+            if (kinds[i] != kind || it == pc.end()) continue;
             W[it - pc.begin()] += w[i];
             nplates[it - pc.begin()]++;
         }
@@ -531,6 +537,7 @@ std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>
             used += pc[best];
         }
         BatchPhase P;
+        P.kind = kind;
         for (int k = 0; k < nc; k++)
             for (int t = 0; t < teams[k]; t++) {
                 P.team_base.push_back(P.grid);
@@ -541,11 +548,11 @@ std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>
         P.team_load.assign(T, 0.0);
         std::vector<std::vector<int>> q(T);
         for (int i : order) {
-            if (std::find(pc.begin(), pc.end(), d[i]) == pc.end()) continue;
+            if (kinds[i] != kind || std::find(pc.begin(), pc.end(), d[i]) == pc.end()) continue;
             int bt = -1;
             for (int t = 0; t < T; t++)
                 if (P.team_size[t] == d[i] && (bt < 0 || P.team_load[t] < P.team_load[bt])) bt = t;
-            out.plate_phase[i] = (int)ph;
+            out.plate_phase[i] = (int)out.phases.size();
             out.plate_team[i] = bt;
             P.team_load[bt] += w[i];
             q[bt].push_back(i);
@@ -556,6 +563,7 @@ std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>
             P.queue.insert(P.queue.end(), q[t].begin(), q[t].end());
         }
         out.phases.push_back(std::move(P));
+    }
     }
     return "";
 }

@@ -92,8 +92,10 @@ double estimate_lambda_max(const pg_problem& p, const std::vector<double>& ke64,
 // among the team sizes in proportion to their estimated work (sqrt(n)
 // iterations of n + 300 d node-equivalents), one team per size at least,
 // and each size's plates go to its teams longest first to the least-loaded
-// team.
+// team.  Plates of different kinds (element types: the launch's kernel is
+// specialised for one) never share a phase.
 struct BatchPhase {
+    int kind = 4;                         // nodes per element of all its plates
     int grid = 0;                         // blocks of the launch
     std::vector<int> team_base, team_size;
     std::vector<int> queue_off, queue;    // per team, plates in solve order
@@ -103,8 +105,8 @@ struct BatchSchedule {
     std::vector<BatchPhase> phases;
     std::vector<int> plate_phase, plate_team, plate_size;  // [count]; team index within its phase
 };
-std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>& caps, int sms,
-                           BatchSchedule& out);
+std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>& caps,
+                           const std::vector<int>& kinds, int sms, BatchSchedule& out);
 
 // 64-bit FNV-1a over the problem's mesh, colouring, material and
 // constraint arrays (not F): the key of the plan cache.

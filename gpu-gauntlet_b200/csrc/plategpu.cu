@@ -106,7 +106,7 @@ struct pg_plan {
 // size of the team of blocks that solves it, and the team schedule (one
 // launch per phase).
 struct BatchPhaseDev {
-    int grid = 0;
+    int grid = 0, kind = 4;
     DevBuf<int> block_team, team_base, queue_off, queue;
 };
 struct pg_batch {
@@ -119,8 +119,7 @@ struct pg_batch {
     DevBuf<pg::PcgArgs> args;
     DevBuf<pg::PcgResult> res;
     DevBuf<unsigned long long> times;
-    int ok_smem = 0;
-    const void* ok_fn = nullptr;
+    int ok_smem = 0, ok_precision = 0;
     std::vector<std::vector<float>> hF;   // each plate's current load (for the FP64 fallback)
     std::unique_ptr<pg_batch> fb;         // FP64 batch of the plates whose mixed solve stagnated
     std::vector<int> fb_ids;              // its plates
@@ -800,10 +799,11 @@ std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int co
     }
     // schedule, then check every plate's layout at its team size; lower the
     // capacity of the plates whose parts do not fit and reschedule
-    std::vector<int> caps(count);
+    std::vector<int> caps(count), kinds(count);
+    for (int i = 0; i < count; i++) kinds[i] = (int)probs[i].nodes_per_element;
     for (int i = 0; i < count; i++) caps[i] = batch_capacity(o, b->rings, (int)probs[i].nodes_per_element);
     for (int attempt = 0;; attempt++) {
-        std::string e = pg::schedule_batch(nodes, caps, c->sms, b->sched);
+        std::string e = pg::schedule_batch(nodes, caps, kinds, c->sms, b->sched);
         if (!e.empty()) throw Fail{PG_EUNSUPPORTED, e};
         b->plans.clear();
         bool fits = true;
@@ -829,6 +829,7 @@ std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int co
         for (size_t t = 0; t < P.team_size.size(); t++)
             for (int k = 0; k < P.team_size[t]; k++) bt[P.team_base[t] + k] = (int)t;
         d->grid = P.grid;
+        d->kind = P.kind;
         d->block_team.upload(bt.data(), bt.size(), st);
         d->team_base.upload(P.team_base.data(), P.team_base.size(), st);
         d->queue_off.upload(P.queue_off.data(), P.queue_off.size(), st);
@@ -905,20 +906,29 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
     CK(cudaMemsetAsync(b->abort_flag.p, 0, sizeof(int), st));
     CK(cudaMemsetAsync(b->times.p, 0, b->times.n * sizeof(unsigned long long), st));
     const bool mixed = o.precision == PG_PREC_MIXED;
-    const void* fn = mixed ? (const void*)pg::pcg_batch_kernel<float, true>
-                           : (const void*)pg::pcg_batch_kernel<double, false>;
-    opt_in_smem(c, fn);
+    auto kernel_of = [&](int kind) {
+        if (kind == 4)
+            return mixed ? (const void*)pg::pcg_batch_kernel<4, float, true>
+                         : (const void*)pg::pcg_batch_kernel<4, double, false>;
+        return mixed ? (const void*)pg::pcg_batch_kernel<3, float, true>
+                     : (const void*)pg::pcg_batch_kernel<3, double, false>;
+    };
     int grid_max = 0;
     for (auto& ph : b->phases) grid_max = std::max(grid_max, ph->grid);
-    if (b->ok_fn != fn || b->ok_smem != smem) {
-        int nb = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, pg::kMaxThreads, smem));
-        if (nb < 1 || nb * c->sms < grid_max)
-            throw Fail{PG_EUNSUPPORTED, "batch grid does not fit on the device"};
-        b->ok_fn = fn;
+    if (b->ok_precision != (mixed ? 1 : 2) || b->ok_smem != smem) {
+        for (int kind : {3, 4}) {
+            const void* fk = kernel_of(kind);
+            opt_in_smem(c, fk);
+            int nb = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fk, pg::kMaxThreads, smem));
+            if (nb < 1 || nb * c->sms < grid_max)
+                throw Fail{PG_EUNSUPPORTED, "batch grid does not fit on the device"};
+        }
+        b->ok_precision = mixed ? 1 : 2;  // residency checked for this precision and size
         b->ok_smem = smem;
     }
     for (auto& ph : b->phases) {  // one persistent launch per phase, back to back
+        const void* fn = kernel_of(ph->kind);
         pg::BatchArgs ba{b->args.p, ph->block_team.p, ph->team_base.p, ph->queue_off.p, ph->queue.p,
                          b->times.p};
         void* args[] = {&ba};
@@ -1426,7 +1436,8 @@ int pg_batch_schedule(const uint32_t* node_counts, int count, int sms, int cap, 
     try {
         std::vector<int> nodes(node_counts, node_counts + count);
         pg::BatchSchedule S;
-        if (!pg::schedule_batch(nodes, std::vector<int>(count, cap), sms, S).empty()) return PG_EUNSUPPORTED;
+        if (!pg::schedule_batch(nodes, std::vector<int>(count, cap), std::vector<int>(count, 4), sms, S).empty())
+            return PG_EUNSUPPORTED;
         for (int i = 0; i < count; i++) {
             plate_phase[i] = S.plate_phase[i];
             plate_size[i] = S.plate_size[i];
