@@ -106,9 +106,12 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:  # host-only runs of the plumbing (tests)
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
@@ -125,7 +128,8 @@ def max_over_ranks(world, value, local):
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dev = f"cuda:{local}" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -433,6 +437,8 @@ def run_plategpu(args, world, rank, local):
         e2e.append((time.perf_counter() - t0) * 1e3)
     barrier(world)
     e2e_value = max_over_ranks(world, sum(e2e), local) / (world * e2e_steps)
+    # every rank takes part in the batch (its share of the plates)
+    batch = batch_bench(args, ctx, chk is not None, world, rank, local) if args.batch > 0 else None
 
     if rank != 0:
         ctx.close()
@@ -478,8 +484,8 @@ def run_plategpu(args, world, rank, local):
         "clocks": clocks,
         "accuracy": H.get("accuracy"),
     }
-    if args.batch > 0 and world == 1:
-        line["batch"] = batch_bench(args, ctx, chk is not None)
+    if batch is not None:
+        line["batch"] = batch
     if chk is not None:
         line["cpu_baseline"] = {
             "value": chk["ref_ms"], "unit": "ms", "cores": 1, "kind": "port",
@@ -492,14 +498,18 @@ def run_plategpu(args, world, rank, local):
     ctx.close()
 
 
-def batch_bench(args, ctx, check):
+def batch_bench(args, ctx, check, world=1, rank=0, local=0):
     """The uneven-plate batch (batched solver, one persistent launch per
     phase): solves/s and per-plate p50 / p99 / max, FP64 error on a seeded
-    sample of plates when the checker runs."""
+    sample of plates when the checker runs.  With N ranks the plates are
+    shared out by estimated cost (no collective on the data path); the batch
+    time is the largest over the ranks."""
     import numpy as np
     from plategpu import _lib, workloads
 
-    B = workloads.batch_uneven(count=args.batch)
+    ALL = workloads.batch_uneven(count=args.batch)
+    shards = workloads.shard_lpt([workloads.plate_cost(w) for w in ALL], world)
+    B = [ALL[i] for i in shards[rank]]
     probs = [_lib.Problem(w.mesh, w.material, w.coloring, w.F, w.cons_mask) for w in B]
     # 2e-7: the DKT plates need a tighter residual than the Q4 ones for 1e-6 error
     opts = _lib.make_options(tolerance=2e-7, max_iterations=20000, stop_rule=_lib.PG_STOP_RELATIVE,
@@ -508,21 +518,23 @@ def batch_bench(args, ctx, check):
     b.solve(opts, want_x=False)  # first solve: coarse matrices, set-up kernels
     ms, last = [], None
     for k in range(max(1, args.batch_steps)):
+        barrier(world)
         xs, infos, bi = b.solve(opts, want_x=(k == max(1, args.batch_steps) - 1))
-        ms.append(bi.solve_ms)
+        ms.append(max_over_ranks(world, bi.solve_ms, local))
         last = (xs, infos, bi)
     b.close()
     xs, infos, bi = last
     med = statistics.median(ms)
     its = [i.iterations for i in infos]
     out = {"workload": ("batch_uneven: %d plates, elements per side log-uniform 16-256, 70%% Q4 / "
-                        "30%% DKT, random material, supports and random-field loads" % len(B)),
-           "dof_total": int(sum(3 * w.mesh.nodeCount for w in B)),
+                        "30%% DKT, random material, supports and random-field loads" % len(ALL)),
+           "dof_total": int(sum(3 * w.mesh.nodeCount for w in ALL)),
+           "ranks": world, "plates_per_rank": [len(sh) for sh in shards],
            "method": "mixed_two_level, FP64 re-solve (as a batch) of plates whose mixed solve stagnates",
-           "stop": "||r||/||b|| < 2e-7", "solves_per_s": len(B) / (med * 1e-3), "batch_ms": med,
+           "stop": "||r||/||b|| < 2e-7", "solves_per_s": len(ALL) / (med * 1e-3), "batch_ms": med,
            "batch_ms_all": ms, "plate_ms_p50": bi.plate_ms_p50, "plate_ms_p99": bi.plate_ms_p99,
            "plate_ms_max": bi.plate_ms_max, "phases": bi.phases, "teams": bi.teams,
-           "fallbacks": bi.fallbacks, "converged": bi.converged,
+           "fallbacks_rank0": bi.fallbacks, "converged_rank0": bi.converged,
            "iterations_median": float(np.median(its)), "iterations_max": int(max(its))}
     if check:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))

@@ -211,6 +211,27 @@ def batch_uneven(count: int = 256, seed: int = 5, min_side: int = 16,
     return out
 
 
+def plate_cost(w: Workload) -> float:
+    """Estimated solve work of a plate: about sqrt(n) iterations over n nodes."""
+    n = float(w.mesh.nodeCount)
+    return n * np.sqrt(n)
+
+
+def shard_lpt(costs, parts: int) -> List[List[int]]:
+    """Longest-processing-time assignment of items to `parts` shards: items
+    by decreasing cost (index order on ties) each go to the currently
+    lightest shard (lowest index on ties).  Deterministic, so every rank
+    computes the same shards."""
+    order = sorted(range(len(costs)), key=lambda i: (-float(costs[i]), i))
+    load = [0.0] * parts
+    out: List[List[int]] = [[] for _ in range(parts)]
+    for i in order:
+        k = min(range(parts), key=lambda j: (load[j], j))
+        out[k].append(i)
+        load[k] += float(costs[i])
+    return [sorted(sh) for sh in out]
+
+
 WORKLOADS = {
     "plate_q4_32": plate_q4_32,
     "plate_q4_141": plate_q4_141,

@@ -50,3 +50,14 @@ def test_schedule_rejects_a_plate_larger_than_the_device():
         _lib.batch_schedule([148 * 520 + 1], 148, 520)
     with pytest.raises(_lib.PlateGPUError):  # the 257^2-node plates need 447 nodes per block
         _lib.batch_schedule(uneven_node_counts(), 148, 300)
+
+
+def test_shard_lpt_balances_and_covers():
+    from plategpu.workloads import shard_lpt
+    costs = [float(n) ** 1.5 for n in uneven_node_counts()]
+    for parts in (1, 2, 4, 8):
+        sh = shard_lpt(costs, parts)
+        assert sorted(i for s in sh for i in s) == list(range(len(costs)))
+        loads = [sum(costs[i] for i in s) for s in sh]
+        assert max(loads) <= sum(loads) / parts + max(costs) + 1e-9  # LPT bound
+    assert shard_lpt([3.0, 1.0, 2.0], 2) == [[0], [1, 2]]
