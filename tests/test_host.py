@@ -138,3 +138,51 @@ def test_oracle_moments_of_a_pure_bending_field(oracle):
         assert np.allclose(Mx, D * (c + nu * d), rtol=1e-6)
         assert np.allclose(My, D * (d + nu * c), rtol=1e-6)
         assert np.abs(Mxy).max() < 1e-6 * abs(D * c)
+
+
+def test_unstructured_mesh_colouring_and_plans(oracle):
+    """A plate with holes (Delaunay triangles, shuffled node numbers): greedy
+    colouring agrees with the oracle and is valid, and the host partition
+    keeps its invariants at several part counts and both halo widths."""
+    import unstructured as U
+    from plategpu import _lib
+
+    wl = U.workload(h=0.2)
+    m = wl.mesh
+    el = m.elements.reshape(-1, 3)
+    xy = m.nodes.reshape(-1, 2).astype(np.float64)
+    d = xy[el]
+    area2 = (d[:, 1, 0] - d[:, 0, 0]) * (d[:, 2, 1] - d[:, 0, 1]) - \
+        (d[:, 2, 0] - d[:, 0, 0]) * (d[:, 1, 1] - d[:, 0, 1])
+    assert (area2 > 0).all()
+    assert col.verifyColoring(m, wl.coloring)
+    ec, flat, _counts = oracle.color_greedy(m.nodeCount, m.elementCount, 3, m.elements)
+    np.testing.assert_array_equal(ec, wl.coloring.elementColors)
+    np.testing.assert_array_equal(np.concatenate(wl.coloring.colors), flat)
+    pr = _lib.Problem(m, wl.material, wl.coloring, wl.F, wl.cons_mask)
+    for ctas in (5, 37, 148):
+        for rings in (1, 2):
+            st = _lib.plan_inspect(pr, ctas, rings=rings)
+            assert st["violations"] == 0 and st["parts"] == ctas and st["recolored"] == 0
+
+
+def test_reference_dkt_zero_mode_at_third_vertex_nodes(oracle):
+    """The reference's DKT element (element.ts:642-943 as written) leaves a
+    zero-energy mode at every free node that is the third vertex of all its
+    triangles; the test meshes rotate vertex lists so that none is."""
+    import unstructured as U
+
+    for rotate in (False, True):
+        wl = U.workload(h=0.5, rotate=rotate)
+        m, mat = wl.mesh, wl.material
+        el = m.elements.reshape(-1, 3)
+        front = np.zeros(m.nodeCount, bool)
+        front[el[:, 0]] = True
+        front[el[:, 1]] = True
+        free = ~wl.cons_mask.reshape(-1, 3).all(1)
+        third_only = int((~front & free).sum())
+        ke = oracle.all_ke(m.nodes, m.elements, 3, mat.E, mat.nu, mat.t, elem_t=mat.elem_t, mode=oracle.FP64)
+        w = np.linalg.eigvalsh(oracle.assemble(m.nodeCount, m.elements, 3, ke, wl.cons_mask).toarray())
+        zero = int((np.abs(w) < 1e-14 * w[-1]).sum())
+        assert zero == third_only
+        assert (third_only > 0) == (not rotate)
