@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "multi.cuh"
 #include "plan.h"
 #include "plategpu.h"
 
@@ -93,6 +94,17 @@ struct Plan {
     DevBuf<int> abort_flag;
     DevBuf<unsigned long long> trace;
     DevBuf<pg::PcgResult> res;
+    // load cases solved together (NR cases per launch): their loads,
+    // solutions, exchange buffers and result records
+    int m_nr = 0;
+    unsigned m_tag0 = 0;
+    bool m_ready = false;
+    const void* m_ok_fn = nullptr;
+    int m_ok_smem = 0;
+    DevBuf<float> mF;
+    DevBuf<double> mx;
+    DevBuf<unsigned long long> mllv, mllx, mllp;
+    DevBuf<pg::PcgResult> mres;
 };
 
 }  // namespace
@@ -199,6 +211,53 @@ pg::SmemLayout make_layout(const pg::HostPlan& hp, bool mixed, int ke_mode, bool
     L.u = take(3 * nloc * T);
     if (mixed)
         L.ytd = 3 * ntask_own * 8 <= off - (size_t)L.yt ? L.yt : take(3 * ntask_own * 8);
+    L.kt = take(ke_mode == 2 ? 3 * nd * ntask * T : ke_mode == 1 ? 3 * nd * ntask_own * T : 0);
+    L.nb = take(coarse ? 3 * nloc * T : 0);
+    L.ainv = take(coarse && ainv_smem ? (size_t)3 * hp.max_kagg * hp.C * T : 0);
+    L.nslot = take(coarse ? nloc * 4 : 0);
+    L.gid = take(nloc * 4);
+    L.tptr = take((n1 + 1) * 4);
+    L.tnode = take(hp.npe * ntask * 2);
+    L.cm = take(3 * nloc);
+    L.total = (int)off;
+    return L;
+}
+
+// Shared-memory layout of a launch of NR load cases: every per-DOF vector
+// and the task results hold NR values per entry; the partial sums 6 per case.
+pg::SmemLayout make_layout_multi(const pg::HostPlan& hp, bool mixed, int ke_mode, bool coarse,
+                                 bool ainv_smem, int NR) {
+    const size_t T = mixed ? 4 : 8, nd = 3 * hp.npe, R = NR;
+    const size_t nloc = hp.max_nloc, nown = hp.max_nown, ntask = hp.max_ntask;
+    const size_t ntask_own = hp.max_ntask_own, n1 = std::max(hp.max_n1, hp.max_nown);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const int o = (int)off;
+        off = (off + bytes + 15) & ~(size_t)15;
+        return o;
+    };
+    pg::SmemLayout L{};
+    L.x = take(3 * nown * 8 * R);
+    L.xl = take(mixed ? 3 * nloc * 8 * R : 0);
+    L.red = take(32 * 6 * R * 8);  // [warps][6 NR]
+    L.scal = take(5 * R * 8);      // dots, alpha, beta per case
+    L.sp = take((size_t)6 * R * hp.G * 8);
+    L.qw = take(coarse ? 3 * (size_t)hp.max_kagg * 8 * R : 0);
+    L.cs = take(coarse ? 2 * 3 * (size_t)hp.max_kagg * 8 * R : 0);
+    L.cv = take(coarse ? 2 * 3 * (size_t)hp.max_kagg * 8 * R : 0);
+    L.ctl = take(4 * 4);
+    L.clk = take(8 * 8);
+    L.r = take(3 * nloc * T * R);
+    L.p = take(3 * nloc * T * R);
+    L.s = take(3 * nloc * T * R);
+    L.B = take(9 * nloc * T);
+    // yt, w, u back to back: the FP64 residual's task results (ytd) reuse
+    // them when they fit (u is rebuilt from r after every replacement)
+    L.yt = take(3 * ntask * T * R);
+    L.w = take(3 * nloc * T * R);
+    L.u = take(3 * nloc * T * R);
+    if (mixed)
+        L.ytd = 3 * ntask_own * 8 * R <= off - (size_t)L.yt ? L.yt : take(3 * ntask_own * 8 * R);
     L.kt = take(ke_mode == 2 ? 3 * nd * ntask * T : ke_mode == 1 ? 3 * nd * ntask_own * T : 0);
     L.nb = take(coarse ? 3 * nloc * T : 0);
     L.ainv = take(coarse && ainv_smem ? (size_t)3 * hp.max_kagg * hp.C * T : 0);
@@ -730,6 +789,156 @@ void solve_with_fallback(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info
     fi->solve_ms += first_ms;
 }
 
+// Layout of an NR-case launch: the first of the single solve's preferences
+// that fits; false when none does (the plate's parts are then solved with
+// fewer cases per launch).
+bool choose_layout_multi(pg_ctx* c, const pg::HostPlan& hp, const pg_options& o, int NR, int* ke_mode,
+                         bool* ainv_smem, pg::SmemLayout* out) {
+    const bool mixed = o.precision == PG_PREC_MIXED, coarse = o.preconditioner == PG_PRECOND_TWO_LEVEL;
+    const int full = hp.rings == 2 ? 2 : 1;
+    const bool ke_first = 3 * 3 * hp.npe * (size_t)hp.max_ntask_own >= (size_t)3 * hp.max_kagg * hp.C;
+    const int cand[6][2] = {{full, 1}, {1, 1}, {ke_first ? full : 0, ke_first ? 0 : 1},
+                            {ke_first ? 1 : 0, ke_first ? 0 : 1}, {0, 1}, {0, 0}};
+    for (auto& cd : cand) {
+        *ke_mode = cd[0];
+        *ainv_smem = coarse && cd[1];
+        *out = make_layout_multi(hp, mixed, *ke_mode, coarse, *ainv_smem, NR);
+        if (out->total <= c->max_smem) return true;
+    }
+    return false;
+}
+
+const void* multi_kernel(int npe, bool mixed, int NR) {
+    if (npe == 4) {
+        if (NR == 2) return mixed ? (const void*)pg::pcg_multi_kernel<4, float, true, 2>
+                                  : (const void*)pg::pcg_multi_kernel<4, double, false, 2>;
+        return mixed ? (const void*)pg::pcg_multi_kernel<4, float, true, 4>
+                     : (const void*)pg::pcg_multi_kernel<4, double, false, 4>;
+    }
+    if (NR == 2) return mixed ? (const void*)pg::pcg_multi_kernel<3, float, true, 2>
+                              : (const void*)pg::pcg_multi_kernel<3, double, false, 2>;
+    return mixed ? (const void*)pg::pcg_multi_kernel<3, float, true, 4>
+                 : (const void*)pg::pcg_multi_kernel<3, double, false, 4>;
+}
+
+// count <= NR load cases of plan pl in one launch of the NR-case kernel
+// (cases count..NR-1 get a zero load and stop at once).  F[k] / x[k] are
+// host vectors of 3 Nn; infos (optional) gets one record per case.  Cases
+// whose mixed solve stagnated are solved again, one by one, in FP64.
+void run_solve_multi(pg_ctx* c, Plan* pl, const pg_options& o, int NR, int count, const float* const* F,
+                     double* const* x, pg_info* infos) {
+    const pg::HostPlan& hp = pl->hp;
+    const bool mixed = o.precision == PG_PREC_MIXED;
+    const size_t n = 3 * (size_t)hp.Nn;
+    prepare_plan_data(c, pl, o);
+    int ke_mode = 0;
+    bool ainv_smem = false;
+    pg::SmemLayout L{};
+    if (!choose_layout_multi(c, hp, o, NR, &ke_mode, &ainv_smem, &L))
+        throw Fail{PG_EUNSUPPORTED, "load-case partition too large for shared memory"};
+    cudaStream_t st = c->stream;
+    if (pl->m_nr != NR) {
+        pl->mF.alloc(n * NR);
+        pl->mx.alloc(n * NR);
+        pl->mllv.alloc(2 * n * NR * 2);
+        pl->mllx.alloc(n * NR * 2);
+        pl->mllp.alloc(2 * (size_t)pg::kRep * pl->G * pg::multi_slot_words<4>() + 2);
+        pl->mres.alloc(NR);
+        pl->m_nr = NR;
+        pl->m_ready = false;
+    }
+    ensure_staging(c, n * NR);
+    for (int k = 0; k < NR; k++) {
+        if (k < count)
+            std::memcpy(c->hF + k * n, F[k], n * sizeof(float));
+        else
+            std::memset(c->hF + k * n, 0, n * sizeof(float));
+    }
+    CK(cudaEventRecord(c->ev[0], st));
+    run_setup(c, pl);
+    CK(cudaMemcpyAsync(pl->mF.p, c->hF, n * NR * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(c->ev[1], st));
+    if (!pl->m_ready || pl->m_tag0 > 0xf0000000u) {
+        CK(cudaMemsetAsync(pl->mllv.p, 0, pl->mllv.n * sizeof(unsigned long long), st));
+        CK(cudaMemsetAsync(pl->mllx.p, 0, pl->mllx.n * sizeof(unsigned long long), st));
+        CK(cudaMemsetAsync(pl->mllp.p, 0, pl->mllp.n * sizeof(unsigned long long), st));
+        pl->m_tag0 = 0;
+    }
+    pl->m_ready = false;
+    CK(cudaMemsetAsync(pl->mres.p, 0, NR * sizeof(pg::PcgResult), st));
+    CK(cudaMemsetAsync(pl->abort_flag.p, 0, sizeof(int), st));
+    pg::PcgArgs a = fill_args(pl, o, L, ke_mode, ainv_smem, pl->abort_flag.p, pl->mres.p);
+    a.F = pl->mF.p;
+    a.x = pl->mx.p;
+    a.llv = pl->mllv.p;
+    a.llx = pl->mllx.p;
+    a.llp = pl->mllp.p;
+    a.tag0 = pl->m_tag0;
+    a.timing = 0;
+    a.test_stall = 0;
+    a.trace_it = -1;
+    const void* fn = multi_kernel(hp.npe, mixed, NR);
+    opt_in_smem(c, fn);
+    if (pl->m_ok_fn != fn || pl->m_ok_smem != L.total) {
+        int nb = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, pg::kMaxThreads, L.total));
+        if (nb < 1 || nb * c->sms < pl->G)
+            throw Fail{PG_EUNSUPPORTED, "load-case grid does not fit on the device"};
+        pl->m_ok_fn = fn;
+        pl->m_ok_smem = L.total;
+    }
+    void* args[] = {&a};
+    CK(cudaLaunchCooperativeKernel(fn, dim3(pl->G), dim3(pg::kMaxThreads), args, L.total, st));
+    CK(cudaEventRecord(c->ev[2], st));
+    std::vector<pg::PcgResult> r(NR);
+    if (x) CK(cudaMemcpyAsync(c->hx, pl->mx.p, n * count * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(r.data(), pl->mres.p, NR * sizeof(pg::PcgResult), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    bool clean = r[0].wait_failures == 0;
+    unsigned last = 0;
+    for (int k = 0; k < NR; k++) {
+        clean = clean && r[k].status == pg::ST_OK;
+        last = std::max(last, r[k].last_tag);
+    }
+    if (clean) {
+        pl->m_tag0 = last;
+        pl->m_ready = true;
+    }
+    float ms_setup = 0, ms_solve = 0;
+    CK(cudaEventElapsedTime(&ms_setup, c->ev[0], c->ev[1]));
+    CK(cudaEventElapsedTime(&ms_solve, c->ev[1], c->ev[2]));
+    if (x)
+        for (int k = 0; k < count; k++) std::memcpy(x[k], c->hx + k * n, n * sizeof(double));
+    for (int k = 0; k < count; k++) {
+        if (infos) {
+            std::memset(&infos[k], 0, sizeof(pg_info));
+            fill_info(&infos[k], r[k], pl, o, pg::kMaxThreads, L.total);
+            infos[k].status = r[k].status;
+            infos[k].setup_ms = ms_setup;
+            infos[k].solve_ms = ms_solve;
+            infos[k].plan_cached = 1;
+        }
+    }
+    if (r[0].wait_failures > 0) throw_on_failure(r[0]);
+    for (int k = 0; k < count; k++) throw_on_failure(r[k]);
+    if (!mixed || !o.fallback) return;
+    pg_options o64 = o;
+    o64.precision = PG_PREC_FP64;
+    for (int k = 0; k < count; k++) {
+        if (r[k].stop_reason != PG_STOP_STAGNATED) continue;
+        CK(cudaMemcpyAsync(pl->F.p, F[k], n * sizeof(float), cudaMemcpyHostToDevice, st));
+        pg_info fi{};
+        run_solve(c, pl, o64, &fi, x ? (void*)x[k] : nullptr, cudaMemcpyDeviceToHost);
+        if (infos) {
+            const double first_ms = infos[k].solve_ms;
+            infos[k] = fi;
+            infos[k].fallback = 1;
+            infos[k].solve_ms += first_ms;
+            infos[k].plan_cached = 1;
+        }
+    }
+}
+
 template <typename F>
 int guarded(pg_ctx* c, pg_info* info, F&& body) {
     if (!c) return PG_EINVAL;
@@ -1165,6 +1374,64 @@ int pg_solve(pg_ctx* c, const pg_problem* p, const pg_options* opt, double* x_ou
         solve_with_fallback(c, pl, o, info, c->hx, cudaMemcpyDeviceToHost);
         std::memcpy(x_out, c->hx, n * sizeof(double));
         if (info) info->plan_cached = cached ? 1 : 0;
+    });
+}
+
+int pg_solve_load_cases(pg_ctx* c, const pg_problem* p, int count, const float* F, const pg_options* opt,
+                        int cases_per_launch, double* x_out, pg_info* infos) {
+    if (infos && count > 0) std::memset(infos, 0, (size_t)count * sizeof(pg_info));
+    return guarded(c, nullptr, [&] {
+        check_problem(p, false);
+        if (count < 1 || !F) throw Fail{PG_EINVAL, "need count >= 1 load cases and F"};
+        if (cases_per_launch != 0 && cases_per_launch != 1 && cases_per_launch != 2 && cases_per_launch != 4)
+            throw Fail{PG_EINVAL, "cases_per_launch must be 0 (automatic), 1, 2 or 4"};
+        pg_options o;
+        fill_options(opt, &o);
+        const size_t n = 3 * (size_t)p->node_count;
+        if (n && !x_out) throw Fail{PG_EINVAL, "x_out is NULL"};
+        for (size_t i = 0; i < n * count; i++)
+            if (!std::isfinite(F[i])) throw Fail{PG_ENONFINITE, "F contains NaN or Inf"};
+        if (n == 0) {
+            if (infos)
+                for (int k = 0; k < count; k++) { infos[k].converged = 1; infos[k].stop_reason = PG_STOP_ZERO_RHS; }
+            return;
+        }
+        const int G = o.ctas ? std::min(o.ctas, (int)p->node_count) : auto_ctas(c, (int)p->node_count);
+        bool cached = false;
+        Plan* pl = get_plan(c, *p, G, halo_rings(o), &cached);
+        prepare_plan_data(c, pl, o);
+        // widest group whose layout fits (automatic: 4, else 2, else 1)
+        auto fits = [&](int NR) {
+            int km = 0;
+            bool ai = false;
+            pg::SmemLayout L{};
+            return choose_layout_multi(c, pl->hp, o, NR, &km, &ai, &L);
+        };
+        int W = cases_per_launch;
+        if (W == 0) W = fits(4) ? 4 : fits(2) ? 2 : 1;
+        else if (W > 1 && !fits(W)) throw Fail{PG_EUNSUPPORTED, "load-case partition too large for shared memory"};
+        for (int k0 = 0; k0 < count;) {
+            const int m = std::min(W, count - k0);
+            std::vector<const float*> Fk(m);
+            std::vector<double*> xk(m);
+            for (int k = 0; k < m; k++) {
+                Fk[k] = F + (size_t)(k0 + k) * n;
+                xk[k] = x_out + (size_t)(k0 + k) * n;
+            }
+            pg_info* ik = infos ? infos + k0 : nullptr;
+            if (m == 1) {
+                ensure_staging(c, n);
+                std::memcpy(c->hF, Fk[0], n * sizeof(float));
+                CK(cudaMemcpyAsync(pl->F.p, c->hF, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+                solve_with_fallback(c, pl, o, ik, c->hx, cudaMemcpyDeviceToHost);
+                std::memcpy(xk[0], c->hx, n * sizeof(double));
+            } else {
+                run_solve_multi(c, pl, o, (m == 2 && (W == 2 || fits(2))) ? 2 : W, m, Fk.data(), xk.data(), ik);
+            }
+            if (ik)
+                for (int k = 0; k < m; k++) ik[k].plan_cached = (cached || k0 > 0) ? 1 : 0;
+            k0 += m;
+        }
     });
 }
 

@@ -13,7 +13,8 @@ from .coloring import (computeElementColoring, computeElementColoringGreedy, get
                        verifyColoring)
 from .problem import (applyBCsToRHS, buildLoadVector, constrained_mask, identifyConstrainedDOFs,
                       pressure_load_vector)
-from .solver import clearPipelineCache, isWebGPUAvailable, solveGPU, solveGPUAsync
+from .solver import (clearPipelineCache, isWebGPUAvailable, solveGPU, solveGPUAsync,
+                     solveGPULoadCases)
 from .postprocess import (computeMoments, extractVerticalDisplacements, findMaxDisplacement,
                           findMaxMoments)
 from ._lib import PlateGPUError

@@ -20,6 +20,8 @@ PG_PREC_FP64, PG_PREC_MIXED = 0, 1
 PG_STOP_REFERENCE, PG_STOP_RELATIVE = 0, 1
 PG_PRECOND_BLOCK_JACOBI, PG_PRECOND_TWO_LEVEL = 0, 1
 PG_SMOOTHER_BLOCK_JACOBI, PG_SMOOTHER_CHEBYSHEV = 0, 1
+(PG_STOP_CONVERGED, PG_STOP_MAX_ITER, PG_STOP_BREAKDOWN, PG_STOP_ZERO_RHS,
+ PG_STOP_STAGNATED) = range(5)  # pg_stop_reason
 STOP_REASONS = {0: "converged", 1: "max_iterations", 2: "breakdown", 3: "zero_rhs",
                 4: "stagnated"}
 
@@ -29,7 +31,7 @@ EXPORTED = ("pg_options_default", "pg_is_available", "pg_create", "pg_destroy", 
             "pg_plan_destroy", "pg_apply_k", "pg_apply_k_static",
             "pg_block_jacobi", "pg_element_stiffness", "pg_plan_inspect",
             "pg_plan_inspect_halo", "pg_batch_create", "pg_batch_solve", "pg_batch_destroy",
-            "pg_solve_batch", "pg_batch_schedule", "pg_moments", "pg_plan_moments_device")
+            "pg_solve_batch", "pg_batch_schedule", "pg_moments", "pg_plan_moments_device", "pg_solve_load_cases")
 
 
 class PgProblem(C.Structure):
@@ -167,6 +169,8 @@ def load() -> C.CDLL:
     L.pg_set_stream.restype = I
     L.pg_solve.argtypes = [P, C.POINTER(PgProblem), C.POINTER(PgOptions), P, C.POINTER(PgInfo)]
     L.pg_solve.restype = I
+    L.pg_solve_load_cases.argtypes = [P, C.POINTER(PgProblem), I, P, C.POINTER(PgOptions), I, P, P]
+    L.pg_solve_load_cases.restype = I
     L.pg_plan_create.argtypes = [P, C.POINTER(PgProblem), C.POINTER(PgOptions), C.POINTER(P)]
     L.pg_plan_create.restype = I
     L.pg_plan_solve_device.argtypes = [P, C.POINTER(PgOptions), P, P, C.POINTER(PgInfo)]
@@ -329,6 +333,20 @@ class Context:
         st = self.L.pg_solve(self.h, C.byref(prob.struct), C.byref(opts), _ptr(x), C.byref(info))
         self._check(st)
         return x, info
+
+    def solve_load_cases(self, prob: Problem, F, opts: PgOptions, cases_per_launch: int = 0):
+        """pg_solve_load_cases: F [k][3 Nn] loads of one plate -> (x [k][3 Nn]
+        FP64, list of k PgInfo)."""
+        F = np.ascontiguousarray(F, np.float32)
+        if F.ndim != 2:
+            raise ValueError("F must be [cases][3 * node_count]")
+        k = F.shape[0]
+        x = np.zeros(F.shape, np.float64)
+        infos = (PgInfo * k)()
+        st = self.L.pg_solve_load_cases(self.h, C.byref(prob.struct), k, _ptr(F), C.byref(opts),
+                                        int(cases_per_launch), _ptr(x), infos)
+        self._check(st)
+        return x, list(infos)
 
     def plan(self, prob: Problem, opts: PgOptions) -> "DevicePlan":
         return DevicePlan(self, prob, opts)

@@ -9,12 +9,14 @@ fields.  Deliberate differences: there is no CPU fallback -- forceCPU, a
 missing library or a missing device raise PlateGPUError instead of quietly
 solving on the CPU (usedGPU is therefore always True); NaN/Inf in F raise
 PG_ENONFINITE.  solveGPUAsync returns an awaitable, as the TypeScript
-function returns a Promise.
+function returns a Promise.  solveGPULoadCases solves several loads of one
+plate together (the reference calls solveGPU once per load).
 """
 from __future__ import annotations
 
 import asyncio
-from typing import Dict, Optional
+import time
+from typing import Dict, List, Optional
 
 import numpy as np
 
@@ -66,6 +68,16 @@ def _option(table, value, name):
     return table[value]
 
 
+def _make_options(options: GPUSolverOptions) -> _lib.PgOptions:
+    return _lib.make_options(
+        tolerance=1e-6 if options.tolerance is None else options.tolerance,
+        max_iterations=1000 if options.maxIterations is None else options.maxIterations,
+        precision=_option(_PREC, options.precision, "precision"),
+        stop_rule=_option(_STOP, options.stopRule, "stopRule"),
+        preconditioner=_option(_PRECOND, options.preconditioner, "preconditioner"),
+        smoother=_option(_SMOOTHER, options.smoother, "smoother"))
+
+
 def solveGPU(mesh: PlateMesh, material: PlateMaterial, coloring: Optional[ElementColoring],
              F: np.ndarray, constrainedDOFs, options: Optional[GPUSolverOptions] = None,
              device: int = 0) -> GPUSolveResult:
@@ -78,13 +90,7 @@ def solveGPU(mesh: PlateMesh, material: PlateMaterial, coloring: Optional[Elemen
     if F.size != 3 * mesh.nodeCount:
         raise _lib.PlateGPUError(_lib.PG_EINVAL,
                                  f"F has {F.size} entries, expected {3 * mesh.nodeCount}")
-    opts = _lib.make_options(
-        tolerance=1e-6 if options.tolerance is None else options.tolerance,
-        max_iterations=1000 if options.maxIterations is None else options.maxIterations,
-        precision=_option(_PREC, options.precision, "precision"),
-        stop_rule=_option(_STOP, options.stopRule, "stopRule"),
-        preconditioner=_option(_PRECOND, options.preconditioner, "preconditioner"),
-        smoother=_option(_SMOOTHER, options.smoother, "smoother"))
+    opts = _make_options(options)
     ctx = get_context(device)
     prob = _lib.Problem(mesh, material, coloring, F, _mask(mesh, constrainedDOFs))
     x, info = ctx.solve(prob, opts)
@@ -93,6 +99,35 @@ def solveGPU(mesh: PlateMesh, material: PlateMaterial, coloring: Optional[Elemen
                           finalResidual=float(info.final_residual),
                           converged=bool(info.converged), gpuTimeMs=float(info.total_ms),
                           usedGPU=True, info=info.as_dict())
+
+
+def solveGPULoadCases(mesh: PlateMesh, material: PlateMaterial, coloring: Optional[ElementColoring],
+                      loads, constrainedDOFs, options: Optional[GPUSolverOptions] = None,
+                      device: int = 0, casesPerLaunch: int = 0) -> List[GPUSolveResult]:
+    """solveGPU for several loads of one plate (pg_solve_load_cases): one
+    GPUSolveResult per load, in order.  The loads share the plate's set-up
+    and run in lockstep, up to casesPerLaunch (0 = automatic) per persistent
+    launch; gpuTimeMs is the wall clock of the whole call."""
+    options = options or GPUSolverOptions()
+    if options.forceCPU:
+        raise _lib.PlateGPUError(_lib.PG_EUNSUPPORTED,
+                                 "forceCPU requested: this solver has no CPU path")
+    F = np.stack([np.asarray(f, np.float32).reshape(-1) for f in loads]) if len(loads) else None
+    if F is None or F.shape[1] != 3 * mesh.nodeCount:
+        raise _lib.PlateGPUError(_lib.PG_EINVAL, f"each load needs {3 * mesh.nodeCount} entries")
+    opts = _make_options(options)
+    ctx = get_context(device)
+    prob = _lib.Problem(mesh, material, coloring, F[0], _mask(mesh, constrainedDOFs))
+    t0 = time.perf_counter()
+    X, infos = ctx.solve_load_cases(prob, F, opts, casesPerLaunch)
+    ms = (time.perf_counter() - t0) * 1e3
+    out = []
+    for x, info in zip(X, infos):
+        out.append(GPUSolveResult(solution=x if options.returnFloat64 else x.astype(np.float32),
+                                  iterations=int(info.iterations), finalResidual=float(info.final_residual),
+                                  converged=bool(info.converged), gpuTimeMs=ms, usedGPU=True,
+                                  info=info.as_dict()))
+    return out
 
 
 async def solveGPUAsync(*args, **kwargs) -> GPUSolveResult:

@@ -27,6 +27,9 @@
  *                    them (gpu/solver.ts:130-131)
  *   pg_is_available  isWebGPUAvailable  src/lib/plate/gpu/context.ts:19
  *   pg_clear_cache   clearPipelineCache src/lib/plate/gpu/solver.ts:601-603
+ *   pg_solve_load_cases  solveGPU called once per load of the same plate
+ *                    (gpu/solver.ts:80-104); the lockstep solve of several
+ *                    loads has no reference counterpart
  *
  * Semantics kept from the reference: F arrives with the boundary conditions
  * applied (applyBCsToRHS); constrained DOFs are identity rows, (K p)_c = p_c,
@@ -203,6 +206,23 @@ int pg_set_stream(pg_ctx* ctx, void* stream);
  * narrows it to the reference's Float32Array).  info may be NULL. */
 int pg_solve(pg_ctx* ctx, const pg_problem* prob, const pg_options* opt, double* x_out,
              pg_info* info);
+
+/* Load cases: solves K x_k = F_k for `count` loads of one plate (prob->F is
+ * not read).  F: [count][3*node_count] float, x_out: [count][3*node_count]
+ * FP64, infos (optional): [count].  Up to cases_per_launch cases (0 =
+ * automatic: 4 when the plate's parts fit in shared memory with four, else
+ * 2, else 1; or 1, 2, 4) run in lockstep in one persistent launch: one
+ * exchange round per iteration for all of them, each element block read
+ * once for all of them, each case with its own PCG scalars and stop.  The
+ * launch runs until its last case stops; each case's info carries that
+ * launch's solve_ms.  In mixed precision a residual replacement asked for
+ * by one case runs for all (only the cases that asked replace their
+ * residual), and a case that stagnates is solved again alone in FP64
+ * (pg_options.fallback).  A solve of one load (pg_solve) is the
+ * reference's solveGPU (gpu/solver.ts:80-104); the reference solves load
+ * cases by calling it once per load. */
+int pg_solve_load_cases(pg_ctx* ctx, const pg_problem* prob, int count, const float* F,
+                        const pg_options* opt, int cases_per_launch, double* x_out, pg_info* infos);
 
 /* Device-resident solves.  A plan holds the partition of one mesh and its
  * device copies (nodes, elements, colouring, constraints, material).  The
