@@ -85,6 +85,9 @@ def parse_args():
     ap.add_argument("--batch", type=int, default=256,
                     help="plates of the uneven batch measured beside the headline (0 = skip)")
     ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--cases", type=int, default=4,
+                    help="load cases of the workload plate solved together (0 = skip)")
+    ap.add_argument("--cases-steps", type=int, default=5)
     args = ap.parse_args()
     bj, tl = TOLERANCES.get(args.workload, (1e-6, 1e-6))
     args.tol_bj = bj if args.tol_bj is None else args.tol_bj
@@ -437,6 +440,8 @@ def run_plategpu(args, world, rank, local):
         e2e.append((time.perf_counter() - t0) * 1e3)
     barrier(world)
     e2e_value = max_over_ranks(world, sum(e2e), local) / (world * e2e_steps)
+    cases = (cases_bench(args, ctx, wl, prob, H, head, chk is not None, world, local)
+             if args.cases > 0 else None)
     # every rank takes part in the batch (its share of the plates)
     batch = batch_bench(args, ctx, chk is not None, world, rank, local) if args.batch > 0 else None
 
@@ -484,6 +489,8 @@ def run_plategpu(args, world, rank, local):
         "clocks": clocks,
         "accuracy": H.get("accuracy"),
     }
+    if cases is not None:
+        line["load_cases"] = cases
     if batch is not None:
         line["batch"] = batch
     if chk is not None:
@@ -496,6 +503,100 @@ def run_plategpu(args, world, rank, local):
         line["cpu_baseline"] = None
     print(json.dumps(line), flush=True)
     ctx.close()
+
+
+def _lib_options_copy(o, **changes):
+    """A copy of a PgOptions with some fields changed."""
+    import ctypes
+
+    c = type(o)()
+    ctypes.memmove(ctypes.byref(c), ctypes.byref(o), ctypes.sizeof(o))
+    for k, v in changes.items():
+        setattr(c, k, v)
+    return c
+
+
+def case_loads(wl, k, seed=21):
+    """k loads of the workload plate: its own load first, then seeded
+    pressures with 16 point loads each (BCs applied)."""
+    import numpy as np
+    from plategpu import problem
+
+    rng = np.random.default_rng(seed)
+    out = [wl.F]
+    for _ in range(k - 1):
+        F = problem.pressure_load_vector(wl.mesh, rng.uniform(1e3, 8e3))
+        for n in rng.choice(wl.mesh.nodeCount, 16, replace=False):
+            F[3 * int(n)] += rng.uniform(1e3, 1e4)
+        F32 = F.astype(np.float32)
+        problem.applyBCsToRHS(F32, wl.constrainedDOFs)
+        out.append(F32)
+    return np.stack(out)
+
+
+def cases_bench(args, ctx, wl, prob, H, method, check, world=1, local=0):
+    """Load cases: args.cases loads of the workload plate through
+    pg_solve_load_cases with the headline method (several cases in lockstep
+    per persistent launch).  Device time of the launches and host wall clock
+    of the whole call, per case, against the same loads solved one by one
+    through pg_solve; FP64 error of every case when the checker runs."""
+    import numpy as np
+
+    F = case_loads(wl, args.cases)
+    # the seeded loads need a tighter stop than the workload's own load for
+    # an FP64-checked error of 1e-6 (5e-6 leaves up to 1.4e-6)
+    opts = _lib_options_copy(H["opts"], tolerance=min(H["opts"].tolerance, 2e-6))
+    for _ in range(2):
+        ctx.solve_load_cases(prob, F, opts)
+    dev, wall, one_dev, one_wall, last = [], [], [], [], None
+    for _ in range(max(1, args.cases_steps)):
+        barrier(world)
+        t0 = time.perf_counter()
+        X, infos = ctx.solve_load_cases(prob, F, opts)
+        wall.append(max_over_ranks(world, (time.perf_counter() - t0) * 1e3, local))
+        # the cases of one launch share its solve_ms
+        launches = {}
+        for i, inf in enumerate(infos):
+            launches.setdefault((inf.solve_ms, inf.setup_ms), i)
+        dev.append(max_over_ranks(world, sum(k[0] for k in launches), local))
+        last = (X, infos)
+        # the same loads one by one (pg_solve)
+        barrier(world)
+        t0 = time.perf_counter()
+        d = 0.0
+        for f in F:
+            prob.set_F(f)
+            d += ctx.solve(prob, opts)[1].solve_ms
+        one_wall.append(max_over_ranks(world, (time.perf_counter() - t0) * 1e3, local))
+        one_dev.append(max_over_ranks(world, d, local))
+    prob.set_F(wl.F)
+    X, infos = last
+    k = args.cases
+    out = {"cases": k, "method": method, "stop": f"||r||/||b|| < {opts.tolerance:g}",
+           "device_ms_per_case": statistics.median(dev) / k,
+           "e2e_ms_per_case": statistics.median(wall) / k,
+           "one_by_one_device_ms_per_case": statistics.median(one_dev) / k,
+           "one_by_one_e2e_ms_per_case": statistics.median(one_wall) / k,
+           "iterations": [int(i.iterations) for i in infos],
+           "reliable_updates": [int(i.reliable_updates) for i in infos],
+           "fallbacks": int(sum(i.fallback for i in infos)),
+           "shared_bytes": int(infos[0].shared_bytes),
+           "h2d_bytes": int(F.nbytes), "d2h_bytes": int(8 * F.size)}
+    out["speedup_device"] = out["one_by_one_device_ms_per_case"] / out["device_ms_per_case"]
+    out["speedup_e2e"] = out["one_by_one_e2e_ms_per_case"] / out["e2e_ms_per_case"]
+    if check:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        m, mat = wl.mesh, wl.material
+        ke = O.all_ke(m.nodes, m.elements, m.nodesPerElement, mat.E, mat.nu, mat.t, elem_t=mat.elem_t,
+                      mode=O.FP64)
+        errs = []
+        for f, x in zip(F, X):
+            xt, _ = O.truth_solve(m.nodeCount, m.elements, m.nodesPerElement, ke, wl.cons_mask,
+                                  f.astype(np.float64))
+            errs.append(float(np.linalg.norm(x - xt) / np.linalg.norm(xt)))
+        out["rel_l2_vs_fp64_truth"] = errs
+    return out
 
 
 def batch_bench(args, ctx, check, world=1, rank=0, local=0):

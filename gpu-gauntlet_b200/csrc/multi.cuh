@@ -363,6 +363,8 @@ __device__ __forceinline__ void pcg_multi_body(const PcgArgs& a, const int g, un
         for (int q = tid; q < nn1 * NR; q += nt) smooth(q / NR);
         __syncthreads();
     }
+    PhaseClock clk;
+    clk.start(a.timing && g == 0 && tid == 0, (long long*)(sm + L.clk));
     Waiter wt;
     wt.start(a.timeout_ns, a.abort_flag, &a.res->wait_failures);
     unsigned e = a.tag0 + 1, xe = a.tag0 + 1;
@@ -411,6 +413,7 @@ __device__ __forceinline__ void pcg_multi_body(const PcgArgs& a, const int g, un
         // ---- w = A u on owned rows, every case ----
         task_matvec_multi<NPE, T, T, NR>(u, yt, nta, ntm, tn, nta, kt, kstride);
         __syncthreads();
+        clk.lap(0);
         // ---- gather, BC rows, dot products, publish w ----
         double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         unsigned long long* vb = a.llv + (size_t)(e & 1) * N3 * NR * 2;
@@ -442,18 +445,21 @@ __device__ __forceinline__ void pcg_multi_body(const PcgArgs& a, const int g, un
                 }
             }
         }
+        clk.lap(1);
         if (a.coarse) {
             block_publish_multi<NR, 6>(v, red, pb, a.G, g, e);
         } else {
             double v3[3] = {v[0], v[1], v[2]};
             block_publish_multi<NR, 3>(v3, red, pb, a.G, g, e);
         }
+        clk.lap(2);
         {
             const bool ok = exchange_round_multi<T, NR>(pb, a.G, KP * NR, vb, w, no, nloc, gid, g, e, sp, wt);
             if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
             sum_partials<3 * NR>(sp, a.G, KP * NR, scal);
         }
         e++;
+        clk.lap(4);
         // ---- decisions: lane k of warp 0 for case k ----
         __syncwarp();
         if (tid < 32) {
@@ -521,11 +527,13 @@ __device__ __forceinline__ void pcg_multi_body(const PcgArgs& a, const int g, un
                 ctl[0] = act;
                 ctl[2] = (int)ru;
             }
+            clk.lap(6);
         }
         if (a.coarse) coarse_apply_multi<T, NR>(Ai, a.G, rows, sp, KP * NR, 3 * NR, qw, 1);
         __syncthreads();
         const int act = ctl[0];
         if (act == ACT_STOP) break;
+        clk.lap(5);
 
         if (MIXED && act == ACT_RU) {
             // ---- FP64 residuals F - K x of every case; the cases that asked
@@ -648,6 +656,7 @@ __device__ __forceinline__ void pcg_multi_body(const PcgArgs& a, const int g, un
             }
             __syncthreads();
             if (ctl[0] == ACT_STOP) break;
+            clk.lap(7);
             continue;
         }
 
@@ -702,9 +711,11 @@ __device__ __forceinline__ void pcg_multi_body(const PcgArgs& a, const int g, un
             }
         }
         __syncthreads();
+        clk.lap(7);
         if (cheb) {
             task_matvec_multi<NPE, T, T, NR>(u, yt, nta, nta, tn, nta, kt, kstride, ksplit, ktg + t0, (size_t)a.NT);
             __syncthreads();
+            clk.lap(3);
             for (int q = tid; q < nn1 * NR; q += nt) {
                 const int n = q / NR;
                 smooth(n);
@@ -715,6 +726,7 @@ __device__ __forceinline__ void pcg_multi_body(const PcgArgs& a, const int g, un
                 }
             }
             __syncthreads();
+            clk.lap(7);
         }
         if (a.coarse) cb ^= 1;
     }
@@ -793,6 +805,7 @@ __device__ __forceinline__ void pcg_multi_body(const PcgArgs& a, const int g, un
         R.reliable_updates = cs.nru;
         R.reductions = (int)(e - 1 - a.tag0);
         R.last_tag = e > xe ? e : xe;
+        for (int k = 0; k < 8; k++) R.phase_cycles[k] = clk.on ? clk.t[k] : 0;
     }
 }
 

@@ -874,7 +874,6 @@ void run_solve_multi(pg_ctx* c, Plan* pl, const pg_options& o, int NR, int count
     a.llx = pl->mllx.p;
     a.llp = pl->mllp.p;
     a.tag0 = pl->m_tag0;
-    a.timing = 0;
     a.test_stall = 0;
     a.trace_it = -1;
     const void* fn = multi_kernel(hp.npe, mixed, NR);
@@ -917,6 +916,7 @@ void run_solve_multi(pg_ctx* c, Plan* pl, const pg_options& o, int NR, int count
             infos[k].setup_ms = ms_setup;
             infos[k].solve_ms = ms_solve;
             infos[k].plan_cached = 1;
+            for (int q = 0; q < 8; q++) infos[k].phase_us[q] = r[0].phase_cycles[q] / (c->clock_khz * 1e-3);
         }
     }
     if (r[0].wait_failures > 0) throw_on_failure(r[0]);
@@ -1400,15 +1400,26 @@ int pg_solve_load_cases(pg_ctx* c, const pg_problem* p, int count, const float* 
         bool cached = false;
         Plan* pl = get_plan(c, *p, G, halo_rings(o), &cached);
         prepare_plan_data(c, pl, o);
-        // widest group whose layout fits (automatic: 4, else 2, else 1)
-        auto fits = [&](int NR) {
-            int km = 0;
+        // group width: automatic = the widest whose layout keeps the Ke
+        // blocks in shared memory, else the widest that fits.  Ke blocks read
+        // from L2 by every block twice per iteration cost more than a wider
+        // group saves (60k-DOF plate, mixed two-level Chebyshev: four cases
+        // per launch with Ke in L2 1.64 ms per case, two with Ke in shared
+        // memory 1.35, one 1.71)
+        auto fits = [&](int NR, int* km = nullptr) {
+            int m = 0;
             bool ai = false;
             pg::SmemLayout L{};
-            return choose_layout_multi(c, pl->hp, o, NR, &km, &ai, &L);
+            const bool ok = choose_layout_multi(c, pl->hp, o, NR, &m, &ai, &L);
+            if (km) *km = m;
+            return ok;
         };
         int W = cases_per_launch;
-        if (W == 0) W = fits(4) ? 4 : fits(2) ? 2 : 1;
+        if (W == 0) {
+            int km4 = 0, km2 = 0;
+            const bool f4 = fits(4, &km4), f2 = fits(2, &km2);
+            W = (f4 && km4 > 0) ? 4 : (f2 && km2 > 0) ? 2 : f4 ? 4 : f2 ? 2 : 1;
+        }
         else if (W > 1 && !fits(W)) throw Fail{PG_EUNSUPPORTED, "load-case partition too large for shared memory"};
         for (int k0 = 0; k0 < count;) {
             const int m = std::min(W, count - k0);

@@ -210,8 +210,9 @@ int pg_solve(pg_ctx* ctx, const pg_problem* prob, const pg_options* opt, double*
 /* Load cases: solves K x_k = F_k for `count` loads of one plate (prob->F is
  * not read).  F: [count][3*node_count] float, x_out: [count][3*node_count]
  * FP64, infos (optional): [count].  Up to cases_per_launch cases (0 =
- * automatic: 4 when the plate's parts fit in shared memory with four, else
- * 2, else 1; or 1, 2, 4) run in lockstep in one persistent launch: one
+ * automatic: the widest of 4 and 2 whose shared-memory layout still holds
+ * the element blocks, else the widest that fits, else 1; or 1, 2, 4) run in
+ * lockstep in one persistent launch: one
  * exchange round per iteration for all of them, each element block read
  * once for all of them, each case with its own PCG scalars and stop.  The
  * launch runs until its last case stops; each case's info carries that
