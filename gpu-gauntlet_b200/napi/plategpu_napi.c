@@ -77,6 +77,8 @@ napi_status napi_create_error(napi_env, napi_value, napi_value, napi_value*);
 napi_status napi_set_named_property(napi_env, napi_value, const char*, napi_value);
 napi_status napi_create_function(napi_env, const char*, size_t, napi_callback, void*, napi_value*);
 napi_status napi_throw_error(napi_env, const char*, const char*);
+napi_status napi_create_array_with_length(napi_env, size_t, napi_value*);
+napi_status napi_set_element(napi_env, napi_value, uint32_t, napi_value);
 #define NAPI_AUTO_LENGTH ((size_t)-1)
 
 /* ---- one solver context per process, created on first use ---- */
@@ -106,6 +108,8 @@ typedef struct {
     pg_info info;
     void* owned[7]; /* copies of the input arrays */
     double* x;
+    int cases;       /* > 0: a load-case job (pg_solve_load_cases), F holds `cases` loads */
+    pg_info* infos;  /* [cases] */
     int status;
     char error[512];
 } SolveJob;
@@ -113,6 +117,7 @@ typedef struct {
 static void job_free(SolveJob* j) {
     for (int i = 0; i < 7; i++) free(j->owned[i]);
     free(j->x);
+    free(j->infos);
     free(j);
 }
 
@@ -161,7 +166,10 @@ static void solve_execute(napi_env env, void* data) {
         strncpy(j->error, pg_last_error(NULL), sizeof j->error - 1);
         return;
     }
-    j->status = pg_solve(ctx, &j->prob, &j->opt, j->x, &j->info);
+    if (j->cases > 0)
+        j->status = pg_solve_load_cases(ctx, &j->prob, j->cases, j->prob.F, &j->opt, 0, j->x, j->infos);
+    else
+        j->status = pg_solve(ctx, &j->prob, &j->opt, j->x, &j->info);
     if (j->status != PG_OK) strncpy(j->error, pg_last_error(ctx), sizeof j->error - 1);
 }
 
@@ -169,6 +177,29 @@ static void set_num(napi_env env, napi_value o, const char* k, double v) {
     napi_value n;
     napi_create_double(env, v, &n);
     napi_set_named_property(env, o, k, n);
+}
+
+/* The result object of case k of a load-case job, or of the one solve (k < 0). */
+static napi_value result_object(napi_env env, const SolveJob* j, int k) {
+    const size_t n = 3 * (size_t)j->prob.node_count;
+    const pg_info* in = k < 0 ? &j->info : &j->infos[k];
+    void* buf = NULL;
+    napi_value ab, arr, res, b;
+    napi_create_arraybuffer(env, n * sizeof(double), &buf, &ab);
+    if (n) memcpy(buf, j->x + (k < 0 ? 0 : (size_t)k * n), n * sizeof(double));
+    napi_create_typedarray(env, napi_float64_array, n, ab, 0, &arr);
+    napi_create_object(env, &res);
+    napi_set_named_property(env, res, "solution", arr);
+    set_num(env, res, "iterations", in->iterations);
+    set_num(env, res, "finalResidual", in->final_residual);
+    napi_get_boolean(env, in->converged != 0, &b);
+    napi_set_named_property(env, res, "converged", b);
+    set_num(env, res, "gpuTimeMs", in->total_ms);
+    set_num(env, res, "trueRelResidual", in->true_rel_residual);
+    set_num(env, res, "setupMs", in->setup_ms);
+    set_num(env, res, "solveMs", in->solve_ms);
+    set_num(env, res, "stopReason", in->stop_reason);
+    return res;
 }
 
 static void solve_complete(napi_env env, napi_status status, void* data) {
@@ -179,31 +210,22 @@ static void solve_complete(napi_env env, napi_status status, void* data) {
         napi_create_string_utf8(env, j->error[0] ? j->error : "solve failed", NAPI_AUTO_LENGTH, &msg);
         napi_create_error(env, code, msg, &err);
         napi_reject_deferred(env, j->deferred, err);
+    } else if (j->cases > 0) {
+        napi_value list;
+        napi_create_array_with_length(env, (size_t)j->cases, &list);
+        for (int k = 0; k < j->cases; k++)
+            napi_set_element(env, list, (uint32_t)k, result_object(env, j, k));
+        napi_resolve_deferred(env, j->deferred, list);
     } else {
-        const size_t n = 3 * (size_t)j->prob.node_count;
-        void* buf = NULL;
-        napi_value ab, arr, res, b;
-        napi_create_arraybuffer(env, n * sizeof(double), &buf, &ab);
-        if (n) memcpy(buf, j->x, n * sizeof(double));
-        napi_create_typedarray(env, napi_float64_array, n, ab, 0, &arr);
-        napi_create_object(env, &res);
-        napi_set_named_property(env, res, "solution", arr);
-        set_num(env, res, "iterations", j->info.iterations);
-        set_num(env, res, "finalResidual", j->info.final_residual);
-        napi_get_boolean(env, j->info.converged != 0, &b);
-        napi_set_named_property(env, res, "converged", b);
-        set_num(env, res, "gpuTimeMs", j->info.total_ms);
-        set_num(env, res, "trueRelResidual", j->info.true_rel_residual);
-        set_num(env, res, "setupMs", j->info.setup_ms);
-        set_num(env, res, "solveMs", j->info.solve_ms);
-        set_num(env, res, "stopReason", j->info.stop_reason);
-        napi_resolve_deferred(env, j->deferred, res);
+        napi_resolve_deferred(env, j->deferred, result_object(env, j, -1));
     }
     napi_delete_async_work(env, j->work);
     job_free(j);
 }
 
-static napi_value js_solve(napi_env env, napi_callback_info info) {
+/* solve(problem) and solveLoadCases(problem): problem.F holds one load, or
+ * problem.cases loads back to back. */
+static napi_value start_job(napi_env env, napi_callback_info info, int load_cases) {
     size_t argc = 1;
     napi_value argv[1], promise, name;
     if (napi_get_cb_info(env, info, &argc, argv, NULL, NULL) != 0 || argc < 1) {
@@ -215,7 +237,7 @@ static napi_value js_solve(napi_env env, napi_callback_info info) {
         napi_throw_error(env, "PG_ENOMEM", "out of memory");
         return NULL;
     }
-    double nn, ne, npe, E, nu, t, tol, maxit, prec, pre, smo, stop;
+    double nn, ne, npe, E, nu, t, tol, maxit, prec, pre, smo, stop, cases;
     napi_value o = argv[0];
     int bad = get_number(env, o, "nodeCount", -1, &nn) | get_number(env, o, "elementCount", -1, &ne) |
               get_number(env, o, "nodesPerElement", 4, &npe) | get_number(env, o, "E", 0, &E) |
@@ -225,8 +247,10 @@ static napi_value js_solve(napi_env env, napi_callback_info info) {
               get_number(env, o, "precision", PG_PREC_FP64, &prec) |
               get_number(env, o, "preconditioner", PG_PRECOND_BLOCK_JACOBI, &pre) |
               get_number(env, o, "smoother", PG_SMOOTHER_BLOCK_JACOBI, &smo) |
-              get_number(env, o, "stopRule", PG_STOP_REFERENCE, &stop);
-    if (bad || nn < 0 || ne < 0 || nn > 67108864.0 || ne > 67108864.0) {
+              get_number(env, o, "stopRule", PG_STOP_REFERENCE, &stop) |
+              get_number(env, o, "cases", 1, &cases);
+    if (!load_cases) cases = 1;
+    if (bad || nn < 0 || ne < 0 || nn > 67108864.0 || ne > 67108864.0 || cases < 1 || cases > 65536.0) {
         job_free(j);
         napi_throw_error(env, "PG_EINVAL", "problem needs nodeCount, elementCount, E, nu, t");
         return NULL;
@@ -248,13 +272,20 @@ static napi_value js_solve(napi_env env, napi_callback_info info) {
         copy_array(env, o, "colorOffsets", napi_uint32_array, 4, ncolors + 1, 1, &j->owned[2]) ||
         copy_array(env, o, "elementsByColor", napi_uint32_array, 4, Ne, 1, &j->owned[3]) ||
         copy_array(env, o, "elemT", napi_float32_array, 4, Ne, 1, &j->owned[4]) ||
-        copy_array(env, o, "F", napi_float32_array, 4, 3 * Nn, 0, &j->owned[5]) ||
+        copy_array(env, o, "F", napi_float32_array, 4, 3 * Nn * (size_t)cases, 0, &j->owned[5]) ||
         copy_array(env, o, "constrained", napi_uint8_array, 1, 3 * Nn, 0, &j->owned[6])) {
         job_free(j);
         napi_throw_error(env, "PG_EINVAL", "problem arrays missing or of the wrong type / length");
         return NULL;
     }
-    j->x = (double*)malloc(3 * Nn * sizeof(double) + 8);
+    j->cases = load_cases ? (int)cases : 0;
+    j->x = (double*)malloc(3 * Nn * (size_t)cases * sizeof(double) + 8);
+    if (load_cases) j->infos = (pg_info*)calloc((size_t)cases, sizeof(pg_info));
+    if (!j->x || (load_cases && !j->infos)) {
+        job_free(j);
+        napi_throw_error(env, "PG_ENOMEM", "out of memory");
+        return NULL;
+    }
     j->prob.node_count = (uint32_t)Nn;
     j->prob.element_count = (uint32_t)Ne;
     j->prob.nodes_per_element = (uint32_t)k;
@@ -287,6 +318,12 @@ static napi_value js_solve(napi_env env, napi_callback_info info) {
     return promise;
 }
 
+static napi_value js_solve(napi_env env, napi_callback_info info) { return start_job(env, info, 0); }
+
+static napi_value js_solve_load_cases(napi_env env, napi_callback_info info) {
+    return start_job(env, info, 1);
+}
+
 static napi_value js_is_available(napi_env env, napi_callback_info info) {
     (void)info;
     napi_value b;
@@ -309,6 +346,8 @@ napi_value napi_register_module_v1(napi_env env, napi_value exports) {
     napi_value f;
     napi_create_function(env, "solve", NAPI_AUTO_LENGTH, js_solve, NULL, &f);
     napi_set_named_property(env, exports, "solve", f);
+    napi_create_function(env, "solveLoadCases", NAPI_AUTO_LENGTH, js_solve_load_cases, NULL, &f);
+    napi_set_named_property(env, exports, "solveLoadCases", f);
     napi_create_function(env, "isAvailable", NAPI_AUTO_LENGTH, js_is_available, NULL, &f);
     napi_set_named_property(env, exports, "isAvailable", f);
     napi_create_function(env, "clearCache", NAPI_AUTO_LENGTH, js_clear_cache, NULL, &f);

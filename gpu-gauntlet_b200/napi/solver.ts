@@ -50,6 +50,7 @@ interface AddonResult {
 
 interface Addon {
   solve(problem: Record<string, unknown>): Promise<AddonResult>;
+  solveLoadCases(problem: Record<string, unknown>): Promise<AddonResult[]>;
   isAvailable(): boolean;
   clearCache(): void;
 }
@@ -86,14 +87,14 @@ export function clearPipelineCache(): void {
   }
 }
 
-export async function solveGPU(
+function addonProblem(
   mesh: PlateMesh,
   material: PlateMaterial,
   coloring: ElementColoring,
   F: Float32Array,
   constrainedDOFs: Set<number>,
-  options: GPUSolverOptions = {}
-): Promise<GPUSolveResult> {
+  options: GPUSolverOptions
+): Record<string, unknown> {
   if (options.forceCPU) {
     throw new Error('PG_EUNSUPPORTED: forceCPU requested; this solver has no CPU path');
   }
@@ -109,7 +110,7 @@ export async function solveGPU(
   for (let c = 0; c < coloring.colorCount; c++) {
     elementsByColor.set(coloring.colors[c], colorOffsets[c]);
   }
-  const r = await loadAddon().solve({
+  return {
     nodeCount: mesh.nodeCount,
     elementCount: mesh.elementCount,
     nodesPerElement,
@@ -128,7 +129,10 @@ export async function solveGPU(
     preconditioner: options.preconditioner === 'two-level' ? 1 : 0,
     smoother: options.smoother === 'chebyshev' ? 1 : 0,
     stopRule: options.stopRule === 'relative' ? 1 : 0,
-  });
+  };
+}
+
+function toResult(r: AddonResult): GPUSolveResult {
   return {
     solution: Float32Array.from(r.solution),
     iterations: r.iterations,
@@ -137,4 +141,44 @@ export async function solveGPU(
     gpuTimeMs: r.gpuTimeMs,
     usedGPU: true,
   };
+}
+
+export async function solveGPU(
+  mesh: PlateMesh,
+  material: PlateMaterial,
+  coloring: ElementColoring,
+  F: Float32Array,
+  constrainedDOFs: Set<number>,
+  options: GPUSolverOptions = {}
+): Promise<GPUSolveResult> {
+  const r = await loadAddon().solve(addonProblem(mesh, material, coloring, F, constrainedDOFs, options));
+  return toResult(r);
+}
+
+/**
+ * Several loads of one plate (the reference calls solveGPU once per load):
+ * the loads run in lockstep on the GPU, up to four per persistent launch,
+ * each with its own iterations and stop.  One result per load, in order;
+ * gpuTimeMs is the wall clock of the whole call.
+ */
+export async function solveGPULoadCases(
+  mesh: PlateMesh,
+  material: PlateMaterial,
+  coloring: ElementColoring,
+  loads: Float32Array[],
+  constrainedDOFs: Set<number>,
+  options: GPUSolverOptions = {}
+): Promise<GPUSolveResult[]> {
+  const n = mesh.nodeCount * 3;
+  const all = new Float32Array(n * loads.length);
+  loads.forEach((f, k) => {
+    if (f.length !== n) throw new Error(`PG_EINVAL: load ${k} has ${f.length} entries, expected ${n}`);
+    all.set(f, k * n);
+  });
+  const problem = addonProblem(mesh, material, coloring, all, constrainedDOFs, options);
+  problem.cases = loads.length;
+  const t0 = Date.now();
+  const rs = await loadAddon().solveLoadCases(problem);
+  const ms = Date.now() - t0;
+  return rs.map((r) => ({ ...toResult(r), gpuTimeMs: ms }));
 }

@@ -22,7 +22,7 @@ def test_addon_builds_and_exports_entry():
     needed = {u for u in undefined if u.startswith("napi_")}
     assert {"napi_create_promise", "napi_create_async_work", "napi_queue_async_work",
             "napi_resolve_deferred", "napi_reject_deferred"} <= needed
-    assert {"pg_solve", "pg_create", "pg_last_error"} <= undefined
+    assert {"pg_solve", "pg_solve_load_cases", "pg_create", "pg_last_error"} <= undefined
 
 
 def test_typescript_wrapper_keeps_reference_signature():
@@ -32,3 +32,4 @@ def test_typescript_wrapper_keeps_reference_signature():
             "  options: GPUSolverOptions = {}\n): Promise<GPUSolveResult>") in src
     for name in ("isWebGPUAvailable", "clearPipelineCache"):
         assert f"export function {name}(" in src
+    assert "export async function solveGPULoadCases(" in src
