@@ -228,6 +228,40 @@ __global__ void bc_copy_kernel(int n, const uint8_t* __restrict__ cons,
     if (i < n && cons[i]) y[i] = x[i];
 }
 
+// r = F - y narrowed to FP32, 0 on constrained rows (y = K x): the load of
+// an FP64 correction solve K d = F - K x.  r may be F itself.
+__global__ void residual_f32_kernel(int n, const uint8_t* cons, const float* F, const double* y, float* r) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = cons[i] ? 0.0f : (float)((double)F[i] - y[i]);
+}
+
+// x += a
+__global__ void add_kernel(int n, const double* __restrict__ a, double* __restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] += a[i];
+}
+
+// out[0] += sum (F - y)^2, out[1] += sum F^2 over the unconstrained rows
+// (y = K x): the true residual of x.  out must start at zero.
+__global__ void residual_norms_kernel(int n, const uint8_t* __restrict__ cons, const float* __restrict__ F,
+                                      const double* __restrict__ y, double* out) {
+    double a = 0.0, b = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (!cons[i]) {
+            const double f = (double)F[i], r = f - y[i];
+            a += r * r;
+            b += f * f;
+        }
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, a);
+        atomicAdd(out + 1, b);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // tagged exchange between blocks (no grid barrier)
 // ---------------------------------------------------------------------------

@@ -105,6 +105,10 @@ struct Plan {
     DevBuf<double> mx;
     DevBuf<unsigned long long> mllv, mllx, mllp;
     DevBuf<pg::PcgResult> mres;
+    // FP64 correction after a stagnated mixed solve: the mixed x, K x and
+    // the FP32 residual
+    DevBuf<double> xw, kx, nrm;
+    DevBuf<float> rf;
 };
 
 }  // namespace
@@ -775,18 +779,93 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_
 // run_solve, and when a mixed solve stagnated (with o.fallback) the same
 // solve again in FP64 on the same plan; info then describes the FP64 solve,
 // with fallback = 1 and solve_ms covering both.
+// y = K x on the device (colour by colour, then the identity rows of the
+// constrained DOFs), queued on the context stream.  The plan's set-up must
+// have run.
+void queue_apply_k(pg_ctx* c, Plan* pl, const double* x, double* y) {
+    const pg::HostPlan& hp = pl->hp;
+    const size_t n = 3 * (size_t)hp.Nn;
+    CK(cudaMemsetAsync(y, 0, n * sizeof(double), c->stream));
+    for (int col = 0; col < hp.colors; col++) {
+        const int off = (int)hp.color_offsets[col], cnt = (int)hp.color_offsets[col + 1] - off;
+        if (cnt > 0)
+            pg::applyk_color_kernel<<<(cnt + 127) / 128, 128, 0, c->stream>>>(
+                cnt, pl->cob_list.p + off, hp.npe, pl->mesh_elements.p, pl->ke64.p, x, y);
+        CK(cudaGetLastError());
+    }
+    pg::bc_copy_kernel<<<((int)n + 255) / 256, 256, 0, c->stream>>>((int)n, pl->cons.p, x, y);
+    CK(cudaGetLastError());
+}
+
+// Queues ||F - K x||^2 and ||F||^2 of plan pl into pl->nrm (uses pl->kx).
+void queue_true_residual(pg_ctx* c, Plan* pl, const double* x, const float* F) {
+    const int n = 3 * pl->hp.Nn;
+    if (pl->kx.n != (size_t)n) pl->kx.alloc(n);
+    if (pl->nrm.n != 2) pl->nrm.alloc(2);
+    queue_apply_k(c, pl, x, pl->kx.p);
+    CK(cudaMemsetAsync(pl->nrm.p, 0, 2 * sizeof(double), c->stream));
+    const int blocks = std::max(1, std::min(4 * c->sms, (n + 255) / 256));
+    pg::residual_norms_kernel<<<blocks, 256, 0, c->stream>>>(n, pl->cons.p, F, pl->kx.p, pl->nrm.p);
+    CK(cudaGetLastError());
+}
+
+// Stop of an FP64 correction K d = F - K x_m: the caller's rule on x_m + d
+// (||r|| < tol or ||r|| / ||F|| < tol; or the relative test alone) as a
+// relative tolerance on the correction's load, whose norm is r0.
+double correction_tolerance(const pg_options& o, double bnorm, double r0) {
+    const double target = o.stop_rule == PG_STOP_REFERENCE ? std::max(o.tolerance, o.tolerance * bnorm)
+                                                           : o.tolerance * bnorm;
+    return r0 > 0 ? std::min(0.5, target / r0) : o.tolerance;
+}
+
+// After a mixed solve of pl stagnated (pl->x holds its x_m, pl->F the
+// load): solves K d = F - K x_m in FP64, its load the FP32-rounded residual
+// and its stop scaled to the residual x_m already reached, then x = x_m + d
+// into x_dst.  mi: the mixed solve's record in (its final residual is the
+// FP64 true residual of x_m), the result's out.
+void fp64_correction(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* mi, void* x_dst,
+                     cudaMemcpyKind kind) {
+    const size_t n = 3 * (size_t)pl->hp.Nn;
+    const int ni = (int)n;
+    const double bnorm = mi->b_norm, r0 = mi->final_residual;
+    cudaStream_t st = c->stream;
+    if (pl->xw.n != n) pl->xw.alloc(n);
+    if (pl->kx.n != n) pl->kx.alloc(n);
+    if (pl->rf.n != n) pl->rf.alloc(n);
+    // the load kept in rf; the correction's load into F (what run_solve reads)
+    CK(cudaMemcpyAsync(pl->rf.p, pl->F.p, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(pl->xw.p, pl->x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    queue_apply_k(c, pl, pl->xw.p, pl->kx.p);
+    pg::residual_f32_kernel<<<(ni + 255) / 256, 256, 0, st>>>(ni, pl->cons.p, pl->rf.p, pl->kx.p, pl->F.p);
+    CK(cudaGetLastError());
+    pg_options o64 = o;
+    o64.precision = PG_PREC_FP64;
+    o64.stop_rule = PG_STOP_RELATIVE;
+    o64.tolerance = correction_tolerance(o, bnorm, r0);
+    pg_info fi{};
+    run_solve(c, pl, o64, &fi, nullptr, kind);
+    pg::add_kernel<<<(ni + 255) / 256, 256, 0, st>>>(ni, pl->xw.p, pl->x.p);
+    CK(cudaGetLastError());
+    queue_true_residual(c, pl, pl->x.p, pl->rf.p);
+    double nrm[2] = {0.0, 0.0};
+    CK(cudaMemcpyAsync(nrm, pl->nrm.p, sizeof nrm, cudaMemcpyDeviceToHost, st));
+    if (x_dst) CK(cudaMemcpyAsync(x_dst, pl->x.p, n * sizeof(double), kind, st));
+    CK(cudaStreamSynchronize(st));
+    const double mixed_ms = mi->setup_ms + mi->solve_ms;
+    *mi = fi;
+    mi->true_rel_residual = nrm[1] > 0 ? std::sqrt(nrm[0] / nrm[1]) : 0.0;
+    mi->b_norm = bnorm;
+    mi->fallback = 1;
+    mi->solve_ms += mixed_ms;
+}
+
 void solve_with_fallback(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_dst = nullptr,
                          cudaMemcpyKind kind = cudaMemcpyDeviceToDevice) {
     pg_info local{};
     pg_info* fi = info ? info : &local;
     run_solve(c, pl, o, fi, x_dst, kind);
     if (o.precision != PG_PREC_MIXED || !o.fallback || fi->stop_reason != PG_STOP_STAGNATED) return;
-    const double first_ms = fi->setup_ms + fi->solve_ms;
-    pg_options o64 = o;
-    o64.precision = PG_PREC_FP64;
-    run_solve(c, pl, o64, fi, x_dst, kind);
-    fi->fallback = 1;
-    fi->solve_ms += first_ms;
+    fp64_correction(c, pl, o, fi, x_dst, kind);
 }
 
 // Layout of an NR-case launch: the first of the single solve's preferences
@@ -922,18 +1001,18 @@ void run_solve_multi(pg_ctx* c, Plan* pl, const pg_options& o, int NR, int count
     if (r[0].wait_failures > 0) throw_on_failure(r[0]);
     for (int k = 0; k < count; k++) throw_on_failure(r[k]);
     if (!mixed || !o.fallback) return;
-    pg_options o64 = o;
-    o64.precision = PG_PREC_FP64;
     for (int k = 0; k < count; k++) {
         if (r[k].stop_reason != PG_STOP_STAGNATED) continue;
+        // the case's x_m and load into the plan's one-load buffers, then the
+        // FP64 correction as for a one-load solve
+        CK(cudaMemcpyAsync(pl->x.p, pl->mx.p + k * n, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(pl->F.p, F[k], n * sizeof(float), cudaMemcpyHostToDevice, st));
         pg_info fi{};
-        run_solve(c, pl, o64, &fi, x ? (void*)x[k] : nullptr, cudaMemcpyDeviceToHost);
+        fill_info(&fi, r[k], pl, o, pg::kMaxThreads, L.total);
+        fi.solve_ms = ms_solve;
+        fp64_correction(c, pl, o, &fi, x ? (void*)x[k] : nullptr, cudaMemcpyDeviceToHost);
         if (infos) {
-            const double first_ms = infos[k].solve_ms;
             infos[k] = fi;
-            infos[k].fallback = 1;
-            infos[k].solve_ms += first_ms;
             infos[k].plan_cached = 1;
         }
     }
@@ -1061,7 +1140,7 @@ std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int co
 }
 
 void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* const* x_out,
-               pg_info* infos, pg_batch_info* bi);
+               pg_info* infos, pg_batch_info* bi, const double* tols = nullptr);
 
 double percentile(std::vector<double> v, double q) {
     if (v.empty()) return 0.0;
@@ -1071,8 +1150,9 @@ double percentile(std::vector<double> v, double q) {
     return v[lo] + (pos - (double)lo) * (v[hi] - v[lo]);
 }
 
+// tols (optional): a stop tolerance per plate in place of o.tolerance.
 void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* const* x_out,
-               pg_info* infos, pg_batch_info* bi) {
+               pg_info* infos, pg_batch_info* bi, const double* tols) {
     pg_ctx* c = b->ctx;
     const int count = (int)b->plans.size();
     if (halo_rings(o) != b->rings)
@@ -1108,6 +1188,7 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
         ai.timing = 0;
         ai.test_stall = 0;
         ai.trace_it = -1;
+        if (tols) ai.tol = tols[i];
         a[i] = ai;
         smem = std::max(smem, L.total);
     }
@@ -1188,9 +1269,10 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
         bi->shared_bytes = smem;
     }
     for (int i = 0; i < count; i++) throw_on_failure(r[i]);
-    // plates whose mixed solve stagnated: solved again in FP64 as a batch of
-    // their own (planned for FP64 shared-memory capacity, kept while the same
-    // plates stagnate)
+    // plates whose mixed solve stagnated: an FP64 correction K d = F - K x_m
+    // for each, solved as a batch of their own (planned for FP64
+    // shared-memory capacity, kept while the same plates stagnate), each with
+    // its stop scaled to the residual its x_m reached; then x = x_m + d
     if (o.precision != PG_PREC_MIXED || !o.fallback) return;
     std::vector<int> failed;
     for (int i = 0; i < count; i++)
@@ -1199,9 +1281,26 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
     if (failed.empty()) return;
     pg_options o64 = o;
     o64.precision = PG_PREC_FP64;
+    o64.stop_rule = PG_STOP_RELATIVE;
     const int nf = (int)failed.size();
+    std::vector<std::vector<float>> rh(nf);
     std::vector<const float*> Ff(nf);
-    for (int k = 0; k < nf; k++) Ff[k] = b->hF[failed[k]].data();
+    std::vector<double> tols_f(nf);
+    for (int k = 0; k < nf; k++) {
+        Plan* pl = b->plans[failed[k]].get();
+        const size_t n = 3 * (size_t)pl->hp.Nn;
+        const int ni = (int)n;
+        if (pl->kx.n != n) pl->kx.alloc(n);
+        if (pl->rf.n != n) pl->rf.alloc(n);
+        queue_apply_k(c, pl, pl->x.p, pl->kx.p);
+        pg::residual_f32_kernel<<<(ni + 255) / 256, 256, 0, st>>>(ni, pl->cons.p, pl->F.p, pl->kx.p, pl->rf.p);
+        CK(cudaGetLastError());
+        rh[k].resize(n);
+        CK(cudaMemcpyAsync(rh[k].data(), pl->rf.p, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+        Ff[k] = rh[k].data();
+        tols_f[k] = correction_tolerance(o, r[failed[k]].b_norm, r[failed[k]].final_residual);
+    }
+    CK(cudaStreamSynchronize(st));
     if (!b->fb || b->fb_ids != failed) {
         std::vector<pg_problem> fp(nf);
         for (int k = 0; k < nf; k++) {
@@ -1212,17 +1311,39 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
         b->fb = build_batch(c, fp.data(), nf, o64);
         b->fb_ids = failed;
     }
+    std::vector<std::vector<double>> d(nf);
     std::vector<double*> xf(nf, nullptr);
-    if (x_out)
-        for (int k = 0; k < nf; k++) xf[k] = x_out[failed[k]];
+    for (int k = 0; k < nf; k++) {
+        d[k].resize(3 * (size_t)b->plans[failed[k]]->hp.Nn);
+        xf[k] = d[k].data();
+    }
     std::vector<pg_info> inf(nf);
     pg_batch_info fbi{};
-    run_batch(b->fb.get(), o64, Ff.data(), x_out ? xf.data() : nullptr, inf.data(), &fbi);
+    run_batch(b->fb.get(), o64, Ff.data(), xf.data(), inf.data(), &fbi, tols_f.data());
+    // x = x_m + d on each plate's plan, and the true residual of that x
+    std::vector<double> nrm(2 * (size_t)nf, 0.0);
+    for (int k = 0; k < nf; k++) {
+        const int i = failed[k];
+        Plan* pl = b->plans[i].get();
+        const size_t n = d[k].size();
+        const int ni = (int)n;
+        if (pl->xw.n != n) pl->xw.alloc(n);
+        CK(cudaMemcpyAsync(pl->xw.p, d[k].data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+        pg::add_kernel<<<(ni + 255) / 256, 256, 0, st>>>(ni, pl->xw.p, pl->x.p);
+        CK(cudaGetLastError());
+        queue_true_residual(c, pl, pl->x.p, pl->F.p);
+        CK(cudaMemcpyAsync(nrm.data() + 2 * k, pl->nrm.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (x_out && x_out[i])
+            CK(cudaMemcpyAsync(x_out[i], pl->x.p, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));  // d[k] and the pageable x_out[i] are host memory
+    }
     for (int k = 0; k < nf; k++) {
         const int i = failed[k];
         if (infos) {
-            const double mixed_ms = infos[i].solve_ms;
+            const double mixed_ms = infos[i].solve_ms, bn = r[i].b_norm;
             infos[i] = inf[k];
+            infos[i].true_rel_residual = nrm[2 * k + 1] > 0 ? std::sqrt(nrm[2 * k] / nrm[2 * k + 1]) : 0.0;
+            infos[i].b_norm = bn;
             infos[i].fallback = 1;
             infos[i].solve_ms += mixed_ms;
         }
@@ -1502,17 +1623,7 @@ int pg_apply_k(pg_ctx* c, const pg_problem* p, const double* x, double* y) {
         DevBuf<double> dx, dy;
         dx.upload(x, n, c->stream);
         dy.alloc(n);
-        CK(cudaMemsetAsync(dy.p, 0, n * sizeof(double), c->stream));
-        const pg::HostPlan& hp = pl->hp;
-        for (int col = 0; col < hp.colors; col++) {
-            const int off = (int)hp.color_offsets[col], cnt = (int)hp.color_offsets[col + 1] - off;
-            if (cnt > 0)
-                pg::applyk_color_kernel<<<(cnt + 127) / 128, 128, 0, c->stream>>>(
-                    cnt, pl->cob_list.p + off, hp.npe, pl->mesh_elements.p, pl->ke64.p, dx.p, dy.p);
-            CK(cudaGetLastError());
-        }
-        pg::bc_copy_kernel<<<((int)n + 255) / 256, 256, 0, c->stream>>>((int)n, pl->cons.p, dx.p, dy.p);
-        CK(cudaGetLastError());
+        queue_apply_k(c, pl, dx.p, dy.p);
         CK(cudaMemcpyAsync(y, dy.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
     });

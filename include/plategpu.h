@@ -135,9 +135,11 @@ typedef struct pg_options {
                                      (pg_info.trace_ns) */
     int32_t smoother;             /* pg_smoother, default PG_SMOOTHER_BLOCK_JACOBI (also the
                                      smoother of the two-level preconditioner) */
-    int32_t fallback;             /* mixed precision: 1 (default) re-solves in FP64 when the
-                                     mixed solve stagnates (PG_STOP_STAGNATED); 0 returns
-                                     the stagnated result */
+    int32_t fallback;             /* mixed precision: 1 (default) continues in FP64 when the
+                                     mixed solve stagnates (PG_STOP_STAGNATED): an FP64 solve
+                                     of the correction K d = F - K x_m from the stagnated x_m,
+                                     stopped by the same rule on x_m + d; 0 returns the
+                                     stagnated result */
 } pg_options;
 
 /* Per-solve result (GPUSolveResult plus extended statistics). */
@@ -161,9 +163,10 @@ typedef struct pg_info {
                                      one per residual replacement) */
     int32_t shared_bytes;         /* dynamic shared memory per block */
     int32_t coarse_dim;           /* two-level: coarse DOFs kept (0 otherwise) */
-    int32_t fallback;             /* 1 when a stagnated mixed solve was redone in FP64 (the
-                                     result fields are then the FP64 solve's; solve_ms
-                                     covers both) */
+    int32_t fallback;             /* 1 when a stagnated mixed solve was finished by an FP64
+                                     correction (iterations, stop_reason and converged are
+                                     then the correction's; the residuals refer to the final
+                                     x and F; solve_ms covers both) */
     double phase_us[8];           /* with phase_timing, block 0's time (SM cycles at
                                      the nominal clock) in: K.u; gather, dots and
                                      publishing w; block reduction and publishing the

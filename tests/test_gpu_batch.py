@@ -92,7 +92,7 @@ def test_mixed_precision_falls_back_to_fp64_when_it_stagnates(gpu_ctx, oracle, s
     halving the residual) and the FP64 re-solve.  A replacement after every
     update (reliable_interval = 1) cannot halve the residual each time, so
     the rule fires within a few updates; with the default fallback the call
-    then re-solves in FP64 to the requested accuracy."""
+    then finishes in FP64 to the requested accuracy."""
     wl = small_batch[1]
     pr = _lib.Problem(wl.mesh, wl.material, wl.coloring, wl.F, wl.cons_mask)
     kw = dict(tolerance=1e-9, max_iterations=20000, stop_rule=_lib.PG_STOP_RELATIVE,
@@ -109,3 +109,47 @@ def test_mixed_precision_falls_back_to_fp64_when_it_stagnates(gpu_ctx, oracle, s
     assert bi.converged == 4 and bi.fallbacks == sum(inf.fallback for inf in infos) >= 1
     for w, x, inf in zip(small_batch[:4], xs, infos):
         assert inf.converged and rel_err(x, truth(oracle, w)) < 1e-6
+
+
+def oracle_true_rel(oracle, wl, x):
+    """||F - K x|| / ||F|| with the oracle's FP64 operator."""
+    m, mat = wl.mesh, wl.material
+    ke = oracle.all_ke(m.nodes, m.elements, m.nodesPerElement, mat.E, mat.nu, mat.t,
+                       elem_t=mat.elem_t, mode=oracle.FP64)
+    offs, flat = wl.coloring.flat()
+    kx = oracle.apply_k(m.nodeCount, m.elements, m.nodesPerElement, ke, offs, flat, wl.cons_mask,
+                        np.asarray(x, np.float64), oracle.FP64)
+    F = wl.F.astype(np.float64)
+    F[wl.cons_mask != 0] = 0.0
+    return float(np.linalg.norm(F - kx) / np.linalg.norm(F))
+
+
+def test_fp64_correction_starts_from_the_mixed_solution(gpu_ctx, oracle, small_batch):
+    """After a stagnated mixed solve the FP64 stage solves the correction
+    K d = F - K x_m from the stagnated x_m: fewer iterations than an FP64
+    solve from zero to the same stop, and the reported true residual is that
+    of the returned x (checked with the oracle's FP64 operator).  A relative
+    residual of 1e-13 is out of FP32's reach, so the mixed stage stagnates."""
+    wl = workloads.plate_q4_32()
+    pr = _lib.Problem(wl.mesh, wl.material, wl.coloring, wl.F, wl.cons_mask)
+    kw = dict(tolerance=1e-13, max_iterations=20000, stop_rule=_lib.PG_STOP_RELATIVE)
+    x, info = gpu_ctx.solve(pr, _lib.make_options(precision=_lib.PG_PREC_MIXED, **kw))
+    _x64, cold = gpu_ctx.solve(pr, _lib.make_options(precision=_lib.PG_PREC_FP64, **kw))
+    assert info.fallback == 1 and info.converged and cold.converged
+    assert info.iterations < 0.8 * cold.iterations
+    # the true residual of the returned x; at this depth both it and the
+    # oracle's value are FP64 rounding of F - K x (different summation
+    # orders), so they agree to a factor, not to digits
+    rel = oracle_true_rel(oracle, wl, x)
+    assert 0.5 * rel <= info.true_rel_residual <= 2.0 * rel
+    assert rel < 1e-11
+    assert rel_err(x, truth(oracle, wl)) < 1e-6
+    # the batch path: the same plate among others
+    probs = probs_of(small_batch[:3]) + [pr]
+    xs, infos, bi = gpu_ctx.solve_batch(probs, _lib.make_options(precision=_lib.PG_PREC_MIXED, **kw))
+    assert infos[3].fallback == 1 and infos[3].converged
+    assert infos[3].iterations < 0.8 * cold.iterations
+    rel_b = oracle_true_rel(oracle, wl, xs[3])
+    assert 0.5 * rel_b <= infos[3].true_rel_residual <= 2.0 * rel_b
+    for w, xb in zip(small_batch[:3] + [wl], xs):
+        assert rel_err(xb, truth(oracle, w)) < 1e-6
