@@ -631,7 +631,8 @@ def batch_bench(args, ctx, check, world=1, rank=0, local=0):
                         "30%% DKT, random material, supports and random-field loads" % len(ALL)),
            "dof_total": int(sum(3 * w.mesh.nodeCount for w in ALL)),
            "ranks": world, "plates_per_rank": [len(sh) for sh in shards],
-           "method": "mixed_two_level, FP64 re-solve (as a batch) of plates whose mixed solve stagnates",
+           "method": ("mixed_two_level; plates whose mixed solve stagnates finish with an FP64 "
+                      "correction from the mixed solution (as a batch)"),
            "stop": "||r||/||b|| < 2e-7", "solves_per_s": len(ALL) / (med * 1e-3), "batch_ms": med,
            "batch_ms_all": ms, "plate_ms_p50": bi.plate_ms_p50, "plate_ms_p99": bi.plate_ms_p99,
            "plate_ms_max": bi.plate_ms_max, "phases": bi.phases, "teams": bi.teams,
