@@ -454,7 +454,14 @@ __device__ __forceinline__ void pcg_multi_body(const PcgArgs& a, const int g, un
         }
         clk.lap(2);
         {
-            const bool ok = exchange_round_multi<T, NR>(pb, a.G, KP * NR, vb, w, no, nloc, gid, g, e, sp, wt);
+            bool ok = exchange_round_multi<T, NR>(pb, a.G, KP * NR, vb, w, no, nloc, gid, g, e, sp, wt);
+            if (a.test_stall && it == 0 && tid == 0) {
+                // the two spare words after the partial-sum buffers: a tag no
+                // block writes, so the wait must run out
+                double never;
+                ok = ok && poll<double>(a.llp + (size_t)2 * kRep * a.G * multi_slot_words<4>(), 0xffffffffu,
+                                        never, wt);
+            }
             if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
             sum_partials<3 * NR>(sp, a.G, KP * NR, scal);
         }

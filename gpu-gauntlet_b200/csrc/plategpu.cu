@@ -953,7 +953,6 @@ void run_solve_multi(pg_ctx* c, Plan* pl, const pg_options& o, int NR, int count
     a.llx = pl->mllx.p;
     a.llp = pl->mllp.p;
     a.tag0 = pl->m_tag0;
-    a.test_stall = 0;
     a.trace_it = -1;
     const void* fn = multi_kernel(hp.npe, mixed, NR);
     opt_in_smem(c, fn);

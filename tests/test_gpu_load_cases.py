@@ -151,3 +151,28 @@ def test_mirror_and_arguments(gpu_ctx, c1):
     with pytest.raises(PlateGPUError) as e:
         gpu_ctx.solve_load_cases(prob(c1), bad, opts)
     assert e.value.code == _lib.PG_ENONFINITE
+
+
+def test_wait_timeout_reports_and_context_survives(gpu_ctx, c1):
+    """The test hook makes block 0 wait once for a tag no block writes: the
+    lockstep launch ends with PG_ETIMEOUT after the wait limit, and the next
+    call on the same plate and context solves normally."""
+    F = loads(c1, 4, seed=9)
+    bad = _lib.make_options(tolerance=1e-8, max_iterations=5000, test_stall=True, wait_timeout_ms=50)
+    with pytest.raises(PlateGPUError) as e:
+        gpu_ctx.solve_load_cases(prob(c1), F, bad, cases_per_launch=4)
+    assert e.value.code == _lib.PG_ETIMEOUT
+    X, infos = gpu_ctx.solve_load_cases(prob(c1), F, _lib.make_options(tolerance=1e-8, max_iterations=5000),
+                                        cases_per_launch=4)
+    assert all(i.converged for i in infos)
+
+
+@pytest.mark.parametrize("ctas", [37, 148])
+def test_grid_size_and_fp64_width_four(gpu_ctx, oracle, c1, ctas):
+    F = loads(c1, 4, seed=13)
+    opts = _lib.make_options(tolerance=1e-9, max_iterations=20000, stop_rule=_lib.PG_STOP_RELATIVE,
+                             ctas=ctas, preconditioner=TL)
+    X, infos = gpu_ctx.solve_load_cases(prob(c1), F, opts, cases_per_launch=4)
+    for x, info, xt in zip(X, infos, truths(oracle, c1, F)):
+        assert info.converged and info.ctas == ctas
+        assert rel_err(x, xt) < 1e-6
