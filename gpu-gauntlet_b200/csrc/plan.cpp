@@ -568,55 +568,4 @@ std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>
     return "";
 }
 
-uint64_t problem_hash(const pg_problem& p) {
-    uint64_t h = 0x9e3779b97f4a7c15ull;
-    auto mix = [&](uint64_t v) {
-        h ^= v + 0x9e3779b97f4a7c15ull + (h << 6) + (h >> 2);
-        h *= 0xff51afd7ed558ccdull;
-        h ^= h >> 33;
-    };
-    // arrays in four independent lanes of multiply-xorshift (32 bytes per
-    // step, so the four multiplications overlap), folded into h at the end:
-    // this runs on every pg_solve, over the whole mesh
-    auto bytes = [&](const void* d, size_t n) {
-        if (!d) { mix(0xdeadull); return; }
-        const unsigned char* b = (const unsigned char*)d;
-        uint64_t l[4] = {0x243f6a8885a308d3ull, 0x13198a2e03707344ull, 0xa4093822299f31d0ull,
-                         0x082efa98ec4e6c89ull};
-        size_t i = 0;
-        for (; i + 32 <= n; i += 32) {
-            uint64_t v[4];
-            std::memcpy(v, b + i, 32);
-            for (int k = 0; k < 4; k++) {
-                l[k] = (l[k] ^ v[k]) * 0x9fb21c651e98df25ull;
-                l[k] ^= l[k] >> 29;
-            }
-        }
-        for (int k = 0; k < 4; k++) mix(l[k]);
-        for (; i + 8 <= n; i += 8) {
-            uint64_t v;
-            std::memcpy(&v, b + i, 8);
-            mix(v);
-        }
-        uint64_t tail = 0;
-        std::memcpy(&tail, b + i, n - i);
-        mix(tail ^ (uint64_t)n);
-    };
-    mix(p.node_count);
-    mix(p.element_count);
-    mix(p.nodes_per_element);
-    mix(p.color_count);
-    bytes(p.nodes, 2 * sizeof(float) * p.node_count);
-    bytes(p.elements, sizeof(uint32_t) * p.nodes_per_element * p.element_count);
-    if (p.color_count) {
-        bytes(p.color_offsets, sizeof(uint32_t) * (p.color_count + 1));
-        bytes(p.elements_by_color, sizeof(uint32_t) * p.element_count);
-    }
-    bytes(p.constrained, 3 * (size_t)p.node_count);
-    double mat[3] = {p.E, p.nu, p.t};
-    bytes(mat, sizeof(mat));
-    bytes(p.elem_t, p.elem_t ? sizeof(float) * p.element_count : 0);
-    return h;
-}
-
 }  // namespace pg

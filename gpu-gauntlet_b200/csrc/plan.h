@@ -108,8 +108,4 @@ struct BatchSchedule {
 std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>& caps,
                            const std::vector<int>& kinds, int sms, BatchSchedule& out);
 
-// 64-bit FNV-1a over the problem's mesh, colouring, material and
-// constraint arrays (not F): the key of the plan cache.
-uint64_t problem_hash(const pg_problem& p);
-
 }  // namespace pg

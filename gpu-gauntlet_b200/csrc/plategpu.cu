@@ -60,14 +60,16 @@ struct DevBuf {
 };
 
 struct Plan {
-    uint64_t key = 0;
     int G = 0;
     pg::HostPlan hp;
-    // host copies of the mesh arrays the coarse-space set-up reads later
+    // host copies of the problem's arrays: read by the coarse-space set-up,
+    // and compared with a new problem's to find its plan in the cache
     std::vector<float> h_nodes;
     std::vector<uint32_t> h_elements;
     std::vector<uint8_t> h_cons;
     std::vector<float> h_elem_t;
+    uint32_t h_color_count = 0;
+    std::vector<uint32_t> h_color_off, h_by_color;  // the caller's colouring
     pg_problem prob_view{};
     double E = 0, nu = 0, t = 0;
     bool has_elem_t = false;
@@ -293,6 +295,11 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G, int ring
     pl->prob_view.elements_by_color = nullptr;
     if (p.elem_t) pl->h_elem_t.assign(p.elem_t, p.elem_t + (size_t)p.element_count);
     pl->prob_view.elem_t = p.elem_t ? pl->h_elem_t.data() : nullptr;
+    pl->h_color_count = p.color_count;
+    if (p.color_count) {
+        pl->h_color_off.assign(p.color_offsets, p.color_offsets + p.color_count + 1);
+        pl->h_by_color.assign(p.elements_by_color, p.elements_by_color + p.element_count);
+    }
     pl->E = p.E;
     pl->nu = p.nu;
     pl->t = p.t;
@@ -339,10 +346,32 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G, int ring
     return pl;
 }
 
+// Whether p is the problem plan pl was made from: mesh, colouring,
+// constraints and material compared in full (the load is not part of a
+// plan).  Exact, and faster than hashing the arrays (memcmp stops at the
+// first difference and otherwise streams at memory speed).
+bool same_problem(const Plan& pl, const pg_problem& p) {
+    const pg_problem& q = pl.prob_view;
+    if (q.node_count != p.node_count || q.element_count != p.element_count ||
+        q.nodes_per_element != p.nodes_per_element || pl.h_color_count != p.color_count || q.E != p.E ||
+        q.nu != p.nu || q.t != p.t || (q.elem_t != nullptr) != (p.elem_t != nullptr))
+        return false;
+    auto same = [](const void* a, const void* b, size_t bytes) {
+        return bytes == 0 || std::memcmp(a, b, bytes) == 0;
+    };
+    const size_t Nn = p.node_count, Ne = p.element_count;
+    return same(pl.h_cons.data(), p.constrained, 3 * Nn) &&
+           same(pl.h_nodes.data(), p.nodes, 2 * Nn * sizeof(float)) &&
+           same(pl.h_elements.data(), p.elements, (size_t)p.nodes_per_element * Ne * sizeof(uint32_t)) &&
+           (!p.color_count ||
+            (same(pl.h_color_off.data(), p.color_offsets, (p.color_count + 1) * sizeof(uint32_t)) &&
+             same(pl.h_by_color.data(), p.elements_by_color, Ne * sizeof(uint32_t)))) &&
+           (!p.elem_t || same(pl.h_elem_t.data(), p.elem_t, Ne * sizeof(float)));
+}
+
 Plan* get_plan(pg_ctx* c, const pg_problem& p, int G, int rings, bool* cached) {
-    const uint64_t key = pg::problem_hash(p);
     for (auto it = c->plans.begin(); it != c->plans.end(); ++it) {
-        if ((*it)->key == key && (*it)->G == G && (*it)->hp.rings == rings) {
+        if ((*it)->G == G && (*it)->hp.rings == rings && same_problem(**it, p)) {
             c->plans.splice(c->plans.begin(), c->plans, it);
             *cached = true;
             return c->plans.front().get();
@@ -350,7 +379,6 @@ Plan* get_plan(pg_ctx* c, const pg_problem& p, int G, int rings, bool* cached) {
     }
     *cached = false;
     auto pl = build_plan(c, p, G, rings);
-    pl->key = key;
     c->plans.push_front(std::move(pl));
     while (c->plans.size() > kMaxPlans) c->plans.pop_back();
     return c->plans.front().get();

@@ -243,3 +243,36 @@ def test_plan_cache_reused(gpu_ctx, c1):
     pr.set_F(c1.F * 2)
     x, info = gpu_ctx.solve(pr, o)
     assert info.plan_cached == 1
+
+
+def test_plan_cache_compares_every_array(gpu_ctx, c1):
+    """A plan is reused for a problem equal in every mesh, colouring,
+    constraint and material array (copies in other memory included), and
+    not when any one of them differs -- here the last node coordinate, the
+    last colour list entry, one constraint and the thickness."""
+    o = _lib.make_options(ctas=13, tolerance=1e-8, stop_rule=_lib.PG_STOP_RELATIVE)
+    m, mat = c1.mesh, c1.material
+    gpu_ctx.solve(_lib.Problem(m, mat, c1.coloring, c1.F, c1.cons_mask), o)
+    copy = type(m)(**{**m.__dict__, "nodes": m.nodes.copy(), "elements": m.elements.copy()})
+    _x, info = gpu_ctx.solve(_lib.Problem(copy, mat, c1.coloring, c1.F, c1.cons_mask.copy()), o)
+    assert info.plan_cached == 1
+    nodes = m.nodes.copy()
+    nodes[-1] += np.float32(1e-3)
+    moved = type(m)(**{**m.__dict__, "nodes": nodes})
+    _x, info = gpu_ctx.solve(_lib.Problem(moved, mat, c1.coloring, c1.F, c1.cons_mask), o)
+    assert info.plan_cached == 0
+    cons = c1.cons_mask.copy()
+    free = np.flatnonzero(cons == 0)
+    cons[free[len(free) // 2]] = 1
+    F = c1.F.copy()
+    F[cons != 0] = 0
+    _x, info = gpu_ctx.solve(_lib.Problem(m, mat, c1.coloring, F, cons), o)
+    assert info.plan_cached == 0
+    thin = PlateMaterial(mat.E, mat.nu, mat.t * 0.5)
+    _x, info = gpu_ctx.solve(_lib.Problem(m, thin, c1.coloring, c1.F, c1.cons_mask), o)
+    assert info.plan_cached == 0
+    colors = [c.copy() for c in c1.coloring.colors]
+    colors[-1] = colors[-1][::-1].copy()  # same colouring, other order within a colour
+    col2 = ElementColoring(colors, c1.coloring.elementColors, c1.coloring.colorCount)
+    _x, info = gpu_ctx.solve(_lib.Problem(m, mat, col2, c1.F, c1.cons_mask), o)
+    assert info.plan_cached == 0
