@@ -1116,9 +1116,18 @@ std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int co
     // capacity of the plates whose parts do not fit and reschedule
     std::vector<int> caps(count), kinds(count);
     for (int i = 0; i < count; i++) kinds[i] = (int)probs[i].nodes_per_element;
-    for (int i = 0; i < count; i++) caps[i] = batch_capacity(o, b->rings, (int)probs[i].nodes_per_element);
+    for (int i = 0; i < count; i++) {
+        caps[i] = batch_capacity(o, b->rings, (int)probs[i].nodes_per_element);
+        // a plate too large for the whole device at the first guess gets the
+        // whole device anyway; its layout (element blocks and A_c^-1 rows then
+        // possibly in L2, as in a one-plate solve) is checked below
+        caps[i] = std::max(caps[i], (nodes[i] + c->sms - 1) / c->sms);
+    }
     for (int attempt = 0;; attempt++) {
         std::string e = pg::schedule_batch(nodes, caps, kinds, c->sms, b->sched);
+        if (!e.empty() && attempt > 0)
+            throw Fail{PG_EUNSUPPORTED, "a plate of the batch does not fit in shared memory even on the whole "
+                                        "device with these options"};
         if (!e.empty()) throw Fail{PG_EUNSUPPORTED, e};
         b->plans.clear();
         bool fits = true;
