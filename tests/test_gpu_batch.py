@@ -153,3 +153,29 @@ def test_fp64_correction_starts_from_the_mixed_solution(gpu_ctx, oracle, small_b
     assert 0.5 * rel_b <= infos[3].true_rel_residual <= 2.0 * rel_b
     for w, xb in zip(small_batch[:3] + [wl], xs):
         assert rel_err(xb, truth(oracle, w)) < 1e-6
+
+
+def test_plate_larger_than_the_first_capacity_guess_gets_the_whole_device(gpu_ctx, small_batch):
+    """A 59,536-node DKT plate needs more than 400 nodes per block on 148
+    blocks, above the batch's first FP64 capacity guess: it gets a team of the
+    whole device with the layout a one-plate solve uses, and gives the
+    one-plate solve's result (same partition, same iterates)."""
+    from plategpu import coloring, mesher, problem
+    from plategpu.types import PlateMaterial, PlateSupport
+
+    m = mesher.split_triangle_mesh(10, 10, 243, 243, jitter=0.2, seed=4)
+    sup = [PlateSupport("fixed", "all_edges")]
+    cons = problem.identifyConstrainedDOFs(m, sup)
+    F = problem.pressure_load_vector(m, 2e3).astype(np.float32)
+    problem.applyBCsToRHS(F, cons)
+    big = workloads.Workload("dkt243", m, PlateMaterial(2.1e11, 0.3, 0.12),
+                             coloring.computeElementColoringGreedy(m), sup, cons, F)
+    assert m.nodeCount > 148 * 400
+    kw = dict(tolerance=1e-9, max_iterations=20000, stop_rule=_lib.PG_STOP_RELATIVE,
+              precision=_lib.PG_PREC_FP64, preconditioner=_lib.PG_PRECOND_TWO_LEVEL)
+    probs = probs_of([small_batch[0], small_batch[2]]) + probs_of([big])
+    xs, infos, bi = gpu_ctx.solve_batch(probs, _lib.make_options(**kw))
+    assert infos[2].converged and infos[2].ctas == 148
+    x1, one = gpu_ctx.solve(probs[2], _lib.make_options(ctas=148, **kw))
+    assert abs(infos[2].iterations - one.iterations) <= 1
+    assert rel_err(xs[2], x1) < 1e-9
