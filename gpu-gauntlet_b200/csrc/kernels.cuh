@@ -228,6 +228,24 @@ __global__ void bc_copy_kernel(int n, const uint8_t* __restrict__ cons,
     if (i < n && cons[i]) y[i] = x[i];
 }
 
+// Start vector of the lambda_max(D^-1 K) power iteration: 1 + 0.5 sin(0.7 i),
+// 0 on constrained DOFs.
+__global__ void power_start_kernel(int n, const uint8_t* __restrict__ cons, double* __restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = cons[i] ? 0.0 : 1.0 + 0.5 * sin(0.7 * (double)i);
+}
+
+// z = D^-1 y node by node, D^-1 the 3x3 block inverses (FP64).
+__global__ void binv_apply_kernel(int Nn, const double* __restrict__ binv, const double* __restrict__ y,
+                                  double* __restrict__ z) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Nn) return;
+    const double* B = binv + 9 * (size_t)k;
+    const double y0 = y[3 * k], y1 = y[3 * k + 1], y2 = y[3 * k + 2];
+#pragma unroll
+    for (int d = 0; d < 3; d++) z[3 * k + d] = B[3 * d] * y0 + B[3 * d + 1] * y1 + B[3 * d + 2] * y2;
+}
+
 // r = F - y narrowed to FP32, 0 on constrained rows (y = K x): the load of
 // an FP64 correction solve K d = F - K x.  r may be F itself.
 __global__ void residual_f32_kernel(int n, const uint8_t* cons, const float* F, const double* y, float* r) {

@@ -416,50 +416,6 @@ std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, H
     return "";
 }
 
-double estimate_lambda_max(const pg_problem& p, const std::vector<double>& ke64,
-                           const std::vector<double>& binv64, int iters) {
-    const int Nn = (int)p.node_count, Ne = (int)p.element_count, npe = (int)p.nodes_per_element;
-    const int nd = 3 * npe, n = 3 * Nn;
-    if (n == 0) return 1.0;
-    std::vector<double> x(n), y(n);
-    for (int i = 0; i < n; i++) x[i] = p.constrained[i] ? 0.0 : 1.0 + 0.5 * std::sin(0.7 * i);
-    double lam = 1.0;
-    for (int it = 0; it < iters; it++) {
-        // y = A x with A = K_ff (+) I_cc
-        std::fill(y.begin(), y.end(), 0.0);
-        for (int e = 0; e < Ne; e++) {
-            const double* K = ke64.data() + (size_t)e * nd * nd;
-            const uint32_t* en = p.elements + (size_t)e * npe;
-            for (int i = 0; i < nd; i++) {
-                const int gi = 3 * (int)en[i / 3] + i % 3;
-                if (p.constrained[gi]) continue;
-                double acc = 0;
-                for (int j = 0; j < nd; j++) {
-                    const int gj = 3 * (int)en[j / 3] + j % 3;
-                    if (!p.constrained[gj]) acc += K[i * nd + j] * x[gj];
-                }
-                y[gi] += acc;
-            }
-        }
-        for (int i = 0; i < n; i++)
-            if (p.constrained[i]) y[i] = x[i];
-        // x = D^-1 y, normalised; |D^-1 A x| -> lambda_max for |x| = 1
-        double nrm = 0;
-        for (int k = 0; k < Nn; k++)
-            for (int d = 0; d < 3; d++) {
-                const double* Bk = binv64.data() + 9 * (size_t)k + 3 * d;
-                const double v = Bk[0] * y[3 * k] + Bk[1] * y[3 * k + 1] + Bk[2] * y[3 * k + 2];
-                x[3 * k + d] = v;
-                nrm += v * v;
-            }
-        nrm = std::sqrt(nrm);
-        if (!(nrm > 0) || !std::isfinite(nrm)) return (double)npe;
-        for (int i = 0; i < n; i++) x[i] /= nrm;
-        lam = nrm;
-    }
-    return lam;
-}
-
 std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>& caps,
                            const std::vector<int>& kinds, int sms, BatchSchedule& out) {
     out = BatchSchedule{};

@@ -75,13 +75,6 @@ std::string build_partition(const pg_problem& p, int G, int rings, HostPlan& pla
 // lists, and the rows of A_c^-1 = (P^T A P)^-1 each part needs.
 std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, HostPlan& plan);
 
-// Largest eigenvalue of D^-1 A (D the 3x3 nodal block diagonal, A = K_ff
-// (+) I_cc) by `iters` power iterations from a fixed start vector, with
-// D^-1 given as binv64 ([Nn][9]) and A element by element from ke64.
-// Underestimates slightly; block Jacobi bounds it by nodes_per_element.
-double estimate_lambda_max(const pg_problem& p, const std::vector<double>& ke64,
-                           const std::vector<double>& binv64, int iters);
-
 // Team schedule of a batch of independent plates.  A plate of n nodes gets
 // a team of d blocks: a power of two, or every block of the device for the
 // largest plates, with at most caps[i] nodes per block (so its parts fit in

@@ -109,7 +109,7 @@ struct Plan {
     DevBuf<pg::PcgResult> mres;
     // FP64 correction after a stagnated mixed solve: the mixed x, K x and
     // the FP32 residual
-    DevBuf<double> xw, kx, nrm;
+    DevBuf<double> xw, kx, nrm, pw;
     DevBuf<float> rf;
 };
 
@@ -416,6 +416,76 @@ void run_setup(pg_ctx* c, Plan* pl) {
     CK(cudaGetLastError());
 }
 
+// y = K x on the device (colour by colour, then the identity rows of the
+// constrained DOFs), queued on the context stream.  The plan's set-up must
+// have run.
+void queue_apply_k(pg_ctx* c, Plan* pl, const double* x, double* y) {
+    const pg::HostPlan& hp = pl->hp;
+    const size_t n = 3 * (size_t)hp.Nn;
+    CK(cudaMemsetAsync(y, 0, n * sizeof(double), c->stream));
+    for (int col = 0; col < hp.colors; col++) {
+        const int off = (int)hp.color_offsets[col], cnt = (int)hp.color_offsets[col + 1] - off;
+        if (cnt > 0)
+            pg::applyk_color_kernel<<<(cnt + 127) / 128, 128, 0, c->stream>>>(
+                cnt, pl->cob_list.p + off, hp.npe, pl->mesh_elements.p, pl->ke64.p, x, y);
+        CK(cudaGetLastError());
+    }
+    pg::bc_copy_kernel<<<((int)n + 255) / 256, 256, 0, c->stream>>>((int)n, pl->cons.p, x, y);
+    CK(cudaGetLastError());
+}
+
+// lambda_max(D^-1 K) by `iters` power steps on the device from the start
+// vector 1 + 0.5 sin(0.7 i) (0 on constrained DOFs): |z_iters| / |z_(iters-1)|
+// with z_(k+1) = D^-1 K z_k.  The iterates are left unnormalised; their
+// growth, at most about 9^iters for the plate operators, stays far inside
+// FP64's range.  queue_power_steps queues the steps (z_iters ends in pl->xw
+// for even iters, else pl->pw; z_(iters-1) in the other), lambda_from_power
+// reads them back once the stream has run them and sums the two norms on
+// the host, in order.
+void queue_power_steps(pg_ctx* c, Plan* pl, int iters) {
+    const pg::HostPlan& hp = pl->hp;
+    const size_t n = 3 * (size_t)hp.Nn;
+    if (n == 0) return;
+    run_setup(c, pl);
+    if (pl->xw.n != n) pl->xw.alloc(n);
+    if (pl->kx.n != n) pl->kx.alloc(n);
+    if (pl->pw.n != n) pl->pw.alloc(n);
+    cudaStream_t st = c->stream;
+    double* a = pl->xw.p;
+    double* b = pl->pw.p;
+    pg::power_start_kernel<<<((int)n + 255) / 256, 256, 0, st>>>((int)n, pl->cons.p, a);
+    CK(cudaGetLastError());
+    for (int it = 0; it < iters; it++) {
+        queue_apply_k(c, pl, a, pl->kx.p);
+        pg::binv_apply_kernel<<<(hp.Nn + 255) / 256, 256, 0, st>>>(hp.Nn, pl->binv64.p, pl->kx.p, b);
+        CK(cudaGetLastError());
+        std::swap(a, b);
+    }
+}
+
+double lambda_from_power(pg_ctx* c, Plan* pl, int iters) {
+    const size_t n = 3 * (size_t)pl->hp.Nn;
+    if (n == 0 || iters < 1) return 1.0;
+    const double* last = iters % 2 == 0 ? pl->xw.p : pl->pw.p;
+    const double* prev = iters % 2 == 0 ? pl->pw.p : pl->xw.p;
+    std::vector<double> za(n), zb(n);
+    CK(cudaMemcpyAsync(za.data(), last, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(zb.data(), prev, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double na = 0.0, nb = 0.0;
+    for (size_t i = 0; i < n; i++) {
+        na += za[i] * za[i];
+        nb += zb[i] * zb[i];
+    }
+    const double lam = nb > 0 ? std::sqrt(na / nb) : 0.0;
+    return std::isfinite(lam) && lam > 0 ? lam : (double)pl->hp.npe;
+}
+
+double device_lambda_max(pg_ctx* c, Plan* pl, int iters) {
+    queue_power_steps(c, pl, iters);
+    return lambda_from_power(c, pl, iters);
+}
+
 void fill_options(const pg_options* in, pg_options* o) {
     pg_options_default(o);
     if (!in) return;
@@ -477,21 +547,10 @@ void upload_coarse(pg_ctx* c, Plan* pl) {
 }
 
 // Largest eigenvalue of D^-1 K for the polynomial smoother, estimated once
-// per plan on the host from the device's element matrices and block inverses.
+// per plan by power steps on the device.
 void ensure_smoother(pg_ctx* c, Plan* pl) {
     if (pl->lambda_max > 0) return;
-    const pg::HostPlan& hp = pl->hp;
-    run_setup(c, pl);
-    const size_t kk = 9 * (size_t)hp.npe * hp.npe;
-    std::vector<double> ke(std::max<size_t>(1, (size_t)hp.Ne * kk)), binv(9 * (size_t)hp.Nn);
-    if (hp.Ne > 0)
-        CK(cudaMemcpyAsync(ke.data(), pl->ke64.p, (size_t)hp.Ne * kk * sizeof(double),
-                           cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(binv.data(), pl->binv64.p, binv.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                       c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    const double lam = pg::estimate_lambda_max(pl->prob_view, ke, binv, 30);
-    pl->lambda_max = std::isfinite(lam) && lam > 0 ? lam : (double)hp.npe;
+    pl->lambda_max = device_lambda_max(c, pl, 30);
 }
 
 // Coefficients of u = a t - b D^-1 K t (t = D^-1 r): two steps of the
@@ -517,24 +576,29 @@ void prepare_plan_data(pg_ctx* c, Plan* pl, const pg_options& o) {
     if (o.smoother == PG_SMOOTHER_CHEBYSHEV) ensure_smoother(c, pl);
 }
 
-// prepare_plan_data for many plans (a batch): the element matrices and block
-// inverses come down in chunks of plates, the host work (coarse matrices,
-// eigenvalue estimates) runs on worker threads, and the results go back up.
+// prepare_plan_data for many plans (a batch): the eigenvalue estimates run on
+// the device for all plates before one wait; for the coarse matrices the
+// element matrices come down in chunks of plates, the host work runs on
+// worker threads, and the results go back up.
 void prepare_many(pg_ctx* c, const std::vector<Plan*>& pls, const pg_options& o) {
     const bool coarse = o.preconditioner == PG_PRECOND_TWO_LEVEL;
     const bool cheb = o.smoother == PG_SMOOTHER_CHEBYSHEV;
-    std::vector<Plan*> todo;
+    std::vector<Plan*> todo, lam_todo;
     for (Plan* pl : pls) {
         if (cheb && pl->hp.rings != 2)
             throw Fail{PG_EINVAL, "the Chebyshev smoother needs a plan made with it (2-ring halo)"};
-        if ((coarse && !pl->hp.coarse) || (cheb && !(pl->lambda_max > 0))) todo.push_back(pl);
+        if (coarse && !pl->hp.coarse) todo.push_back(pl);
+        if (cheb && !(pl->lambda_max > 0)) lam_todo.push_back(pl);
     }
+    // eigenvalue estimates: every plate's power steps queued back to back
+    for (Plan* pl : lam_todo) queue_power_steps(c, pl, 30);
+    for (Plan* pl : lam_todo) pl->lambda_max = lambda_from_power(c, pl, 30);
     const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
     for (size_t i = 0; i < todo.size();) {
         size_t j = i, elems = 0;
         while (j < todo.size() && (j == i || elems + (size_t)todo[j]->hp.Ne <= 1500000)) elems += todo[j++]->hp.Ne;
         const size_t m = j - i;
-        std::vector<std::vector<double>> ke(m), binv(m);
+        std::vector<std::vector<double>> ke(m);
         for (size_t k = 0; k < m; k++) {
             Plan* pl = todo[i + k];
             run_setup(c, pl);
@@ -543,23 +607,15 @@ void prepare_many(pg_ctx* c, const std::vector<Plan*>& pls, const pg_options& o)
             if (pl->hp.Ne > 0)
                 CK(cudaMemcpyAsync(ke[k].data(), pl->ke64.p, (size_t)pl->hp.Ne * kk * sizeof(double),
                                    cudaMemcpyDeviceToHost, c->stream));
-            if (cheb && !(pl->lambda_max > 0)) {
-                binv[k].resize(9 * (size_t)pl->hp.Nn);
-                CK(cudaMemcpyAsync(binv[k].data(), pl->binv64.p, binv[k].size() * sizeof(double),
-                                   cudaMemcpyDeviceToHost, c->stream));
-            }
         }
         CK(cudaStreamSynchronize(c->stream));
         std::vector<std::string> err(m);
-        std::vector<double> lam(m, 0.0);
         std::atomic<size_t> next{0};
         auto work = [&]() {
             for (size_t k; (k = next.fetch_add(1)) < m;) {
                 Plan* pl = todo[i + k];
                 try {
-                    if (coarse && !pl->hp.coarse) err[k] = pg::build_coarse(pl->prob_view, ke[k], pl->hp);
-                    if (err[k].empty() && cheb && !(pl->lambda_max > 0))
-                        lam[k] = pg::estimate_lambda_max(pl->prob_view, ke[k], binv[k], 30);
+                    err[k] = pg::build_coarse(pl->prob_view, ke[k], pl->hp);
                 } catch (...) {
                     err[k] = "host set-up of the batch failed";
                 }
@@ -572,9 +628,7 @@ void prepare_many(pg_ctx* c, const std::vector<Plan*>& pls, const pg_options& o)
         for (size_t k = 0; k < m; k++) {
             if (!err[k].empty()) throw Fail{PG_EINVAL, err[k]};
             Plan* pl = todo[i + k];
-            if (coarse && pl->hp.coarse && pl->ainv64.n == 0) upload_coarse(c, pl);
-            if (cheb && !(pl->lambda_max > 0))
-                pl->lambda_max = std::isfinite(lam[k]) && lam[k] > 0 ? lam[k] : (double)pl->hp.npe;
+            if (pl->hp.coarse && pl->ainv64.n == 0) upload_coarse(c, pl);
         }
         i = j;
     }
@@ -807,24 +861,6 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_
 // run_solve, and when a mixed solve stagnated (with o.fallback) the same
 // solve again in FP64 on the same plan; info then describes the FP64 solve,
 // with fallback = 1 and solve_ms covering both.
-// y = K x on the device (colour by colour, then the identity rows of the
-// constrained DOFs), queued on the context stream.  The plan's set-up must
-// have run.
-void queue_apply_k(pg_ctx* c, Plan* pl, const double* x, double* y) {
-    const pg::HostPlan& hp = pl->hp;
-    const size_t n = 3 * (size_t)hp.Nn;
-    CK(cudaMemsetAsync(y, 0, n * sizeof(double), c->stream));
-    for (int col = 0; col < hp.colors; col++) {
-        const int off = (int)hp.color_offsets[col], cnt = (int)hp.color_offsets[col + 1] - off;
-        if (cnt > 0)
-            pg::applyk_color_kernel<<<(cnt + 127) / 128, 128, 0, c->stream>>>(
-                cnt, pl->cob_list.p + off, hp.npe, pl->mesh_elements.p, pl->ke64.p, x, y);
-        CK(cudaGetLastError());
-    }
-    pg::bc_copy_kernel<<<((int)n + 255) / 256, 256, 0, c->stream>>>((int)n, pl->cons.p, x, y);
-    CK(cudaGetLastError());
-}
-
 // Queues ||F - K x||^2 and ||F||^2 of plan pl into pl->nrm (uses pl->kx).
 void queue_true_residual(pg_ctx* c, Plan* pl, const double* x, const float* F) {
     const int n = 3 * pl->hp.Nn;
