@@ -270,6 +270,22 @@ std::string build_partition(const pg_problem& p, int G, int rings, HostPlan& pla
     return "";
 }
 
+// sum_{k in [k0, k1)} a[k] b[k] in four interleaved partial sums (the
+// dependent additions of a single running sum would bound the dense steps
+// of the coarse set-up by the adder's latency)
+static double dot4(const double* a, const double* b, int k0, int k1) {
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    int k = k0;
+    for (; k + 4 <= k1; k += 4) {
+        s0 += a[k] * b[k];
+        s1 += a[k + 1] * b[k + 1];
+        s2 += a[k + 2] * b[k + 2];
+        s3 += a[k + 3] * b[k + 3];
+    }
+    for (; k < k1; k++) s0 += a[k] * b[k];
+    return (s0 + s1) + (s2 + s3);
+}
+
 std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, HostPlan& plan) {
     const int G = plan.G, Nn = plan.Nn, npe = plan.npe, nd = 3 * npe;
     const int C = 3 * G;
@@ -339,8 +355,8 @@ std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, H
     for (int i = 0; i < C; i++) dmax = std::max(dmax, Ac[(size_t)i * C + i]);
     plan.dropped_modes = 0;
     for (int j = 0; j < C; j++) {
-        double d = Ac[(size_t)j * C + j];
-        for (int k = 0; k < j; k++) d -= Lm[(size_t)j * C + k] * Lm[(size_t)j * C + k];
+        const double* lrow = Lm.data() + (size_t)j * C;
+        const double d = Ac[(size_t)j * C + j] - dot4(lrow, lrow, 0, j);
         if (!(d > 1e-13 * dmax)) {
             keep[j] = 0;
             plan.dropped_modes++;
@@ -349,28 +365,27 @@ std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, H
         const double ljj = std::sqrt(d);
         Lm[(size_t)j * C + j] = ljj;
         for (int i = j + 1; i < C; i++) {
-            double s = Ac[(size_t)i * C + j];
-            for (int k = 0; k < j; k++) s -= Lm[(size_t)i * C + k] * Lm[(size_t)j * C + k];
+            const double s = Ac[(size_t)i * C + j] - dot4(Lm.data() + (size_t)i * C, lrow, 0, j);
             Lm[(size_t)i * C + j] = s / ljj;
         }
     }
-    // inverse of L (lower), dropped columns stay zero
-    std::vector<double> Li((size_t)C * C, 0.0);
+    // inverse of L (lower), dropped columns stay zero; kept transposed
+    // (Lt[j][k] = (L^-1)[k][j]) so that both loops below run along rows
+    std::vector<double> Lt((size_t)C * C, 0.0);
     for (int j = 0; j < C; j++) {
         if (!keep[j]) continue;
-        Li[(size_t)j * C + j] = 1.0 / Lm[(size_t)j * C + j];
+        double* lj = Lt.data() + (size_t)j * C;
+        lj[j] = 1.0 / Lm[(size_t)j * C + j];
         for (int i = j + 1; i < C; i++) {
             if (!keep[i]) continue;
-            double s = 0;
-            for (int k = j; k < i; k++) s += Lm[(size_t)i * C + k] * Li[(size_t)k * C + j];
-            Li[(size_t)i * C + j] = -s / Lm[(size_t)i * C + i];
+            const double* li = Lm.data() + (size_t)i * C;
+            lj[i] = -dot4(li, lj, j, i) / li[i];
         }
     }
     std::vector<double> Ainv((size_t)C * C, 0.0);  // L^-T L^-1
     for (int i = 0; i < C; i++)
         for (int j = 0; j <= i; j++) {
-            double s = 0;
-            for (int k = i; k < C; k++) s += Li[(size_t)k * C + i] * Li[(size_t)k * C + j];
+            const double s = dot4(Lt.data() + (size_t)i * C, Lt.data() + (size_t)j * C, i, C);
             Ainv[(size_t)i * C + j] = s;
             Ainv[(size_t)j * C + i] = s;
         }
@@ -381,6 +396,7 @@ std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, H
     plan.cagg.clear();
     plan.ainv_off.assign(G + 1, 0);
     plan.ainv.clear();
+    plan.ainv.reserve((size_t)G * 3 * 10 * C);  // about 9 aggregates per part; grows if needed
     plan.max_kagg = 0;
     std::vector<int> slot_of(G, -1);
     for (int g = 0; g < G; g++) {
