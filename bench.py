@@ -212,6 +212,32 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback (6.65 TB/s earlier measurement on this pool)"
 
 
+def l2_copy_peak(local):
+    """Copy bandwidth (read + write bytes per second, GB/s) with a working
+    set of 2 x 32 MB, which stays in L2, measured in this run with CUDA
+    events.  Smaller copies are bound by launch latency and 2 x 48 MB
+    already spills to HBM (measured: 6.9, 8.2 and 6.1 TB/s at 2 x 24, 32 and
+    48 MB), so this is a lower bound of the L2 roof against which the
+    persistent kernel is also compared (its vectors live in shared memory
+    and L2)."""
+    import torch
+
+    a = torch.ones(8 << 20, dtype=torch.float32, device=f"cuda:{local}")
+    b = torch.empty_like(a)
+    for _ in range(10):
+        b.copy_(a)
+    s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s_.record()
+    reps = 400
+    for _ in range(reps):
+        b.copy_(a)
+    e_.record()
+    torch.cuda.synchronize()
+    ms = s_.elapsed_time(e_)
+    return 2.0 * a.numel() * 4 * reps / (ms * 1e-3) / 1e9
+
+
 def ncu_traffic(kernel_tag, workload):
     """DRAM bytes per launch from the committed ncu summary, if present."""
     p = os.path.join(ROOT, "profiles", f"{kernel_tag}_{workload}.txt")
@@ -475,6 +501,7 @@ def run_plategpu(args, world, rank, local):
     alg_bytes = float(WORDS[VARIANTS[head][2]]) * n * word * iters
     peak, peak_src = hbm_peak()
     achieved = alg_bytes / (H["kernel_ms"] * 1e-3) / 1e9
+    l2_peak = l2_copy_peak(local)
     kernel_tag = "pcg_" + head
     line = {
         "metric": METRIC, "value": H["value"], "unit": "ms", "n_gpus": world,
@@ -499,7 +526,10 @@ def run_plategpu(args, world, rank, local):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": ncu_traffic(kernel_tag, args.workload),
                      "kernel": f"{kernel_tag}_kernel", "peak_source": peak_src,
-                     "algorithmic_bytes_per_launch": alg_bytes},
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "l2": {"peak": l2_peak, "frac": achieved / l2_peak, "unit": "GB/s",
+                            "peak_source": ("copy with a 2 x 32 MB working set, L2-resident, measured "
+                                            "in this run (a lower bound of the L2 bandwidth)")}},
         "e2e": {"value": e2e_value, "unit": "ms", "h2d_bytes_per_step": 4 * n,
                 "d2h_bytes_per_step": 8 * n + 64},
         "first_solve_new_mesh_ms": cold_ms,
