@@ -2,9 +2,20 @@
 //
 //   ke_kernel          element stiffness, FP64 (and an FP32 copy), per element
 //   binv_kernel        3x3 block diagonal, constrained rule, FP64 inversion
-//   applyk_*_kernel    y = K x colour by colour (test hook, reference layout)
+//   task_ke_kernel     the per-task 3 x 3npe blocks the PCG kernels read
+//   applyk_*_kernel    y = K x colour by colour (test hook, reference layout;
+//                      also the FP64 K x of the set-up and correction steps)
+//   power_start_kernel, binv_apply_kernel
+//                      lambda_max(D^-1 K) power steps for the Chebyshev smoother
+//   residual_*_kernel, add_kernel
+//                      FP64 correction after a stagnated mixed solve
+//   elem_moments_kernel, node_moments_kernel
+//                      nodal bending moments
 //   pcg_kernel         persistent cooperative PCG: the whole solve in one
 //                      launch, one grid-wide wait per iteration
+//   pcg_batch_kernel   many plates, one team of blocks per plate queue
+//   (pcg_multi_kernel, several load cases of one plate in lockstep, is in
+//   multi.cuh)
 //
 // PCG form.  The reference runs textbook PCG (pcg.ts:98-215) with three
 // reductions per iteration.  Here the Chronopoulos-Gear recurrence computes
