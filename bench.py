@@ -2,21 +2,32 @@
 """Benchmark: milliseconds per 60k-DOF plate solve at FP64-checked error 1e-6.
 
 One step = one complete solve of the plate_q4_141 workload (141x141 Q4
-Mindlin, 60,492 DOF, seeded synthetic loads and column supports): element
-stiffness and block-Jacobi set-up on the GPU, then the persistent PCG
-launch, inputs resident in HBM.  ``value`` is milliseconds per solve for the
-whole job (lower is better); ``e2e`` is the same through the public C ABI
-(pg_solve) from host buffers, copies included.  L2 is flushed (256 MiB
-write) between timed steps; each step is timed with CUDA events on the
-solver's stream.
+Mindlin, 60,492 DOF, seeded synthetic loads and column supports) through
+pg_plan_solve_device: the persistent PCG launch with its result readback,
+inputs resident in HBM (the plan's element stiffness, block-Jacobi and
+coarse set-up ran in the warm-up and is cached).  Seven methods are timed
+(FP64 / mixed precision x block Jacobi / two-level x Chebyshev smoother);
+``value`` is the fastest whose FP64-checked error is <= 1e-6, in ms per
+solve for the whole job (lower is better).  ``e2e`` is the same through
+the public C ABI (pg_solve) from host buffers, copies included;
+``first_solve_new_mesh_ms`` a first pg_solve in a new context (the plan's
+set-up included).  L2 is flushed (256 MiB write) between timed steps; each
+step is timed with CUDA events on the solver's stream.  ``roofline``
+compares the PCG kernel's algorithmic bytes per second with the measured
+HBM copy peak and with an in-run L2-resident copy.
 
-Multi-GPU: a single plate does not shard (the solve is bound by grid-wide
-synchronisation latency), so --gpus N runs N independent replicas, one per
-rank, and ``value`` = max-over-ranks time / (N * steps).
+Further sections of the line: ``load_cases`` (four loads of the plate
+through pg_solve_load_cases against the same loads one by one),
+``other_configs`` (plate_q4_32, plate_dkt_200 and the unstructured
+plate_holes_dkt, four methods each), ``batch`` (a 256-plate uneven batch,
+Q4 and DKT, sides 16-256, four methods, the fastest that meets the error
+bar reported) and ``cpu_baseline`` (the reference-precision CPU solver,
+one core).  --cases 0, --other-configs 0, --batch 0 skip sections.
 
-The line also carries ``batch``: solves/s and per-plate p50/p99 of a
-256-plate uneven batch (Q4 and DKT, sides 16-256) through the batched
-solver (--batch 0 skips it).
+Multi-GPU: a single plate does not shard (the solve is bound by the
+latency of the exchange between blocks), so --gpus N runs N independent
+replicas, one per rank, and ``value`` = max-over-ranks time / (N * steps);
+the batch is sharded across the ranks by estimated cost.
 
 --impl reference times the reference's CPU algorithm (the oracle's
 restatement of solvePCG + applyGlobalK in reference precision; the
