@@ -585,10 +585,9 @@ void prepare_many(pg_ctx* c, const std::vector<Plan*>& pls, const pg_options& o)
     const bool cheb = o.smoother == PG_SMOOTHER_CHEBYSHEV;
     std::vector<Plan*> todo, lam_todo;
     for (Plan* pl : pls) {
-        if (cheb && pl->hp.rings != 2)
-            throw Fail{PG_EINVAL, "the Chebyshev smoother needs a plan made with it (2-ring halo)"};
         if (coarse && !pl->hp.coarse) todo.push_back(pl);
-        if (cheb && !(pl->lambda_max > 0)) lam_todo.push_back(pl);
+        // plates on a 1-ring halo run with block Jacobi (plate_options)
+        if (cheb && pl->hp.rings == 2 && !(pl->lambda_max > 0)) lam_todo.push_back(pl);
     }
     // eigenvalue estimates: every plate's power steps queued back to back
     for (Plan* pl : lam_todo) queue_power_steps(c, pl, 30);
@@ -1134,6 +1133,16 @@ int batch_capacity(const pg_options& o, int rings, int npe) {
     return cap[mixed ? 1 : 0][npe == 3 ? 1 : 0][rings == 2 ? 1 : 0];
 }
 
+// The options a plate of a batch runs with: the batch's, but the
+// block-Jacobi smoother where the plate's plan has a 1-ring halo (a plate
+// whose 2-ring layout for the Chebyshev smoother does not fit in shared
+// memory even on the whole device).
+pg_options plate_options(const pg_options& o, const Plan* pl) {
+    pg_options oi = o;
+    if (pl->hp.rings != 2) oi.smoother = PG_SMOOTHER_BLOCK_JACOBI;
+    return oi;
+}
+
 std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int count,
                                       const pg_options& o) {
     auto b = std::make_unique<pg_batch>();
@@ -1150,10 +1159,10 @@ std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int co
     }
     // schedule, then check every plate's layout at its team size; lower the
     // capacity of the plates whose parts do not fit and reschedule
-    std::vector<int> caps(count), kinds(count);
+    std::vector<int> caps(count), kinds(count), rings(count, b->rings);
     for (int i = 0; i < count; i++) kinds[i] = (int)probs[i].nodes_per_element;
     for (int i = 0; i < count; i++) {
-        caps[i] = batch_capacity(o, b->rings, (int)probs[i].nodes_per_element);
+        caps[i] = batch_capacity(o, rings[i], (int)probs[i].nodes_per_element);
         // a plate too large for the whole device at the first guess gets the
         // whole device anyway; its layout (element blocks and A_c^-1 rows then
         // possibly in L2, as in a one-plate solve) is checked below
@@ -1169,18 +1178,26 @@ std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int co
         bool fits = true;
         for (int i = 0; i < count; i++) {
             const int G = b->sched.plate_size[i];
-            b->plans.push_back(build_plan(c, probs[i], G, b->rings));
+            b->plans.push_back(build_plan(c, probs[i], G, rings[i]));
             int ke_mode = 0;
             bool ainv = false;
             try {
-                choose_layout(c, b->plans.back()->hp, o, &ke_mode, &ainv);
+                choose_layout(c, b->plans.back()->hp, plate_options(o, b->plans.back().get()), &ke_mode, &ainv);
             } catch (const Fail&) {
                 fits = false;
-                caps[i] = caps[i] * 3 / 4;
+                if (rings[i] == 2 && G == c->sms) {
+                    // the 2-ring halo does not fit even on the whole device:
+                    // this plate runs with a 1-ring halo and block Jacobi
+                    rings[i] = 1;
+                    caps[i] = std::max(batch_capacity(o, 1, (int)probs[i].nodes_per_element),
+                                       (nodes[i] + c->sms - 1) / c->sms);
+                } else {
+                    caps[i] = caps[i] * 3 / 4;
+                }
             }
         }
         if (fits) break;
-        if (attempt == 5) throw Fail{PG_EUNSUPPORTED, "batch plates too large for shared memory"};
+        if (attempt == 7) throw Fail{PG_EUNSUPPORTED, "batch plates too large for shared memory"};
     }
     cudaStream_t st = c->stream;
     for (const pg::BatchPhase& P : b->sched.phases) {
@@ -1252,11 +1269,12 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
     int smem = 0;
     for (int i = 0; i < count; i++) {
         Plan* pl = b->plans[i].get();
+        const pg_options oi = plate_options(o, pl);
         int ke_mode = 0;
         bool ainv = false;
-        const pg::SmemLayout L = choose_layout(c, pl->hp, o, &ke_mode, &ainv);
+        const pg::SmemLayout L = choose_layout(c, pl->hp, oi, &ke_mode, &ainv);
         reset_for_launch(c, pl, b->res.p + i);
-        pg::PcgArgs ai = fill_args(pl, o, L, ke_mode, ainv, b->abort_flag.p, b->res.p + i);
+        pg::PcgArgs ai = fill_args(pl, oi, L, ke_mode, ainv, b->abort_flag.p, b->res.p + i);
         ai.timing = 0;
         ai.test_stall = 0;
         ai.trace_it = -1;
@@ -1318,7 +1336,8 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
         converged += r[i].converged ? 1 : 0;
         if (infos) {
             std::memset(&infos[i], 0, sizeof(pg_info));
-            fill_info(&infos[i], r[i], b->plans[i].get(), o, pg::kMaxThreads, a[i].L.total);
+            fill_info(&infos[i], r[i], b->plans[i].get(), plate_options(o, b->plans[i].get()),
+                      pg::kMaxThreads, a[i].L.total);
             infos[i].status = r[i].status;
             infos[i].solve_ms = plate_ms[i];
             infos[i].plan_cached = 1;

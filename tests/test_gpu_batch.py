@@ -179,3 +179,31 @@ def test_plate_larger_than_the_first_capacity_guess_gets_the_whole_device(gpu_ct
     x1, one = gpu_ctx.solve(probs[2], _lib.make_options(ctas=148, **kw))
     assert abs(infos[2].iterations - one.iterations) <= 1
     assert rel_err(xs[2], x1) < 1e-9
+
+
+def test_plate_too_large_for_the_smoother_halo_runs_with_block_jacobi(gpu_ctx, small_batch):
+    """With the Chebyshev smoother a 66,049-node DKT plate's 2-ring layout
+    does not fit in FP64 even on the whole device: that plate runs with a
+    1-ring halo and block-Jacobi smoothing (lambda_max reported 0) and gives
+    the one-plate result of that method, while the other plates keep the
+    smoother."""
+    from plategpu import coloring, mesher, problem
+    from plategpu.types import PlateMaterial, PlateSupport
+
+    m = mesher.split_triangle_mesh(10, 10, 256, 256, jitter=0.2, seed=8)
+    sup = [PlateSupport("fixed", "all_edges")]
+    cons = problem.identifyConstrainedDOFs(m, sup)
+    F = problem.pressure_load_vector(m, 2e3).astype(np.float32)
+    problem.applyBCsToRHS(F, cons)
+    big = workloads.Workload("dkt256", m, PlateMaterial(2.1e11, 0.3, 0.1),
+                             coloring.computeElementColoringGreedy(m), sup, cons, F)
+    kw = dict(tolerance=1e-9, max_iterations=20000, stop_rule=_lib.PG_STOP_RELATIVE,
+              precision=_lib.PG_PREC_FP64, preconditioner=_lib.PG_PRECOND_TWO_LEVEL)
+    probs = probs_of([small_batch[0], small_batch[2]]) + probs_of([big])
+    xs, infos, bi = gpu_ctx.solve_batch(probs, _lib.make_options(smoother=_lib.PG_SMOOTHER_CHEBYSHEV, **kw))
+    assert bi.converged == 3
+    assert infos[0].smoother_lambda_max > 0 and infos[1].smoother_lambda_max > 0
+    assert infos[2].smoother_lambda_max == 0 and infos[2].ctas == 148
+    x1, one = gpu_ctx.solve(probs[2], _lib.make_options(ctas=148, **kw))
+    assert abs(infos[2].iterations - one.iterations) <= 1
+    assert rel_err(xs[2], x1) < 1e-9
