@@ -50,20 +50,23 @@ sys.path.insert(0, os.path.join(ROOT, "gpu-gauntlet_b200"))
 METRIC = "ms per 60k-DOF plate solve at 1e-6 FP64-checked error: learned/mixed vs plain PCG"
 FALLBACK_HBM_GBS = 6650.0
 # name -> (precision, preconditioner, smoother); "fp64" is the plain
-# method.  Each runs at the residual tolerance that gives 5e-7 to 9e-7 FP64
-# error on plate_q4_141 (block Jacobi 1e-6, two-level 5e-6; the two-level
+# method.  Each runs at the residual tolerance of TOLERANCES (the two-level
 # iterates are closer to the solution at equal residual), and the bench
-# checks the error of every variant against the FP64 truth.
+# checks the error of every variant against the FP64 truth on the plate's
+# own load and ACCURACY_LOADS seeded random-field loads.
 VARIANTS = {"fp64": ("fp64", "bj", "bj"), "mixed": ("mixed", "bj", "bj"),
             "mixed_cheb": ("mixed", "bj", "cheb"),
             "fp64_two_level": ("fp64", "tl", "bj"), "mixed_two_level": ("mixed", "tl", "bj"),
             "fp64_two_level_cheb": ("fp64", "tl", "cheb"),
             "mixed_two_level_cheb": ("mixed", "tl", "cheb")}
-# residual tolerances (block Jacobi, two-level) that reach 5e-7 to 9e-7 FP64
-# error: plate_q4_141 as above; the reference's DKT formulation needs a
-# tighter residual for the same error (1.15e-6 at 1e-6, 1.6e-7 at 1e-7);
-# plate_q4_32 runs at its configured rtol 1e-8
-TOLERANCES = {"plate_q4_141": (1e-6, 5e-6), "plate_dkt_200": (1e-7, 1e-7), "plate_q4_32": (1e-8, 1e-8),
+# residual tolerances (block Jacobi, two-level) that keep the FP64 error at
+# or below 1e-6 on the plate's own load and on seeded random-field loads:
+# plate_q4_141 two-level 3e-6 (at 5e-6 a seeded load reached 1.35e-6; at
+# 3e-6 the worst of 17 loads is about 6e-7 in a CPU model of the FP64
+# method); the reference's DKT formulation needs a tighter residual for the
+# same error (1.15e-6 at 1e-6, 1.6e-7 at 1e-7); plate_q4_32 runs at its
+# configured rtol 1e-8
+TOLERANCES = {"plate_q4_141": (1e-6, 3e-6), "plate_dkt_200": (1e-7, 1e-7), "plate_q4_32": (1e-8, 1e-8),
               # FP64 error about 2.5 x the relative residual on this mesh
               "plate_holes_dkt": (2e-7, 2e-7)}
 WORKLOAD_DATA = {
@@ -78,6 +81,12 @@ WORKLOAD_DATA = {
 # schedule: K.p 2, x 3, r 3, block Jacobi 5, p 3); the Chebyshev smoother
 # adds its K.t (2) and a second block-Jacobi product (3)
 WORDS = {"bj": 16, "cheb": 21}
+# seeded random-field loads (Gaussian random field pressure + 0-16 point
+# loads) on which every variant's FP64 error is checked besides the plate's
+# own load; a variant is eligible for the headline only when its largest
+# error over all of them is <= 1e-6
+ACCURACY_LOADS = 16
+ACCURACY_SEED = 77
 
 
 def parse_args():
@@ -275,9 +284,9 @@ def oracle_checks(wl, want_baseline=True):
     F = wl.F.astype(np.float64)
     ke64 = O.all_ke(m.nodes, m.elements, npe, mat.E, mat.nu, mat.t, elem_t=mat.elem_t,
                     mode=O.FP64)
-    xs, rel = O.truth_solve(m.nodeCount, m.elements, npe, ke64, wl.cons_mask, F)
-    A = O.assemble(m.nodeCount, m.elements, npe, ke64, wl.cons_mask)
-    out = {"truth": xs, "A": A}
+    solve = O.truth_factor(m.nodeCount, m.elements, npe, ke64, wl.cons_mask)
+    xs, rel = solve(F)
+    out = {"truth": xs, "A": solve.A, "solve": solve}
     if want_baseline:
         keR = O.all_ke(m.nodes, m.elements, npe, mat.E, mat.nu, mat.t, elem_t=mat.elem_t,
                        mode=O.REF)
@@ -314,8 +323,20 @@ def accuracy(x, chk):
 # arms
 # ---------------------------------------------------------------------------
 
+def bench_config(wl, args):
+    """The workload description that both arms print as `config` (the
+    method each arm ran is reported beside it, not in it)."""
+    return {"workload": args.workload, "dof": wl.n_dof, "elements": wl.mesh.elementCount,
+            "accuracy": "FP64 relative L2 error <= 1e-6 vs the FP64 truth",
+            "l2": "GPU arm: flushed between steps (256 MiB write)",
+            "parallelism": "replicas"}
+
+
 def run_reference(args, world, rank):
-    """The reference CPU algorithm (oracle port, reference precision)."""
+    """The reference CPU algorithm (oracle port, reference precision): each
+    step is one complete solve as solvePlate runs it -- element matrices,
+    block diagonal and its inversion, then PCG to the reference's tolerance
+    1e-6 with the iteration cap raised so that it converges."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -337,27 +358,24 @@ def run_reference(args, world, rank):
         return O.solve_pcg(m.nodeCount, m.elements, npe, ke, offs, flat, wl.cons_mask, bd, F,
                            tol, maxit, O.REF)
 
-    # warm-up: one full solve gives the iteration count of a complete solve
-    _x, full_iters, _r, conv = solve(20000, 1e-6)
-    for _ in range(max(0, args.warmup - 1)):
-        solve(20, 0.0)
-    sample_iters = 150
-    times = []
+    for _ in range(args.warmup):
+        solve(20000, 1e-6)
+    times, full_iters, conv = [], 0, False
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        solve(sample_iters, 0.0)
+        _x, full_iters, _r, conv = solve(20000, 1e-6)
         times.append((time.perf_counter() - t0) * 1e3)
-    step_ms = statistics.mean(times)
-    value = step_ms * full_iters / sample_iters
-    sample = (f"set-up + {sample_iters} PCG iterations per step, scaled by the "
-              f"{full_iters} iterations a full reference-precision solve of {args.workload} "
-              f"takes at tolerance 1e-6 (converged={conv}); single thread")
+    value = statistics.mean(times)
+    sample = (f"one complete reference-precision solve of {args.workload} per step "
+              f"(set-up once + {full_iters} PCG iterations to tolerance 1e-6, "
+              f"converged={conv}) by the C restatement of solvePlate/solvePCG/applyGlobalK; "
+              "single thread (the reference's JavaScript solver runs on one thread)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "ms",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": step_ms, "higher_is_better": False, "scaling": "weak",
+            "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 storage / f64 arithmetic",
-            "data": "synthetic (seeded workload)",
-            "config": {"workload": args.workload, "dof": wl.n_dof, "parallelism": "replicas"},
+            "data": WORKLOAD_DATA.get(args.workload, "synthetic (seeded workload)"),
+            "config": bench_config(wl, args), "iterations": full_iters,
             "cpu_baseline": {"value": value, "unit": "ms", "cores": 1, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0,
@@ -389,8 +407,10 @@ def variant_options(args, name):
         reliable_delta=0.01 if (prec == _lib.PG_PREC_MIXED and smoother == "cheb") else 0.0)
 
 
-def time_variant(args, world, local, ctx, prob, name, stream, F_dev, x_dev, flush):
-    """Warm-up + timed device-resident solves of one variant."""
+def time_variant(args, world, local, ctx, prob, name, stream, F_dev, x_dev, flush, extra_F=None):
+    """Warm-up + timed device-resident solves of one variant; then, untimed,
+    the loads of extra_F (device [k, n] float) with the same plan, whose
+    solutions are returned as "x_extra"."""
     import torch
 
     opts = variant_options(args, name)
@@ -412,6 +432,13 @@ def time_variant(args, world, local, ctx, prob, name, stream, F_dev, x_dev, flus
         barrier(world)
     step_ms = [s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)]
     total = max_over_ranks(world, sum(step_ms), local)
+    x_main = x_dev.cpu().numpy().copy()
+    x_extra = []
+    if extra_F is not None:
+        with torch.cuda.stream(stream):
+            for k in range(extra_F.shape[0]):
+                plan.solve_device(opts, extra_F[k].data_ptr(), x_dev.data_ptr())
+                x_extra.append(x_dev.cpu().numpy().copy())
     plan.close()
     return {"opts": opts, "value": total / (world * args.steps), "step_ms": step_ms,
             "kernel_ms": statistics.mean(i.solve_ms for i in infos),
@@ -421,7 +448,7 @@ def time_variant(args, world, local, ctx, prob, name, stream, F_dev, x_dev, flus
             "reliable_updates": infos[-1].reliable_updates,
             "true_rel_residual": infos[-1].true_rel_residual,
             "ctas": infos[-1].ctas, "threads": infos[-1].threads,
-            "x": x_dev.cpu().numpy().copy()}
+            "x": x_main, "x_extra": x_extra}
 
 
 def run_plategpu(args, world, rank, local):
@@ -445,25 +472,42 @@ def run_plategpu(args, world, rank, local):
         if v not in VARIANTS:
             raise SystemExit(f"unknown variant {v!r}")
 
+    check = rank == 0 and world == 1 and not args.no_cpu_baseline
+    extra_F = None
+    if check and args.workload == "plate_q4_141":
+        extra_F = torch.from_numpy(
+            workloads.random_field_loads(wl, ACCURACY_LOADS, ACCURACY_SEED)).to(f"cuda:{local}")
+
     sampler = ClockSampler(local) if rank == 0 else None
     if sampler:
         sampler.start()
-    res = {v: time_variant(args, world, local, ctx, prob, v, stream, F_dev, x_dev, flush)
+    res = {v: time_variant(args, world, local, ctx, prob, v, stream, F_dev, x_dev, flush, extra_F)
            for v in variants}
     clocks = sampler.stop() if sampler else None
 
     chk = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if check:
         chk = oracle_checks(wl, want_baseline=True)
+        extra_truth = ([chk["solve"](f)[0] for f in extra_F.cpu().numpy()]
+                       if extra_F is not None else [])
         for v in variants:
             res[v]["accuracy"] = accuracy(res[v]["x"], chk)
-    # headline: the fastest variant whose FP64-checked error meets 1e-6
-    # (without the checker, the fastest variant whose true residual met the
-    # tolerance)
+            errs = [res[v]["accuracy"]["rel_l2_vs_fp64_truth"]] + [
+                float(np.linalg.norm(x - xt) / np.linalg.norm(xt))
+                for x, xt in zip(res[v]["x_extra"], extra_truth)]
+            res[v]["accuracy"]["loads"] = {
+                "count": len(errs), "rel_l2_max": max(errs),
+                "rel_l2_p50": float(np.percentile(errs, 50)),
+                "rel_l2_p99": float(np.percentile(errs, 99)),
+                "loads": (f"the plate's own load + {len(errs) - 1} seeded random-field loads "
+                          f"(seed {ACCURACY_SEED})")}
+    # headline: the fastest variant whose FP64-checked error meets 1e-6 on
+    # every load checked (without the checker, the fastest variant whose
+    # true residual met the tolerance)
     def meets(v):
         acc = res[v].get("accuracy")
         if acc is not None:
-            return acc["rel_l2_vs_fp64_truth"] <= 1e-6
+            return acc["loads"]["rel_l2_max"] <= 1e-6
         return res[v]["true_rel_residual"] <= res[v]["tolerance"]
     ok = [v for v in variants if meets(v)] or variants
     head = min(ok, key=lambda v: res[v]["value"])
@@ -521,12 +565,11 @@ def run_plategpu(args, world, rank, local):
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if VARIANTS[head][0] == "fp64" else "f32 inner / f64 refinement",
         "data": WORKLOAD_DATA.get(args.workload, "synthetic (seeded workload)"),
-        "config": {"workload": args.workload, "dof": n, "elements": wl.mesh.elementCount,
-                   "method": head,
+        "config": bench_config(wl, args),
+        "method": {"name": head,
                    "preconditioner": describe_preconditioner(VARIANTS[head], H["coarse_dim"]),
                    "stop": f"||r||/||b|| < {H['tolerance']:g}", "ctas": H["ctas"],
-                   "threads": H["threads"], "l2": "flushed between steps (256 MiB write)",
-                   "parallelism": f"replicas x{world}"},
+                   "threads": H["threads"], "replicas": world},
         "iterations": iters,
         "kernel_ms": H["kernel_ms"], "setup_ms": H["setup_ms"],
         "us_per_iteration": H["kernel_ms"] * 1e3 / max(iters, 1),
@@ -754,20 +797,27 @@ def batch_bench(args, ctx, check, world=1, rank=0, local=0):
     shards = workloads.shard_lpt([workloads.plate_cost(w) for w in ALL], world)
     B = [ALL[i] for i in shards[rank]]
     probs = [_lib.Problem(w.mesh, w.material, w.coloring, w.F, w.cons_mask) for w in B]
-    truths = {}
+    truth_jobs, pool = {}, None
     if check:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as O
+        # FP64 truth (sparse LU) of a sample: the 5 largest plates and a
+        # seeded 5% of the others, computed by worker processes while the GPU
+        # runs
+        import concurrent.futures as cf
+        import multiprocessing as mp
         rng = np.random.default_rng(11)
-        small = [i for i, w in enumerate(B) if w.mesh.nodeCount <= 30000]
-        for i in rng.choice(small, size=min(6, len(small)), replace=False).tolist():
+        by_size = sorted(range(len(B)), key=lambda i: -B[i].mesh.nodeCount)
+        rest = by_size[5:]
+        pick = by_size[:5] + rng.choice(rest, size=min(len(rest), max(6, (len(B) + 19) // 20)),
+                                        replace=False).tolist()
+        pool = cf.ProcessPoolExecutor(max_workers=min(len(pick), max(1, (os.cpu_count() or 2) - 1), 16),
+                                      mp_context=mp.get_context("spawn"))
+        for i in pick:
             w = B[i]
             m, mat = w.mesh, w.material
-            ke = O.all_ke(m.nodes, m.elements, m.nodesPerElement, mat.E, mat.nu, mat.t,
-                          elem_t=mat.elem_t, mode=O.FP64)
-            truths[i] = O.truth_solve(m.nodeCount, m.elements, m.nodesPerElement, ke, w.cons_mask, w.F)[0]
+            truth_jobs[i] = pool.submit(_truth_job, m.nodeCount, m.nodes, m.elements, m.nodesPerElement,
+                                        mat.E, mat.nu, mat.t, mat.elem_t, w.cons_mask, w.F)
     methods = BATCH_METHODS if args.batch_fp64 else BATCH_METHODS[:1]
-    rows = {}
+    rows, per_plate, fallback_plates, truth_note = {}, {}, [], None
     for name in methods:
         opts = batch_options(name)
         steps = 1 if name == "fp64_block_jacobi" else max(1, args.batch_steps)
@@ -787,6 +837,10 @@ def batch_bench(args, ctx, check, world=1, rank=0, local=0):
             rows[name] = {"unavailable": err or "failed on another rank"}
             continue
         xs, infos, bi = last
+        if check and name == methods[0]:
+            # plates that stagnated in mixed precision and were finished by
+            # the FP64 correction
+            fallback_plates = [i for i, inf in enumerate(infos) if inf.fallback]
         med = statistics.median(t)
         its = [i.iterations for i in infos]
         row = {"solves_per_s": len(ALL) / (med * 1e-3), "batch_ms": med, "batch_ms_all": t,
@@ -794,17 +848,46 @@ def batch_bench(args, ctx, check, world=1, rank=0, local=0):
                "plate_ms_max": bi.plate_ms_max, "phases": bi.phases, "teams": bi.teams,
                "fallbacks_rank0": bi.fallbacks, "converged_rank0": bi.converged,
                "iterations_median": float(np.median(its)), "iterations_max": int(max(its))}
-        if truths:
-            row["rel_l2_vs_fp64_truth_sample"] = {
-                B[i].name: float(np.linalg.norm(xs[i] - xt) / np.linalg.norm(xt)) for i, xt in truths.items()}
+        if check:
+            per_plate[name] = xs
         rows[name] = row
+
+    if check:
+        # every plate of every method against an FP64 two-level solve of the
+        # same plate to ||r||/||b|| < 1e-12 (the LU truths below pin that
+        # solve), and the LU-truth sample
+        tight = batch_options("fp64_two_level")
+        tight.tolerance = 1e-12
+        tb = ctx.batch(probs, tight)
+        xt_all = tb.solve(tight)[0]
+        tb.close()
+        truths = {i: f.result()[0] for i, f in truth_jobs.items()}
+        pool.shutdown()
+        for name, xs in per_plate.items():
+            errs = [float(np.linalg.norm(x - t) / np.linalg.norm(t)) for x, t in zip(xs, xt_all)]
+            rows[name]["rel_l2_vs_fp64_tight_all"] = {
+                "plates": len(errs), "max": max(errs), "p50": float(np.median(errs)),
+                "worst_plate": B[int(np.argmax(errs))].name}
+            samp = {B[i].name: float(np.linalg.norm(xs[i] - t) / np.linalg.norm(t))
+                    for i, t in truths.items()}
+            rows[name]["rel_l2_vs_fp64_truth_sample"] = samp
+            rows[name]["max_rel_l2_vs_fp64_truth"] = max(samp.values())
+            if name == methods[0]:
+                fb = [float(np.linalg.norm(xs[i] - xt_all[i]) / np.linalg.norm(xt_all[i]))
+                      for i in fallback_plates]
+                rows[name]["fallback_plates_rel_l2_vs_fp64_tight_max"] = max(fb) if fb else None
+        tight_vs_truth = [float(np.linalg.norm(xt_all[i] - t) / np.linalg.norm(t)) for i, t in truths.items()]
+        truth_note = {"sample_plates": len(truths),
+                      "sample": "the 5 largest plates and a seeded 5% of the others (sparse LU)",
+                      "tight_fp64_vs_truth_max": max(tight_vs_truth) if tight_vs_truth else None}
 
     def meets(name):
         r = rows[name]
         if "unavailable" in r or r["converged_rank0"] != len(B):
             return False
         e = r.get("rel_l2_vs_fp64_truth_sample")
-        return e is None or max(e.values()) <= 1e-6
+        a = r.get("rel_l2_vs_fp64_tight_all")
+        return (e is None or max(e.values()) <= 1e-6) and (a is None or a["max"] <= 1e-6)
 
     ok = [n for n in rows if meets(n)] or [n for n in rows if "unavailable" not in rows[n]]
     head = min(ok, key=lambda n: rows[n]["batch_ms"])
@@ -815,7 +898,18 @@ def batch_bench(args, ctx, check, world=1, rank=0, local=0):
            "method": head, "stop": "||r||/||b|| < 2e-7"}
     out.update(rows[head])
     out["methods"] = rows
+    if check:
+        out["accuracy_check"] = truth_note
     return out
+
+
+def _truth_job(Nn, nodes, elements, npe, E, nu, t, elem_t, cons, F):
+    """FP64 truth of one plate (oracle, in a worker process)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    ke = O.all_ke(nodes, elements, npe, E, nu, t, elem_t=elem_t, mode=O.FP64)
+    return O.truth_solve(Nn, elements, npe, ke, cons, F)
 
 
 def main():

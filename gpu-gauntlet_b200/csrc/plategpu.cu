@@ -16,6 +16,7 @@
 #include <thread>
 #include <vector>
 
+#include "internal.h"
 #include "kernels.cuh"
 #include "multi.cuh"
 #include "plan.h"
@@ -501,7 +502,8 @@ void fill_options(const pg_options* in, pg_options* o) {
     if (o->threads < 0 || o->threads > pg::kMaxThreads || (o->threads % 32) != 0)
         throw Fail{PG_EINVAL, "threads must be a multiple of 32 in [32, 576] (0 = automatic)"};
     if (o->ctas < 0) throw Fail{PG_EINVAL, "ctas must be >= 0"};
-    if (!(o->wait_timeout_ms >= 0)) throw Fail{PG_EINVAL, "wait_timeout_ms must be >= 0"};
+    if (!(o->wait_timeout_ms >= 0) || !std::isfinite(o->wait_timeout_ms) || o->wait_timeout_ms > 600000.0)
+        throw Fail{PG_EINVAL, "wait_timeout_ms must be finite and in [0, 600000]"};
     if (o->preconditioner != PG_PRECOND_BLOCK_JACOBI && o->preconditioner != PG_PRECOND_TWO_LEVEL)
         throw Fail{PG_EINVAL, "unknown preconditioner"};
     if (o->smoother != PG_SMOOTHER_BLOCK_JACOBI && o->smoother != PG_SMOOTHER_CHEBYSHEV)
@@ -1192,12 +1194,19 @@ std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int co
                     caps[i] = std::max(batch_capacity(o, 1, (int)probs[i].nodes_per_element),
                                        (nodes[i] + c->sms - 1) / c->sms);
                 } else {
-                    caps[i] = caps[i] * 3 / 4;
+                    // the next attempt gets at least twice as many blocks (a cap
+                    // below n/G), past the largest power of two the whole device,
+                    // and never less than the whole device's share, so a plate
+                    // that keeps failing reaches the whole-device attempt (and,
+                    // with a 2-ring halo, the 1-ring fallback above)
+                    const int floor_cap = (nodes[i] + c->sms - 1) / c->sms;
+                    const int below = std::max(1, (nodes[i] - 1) / std::max(1, G));
+                    caps[i] = std::max(floor_cap, std::min(caps[i] * 3 / 4, below));
                 }
             }
         }
         if (fits) break;
-        if (attempt == 7) throw Fail{PG_EUNSUPPORTED, "batch plates too large for shared memory"};
+        if (attempt == 11) throw Fail{PG_EUNSUPPORTED, "batch plates too large for shared memory"};
     }
     cudaStream_t st = c->stream;
     for (const pg::BatchPhase& P : b->sched.phases) {
@@ -1468,6 +1477,39 @@ void run_moments(pg_ctx* c, Plan* pl, const double* x_dev, double* M_dev) {
 }
 
 }  // namespace
+
+namespace pgi {
+
+std::mutex& ctx_mutex(pg_ctx* c) { return c->mu; }
+int ctx_device(const pg_ctx* c) { return c->device; }
+int ctx_sms(const pg_ctx* c) { return c->sms; }
+cudaStream_t ctx_stream(const pg_ctx* c) { return c->stream; }
+void ctx_set_error(pg_ctx* c, const std::string& msg) { c->err = msg; }
+pg_ctx* plan_ctx(const pg_plan* h) { return h ? h->ctx : nullptr; }
+
+std::string plan_operator(pg_plan* h, OperatorView* out) {
+    try {
+        Plan* pl = h->plan.get();
+        run_setup(h->ctx, pl);
+        const pg::HostPlan& hp = pl->hp;
+        out->Nn = hp.Nn;
+        out->Ne = hp.Ne;
+        out->npe = hp.npe;
+        out->inc_ptr = pl->inc_ptr.p;
+        out->inc_idx = pl->inc_idx.p;
+        out->elements = pl->mesh_elements.p;
+        out->ke32 = pl->ke32.p;
+        out->ke64 = pl->ke64.p;
+        out->binv32 = pl->binv32.p;
+        out->binv64 = pl->binv64.p;
+        out->cons = pl->cons.p;
+        return std::string();
+    } catch (const Fail& f) {
+        return f.msg;
+    }
+}
+
+}  // namespace pgi
 
 extern "C" {
 

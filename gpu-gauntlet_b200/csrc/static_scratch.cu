@@ -104,6 +104,9 @@ int fail(int st, char* msg, size_t len, const char* text) {
 
 // Device address of the static scratch on the current device, looked up
 // once per device (cudaGetSymbolAddress must run with that device current).
+// The cached address belongs to the device's current context: after a
+// cudaDeviceReset the module is loaded again and the array may move, so
+// this entry point must not be used across a device reset.
 cudaError_t scratch_address(int dev, double** out) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_scratch_ptr[dev]) {
@@ -162,8 +165,23 @@ extern "C" int pg_apply_k_static(const pg_problem* p, const double* x, double* y
     if (p->element_count > 0 &&
         (!p->elements || !p->color_offsets || !p->elements_by_color || p->color_count == 0))
         return fail(PG_EINVAL, msg, msg_len, "elements or colouring arrays are NULL");
-    if (p->element_count > 0 && p->color_offsets[p->color_count] != p->element_count)
-        return fail(PG_EINVAL, msg, msg_len, "color_offsets must end at element_count");
+    if (p->element_count > 0) {
+        // the offsets are on the host: check all of them before the kernels
+        // index elements_by_color with them
+        if (p->color_offsets[0] != 0 || p->color_offsets[p->color_count] != p->element_count)
+            return fail(PG_EINVAL, msg, msg_len, "color_offsets must start at 0 and end at element_count");
+        for (uint32_t c = 0; c < p->color_count; c++)
+            if (p->color_offsets[c] > p->color_offsets[c + 1])
+                return fail(PG_EINVAL, msg, msg_len, "color_offsets must not decrease");
+    }
+    {
+        // y is cleared before K x is accumulated into it, so x and y must not
+        // overlap (an in-place call would return K 0)
+        const size_t bytes = 3 * (size_t)p->node_count * sizeof(double);
+        const uintptr_t xa = (uintptr_t)x, ya = (uintptr_t)y;
+        if (xa < ya + bytes && ya < xa + bytes)
+            return fail(PG_EINVAL, msg, msg_len, "x and y must not overlap");
+    }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(PG_ECUDA, msg, msg_len, cudaGetErrorString(e));

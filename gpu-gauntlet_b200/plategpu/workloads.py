@@ -202,18 +202,42 @@ def batch_uneven(count: int = 256, seed: int = 5, min_side: int = 16,
         kinds = ["fixed" if rng.uniform() < 0.5 else "pinned" for _ in range(4)]
         supports = _edge_supports(mesh, kinds)
         cons = _prob.identifyConstrainedDOFs(mesh, supports)
-        g = grf_squared_exponential(n, n, WIDTH / n, float(rng.uniform(0.5, 3.0)), rng).reshape(-1)
-        amp = float(rng.uniform(1e3, 1e4))
-        npe = mesh.nodesPerElement
-        el = mesh.elements.astype(np.int64).reshape(-1, npe)
-        q = amp * (1.0 + 0.5 * g[el].mean(axis=1))
-        k = int(rng.integers(0, 17))
-        interior = _interior_nodes(n, n)
-        pts = rng.choice(interior, size=k, replace=False) if k else np.zeros(0, np.int64)
-        F, loads = _finish_loads(mesh, q, pts, rng.uniform(1e3, 1e4, size=k), cons)
+        F, loads = _random_field_load(mesh, n, cons, rng)
         out.append(Workload(name=f"batch{i}_{'dkt' if dkt else 'q4'}_{n}", mesh=mesh,
                             material=material, coloring=coloring, supports=supports,
                             constrainedDOFs=cons, F=F, point_loads=loads))
+    return out
+
+
+def _random_field_load(mesh: PlateMesh, n: int, cons, rng: np.random.Generator):
+    """A Gaussian random field pressure on an n x n-element plate
+    (squared-exponential, length-scale U(0.5, 3) m, amplitude U(1, 10) kPa,
+    element values from the nodal field, q = amp (1 + g / 2) positive
+    downward) plus 0-16 point loads U(1, 10) kN at random interior nodes;
+    float32, BCs applied."""
+    g = grf_squared_exponential(n, n, WIDTH / n, float(rng.uniform(0.5, 3.0)), rng).reshape(-1)
+    amp = float(rng.uniform(1e3, 1e4))
+    npe = mesh.nodesPerElement
+    el = mesh.elements.astype(np.int64).reshape(-1, npe)
+    q = amp * (1.0 + 0.5 * g[el].mean(axis=1))
+    k = int(rng.integers(0, 17))
+    interior = _interior_nodes(n, n)
+    pts = rng.choice(interior, size=k, replace=False) if k else np.zeros(0, np.int64)
+    return _finish_loads(mesh, q, pts, rng.uniform(1e3, 1e4, size=k), cons)
+
+
+def random_field_loads(wl: Workload, count: int, seed: int) -> np.ndarray:
+    """`count` seeded random-field loads of a structured n x n plate
+    (plate_q4_141: the learned preconditioner's training and held-out
+    loads): each a Gaussian random field pressure plus 0-16 point loads as
+    in _random_field_load.  Returns float32 [count, 3 * nodeCount]."""
+    n = int(round(np.sqrt(wl.mesh.elementCount)))
+    if n * n != wl.mesh.elementCount or wl.mesh.nodesPerElement != 4:
+        raise ValueError("random_field_loads needs a structured n x n Q4 plate")
+    rng = np.random.default_rng(seed)
+    out = np.empty((count, wl.n_dof), np.float32)
+    for k in range(count):
+        out[k] = _random_field_load(wl.mesh, n, wl.constrainedDOFs, rng)[0]
     return out
 
 

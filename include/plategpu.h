@@ -335,8 +335,13 @@ int pg_block_jacobi(pg_ctx* ctx, const pg_problem* prob, double* binv_out);
  *     at most 7,281 Q4 or 12,945 DKT elements; larger problems fail with
  *     PG_EINVAL before any work is queued.
  *   - The first call on a device looks up that array's device address
- *     (cudaGetSymbolAddress); make that first call before any stream
- *     capture.
+ *     (cudaGetSymbolAddress) and keeps it; make that first call before any
+ *     stream capture.  The kept address is not valid after a
+ *     cudaDeviceReset of that device: do not use this entry point across a
+ *     device reset.
+ *   - x and y must not overlap (y is cleared before K x is summed into it):
+ *     an overlapping call fails with PG_EINVAL.  color_offsets must start
+ *     at 0, not decrease and end at element_count (PG_EINVAL otherwise).
  *   - Work is queued on `stream` (a cudaStream_t; NULL = legacy default
  *     stream) and the call returns without waiting.  All calls share the
  *     one array, so calls whose work overlaps on the GPU (other streams,
@@ -364,6 +369,115 @@ int pg_plan_inspect(const pg_problem* prob, int ctas, int32_t* stats_out, char* 
  * too, and the invariants cover them). */
 int pg_plan_inspect_halo(const pg_problem* prob, int ctas, int rings, int32_t* stats_out,
                          char* msg, size_t msg_len);
+
+/* ---------------------------------------------------------------------------
+ * Learned two-level preconditioner (no counterpart in the reference, whose
+ * PCG applies only the 3x3 block Jacobi -- src/lib/plate/gpu/shaders/
+ * index.ts:214-262, once per iteration of runGPUPCG, gpu/solver.ts:190-553;
+ * the network's correction is added at that point of the iteration).
+ *
+ * pg_net: a 4-level U-Net over a height x width grid (multiples of 8):
+ * 3 x 3 convolutions without bias, channels 16/32/64/128, ReLU, 2x2 average
+ * pooling, nearest upsampling, skip connections by concatenation; 3 input
+ * and 3 output channels (w, theta_x, theta_y of the node at each pixel).
+ * BF16 weights and activations with FP32 accumulation on the tensor cores
+ * (mma.sync), FP32 master weights and Adam state.  Parameters cross the ABI
+ * in the real (unpadded) layout: per layer [cout][3][3][cin], layers in the
+ * order e0a e0b e1a e1b e2a e2b e3a e3b d2a d2b d1a d1b d0a d0b out.
+ * scales[6]: the input scales applied to the residual's three components
+ * and the output scales applied to the network's three outputs.
+ * ------------------------------------------------------------------------- */
+typedef struct pg_net pg_net;
+int pg_net_create(pg_ctx* ctx, int height, int width, uint64_t seed, pg_net** out);
+void pg_net_destroy(pg_net* net);
+int64_t pg_net_param_count(const pg_net* net);
+/* params (may be NULL): [pg_net_param_count] floats; setting them resets the
+ * Adam state.  scales (may be NULL): 6 floats > 0. */
+int pg_net_set_params(pg_net* net, const float* params, const float* scales);
+int pg_net_get_params(pg_net* net, float* params, float* scales);
+/* Test hooks on device buffers: forward of `batch` images [batch][h][w][3]
+ * (FP32 in and out); backward of the last forward from dL/d out (FP32
+ * [batch][h][w][3]) into dL/d in (device, may be NULL) and the parameter
+ * gradients (host, real layout, may be NULL); one Adam step (lr, betas 0.9
+ * and 0.999, eps 1e-8) with given gradients (host, real layout). */
+int pg_net_forward(pg_net* net, int batch, const float* in_dev, float* out_dev);
+int pg_net_backward(pg_net* net, int batch, const float* gout_dev, float* gin_dev, float* gparams);
+int pg_net_adam_step(pg_net* net, const float* grads, float lr);
+
+/* The learned solver of one plan: the plan's operator and block Jacobi, the
+ * network, and node_pixel [node_count] (host) mapping every node to a
+ * distinct pixel y * width + x of the network's grid.  Neither the plan nor
+ * the network may be destroyed before it. */
+typedef struct pg_learned pg_learned;
+int pg_learned_create(pg_plan* plan, pg_net* net, const int32_t* node_pixel, pg_learned** out);
+void pg_learned_destroy(pg_learned* learned);
+
+/* Residual/error pairs from solver output, on the device: for each of
+ * `count` loads, r = F - K x_k (FP64 K) and e = x* - x_k, with x_k = 0 when
+ * xk_dev is NULL.  F_dev [count][3n] float, xstar_dev / xk_dev [count][3n]
+ * double, R_out / E_out [count][3n] float. */
+int pg_learned_make_pairs(pg_learned* learned, int count, const float* F_dev, const double* xstar_dev,
+                          const double* xk_dev, float* R_out, float* E_out);
+
+#define PG_TRAIN_MAX_EPOCHS 256
+typedef struct pg_train_options {
+    uint32_t struct_size;   /* sizeof(pg_train_options); set by pg_train_options_default */
+    int32_t epochs;         /* default 20 */
+    int32_t batch;          /* pairs per Adam step, default 32 */
+    float lr;               /* Adam learning rate, default 1e-3 */
+    int32_t cosine;         /* 1 (default): cosine decay of lr to 0 over the run */
+    uint64_t seed;          /* shuffles */
+    int32_t val_count;      /* the last val_count pairs are held out for the validation loss */
+    int32_t set_scales;     /* 1 (default): set the network's scales from the pairs */
+} pg_train_options;
+
+typedef struct pg_train_info {
+    int32_t steps, batch;
+    double loss_first_step, loss_last_step;   /* training loss of the first / last step */
+    double val_loss_before, val_loss;         /* validation loss before / after training */
+    double train_ms;                          /* device time of the training graphs */
+    double total_ms;                          /* whole call, host clock */
+    double epoch_loss[PG_TRAIN_MAX_EPOCHS];   /* mean training loss of each epoch */
+    double epoch_val_loss[PG_TRAIN_MAX_EPOCHS];
+} pg_train_info;
+
+void pg_train_options_default(pg_train_options* opt);
+/* Trains the network on `count` residual/error pairs (device, [count][3n]
+ * float; A e = r): each pair is pre-smoothed (t = D^-1 r, r1 = r - K t,
+ * e1 = e - t) and the network is trained with Adam to minimise the
+ * energy-norm error after its correction, (e1 - y)^T K (e1 - y) / e1^T K e1
+ * with y = N(r1), K applied by this library's own element kernels.  One
+ * CUDA graph launch per epoch. */
+int pg_learned_train(pg_learned* learned, int count, const float* R_dev, const float* E_dev,
+                     const pg_train_options* opt, pg_train_info* info);
+/* Test hook: the loss of each of `count` pairs with the current network
+ * (replaces the training set held by `learned`). */
+int pg_learned_loss(pg_learned* learned, int count, const float* R_dev, const float* E_dev, double* loss_out);
+
+typedef struct pg_learned_stats {
+    int32_t mode;                /* as passed */
+    int32_t network_iterations;  /* iterations whose network correction was used */
+    int32_t network_off_at;      /* iteration after which the network was switched off, or -1 */
+    int32_t replacements;        /* FP64 true-residual recomputations */
+} pg_learned_stats;
+
+/* Flexible PCG (Polak-Ribiere) with the two-level preconditioner
+ * z = t + y + D^-1 (r1 - K y), t = D^-1 r, r1 = r - K t, y = N(r1)
+ * (mode 1); an iteration whose network correction does not reduce the
+ * residual uses z = D^-1 r, and after three such iterations in a row the
+ * solve continues as plain block-Jacobi PCG.  mode 0: plain block-Jacobi
+ * PCG in the same loop; mode 2: the smoothing steps without the network
+ * (z = t + D^-1 r1).  FP32 vectors and BF16 network, FP64 x, dot products
+ * and alpha/beta; the stop test (opt: tolerance, max_iterations,
+ * stop_rule) is made on the FP64 true residual F - K x, which also
+ * replaces the recursive residual every 50 iterations.  The whole solve is
+ * one CUDA graph launch (a conditional WHILE node).
+ * _device: F_dev / x_dev device [3n] float / double; otherwise host buffers
+ * (copies included).  info->solve_ms is the graph's device time. */
+int pg_learned_solve_device(pg_learned* learned, const pg_options* opt, int mode, const float* F_dev,
+                            double* x_dev, pg_info* info, pg_learned_stats* stats);
+int pg_learned_solve(pg_learned* learned, const pg_options* opt, int mode, const float* F, double* x_out,
+                     pg_info* info, pg_learned_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -79,19 +79,51 @@ def call_static(torch, dp, x):
     return yd.cpu().numpy()
 
 
-def test_static_matches_apply_k_on_consecutive_calls(gpu_ctx):
+def test_static_matches_apply_k_on_consecutive_calls(gpu_ctx, oracle):
     torch = pytest.importorskip("torch")
     rng = np.random.default_rng(21)
     calls = [q4_case(), dkt_case(), q4_case()]
     for m, mat, col, cons in calls:
         dp = DeviceProblem(torch, m, mat, col, cons)
         hp = _lib.Problem(m, mat, col, None, cons)
+        ke = oracle.all_ke(m.nodes, m.elements, m.nodesPerElement, mat.E, mat.nu, mat.t,
+                           elem_t=mat.elem_t, mode=oracle.FP64)
+        offs, flat = col.flat()
         for _ in range(2):
             x = rng.standard_normal(3 * m.nodeCount)
             y = call_static(torch, dp, x)
             ref = gpu_ctx.apply_k(hp, x)
             assert np.all(np.isfinite(y))
             assert rel_err(y, ref) < 1e-12
+            # and directly against the FP64 oracle's K x (solver.ts:422-483)
+            yo = oracle.apply_k(m.nodeCount, m.elements, m.nodesPerElement, ke, offs, flat, cons, x,
+                                mode=oracle.FP64)
+            assert rel_err(y, yo) < 1e-12
+
+
+def test_static_rejects_overlapping_x_and_y_and_bad_offsets():
+    torch = pytest.importorskip("torch")
+    m, mat, col, cons = q4_case()
+    dp = DeviceProblem(torch, m, mat, col, cons)
+    L = _lib.load()
+    n = 3 * m.nodeCount
+    buf = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
+    msg = C.create_string_buffer(256)
+    # y == x and a y that starts inside x
+    for yoff in (0, 8 * (n // 2)):
+        st = L.pg_apply_k_static(C.byref(dp.struct), buf.data_ptr(), buf.data_ptr() + yoff, None,
+                                 msg, 256)
+        assert st == _lib.PG_EINVAL and "overlap" in msg.value.decode()
+    # colour offsets that start above 0, or decrease, are refused before any
+    # work is queued
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    y = torch.zeros(n, dtype=torch.float64, device="cuda")
+    good = dp.host_offsets.copy()
+    for bad in ([1] + list(good[1:]), [0, 1_000_000] + list(good[2:])):
+        dp.host_offsets[:] = np.asarray(bad, np.uint32)
+        st = L.pg_apply_k_static(C.byref(dp.struct), x.data_ptr(), y.data_ptr(), None, msg, 256)
+        assert st == _lib.PG_EINVAL and "color_offsets" in msg.value.decode()
+    dp.host_offsets[:] = good
 
 
 def test_static_rejects_oversized_problem():
