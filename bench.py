@@ -114,6 +114,10 @@ def parse_args():
     ap.add_argument("--cases", type=int, default=4,
                     help="load cases of the workload plate solved together (0 = skip)")
     ap.add_argument("--cases-steps", type=int, default=5)
+    ap.add_argument("--learned", type=int, default=1,
+                    help="1: also time the learned two-level preconditioner (needs its weight file)")
+    ap.add_argument("--learned-held-out", type=int, default=512,
+                    help="held-out random-field loads evaluated with the learned preconditioner")
     ap.add_argument("--other-configs", type=int, default=1,
                     help="1: also time the other single-plate configs (plate_q4_32, plate_dkt_200, "
                          "plate_holes_dkt)")
@@ -540,6 +544,8 @@ def run_plategpu(args, world, rank, local):
     cold_ctx.close()
     cases = (cases_bench(args, ctx, wl, prob, H, head, chk is not None, world, local)
              if args.cases > 0 else None)
+    lrn = (learned_bench(args, ctx, stream, flush, local, wl, chk, extra_F)
+           if args.learned and rank == 0 else None)
     others = (other_configs_bench(args, ctx, stream, flush, world, local, chk is not None)
               if args.other_configs else None)
     # every rank takes part in the batch (its share of the plates)
@@ -595,6 +601,8 @@ def run_plategpu(args, world, rank, local):
     }
     if cases is not None:
         line["load_cases"] = cases
+    if lrn is not None:
+        line["learned"] = lrn
     if others:
         line["other_configs"] = others
     if batch is not None:
@@ -609,6 +617,146 @@ def run_plategpu(args, world, rank, local):
         line["cpu_baseline"] = None
     print(json.dumps(line), flush=True)
     ctx.close()
+
+
+LEARNED_TOL = 1e-6  # relative FP64 true residual of the learned flexible PCG (see learned_bench)
+
+
+def learned_bench(args, ctx, stream, flush, local, wl, chk, extra_F):
+    """The learned two-level preconditioner on the workload plate: the U-Net
+    trained by ``python -m plategpu.learned train`` (its weight file ships
+    with the package) as the coarse correction inside flexible PCG, one
+    CUDA graph launch per solve.  Timed like the headline variants
+    (device-resident loads, L2 flushed between steps); FP64 error on the same
+    loads as the variants when the checker runs; held-out random-field loads
+    (seeded differently from the training loads) for iterations and time;
+    the same flexible PCG without the network (smoothing steps only, and
+    plain block Jacobi) for the gain; and the network's forward pass alone
+    (batch 1 and 32) against the BF16 tensor-core peak."""
+    import numpy as np
+    import torch
+
+    from plategpu import _lib, learned
+
+    path = learned.DEFAULT_WEIGHTS
+    if args.workload != "plate_q4_141" or not os.path.exists(path):
+        return {"unavailable": f"no trained network for {args.workload} ({os.path.basename(path)} absent)"}
+    ls = learned.LearnedSolver(ctx, wl, weights=path)
+    meta = {}
+    try:
+        meta = learned.load_weights(ls.net, path)
+        n = wl.n_dof
+        F_dev = torch.from_numpy(wl.F).to(f"cuda:{local}")
+        x_dev = torch.zeros(n, dtype=torch.float64, device=f"cuda:{local}")
+        opts = learned.solve_options(LEARNED_TOL, max_iterations=2000)
+        steps = max(3, args.steps // 2)
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                ls.learned.solve_device(opts, F_dev.data_ptr(), x_dev.data_ptr())
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(steps)]
+            infos = []
+            torch.cuda.synchronize()
+            for k in range(steps):
+                flush.fill_(k & 0xFF)
+                ev[k][0].record(stream)
+                infos.append(ls.learned.solve_device(opts, F_dev.data_ptr(), x_dev.data_ptr()))
+                ev[k][1].record(stream)
+            torch.cuda.synchronize()
+        ms = [a.elapsed_time(b) for a, b in ev]
+        info, st = infos[-1]
+        out = {"method": "flexible PCG (Polak-Ribiere), two-level: block-Jacobi smoothing + U-Net "
+                         "correction (BF16 tensor cores), FP64 true-residual stop",
+               "stop": f"||F - K x|| / ||F|| < {LEARNED_TOL:g} (FP64)",
+               "value": statistics.mean(ms), "graph_ms": statistics.mean(i[0].solve_ms for i in infos),
+               "iterations": int(info.iterations), "network_iterations": int(st.network_iterations),
+               "network_off_at": int(st.network_off_at), "true_rel_residual": info.true_rel_residual,
+               "us_per_iteration": 1e3 * statistics.mean(ms) / max(1, info.iterations),
+               "training": {k: meta.get(k) for k in ("loads", "epochs", "steps", "batch", "lr", "val_loss_before",
+                                                     "val_loss", "train_ms", "params", "held_out")}}
+        x_main = x_dev.cpu().numpy().copy()
+        # the same loop without the network
+        for mode, name in ((_lib.LEARNED_SMOOTHING_ONLY, "without_network_smoothing_only"),
+                           (_lib.LEARNED_BLOCK_JACOBI, "without_network_block_jacobi")):
+            o2 = learned.solve_options(LEARNED_TOL, max_iterations=20000)
+            i2, _ = ls.learned.solve_device(o2, F_dev.data_ptr(), x_dev.data_ptr(), mode)
+            out[name] = {"iterations": int(i2.iterations), "ms": float(i2.solve_ms)}
+        out["iteration_gain_vs_smoothing_only"] = (out["without_network_smoothing_only"]["iterations"] /
+                                                   max(1, out["iterations"]))
+        if chk is not None:
+            errs = [float(np.linalg.norm(x_main - chk["truth"]) / np.linalg.norm(chk["truth"]))]
+            if extra_F is not None:
+                for f in extra_F:
+                    ls.learned.solve_device(opts, f.data_ptr(), x_dev.data_ptr())
+                    xt = chk["solve"](f.cpu().numpy())[0]
+                    errs.append(float(np.linalg.norm(x_dev.cpu().numpy() - xt) / np.linalg.norm(xt)))
+            out["accuracy"] = {"loads": {"count": len(errs), "rel_l2_max": max(errs),
+                                         "rel_l2_p50": float(np.percentile(errs, 50)),
+                                         "rel_l2_p99": float(np.percentile(errs, 99))}}
+        # held-out loads: iterations and device time (errors against FP64
+        # two-level solutions to 1e-12)
+        k_h = min(args.learned_held_out, 512)
+        if k_h > 0:
+            H = learned_loads(wl, k_h)
+            xt = learned.tight_solutions(torch, ctx, ls, H)
+            rows = learned.evaluate(torch, ls, H, tolerance=LEARNED_TOL, truth=xt)
+            its = [r["iterations"] for r in rows]
+            out["held_out"] = {"loads": k_h, "seed": learned.HELD_OUT_SEED,
+                               "iterations_p50": float(np.median(its)), "iterations_max": int(max(its)),
+                               "ms_p50": float(np.median([r["ms"] for r in rows])),
+                               "ms_p99": float(np.percentile([r["ms"] for r in rows], 99)),
+                               "converged": int(sum(r["converged"] for r in rows)),
+                               "rel_l2_max_vs_fp64_1e-12": max(r["rel_l2"] for r in rows),
+                               "network_off": int(sum(r["network_off_at"] >= 0 for r in rows))}
+        out["network_forward"] = network_forward_rate(ls.net, local)
+    finally:
+        ls.close()
+    return out
+
+
+def learned_loads(wl, k):
+    from plategpu import learned, workloads
+
+    return workloads.random_field_loads(wl, k, learned.HELD_OUT_SEED)
+
+
+def network_forward_rate(net, local):
+    """Device time of the network's forward pass (pg_net_forward, including
+    the FP32 <-> BF16 packing) at batch 1 and 32, and the convolutions'
+    FLOP rate at batch 32 against the measured BF16 peak."""
+    import torch
+
+    from plategpu import _lib
+
+    from plategpu import learned
+
+    H, W = net.height, net.width
+    flops_px = learned.flops_per_image(H, W)
+    res = {"flop_per_image": flops_px}
+    for B in (1, 32):
+        x = torch.randn(B, H, W, 3, device=f"cuda:{local}")
+        y = torch.empty_like(x)
+        for _ in range(3):
+            net.forward(B, x.data_ptr(), y.data_ptr())
+        torch.cuda.synchronize()
+        s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 20
+        s_.record()
+        for _ in range(reps):
+            net.forward(B, x.data_ptr(), y.data_ptr())
+        e_.record()
+        torch.cuda.synchronize()
+        ms = s_.elapsed_time(e_) / reps
+        res[f"batch{B}_us"] = 1e3 * ms
+        res[f"batch{B}_tflops"] = flops_px * B / (ms * 1e-3) / 1e12
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["bf16_tflops"])
+        res["bf16_peak_tflops"] = peak
+        res["batch32_frac_of_bf16_peak"] = res["batch32_tflops"] / peak
+    except (OSError, KeyError, ValueError):
+        pass
+    return res
 
 
 def _lib_options_copy(o, **changes):

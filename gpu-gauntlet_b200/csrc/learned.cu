@@ -1,0 +1,1759 @@
+// Learned two-level preconditioner: a U-Net coarse correction inside
+// flexible PCG, trained on the GPU by this library's own kernels.
+//
+// The reference (cseifert512/gpu-gauntlet) preconditions its PCG with the
+// 3 x 3 block Jacobi only (src/lib/plate/gpu/shaders/index.ts:214-262,
+// applied once per iteration of runGPUPCG, src/lib/plate/gpu/solver.ts:
+// 190-553).  This file adds, at that point of the iteration, a two-level
+// preconditioner for plates on a structured node grid:
+//
+//   t  = D^-1 r                       block-Jacobi pre-smoothing
+//   r1 = r - K t                      residual after smoothing
+//   y  = N(r1)                        network correction (coarse level)
+//   r2 = r1 - K y
+//   z  = t + y + D^-1 r2              block-Jacobi post-smoothing
+//
+// N maps the residual, laid out as a 3-channel image over the node grid
+// (w, theta_x, theta_y per node), to an approximation of K^-1 r1.  It is a
+// 4-level U-Net (unet.cuh) without biases, so N(c r) = c N(r) for c > 0 and
+// its correction scales with the residual.  Whenever the correction does
+// not reduce the residual (|r2| >= |r1|) that iteration uses z = D^-1 r
+// (plain block Jacobi), and after `fallback_after` such iterations in a
+// row the rest of the solve is plain block-Jacobi PCG.  Because N is
+// nonlinear the outer iteration is flexible PCG with the Polak-Ribiere
+// beta = z_k+1 . (r_k+1 - r_k) / (z_k . r_k) and alpha = p.r / p.Kp.
+//
+// Precision: r, z, p, K p and the network in FP32 / BF16 (FP32
+// accumulation); x, every dot product and the alpha/beta recurrences in
+// FP64; the block inverses are computed in FP64; every `replace_every`
+// iterations, and before the solve may stop, the residual is recomputed as
+// r = F - K x in FP64 and the stop test is made on that true residual.
+//
+// Execution: the whole solve is one CUDA graph launch: a conditional WHILE
+// node whose body is one iteration (about 30 kernels), ended from the
+// device by cudaGraphSetConditional once the true residual meets the
+// tolerance (or the iteration limit, a breakdown or a non-finite value).
+// Training is a second graph whose WHILE body is one Adam step (batch
+// gather, forward, energy-norm loss through the library's own K.p,
+// backward, Adam), so an epoch is one launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "plategpu.h"
+#include "unet.cuh"
+
+using pgn::bf16;
+
+namespace {
+
+struct LFail {
+    int status;
+    std::string msg;
+};
+
+#define LCK(call)                                                                         \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            throw LFail{e_ == cudaErrorMemoryAllocation ? PG_ENOMEM : PG_ECUDA,           \
+                        std::string(#call) + ": " + cudaGetErrorString(e_)};              \
+    } while (0)
+
+template <typename T>
+struct Buf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        release();
+        n = count;
+        if (count) LCK(cudaMalloc(&p, count * sizeof(T)));
+    }
+    void zero(cudaStream_t st) {
+        if (n) LCK(cudaMemsetAsync(p, 0, n * sizeof(T), st));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~Buf() { release(); }
+};
+
+// ---------------------------------------------------------------------------
+// network description (matches oracle/unet_oracle.py LAYERS)
+// ---------------------------------------------------------------------------
+
+struct LayerSpec {
+    int cin, cout;  // real channel counts
+};
+constexpr LayerSpec kSpec[pgn::kLayers] = {
+    {3, 16},   {16, 16},  {16, 32},  {32, 32},  {32, 64},  {64, 64},  {64, 128}, {128, 128},
+    {192, 64}, {64, 64},  {96, 32},  {32, 32},  {48, 16},  {16, 16},  {16, 3}};
+enum { E0A, E0B, E1A, E1B, E2A, E2B, E3A, E3B, D2A, D2B, D1A, D1B, D0A, D0B, OUTL };
+
+int pad16(int c) { return (c + 15) / 16 * 16; }
+
+pgn::LayerTable make_table() {
+    pgn::LayerTable T{};
+    long off = 0, off_f = 0, off_d = 0;
+    for (int k = 0; k < pgn::kLayers; k++) {
+        const int ci = pad16(kSpec[k].cin), co = pad16(kSpec[k].cout);
+        T.l[k] = {ci, co, off, off_f, off_d};
+        off += 9L * ci * co;
+        off_f += 9L * ci * co;
+        off_d += 9L * ci * co;
+    }
+    T.total = off;
+    return T;
+}
+
+long real_param_count() {
+    long s = 0;
+    for (const LayerSpec& l : kSpec) s += 9L * l.cin * l.cout;
+    return s;
+}
+
+// Activations (and, for training, their gradients) of one batch size.
+struct Workspace {
+    int B = 0;
+    bool grads = false;
+    Buf<bf16> in, e0a, cat0, d0a, d0, p1, e1a, cat1, d1a, d1, p2, e2a, cat2, d2a, d2, p3, e3a, e3;
+    Buf<float> out;  // [B][H][W][4], channels 0..2
+    Buf<bf16> gout, g_d0, g_d0a, dcat0, g_d1, g_d1a, dcat1, g_d2, g_d2a, dcat2, g_e3, g_e3a, dp3, g_e2,
+        g_e2a, dp2, g_e1, g_e1a, dp1, g_e0, g_e0a, din;
+};
+
+}  // namespace
+
+struct pg_net {
+    pg_ctx* ctx = nullptr;
+    int H = 0, W = 0;
+    int version = 0;  // bumped when the scales change (solve graphs bake them in)
+    pgn::LayerTable T{};
+    Buf<float> w, m, v, g;  // FP32 master weights, Adam moments, gradients (padded layout)
+    Buf<bf16> wf, wd;       // BF16 forward / input-gradient copies
+    Buf<int> step;          // Adam steps taken (device)
+    float scale[6] = {1, 1, 1, 1, 1, 1};  // input scales (3) and output scales (3)
+    std::map<int, std::unique_ptr<Workspace>> ws;
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// launches
+// ---------------------------------------------------------------------------
+
+int pick_cot(int rows) {
+    for (int c : {64, 48, 32, 16})
+        if (rows % c == 0) return c;
+    return 16;
+}
+
+template <int CIN, int COT, int MODE>
+void conv_launch(const pgn::ConvArgs& a, int rows, cudaStream_t st) {
+    const int smem = pgn::conv_smem_bytes(CIN, COT);
+    const void* fn = (const void*)pgn::conv3x3_kernel<CIN, COT, MODE>;
+    LCK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    dim3 grid((a.W + 7) / 8, ((a.H + 7) / 8) * a.B, rows / COT);
+    pgn::conv3x3_kernel<CIN, COT, MODE><<<grid, pgn::kConvThreads, smem, st>>>(a);
+    LCK(cudaGetLastError());
+}
+
+// Dispatches the (input channels, output tile, epilogue) combinations the
+// network uses.
+void conv(int mode, int cin, int rows, const pgn::ConvArgs& a, cudaStream_t st) {
+    const int cot = pick_cot(rows);
+#define PG_CONV(C, T, M)                                   \
+    if (cin == C && cot == T && mode == M) {               \
+        conv_launch<C, T, M>(a, rows, st);                 \
+        return;                                            \
+    }
+    using namespace pgn;
+    PG_CONV(16, 16, OUT_BF16_RELU) PG_CONV(16, 32, OUT_BF16_RELU) PG_CONV(32, 32, OUT_BF16_RELU)
+    PG_CONV(32, 64, OUT_BF16_RELU) PG_CONV(64, 64, OUT_BF16_RELU) PG_CONV(128, 64, OUT_BF16_RELU)
+    PG_CONV(192, 64, OUT_BF16_RELU) PG_CONV(96, 32, OUT_BF16_RELU) PG_CONV(48, 16, OUT_BF16_RELU)
+    PG_CONV(16, 16, OUT_F32)
+    PG_CONV(16, 16, OUT_BF16_MASKED) PG_CONV(16, 48, OUT_BF16_MASKED) PG_CONV(32, 32, OUT_BF16_MASKED)
+    PG_CONV(32, 48, OUT_BF16_MASKED) PG_CONV(64, 64, OUT_BF16_MASKED) PG_CONV(128, 64, OUT_BF16_MASKED)
+    PG_CONV(128, 64, OUT_BF16) PG_CONV(64, 32, OUT_BF16) PG_CONV(32, 16, OUT_BF16) PG_CONV(16, 16, OUT_BF16)
+#undef PG_CONV
+    throw LFail{PG_EUNSUPPORTED, "no convolution kernel for cin " + std::to_string(cin) + ", tile " +
+                                     std::to_string(cot) + ", mode " + std::to_string(mode)};
+}
+
+pgn::ConvArgs cargs(int B, int H, int W, const bf16* in, int in_cs, const bf16* w, int w_rows, void* out,
+                    int out_cs, int out_coff, int cout_real, const int* skip) {
+    pgn::ConvArgs a{};
+    a.B = B;
+    a.H = H;
+    a.W = W;
+    a.in = in;
+    a.in_cs = in_cs;
+    a.w = w;
+    a.w_rows = w_rows;
+    a.out = out;
+    a.out_cs = out_cs;
+    a.out_coff = out_coff;
+    a.cout_real = cout_real;
+    a.skip = skip;
+    return a;
+}
+
+int ew_grid(long items) { return (int)std::min<long>((items + 255) / 256, 148L * 16); }
+
+// The workspace of batch size B, created on first use; gradient buffers
+// are added to an existing workspace when first needed, so the activation
+// buffers a captured graph points to never move.
+Workspace* workspace(pg_net* n, int B, bool grads) {
+    auto it = n->ws.find(B);
+    Workspace* w = nullptr;
+    cudaStream_t st = pgi::ctx_stream(n->ctx);
+    const size_t P0 = (size_t)B * n->H * n->W, P1 = P0 / 4, P2 = P1 / 4, P3 = P2 / 4;
+    if (it != n->ws.end()) {
+        w = it->second.get();
+        if (w->grads || !grads) return w;
+    } else {
+        auto nw = std::make_unique<Workspace>();
+        w = nw.get();
+        n->ws[B] = std::move(nw);
+        w->B = B;
+        w->in.alloc(P0 * 16);
+        w->e0a.alloc(P0 * 16);
+        w->cat0.alloc(P0 * 48);
+        w->d0a.alloc(P0 * 16);
+        w->d0.alloc(P0 * 16);
+        w->out.alloc(P0 * 4);
+        w->p1.alloc(P1 * 16);
+        w->e1a.alloc(P1 * 32);
+        w->cat1.alloc(P1 * 96);
+        w->d1a.alloc(P1 * 32);
+        w->d1.alloc(P1 * 32);
+        w->p2.alloc(P2 * 32);
+        w->e2a.alloc(P2 * 64);
+        w->cat2.alloc(P2 * 192);
+        w->d2a.alloc(P2 * 64);
+        w->d2.alloc(P2 * 64);
+        w->p3.alloc(P3 * 64);
+        w->e3a.alloc(P3 * 128);
+        w->e3.alloc(P3 * 128);
+        w->in.zero(st);  // channels 3..15 and pixels without a node stay 0
+        w->out.zero(st);
+    }
+    if (grads) {
+        w->grads = true;
+        w->gout.alloc(P0 * 16);
+        w->gout.zero(st);  // channels 3..15 and pixels without a node stay 0
+        w->g_d0.alloc(P0 * 16);
+        w->g_d0a.alloc(P0 * 16);
+        w->dcat0.alloc(P0 * 48);
+        w->g_d1.alloc(P1 * 32);
+        w->g_d1a.alloc(P1 * 32);
+        w->dcat1.alloc(P1 * 96);
+        w->g_d2.alloc(P2 * 64);
+        w->g_d2a.alloc(P2 * 64);
+        w->dcat2.alloc(P2 * 192);
+        w->g_e3.alloc(P3 * 128);
+        w->g_e3a.alloc(P3 * 128);
+        w->dp3.alloc(P3 * 64);
+        w->g_e2.alloc(P2 * 64);
+        w->g_e2a.alloc(P2 * 64);
+        w->dp2.alloc(P2 * 32);
+        w->g_e1.alloc(P1 * 32);
+        w->g_e1a.alloc(P1 * 32);
+        w->dp1.alloc(P1 * 16);
+        w->g_e0.alloc(P0 * 16);
+        w->g_e0a.alloc(P0 * 16);
+        w->din.alloc(P0 * 16);
+    }
+    LCK(cudaStreamSynchronize(st));
+    return w;
+}
+
+// U-Net forward of ws->in ([B][H][W][16], channels 0..2 used) into ws->out.
+void net_forward(pg_net* n, Workspace* w, cudaStream_t st, const int* skip) {
+    const int B = w->B;
+    const int H0 = n->H, W0 = n->W, H1 = H0 / 2, W1 = W0 / 2, H2 = H1 / 2, W2 = W1 / 2, H3 = H2 / 2, W3 = W2 / 2;
+    const pgn::LayerTable& T = n->T;
+    auto wf = [&](int k) { return n->wf.p + T.l[k].off_f; };
+    using namespace pgn;
+    conv(OUT_BF16_RELU, 16, 16, cargs(B, H0, W0, w->in.p, 16, wf(E0A), 16, w->e0a.p, 16, 0, 16, skip), st);
+    conv(OUT_BF16_RELU, 16, 16, cargs(B, H0, W0, w->e0a.p, 16, wf(E0B), 16, w->cat0.p, 48, 0, 16, skip), st);
+    pool2_kernel<<<ew_grid((long)B * H1 * W1 * 2), 256, 0, st>>>(B, H1, W1, w->cat0.p, 48, 16, w->p1.p, 16, skip);
+    conv(OUT_BF16_RELU, 16, 32, cargs(B, H1, W1, w->p1.p, 16, wf(E1A), 32, w->e1a.p, 32, 0, 32, skip), st);
+    conv(OUT_BF16_RELU, 32, 32, cargs(B, H1, W1, w->e1a.p, 32, wf(E1B), 32, w->cat1.p, 96, 0, 32, skip), st);
+    pool2_kernel<<<ew_grid((long)B * H2 * W2 * 4), 256, 0, st>>>(B, H2, W2, w->cat1.p, 96, 32, w->p2.p, 32, skip);
+    conv(OUT_BF16_RELU, 32, 64, cargs(B, H2, W2, w->p2.p, 32, wf(E2A), 64, w->e2a.p, 64, 0, 64, skip), st);
+    conv(OUT_BF16_RELU, 64, 64, cargs(B, H2, W2, w->e2a.p, 64, wf(E2B), 64, w->cat2.p, 192, 0, 64, skip), st);
+    pool2_kernel<<<ew_grid((long)B * H3 * W3 * 8), 256, 0, st>>>(B, H3, W3, w->cat2.p, 192, 64, w->p3.p, 64, skip);
+    conv(OUT_BF16_RELU, 64, 128, cargs(B, H3, W3, w->p3.p, 64, wf(E3A), 128, w->e3a.p, 128, 0, 128, skip), st);
+    conv(OUT_BF16_RELU, 128, 128, cargs(B, H3, W3, w->e3a.p, 128, wf(E3B), 128, w->e3.p, 128, 0, 128, skip), st);
+    up2_kernel<<<ew_grid((long)B * H2 * W2 * 16), 256, 0, st>>>(B, H2, W2, w->e3.p, 128, 128, w->cat2.p, 192, 64, skip);
+    conv(OUT_BF16_RELU, 192, 64, cargs(B, H2, W2, w->cat2.p, 192, wf(D2A), 64, w->d2a.p, 64, 0, 64, skip), st);
+    conv(OUT_BF16_RELU, 64, 64, cargs(B, H2, W2, w->d2a.p, 64, wf(D2B), 64, w->d2.p, 64, 0, 64, skip), st);
+    up2_kernel<<<ew_grid((long)B * H1 * W1 * 8), 256, 0, st>>>(B, H1, W1, w->d2.p, 64, 64, w->cat1.p, 96, 32, skip);
+    conv(OUT_BF16_RELU, 96, 32, cargs(B, H1, W1, w->cat1.p, 96, wf(D1A), 32, w->d1a.p, 32, 0, 32, skip), st);
+    conv(OUT_BF16_RELU, 32, 32, cargs(B, H1, W1, w->d1a.p, 32, wf(D1B), 32, w->d1.p, 32, 0, 32, skip), st);
+    up2_kernel<<<ew_grid((long)B * H0 * W0 * 4), 256, 0, st>>>(B, H0, W0, w->d1.p, 32, 32, w->cat0.p, 48, 16, skip);
+    conv(OUT_BF16_RELU, 48, 16, cargs(B, H0, W0, w->cat0.p, 48, wf(D0A), 16, w->d0a.p, 16, 0, 16, skip), st);
+    conv(OUT_BF16_RELU, 16, 16, cargs(B, H0, W0, w->d0a.p, 16, wf(D0B), 16, w->d0.p, 16, 0, 16, skip), st);
+    conv(OUT_F32, 16, 16, cargs(B, H0, W0, w->d0.p, 16, wf(OUTL), 16, w->out.p, 4, 0, 3, skip), st);
+    LCK(cudaGetLastError());
+}
+
+void wgrad(pg_net* n, int k, int B, int H, int W, const bf16* x, int x_cs, const bf16* g, int g_cs,
+           cudaStream_t st) {
+    const pgn::LayerDesc& L = n->T.l[k];
+    pgn::WgradArgs a{};
+    a.B = B;
+    a.H = H;
+    a.W = W;
+    a.x = x;
+    a.x_cs = x_cs;
+    a.g = g;
+    a.g_cs = g_cs;
+    a.dw = n->g.p + L.off;
+    a.cin = L.cin;
+    a.cout = L.cout;
+    a.tiles = B * ((H + 7) / 8) * ((W + 7) / 8);
+    const int cot = L.cout % 32 == 0 ? 32 : 16, cit = L.cin % 32 == 0 ? 32 : 16;
+    const int gy = L.cout / cot, gz = L.cin / cit;
+    const int gx = std::max(1, std::min(a.tiles, 148 * 4 / (gy * gz)));
+    dim3 grid(gx, gy, gz);
+    if (cot == 32 && cit == 32)
+        pgn::wgrad_kernel<32, 32><<<grid, 128, 0, st>>>(a);
+    else if (cot == 32)
+        pgn::wgrad_kernel<32, 16><<<grid, 64, 0, st>>>(a);
+    else if (cit == 32)
+        pgn::wgrad_kernel<16, 32><<<grid, 64, 0, st>>>(a);
+    else
+        pgn::wgrad_kernel<16, 16><<<grid, 32, 0, st>>>(a);
+    LCK(cudaGetLastError());
+}
+
+// Input gradient of layer k: dX = conv(G, W flipped/transposed), masked by
+// (X > 0) when X is a ReLU output.
+void dgrad(pg_net* n, int k, int B, int H, int W, const bf16* g, bf16* out, int out_cs, const bf16* mask,
+           int mask_cs, cudaStream_t st) {
+    const pgn::LayerDesc& L = n->T.l[k];
+    pgn::ConvArgs a = cargs(B, H, W, g, L.cout, n->wd.p + L.off_d, L.cin, out, out_cs, 0, L.cin, nullptr);
+    a.mask = mask;
+    a.mask_cs = mask_cs;
+    conv(mask ? pgn::OUT_BF16_MASKED : pgn::OUT_BF16, L.cout, L.cin, a, st);
+}
+
+// Backward of the forward pass held in w, from w->gout (dL/d out, [B][H][W][16],
+// channels 0..2): accumulates into n->g (zero it first).  With din, also
+// the gradient of the network input (w->din).
+void net_backward(pg_net* n, Workspace* w, cudaStream_t st, bool din) {
+    const int B = w->B;
+    const int H0 = n->H, W0 = n->W, H1 = H0 / 2, W1 = W0 / 2, H2 = H1 / 2, W2 = W1 / 2, H3 = H2 / 2, W3 = W2 / 2;
+    using namespace pgn;
+    // output layer and level-0 decoder
+    wgrad(n, OUTL, B, H0, W0, w->d0.p, 16, w->gout.p, 16, st);
+    dgrad(n, OUTL, B, H0, W0, w->gout.p, w->g_d0.p, 16, w->d0.p, 16, st);
+    wgrad(n, D0B, B, H0, W0, w->d0a.p, 16, w->g_d0.p, 16, st);
+    dgrad(n, D0B, B, H0, W0, w->g_d0.p, w->g_d0a.p, 16, w->d0a.p, 16, st);
+    wgrad(n, D0A, B, H0, W0, w->cat0.p, 48, w->g_d0a.p, 16, st);
+    dgrad(n, D0A, B, H0, W0, w->g_d0a.p, w->dcat0.p, 48, w->cat0.p, 48, st);
+    up2_bwd_kernel<<<ew_grid((long)B * H1 * W1 * 4), 256, 0, st>>>(B, H1, W1, w->dcat0.p, 48, 16, 32, w->g_d1.p, 32);
+    // level-1 decoder
+    wgrad(n, D1B, B, H1, W1, w->d1a.p, 32, w->g_d1.p, 32, st);
+    dgrad(n, D1B, B, H1, W1, w->g_d1.p, w->g_d1a.p, 32, w->d1a.p, 32, st);
+    wgrad(n, D1A, B, H1, W1, w->cat1.p, 96, w->g_d1a.p, 32, st);
+    dgrad(n, D1A, B, H1, W1, w->g_d1a.p, w->dcat1.p, 96, w->cat1.p, 96, st);
+    up2_bwd_kernel<<<ew_grid((long)B * H2 * W2 * 8), 256, 0, st>>>(B, H2, W2, w->dcat1.p, 96, 32, 64, w->g_d2.p, 64);
+    // level-2 decoder
+    wgrad(n, D2B, B, H2, W2, w->d2a.p, 64, w->g_d2.p, 64, st);
+    dgrad(n, D2B, B, H2, W2, w->g_d2.p, w->g_d2a.p, 64, w->d2a.p, 64, st);
+    wgrad(n, D2A, B, H2, W2, w->cat2.p, 192, w->g_d2a.p, 64, st);
+    dgrad(n, D2A, B, H2, W2, w->g_d2a.p, w->dcat2.p, 192, w->cat2.p, 192, st);
+    up2_bwd_kernel<<<ew_grid((long)B * H3 * W3 * 16), 256, 0, st>>>(B, H3, W3, w->dcat2.p, 192, 64, 128, w->g_e3.p, 128);
+    // bottleneck
+    wgrad(n, E3B, B, H3, W3, w->e3a.p, 128, w->g_e3.p, 128, st);
+    dgrad(n, E3B, B, H3, W3, w->g_e3.p, w->g_e3a.p, 128, w->e3a.p, 128, st);
+    wgrad(n, E3A, B, H3, W3, w->p3.p, 64, w->g_e3a.p, 128, st);
+    dgrad(n, E3A, B, H3, W3, w->g_e3a.p, w->dp3.p, 64, nullptr, 0, st);
+    // level-2 encoder
+    pool2_bwd_add_kernel<<<ew_grid((long)B * H2 * W2 * 8), 256, 0, st>>>(B, H2, W2, w->dcat2.p, w->cat2.p, 192,
+                                                                         w->dp3.p, 64, w->g_e2.p);
+    wgrad(n, E2B, B, H2, W2, w->e2a.p, 64, w->g_e2.p, 64, st);
+    dgrad(n, E2B, B, H2, W2, w->g_e2.p, w->g_e2a.p, 64, w->e2a.p, 64, st);
+    wgrad(n, E2A, B, H2, W2, w->p2.p, 32, w->g_e2a.p, 64, st);
+    dgrad(n, E2A, B, H2, W2, w->g_e2a.p, w->dp2.p, 32, nullptr, 0, st);
+    // level-1 encoder
+    pool2_bwd_add_kernel<<<ew_grid((long)B * H1 * W1 * 4), 256, 0, st>>>(B, H1, W1, w->dcat1.p, w->cat1.p, 96,
+                                                                         w->dp2.p, 32, w->g_e1.p);
+    wgrad(n, E1B, B, H1, W1, w->e1a.p, 32, w->g_e1.p, 32, st);
+    dgrad(n, E1B, B, H1, W1, w->g_e1.p, w->g_e1a.p, 32, w->e1a.p, 32, st);
+    wgrad(n, E1A, B, H1, W1, w->p1.p, 16, w->g_e1a.p, 32, st);
+    dgrad(n, E1A, B, H1, W1, w->g_e1a.p, w->dp1.p, 16, nullptr, 0, st);
+    // level-0 encoder
+    pool2_bwd_add_kernel<<<ew_grid((long)B * H0 * W0 * 2), 256, 0, st>>>(B, H0, W0, w->dcat0.p, w->cat0.p, 48,
+                                                                         w->dp1.p, 16, w->g_e0.p);
+    wgrad(n, E0B, B, H0, W0, w->e0a.p, 16, w->g_e0.p, 16, st);
+    dgrad(n, E0B, B, H0, W0, w->g_e0.p, w->g_e0a.p, 16, w->e0a.p, 16, st);
+    wgrad(n, E0A, B, H0, W0, w->in.p, 16, w->g_e0a.p, 16, st);
+    if (din) dgrad(n, E0A, B, H0, W0, w->g_e0a.p, w->din.p, 16, nullptr, 0, st);
+    LCK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// operator kernels (plate side)
+// ---------------------------------------------------------------------------
+
+struct Op {
+    int Nn;
+    const int* inc_ptr;
+    const int* inc_idx;
+    const uint32_t* el;
+    const float* ke32;
+    const double* ke64;
+    const float* binv32;
+    const uint8_t* cons;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block sums of K values into parts[blockIdx.x * K + k] (blockDim.x <= 1024).
+template <int K>
+__device__ void block_partials(double (&v)[K], double* parts) {
+    __shared__ double red[K][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const double s = warp_sum(v[k]);
+        if (lane == 0) red[k][warp] = s;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const double s = warp_sum(lane < nw ? red[k][lane] : 0.0);
+            if (lane == 0) parts[blockIdx.x * K + k] = s;
+        }
+    }
+}
+
+// Sum of nb blocks' partials, the same fixed order in every block; every
+// thread of the block receives the K sums.
+template <int K>
+__device__ void reduce_parts(const double* parts, int nb, double (&out)[K]) {
+    __shared__ double res[K];
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            double s = 0.0;
+            for (int i = threadIdx.x; i < nb; i += 32) s += parts[i * K + k];
+            s = warp_sum(s);
+            if (threadIdx.x == 0) res[k] = s;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; k++) out[k] = res[k];
+    __syncthreads();
+}
+
+// (K v)_n for node n with v read through getv(m, d) (FP32 element matrices),
+// constrained rows replaced by the identity (y_c = v_c).
+template <int NPE, typename GetV>
+__device__ __forceinline__ void kv_node(const Op& op, int n, GetV getv, float (&out)[3]) {
+    constexpr int ND = 3 * NPE;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    for (int q = op.inc_ptr[n]; q < op.inc_ptr[n + 1]; q++) {
+        const int e = op.inc_idx[q] >> 2, k = op.inc_idx[q] & 3;
+        const float* Ke = op.ke32 + (size_t)e * ND * ND + 3 * k * ND;
+#pragma unroll
+        for (int b = 0; b < NPE; b++) {
+            const int m = (int)op.el[(size_t)e * NPE + b];
+            const float v0 = getv(m, 0), v1 = getv(m, 1), v2 = getv(m, 2);
+            const float* c0 = Ke + 3 * b;
+            s0 += c0[0] * v0 + c0[1] * v1 + c0[2] * v2;
+            s1 += c0[ND] * v0 + c0[ND + 1] * v1 + c0[ND + 2] * v2;
+            s2 += c0[2 * ND] * v0 + c0[2 * ND + 1] * v1 + c0[2 * ND + 2] * v2;
+        }
+    }
+    out[0] = op.cons[3 * n] ? getv(n, 0) : s0;
+    out[1] = op.cons[3 * n + 1] ? getv(n, 1) : s1;
+    out[2] = op.cons[3 * n + 2] ? getv(n, 2) : s2;
+}
+
+__device__ __forceinline__ float binv_row(const float* B9, int d, float a, float b, float c) {
+    return B9[3 * d] * a + B9[3 * d + 1] * b + B9[3 * d + 2] * c;
+}
+
+// ----- training data --------------------------------------------------------
+
+// Residual/error pairs from solver output: r = F - K x_k (FP64), e = x* - x_k.
+template <int NPE>
+__global__ void make_pairs_kernel(Op op, int count, const float* __restrict__ F, const double* __restrict__ xs,
+                                  const double* __restrict__ xk, float* __restrict__ R, float* __restrict__ E) {
+    constexpr int ND = 3 * NPE;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x, p = blockIdx.y;
+    if (n >= op.Nn || p >= count) return;
+    const size_t base = (size_t)p * 3 * op.Nn;
+    double s[3] = {0, 0, 0};
+    if (xk) {
+        for (int q = op.inc_ptr[n]; q < op.inc_ptr[n + 1]; q++) {
+            const int e = op.inc_idx[q] >> 2, k = op.inc_idx[q] & 3;
+            const double* Ke = op.ke64 + (size_t)e * ND * ND + 3 * k * ND;
+            for (int b = 0; b < NPE; b++) {
+                const int m = (int)op.el[(size_t)e * NPE + b];
+                for (int d = 0; d < 3; d++)
+                    for (int c = 0; c < 3; c++) s[d] += Ke[d * ND + 3 * b + c] * xk[base + 3 * m + c];
+            }
+        }
+    }
+    for (int d = 0; d < 3; d++) {
+        const size_t i = base + 3 * n + d;
+        const double kx = xk ? (op.cons[3 * n + d] ? xk[i] : s[d]) : 0.0;
+        R[i] = (float)((double)F[i] - kx);
+        E[i] = (float)(xs[i] - (xk ? xk[i] : 0.0));
+    }
+}
+
+// Pre-smoothed pairs: t = D^-1 r, r1 = r - K t, e1 = e - t.  mode 0 sums
+// r1_c^2 and e1_c^2 (stats[6]); mode 1 writes the scaled r1 into the
+// compact image set img[p][pixel][4] (BF16, channels 0..2), e1 into E1, and
+// e1^T K e1 into den[p].
+template <int NPE>
+__global__ void prep_pairs_kernel(Op op, int count, const float* __restrict__ R, const float* __restrict__ E,
+                                  const int* __restrict__ node_pixel, int HW, int mode, float s0, float s1,
+                                  float s2, double* __restrict__ stats, bf16* __restrict__ img,
+                                  float* __restrict__ E1, double* __restrict__ den) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x, p = blockIdx.y;
+    const bool live = n < op.Nn;
+    const size_t base = (size_t)p * 3 * op.Nn;
+    const float* r = R + base;
+    const float* e = E + base;
+    auto tv = [&](int m, int d) {
+        const float* B9 = op.binv32 + 9 * m;
+        return binv_row(B9, d, r[3 * m], r[3 * m + 1], r[3 * m + 2]);
+    };
+    auto e1v = [&](int m, int d) { return e[3 * m + d] - tv(m, d); };
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    if (live) {
+        float u[3];
+        kv_node<NPE>(op, n, tv, u);
+        float r1[3], e1[3];
+        for (int d = 0; d < 3; d++) {
+            r1[d] = r[3 * n + d] - u[d];
+            e1[d] = e1v(n, d);
+        }
+        if (mode == 0) {
+            for (int d = 0; d < 3; d++) {
+                acc[d] = (double)r1[d] * r1[d];
+                acc[3 + d] = (double)e1[d] * e1[d];
+            }
+        } else {
+            const float sc[3] = {s0, s1, s2};
+            bf16* px = img + ((size_t)p * HW + node_pixel[n]) * 4;
+            for (int d = 0; d < 3; d++) px[d] = __float2bfloat16_rn(sc[d] * r1[d]);
+            px[3] = __float2bfloat16_rn(0.f);
+            for (int d = 0; d < 3; d++) E1[base + 3 * n + d] = e1[d];
+            float ke1[3];
+            kv_node<NPE>(op, n, e1v, ke1);
+            acc[0] = (double)e1[0] * ke1[0] + (double)e1[1] * ke1[1] + (double)e1[2] * ke1[2];
+        }
+    }
+    __shared__ double red[6][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < 6; k++) {
+        const double s = warp_sum(acc[k]);
+        if (lane == 0) red[k][warp] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        if (mode == 0) {
+            for (int k = 0; k < 6; k++) {
+                double s = 0;
+                for (int i = 0; i < nw; i++) s += red[k][i];
+                atomicAdd(stats + k, s);
+            }
+        } else {
+            double s = 0;
+            for (int i = 0; i < nw; i++) s += red[0][i];
+            atomicAdd(den + p, s);
+        }
+    }
+}
+
+// Batch input: in[b][pixel][0..15] = img[idx_b][pixel][0..2] (other channels 0).
+// idx_b = perm[(step - 1) * B + b] when step is given (training), else idx[b].
+__global__ void gather_batch_kernel(int B, int HW, const bf16* __restrict__ img, const int* __restrict__ perm,
+                                    const int* __restrict__ step, bf16* __restrict__ in) {
+    const long total = (long)B * HW;
+    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+        const int b = (int)(q / HW), px = (int)(q - (long)b * HW);
+        const int idx = step ? perm[(size_t)(*step - 1) * B + b] : perm[b];
+        const uint2 v = *reinterpret_cast<const uint2*>(img + ((size_t)idx * HW + px) * 4);
+        uint4 o0, o1;
+        o0.x = v.x;
+        o0.y = v.y & 0xFFFFu;  // channel 3 cleared
+        o0.z = o0.w = 0;
+        o1.x = o1.y = o1.z = o1.w = 0;
+        uint4* dst = reinterpret_cast<uint4*>(in + ((size_t)b * HW + px) * 16);
+        dst[0] = o0;
+        dst[1] = o1;
+    }
+}
+
+// Energy-norm loss of a batch: d = e1 - y, y = s_out * N(r1) (0 on
+// constrained DOFs), loss += (d^T K d) / (B e1^T K e1) into *loss; with
+// gout, dL/d(out) = -2 s_out (K d) / (B e1^T K e1) into gout[b][pixel][0..2].
+template <int NPE>
+__global__ void loss_kernel(Op op, int B, int HW, const int* __restrict__ node_pixel, const float* __restrict__ out,
+                            const float* __restrict__ E1, const double* __restrict__ den,
+                            const int* __restrict__ perm, const int* __restrict__ step, float so0, float so1,
+                            float so2, double* __restrict__ loss_hist, bf16* __restrict__ gout) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
+    const int idx = step ? perm[(size_t)(*step - 1) * B + b] : perm[b];
+    const float so[3] = {so0, so1, so2};
+    const float* e1 = E1 + (size_t)idx * 3 * op.Nn;
+    const float* ob = out + (size_t)b * HW * 4;
+    auto dv = [&](int m, int d) {
+        const float y = op.cons[3 * m + d] ? 0.f : so[d] * ob[(size_t)node_pixel[m] * 4 + d];
+        return e1[3 * m + d] - y;
+    };
+    const double sc = 1.0 / ((double)B * den[idx]);
+    double acc[1] = {0.0};
+    if (n < op.Nn) {
+        float kd[3];
+        kv_node<NPE>(op, n, dv, kd);
+        acc[0] = ((double)dv(n, 0) * kd[0] + (double)dv(n, 1) * kd[1] + (double)dv(n, 2) * kd[2]) * sc;
+        if (gout) {
+            bf16* g = gout + ((size_t)b * HW + node_pixel[n]) * 16;
+            for (int d = 0; d < 3; d++)
+                g[d] = __float2bfloat16_rn(op.cons[3 * n + d] ? 0.f : (float)(-2.0 * sc * so[d] * kd[d]));
+        }
+    }
+    __shared__ double red[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double s = warp_sum(acc[0]);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int i = 0; i < (int)((blockDim.x + 31) >> 5); i++) t += red[i];
+        atomicAdd(loss_hist + (step ? *step - 1 : 0), t);
+    }
+}
+
+__global__ void step_begin_kernel(int* step) { *step += 1; }
+
+__global__ void train_tick_kernel(cudaGraphConditionalHandle h, const int* step, const int* stop) {
+    cudaGraphSetConditional(h, *step < *stop ? 1u : 0u);
+}
+
+// ----- flexible PCG ---------------------------------------------------------
+
+struct FState {
+    int it, done, converged, stop_reason, tr_ran, net_off, net_off_at, bad_count, use_net, skip_net;
+    int iterations, net_iters, replacements, error;
+    double bnorm2, rr, true_rr, alpha, beta, gamma_prev, gamma_next;
+};
+
+struct FArgs {
+    Op op;
+    int HW;
+    const int* node_pixel;
+    bf16* img_in;        // [HW][16]
+    const float* img_out;  // [HW][4]
+    float si0, si1, si2, so0, so1, so2;
+    const float* F;
+    double* x;
+    float *r, *r_prev, *r1, *y, *r2, *z, *p0, *p1, *q;
+    double *pU, *pTR, *pA, *pB, *pC, *pD, *pI;
+    FState* st;
+    int G;
+    double tol2;
+    int stop_rule, maxit, replace_every, mode, fallback_after;
+};
+
+__device__ __forceinline__ bool stop_test(const FArgs& a, double rr, double bn2) {
+    return a.stop_rule == PG_STOP_RELATIVE ? rr < a.tol2 * bn2 : (rr < a.tol2 || rr < a.tol2 * bn2);
+}
+
+__global__ void fp_init_kernel(FArgs a) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[1] = {0.0};
+    if (n < a.op.Nn) {
+        for (int d = 0; d < 3; d++) {
+            const int i = 3 * n + d;
+            const float f = a.F[i];
+            a.x[i] = 0.0;
+            a.r[i] = f;
+            a.r_prev[i] = f;
+            a.p0[i] = a.p1[i] = a.q[i] = 0.f;
+            acc[0] += (double)f * f;
+        }
+    }
+    block_partials<1>(acc, a.pI);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        FState s{};
+        s.gamma_prev = 1.0;
+        *a.st = s;
+    }
+}
+
+// U: x += alpha p, r -= alpha q with alpha = p.r / p.Kp of the last
+// direction (0 at the first iteration).
+__global__ void fp_update_kernel(FArgs a) {
+    FState* st = a.st;
+    const int it = st->it;
+    double alpha = 0.0, bn2 = 0.0;
+    int stop = 0;  // 1 zero rhs, 2 breakdown, 3 non-finite
+    if (it == 0) {
+        double s[1];
+        reduce_parts<1>(a.pI, a.G, s);
+        bn2 = s[0];
+        if (!isfinite(bn2)) stop = 3;
+        else if (bn2 < 1e-60) stop = 1;
+    } else {
+        double s[2];
+        reduce_parts<2>(a.pD, a.G, s);
+        if (!isfinite(s[0]) || !isfinite(s[1])) stop = 3;
+        else if (fabs(s[0]) < 1e-30) stop = 2;
+        else alpha = s[1] / s[0];
+    }
+    const float* p = (it & 1) ? a.p1 : a.p0;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[1] = {0.0};
+    if (n < a.op.Nn && !stop) {
+        for (int d = 0; d < 3; d++) {
+            const int i = 3 * n + d;
+            const float ri = a.r[i];
+            a.x[i] += alpha * (double)p[i];
+            a.r_prev[i] = ri;
+            const float rn = (float)((double)ri - alpha * (double)a.q[i]);
+            a.r[i] = rn;
+            acc[0] += (double)rn * rn;
+        }
+    }
+    block_partials<1>(acc, a.pU);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (it == 0) st->bnorm2 = bn2;
+        st->alpha = alpha;
+        if (stop) {
+            st->done = 1;
+            st->converged = stop == 1;
+            st->stop_reason = stop == 1 ? PG_STOP_ZERO_RHS : PG_STOP_BREAKDOWN;
+            st->error = stop == 3;
+            st->iterations = it;
+            st->skip_net = 1;
+        }
+    }
+}
+
+// TR: when the recursive residual meets the tolerance, every replace_every
+// iterations and at the iteration limit: r = F - K x in FP64 (then rounded),
+// and |F - K x|^2 for the stop test.
+template <int NPE>
+__global__ void fp_true_res_kernel(FArgs a) {
+    constexpr int ND = 3 * NPE;
+    FState* st = a.st;
+    if (st->done) return;
+    const int it = st->it;
+    double s[1];
+    reduce_parts<1>(a.pU, a.G, s);
+    const bool trig = stop_test(a, s[0], st->bnorm2) || (it > 0 && it % a.replace_every == 0) ||
+                      it >= a.maxit || !isfinite(s[0]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->tr_ran = trig;
+        st->rr = s[0];
+        if (trig) st->replacements++;
+    }
+    if (!trig) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[1] = {0.0};
+    if (n < a.op.Nn) {
+        double kx[3] = {0, 0, 0};
+        for (int q = a.op.inc_ptr[n]; q < a.op.inc_ptr[n + 1]; q++) {
+            const int e = a.op.inc_idx[q] >> 2, k = a.op.inc_idx[q] & 3;
+            const double* Ke = a.op.ke64 + (size_t)e * ND * ND + 3 * k * ND;
+            for (int b = 0; b < NPE; b++) {
+                const int m = (int)a.op.el[(size_t)e * NPE + b];
+                const double x0 = a.x[3 * m], x1 = a.x[3 * m + 1], x2 = a.x[3 * m + 2];
+                for (int d = 0; d < 3; d++) kx[d] += Ke[d * ND + 3 * b] * x0 + Ke[d * ND + 3 * b + 1] * x1 +
+                                                     Ke[d * ND + 3 * b + 2] * x2;
+            }
+        }
+        for (int d = 0; d < 3; d++) {
+            const int i = 3 * n + d;
+            const double rt = (double)a.F[i] - (a.op.cons[i] ? a.x[i] : kx[d]);
+            a.r[i] = (float)rt;
+            acc[0] += rt * rt;
+        }
+    }
+    block_partials<1>(acc, a.pTR);
+}
+
+// A: stop decision on the true residual; then r1 = r - K D^-1 r and the
+// network input image (s_in r1).
+template <int NPE>
+__global__ void fp_prep_kernel(FArgs a) {
+    FState* st = a.st;
+    if (st->done) return;
+    const int it = st->it;
+    if (st->tr_ran) {
+        double s[1];
+        reduce_parts<1>(a.pTR, a.G, s);
+        const bool fin = isfinite(s[0]);
+        const bool conv = fin && stop_test(a, s[0], st->bnorm2);
+        if (conv || it >= a.maxit || !fin) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                st->done = 1;
+                st->converged = conv;
+                st->stop_reason = conv ? PG_STOP_CONVERGED : PG_STOP_MAX_ITER;
+                st->error = !fin;
+                st->true_rr = s[0];
+                st->iterations = it;
+                st->skip_net = 1;
+            }
+            return;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->true_rr = s[0];
+    }
+    const bool skip = a.mode != 1 || st->net_off;
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->skip_net = skip;
+    if (a.mode == 0 || (a.mode == 1 && st->net_off)) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[1] = {0.0};
+    if (n < a.op.Nn) {
+        const float* r = a.r;
+        auto tv = [&](int m, int d) {
+            return binv_row(a.op.binv32 + 9 * m, d, r[3 * m], r[3 * m + 1], r[3 * m + 2]);
+        };
+        float u[3];
+        kv_node<NPE>(a.op, n, tv, u);
+        const float sc[3] = {a.si0, a.si1, a.si2};
+        bf16* px = a.img_in + (size_t)a.node_pixel[n] * 16;
+        for (int d = 0; d < 3; d++) {
+            const float r1 = r[3 * n + d] - u[d];
+            a.r1[3 * n + d] = r1;
+            px[d] = __float2bfloat16_rn(sc[d] * r1);
+            acc[0] += (double)r1 * r1;
+        }
+    }
+    block_partials<1>(acc, a.pA);
+}
+
+// B: y = s_out N(r1) (0 on constrained DOFs), r2 = r1 - K y.
+template <int NPE>
+__global__ void fp_net_kernel(FArgs a) {
+    FState* st = a.st;
+    if (st->done || st->skip_net) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const float so[3] = {a.so0, a.so1, a.so2};
+    auto yv = [&](int m, int d) {
+        return a.op.cons[3 * m + d] ? 0.f : so[d] * a.img_out[(size_t)a.node_pixel[m] * 4 + d];
+    };
+    double acc[1] = {0.0};
+    if (n < a.op.Nn) {
+        float v[3];
+        kv_node<NPE>(a.op, n, yv, v);
+        for (int d = 0; d < 3; d++) {
+            const int i = 3 * n + d;
+            const float r2 = a.r1[i] - v[d];
+            a.y[i] = yv(n, d);
+            a.r2[i] = r2;
+            acc[0] += (double)r2 * r2;
+        }
+    }
+    block_partials<1>(acc, a.pB);
+}
+
+// C: z = D^-1 r (+ y + D^-1 r2 when the network's correction reduced the
+// residual; mode 2: + D^-1 r1, the smoothing steps without the network).
+__global__ void fp_prec_kernel(FArgs a) {
+    FState* st = a.st;
+    if (st->done) return;
+    bool use = false;
+    if (a.mode == 1 && !st->skip_net) {
+        double s1[1], s2[1];
+        reduce_parts<1>(a.pA, a.G, s1);
+        reduce_parts<1>(a.pB, a.G, s2);
+        use = s2[0] < s1[0];
+    }
+    const bool smooth2 = a.mode == 2;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[2] = {0.0, 0.0};
+    if (n < a.op.Nn) {
+        const float* B9 = a.op.binv32 + 9 * n;
+        const int i = 3 * n;
+        const float r0 = a.r[i], r1_ = a.r[i + 1], r2_ = a.r[i + 2];
+        float z[3];
+        for (int d = 0; d < 3; d++) z[d] = binv_row(B9, d, r0, r1_, r2_);
+        if (use) {
+            const float q0 = a.r2[i], q1 = a.r2[i + 1], q2 = a.r2[i + 2];
+            for (int d = 0; d < 3; d++) z[d] += a.y[i + d] + binv_row(B9, d, q0, q1, q2);
+        } else if (smooth2) {
+            const float q0 = a.r1[i], q1 = a.r1[i + 1], q2 = a.r1[i + 2];
+            for (int d = 0; d < 3; d++) z[d] += binv_row(B9, d, q0, q1, q2);
+        }
+        for (int d = 0; d < 3; d++) {
+            a.z[i + d] = z[d];
+            acc[0] += (double)z[d] * a.r[i + d];
+            acc[1] += (double)z[d] * a.r_prev[i + d];
+        }
+    }
+    block_partials<2>(acc, a.pC);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->use_net = use;
+        if (a.mode == 1 && !st->skip_net) {
+            st->bad_count = use ? 0 : st->bad_count + 1;
+            st->net_iters += use;
+        }
+    }
+}
+
+// D: beta (Polak-Ribiere), p = z + beta p_old, q = K p.
+template <int NPE>
+__global__ void fp_dir_kernel(FArgs a) {
+    FState* st = a.st;
+    if (st->done) return;
+    const int it = st->it;
+    double s[2];
+    reduce_parts<2>(a.pC, a.G, s);
+    double beta = it == 0 ? 0.0 : (s[0] - s[1]) / st->gamma_prev;
+    if (!isfinite(beta)) beta = 0.0;
+    const float* po = (it & 1) ? a.p1 : a.p0;
+    float* pn = (it & 1) ? a.p0 : a.p1;
+    const float bf = (float)beta;
+    auto pv = [&](int m, int d) { return a.z[3 * m + d] + bf * po[3 * m + d]; };
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[2] = {0.0, 0.0};
+    if (n < a.op.Nn) {
+        float qv[3];
+        kv_node<NPE>(a.op, n, pv, qv);
+        for (int d = 0; d < 3; d++) {
+            const int i = 3 * n + d;
+            const float pi = pv(n, d);
+            pn[i] = pi;
+            a.q[i] = qv[d];
+            acc[0] += (double)pi * qv[d];
+            acc[1] += (double)pi * a.r[i];
+        }
+    }
+    block_partials<2>(acc, a.pD);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->gamma_next = s[0];
+        st->beta = beta;
+    }
+}
+
+__global__ void fp_tick_kernel(FArgs a, cudaGraphConditionalHandle h) {
+    FState* st = a.st;
+    st->gamma_prev = st->gamma_next;
+    if (a.mode == 1 && !st->net_off && st->bad_count >= a.fallback_after) {
+        st->net_off = 1;
+        st->net_off_at = st->it;
+    }
+    st->it += 1;
+    cudaGraphSetConditional(h, (!st->done && st->it <= a.maxit + 1) ? 1u : 0u);
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+
+template <typename F>
+int lguarded(pg_ctx* c, F&& body) {
+    if (!c) return PG_EINVAL;
+    std::lock_guard<std::mutex> lk(pgi::ctx_mutex(c));
+    try {
+        LCK(cudaSetDevice(pgi::ctx_device(c)));
+        body();
+    } catch (const LFail& f) {
+        pgi::ctx_set_error(c, f.msg);
+        return f.status;
+    } catch (const std::bad_alloc&) {
+        pgi::ctx_set_error(c, "host allocation failed");
+        return PG_ENOMEM;
+    }
+    return PG_OK;
+}
+
+}  // namespace
+
+// The learned solver of one plan: the node -> pixel map, the training set,
+// the solve's vectors and its graph.
+struct pg_learned {
+    pg_plan* plan = nullptr;
+    pg_net* net = nullptr;
+    pg_ctx* ctx = nullptr;
+    pgi::OperatorView ov{};
+    Op op{};
+    int HW = 0;
+    Buf<int> node_pixel;
+    // training set
+    int P = 0;
+    Buf<bf16> img;
+    Buf<float> E1;
+    Buf<double> den, stats, loss_hist;
+    Buf<int> perm, stop_step;
+    // solve
+    Buf<float> F, r, r_prev, r1, y, r2, z, p0, p1, q;
+    Buf<double> x, parts;
+    Buf<FState> st;
+    cudaGraphExec_t solve_exec = nullptr;
+    int solve_mode = -1, solve_maxit = -1, solve_rule = -1, solve_version = -1;
+    double solve_tol = -1;
+    cudaGraphExec_t train_exec = nullptr;
+    int train_B = 0;
+    cudaStream_t cap = nullptr;  // capture stream
+    ~pg_learned() {
+        if (solve_exec) cudaGraphExecDestroy(solve_exec);
+        if (train_exec) cudaGraphExecDestroy(train_exec);
+        if (cap) cudaStreamDestroy(cap);
+    }
+};
+
+namespace {
+
+Op make_op(const pgi::OperatorView& v) {
+    return Op{v.Nn, v.inc_ptr, v.inc_idx, v.elements, v.ke32, v.ke64, v.binv32, v.cons};
+}
+
+// Real (unpadded, oracle-order) parameters <-> padded master layout.
+void real_to_padded(const pg_net* n, const float* real, std::vector<float>& pad) {
+    pad.assign(n->T.total, 0.f);
+    long k = 0;
+    for (int l = 0; l < pgn::kLayers; l++) {
+        const pgn::LayerDesc& L = n->T.l[l];
+        for (int co = 0; co < kSpec[l].cout; co++)
+            for (int tap = 0; tap < 9; tap++)
+                for (int ci = 0; ci < kSpec[l].cin; ci++) pad[L.off + ((long)co * 9 + tap) * L.cin + ci] = real[k++];
+    }
+}
+
+void padded_to_real(const pg_net* n, const std::vector<float>& pad, float* real) {
+    long k = 0;
+    for (int l = 0; l < pgn::kLayers; l++) {
+        const pgn::LayerDesc& L = n->T.l[l];
+        for (int co = 0; co < kSpec[l].cout; co++)
+            for (int tap = 0; tap < 9; tap++)
+                for (int ci = 0; ci < kSpec[l].cin; ci++) real[k++] = pad[L.off + ((long)co * 9 + tap) * L.cin + ci];
+    }
+}
+
+void refresh_bf16(pg_net* n, cudaStream_t st) {
+    pgn::weights_to_bf16_kernel<<<ew_grid(n->T.total), 256, 0, st>>>(n->T, n->w.p, n->wf.p, n->wd.p);
+    LCK(cudaGetLastError());
+}
+
+// FP32 [B][H][W][3] <-> the workspace's BF16 [B][H][W][16] / FP32 [B][H][W][4]
+__global__ void pack_in_kernel(long P, const float* __restrict__ src, bf16* __restrict__ dst) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < P; i += (long)gridDim.x * blockDim.x)
+        for (int c = 0; c < 16; c++) dst[i * 16 + c] = __float2bfloat16_rn(c < 3 ? src[i * 3 + c] : 0.f);
+}
+__global__ void unpack_out_kernel(long P, const float* __restrict__ src, float* __restrict__ dst) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < P; i += (long)gridDim.x * blockDim.x)
+        for (int c = 0; c < 3; c++) dst[i * 3 + c] = src[i * 4 + c];
+}
+__global__ void pack_gout_kernel(long P, const float* __restrict__ src, bf16* __restrict__ dst) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < P; i += (long)gridDim.x * blockDim.x)
+        for (int c = 0; c < 16; c++) dst[i * 16 + c] = __float2bfloat16_rn(c < 3 ? src[i * 3 + c] : 0.f);
+}
+__global__ void unpack_din_kernel(long P, const bf16* __restrict__ src, float* __restrict__ dst) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < P; i += (long)gridDim.x * blockDim.x)
+        for (int c = 0; c < 3; c++) dst[i * 3 + c] = __bfloat162float(src[i * 16 + c]);
+}
+
+int grid_nodes(int Nn) { return (Nn + 255) / 256; }
+
+void build_solve_graph(pg_learned* L, const pg_options& o, int mode, int fallback_after, int replace_every) {
+    pg_net* n = L->net;
+    cudaStream_t cs = L->cap;
+    Workspace* w = workspace(n, 1, false);
+    const int G = grid_nodes(L->op.Nn);
+    FArgs a{};
+    a.op = L->op;
+    a.HW = L->HW;
+    a.node_pixel = L->node_pixel.p;
+    a.img_in = w->in.p;
+    a.img_out = w->out.p;
+    a.si0 = n->scale[0];
+    a.si1 = n->scale[1];
+    a.si2 = n->scale[2];
+    a.so0 = n->scale[3];
+    a.so1 = n->scale[4];
+    a.so2 = n->scale[5];
+    a.F = L->F.p;
+    a.x = L->x.p;
+    a.r = L->r.p;
+    a.r_prev = L->r_prev.p;
+    a.r1 = L->r1.p;
+    a.y = L->y.p;
+    a.r2 = L->r2.p;
+    a.z = L->z.p;
+    a.p0 = L->p0.p;
+    a.p1 = L->p1.p;
+    a.q = L->q.p;
+    double* P = L->parts.p;
+    a.pU = P;
+    a.pTR = P + 2 * G;
+    a.pA = P + 4 * G;
+    a.pB = P + 6 * G;
+    a.pC = P + 8 * G;
+    a.pD = P + 10 * G;
+    a.pI = P + 12 * G;
+    a.st = L->st.p;
+    a.G = G;
+    a.tol2 = o.tolerance * o.tolerance;
+    a.stop_rule = o.stop_rule;
+    a.maxit = o.max_iterations;
+    a.replace_every = replace_every;
+    a.mode = mode;
+    a.fallback_after = fallback_after;
+
+    if (L->solve_exec) {
+        cudaGraphExecDestroy(L->solve_exec);
+        L->solve_exec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    LCK(cudaGraphCreate(&g, 0));
+    try {
+        cudaGraphConditionalHandle h;
+        LCK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        // the body's init runs as the first node of the graph, before the loop
+        cudaGraphNode_t init_node, loop;
+        cudaKernelNodeParams kp{};
+        void* init_args[] = {&a};
+        kp.func = (void*)fp_init_kernel;
+        kp.gridDim = dim3(G);
+        kp.blockDim = dim3(256);
+        kp.kernelParams = init_args;
+        LCK(cudaGraphAddKernelNode(&init_node, g, nullptr, 0, &kp));
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        LCK(cudaGraphAddNode(&loop, g, &init_node, 1, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        LCK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        const bool q4 = L->op.inc_ptr && L->ov.npe == 4;
+        fp_update_kernel<<<G, 256, 0, cs>>>(a);
+        if (q4) {
+            fp_true_res_kernel<4><<<G, 256, 0, cs>>>(a);
+            fp_prep_kernel<4><<<G, 256, 0, cs>>>(a);
+        } else {
+            fp_true_res_kernel<3><<<G, 256, 0, cs>>>(a);
+            fp_prep_kernel<3><<<G, 256, 0, cs>>>(a);
+        }
+        if (mode == 1) {
+            net_forward(n, w, cs, &L->st.p->skip_net);
+            if (q4)
+                fp_net_kernel<4><<<G, 256, 0, cs>>>(a);
+            else
+                fp_net_kernel<3><<<G, 256, 0, cs>>>(a);
+        }
+        fp_prec_kernel<<<G, 256, 0, cs>>>(a);
+        if (q4)
+            fp_dir_kernel<4><<<G, 256, 0, cs>>>(a);
+        else
+            fp_dir_kernel<3><<<G, 256, 0, cs>>>(a);
+        fp_tick_kernel<<<1, 1, 0, cs>>>(a, h);
+        cudaError_t ce = cudaGetLastError();
+        cudaGraph_t got = nullptr;
+        cudaError_t ee = cudaStreamEndCapture(cs, &got);
+        LCK(ce);
+        LCK(ee);
+        LCK(cudaGraphInstantiate(&L->solve_exec, g, 0));
+    } catch (...) {
+        cudaGraphDestroy(g);
+        throw;
+    }
+    cudaGraphDestroy(g);
+    L->solve_mode = mode;
+    L->solve_version = n->version;
+    L->solve_maxit = o.max_iterations;
+    L->solve_rule = o.stop_rule;
+    L->solve_tol = o.tolerance;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+int pg_net_create(pg_ctx* ctx, int height, int width, uint64_t seed, pg_net** out) {
+    if (out) *out = nullptr;
+    return lguarded(ctx, [&] {
+        if (!out) throw LFail{PG_EINVAL, "out is NULL"};
+        if (height < 8 || width < 8 || height % 8 || width % 8 || (long)height * width > (1L << 22))
+            throw LFail{PG_EINVAL, "network grid must be at least 8 x 8, multiples of 8, at most 4M pixels"};
+        auto n = std::make_unique<pg_net>();
+        n->ctx = ctx;
+        n->H = height;
+        n->W = width;
+        n->T = make_table();
+        const size_t tot = (size_t)n->T.total;
+        n->w.alloc(tot);
+        n->m.alloc(tot);
+        n->v.alloc(tot);
+        n->g.alloc(tot);
+        n->wf.alloc(tot);
+        n->wd.alloc(tot);
+        n->step.alloc(1);
+        cudaStream_t st = pgi::ctx_stream(ctx);
+        // He-normal initialisation (std sqrt(2 / (9 cin)), sqrt(1 / (9 cin)) for
+        // the linear output layer), padded weights 0
+        std::mt19937_64 rng(seed);
+        std::normal_distribution<double> nd(0.0, 1.0);
+        std::vector<float> real((size_t)real_param_count()), pad;
+        long k = 0;
+        for (int l = 0; l < pgn::kLayers; l++) {
+            const double sd = std::sqrt((l == OUTL ? 1.0 : 2.0) / (9.0 * kSpec[l].cin));
+            for (long i = 0; i < 9L * kSpec[l].cin * kSpec[l].cout; i++) real[k++] = (float)(sd * nd(rng));
+        }
+        real_to_padded(n.get(), real.data(), pad);
+        LCK(cudaMemcpyAsync(n->w.p, pad.data(), tot * sizeof(float), cudaMemcpyHostToDevice, st));
+        n->m.zero(st);
+        n->v.zero(st);
+        n->g.zero(st);
+        n->step.zero(st);
+        refresh_bf16(n.get(), st);
+        LCK(cudaStreamSynchronize(st));
+        *out = n.release();
+    });
+}
+
+void pg_net_destroy(pg_net* n) {
+    if (!n) return;
+    {
+        std::lock_guard<std::mutex> lk(pgi::ctx_mutex(n->ctx));
+        cudaSetDevice(pgi::ctx_device(n->ctx));
+        cudaStreamSynchronize(pgi::ctx_stream(n->ctx));
+        n->ws.clear();
+    }
+    delete n;
+}
+
+int64_t pg_net_param_count(const pg_net* n) { return n ? real_param_count() : 0; }
+
+int pg_net_set_params(pg_net* n, const float* params, const float* scales) {
+    if (!n) return PG_EINVAL;
+    return lguarded(n->ctx, [&] {
+        cudaStream_t st = pgi::ctx_stream(n->ctx);
+        if (params) {
+            std::vector<float> pad;
+            real_to_padded(n, params, pad);
+            LCK(cudaMemcpyAsync(n->w.p, pad.data(), pad.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+            refresh_bf16(n, st);
+            n->m.zero(st);
+            n->v.zero(st);
+            n->step.zero(st);
+        }
+        if (scales) {
+            for (int i = 0; i < 6; i++)
+                if (!(scales[i] > 0) || !std::isfinite(scales[i])) throw LFail{PG_EINVAL, "scales must be > 0"};
+            std::memcpy(n->scale, scales, sizeof n->scale);
+            n->version++;
+        }
+        LCK(cudaStreamSynchronize(st));
+    });
+}
+
+int pg_net_get_params(pg_net* n, float* params, float* scales) {
+    if (!n) return PG_EINVAL;
+    return lguarded(n->ctx, [&] {
+        cudaStream_t st = pgi::ctx_stream(n->ctx);
+        if (params) {
+            std::vector<float> pad(n->T.total);
+            LCK(cudaMemcpyAsync(pad.data(), n->w.p, pad.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+            LCK(cudaStreamSynchronize(st));
+            padded_to_real(n, pad, params);
+        }
+        if (scales) std::memcpy(scales, n->scale, sizeof n->scale);
+    });
+}
+
+int pg_net_forward(pg_net* n, int batch, const float* in_dev, float* out_dev) {
+    if (!n) return PG_EINVAL;
+    return lguarded(n->ctx, [&] {
+        if (batch < 1 || !in_dev || !out_dev) throw LFail{PG_EINVAL, "batch < 1 or NULL buffer"};
+        cudaStream_t st = pgi::ctx_stream(n->ctx);
+        Workspace* w = workspace(n, batch, true);
+        const long P = (long)batch * n->H * n->W;
+        pack_in_kernel<<<ew_grid(P), 256, 0, st>>>(P, in_dev, w->in.p);
+        net_forward(n, w, st, nullptr);
+        unpack_out_kernel<<<ew_grid(P), 256, 0, st>>>(P, w->out.p, out_dev);
+        LCK(cudaGetLastError());
+        LCK(cudaStreamSynchronize(st));
+    });
+}
+
+int pg_net_backward(pg_net* n, int batch, const float* gout_dev, float* gin_dev, float* gparams) {
+    if (!n) return PG_EINVAL;
+    return lguarded(n->ctx, [&] {
+        if (batch < 1 || !gout_dev) throw LFail{PG_EINVAL, "batch < 1 or NULL buffer"};
+        auto it = n->ws.find(batch);
+        if (it == n->ws.end() || !it->second->grads) throw LFail{PG_EINVAL, "call pg_net_forward first"};
+        Workspace* w = it->second.get();
+        cudaStream_t st = pgi::ctx_stream(n->ctx);
+        const long P = (long)batch * n->H * n->W;
+        pack_gout_kernel<<<ew_grid(P), 256, 0, st>>>(P, gout_dev, w->gout.p);
+        n->g.zero(st);
+        net_backward(n, w, st, gin_dev != nullptr);
+        if (gin_dev) unpack_din_kernel<<<ew_grid(P), 256, 0, st>>>(P, w->din.p, gin_dev);
+        LCK(cudaGetLastError());
+        if (gparams) {
+            std::vector<float> pad(n->T.total);
+            LCK(cudaMemcpyAsync(pad.data(), n->g.p, pad.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+            LCK(cudaStreamSynchronize(st));
+            padded_to_real(n, pad, gparams);
+        }
+        LCK(cudaStreamSynchronize(st));
+    });
+}
+
+int pg_net_adam_step(pg_net* n, const float* grads, float lr) {
+    if (!n) return PG_EINVAL;
+    return lguarded(n->ctx, [&] {
+        if (!grads) throw LFail{PG_EINVAL, "grads is NULL"};
+        cudaStream_t st = pgi::ctx_stream(n->ctx);
+        std::vector<float> pad;
+        real_to_padded(n, grads, pad);
+        LCK(cudaMemcpyAsync(n->g.p, pad.data(), pad.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+        step_begin_kernel<<<1, 1, 0, st>>>(n->step.p);
+        pgn::adam_kernel<<<ew_grid(n->T.total), 256, 0, st>>>(n->T, n->w.p, n->m.p, n->v.p, n->g.p, n->step.p, lr,
+                                                              0.9f, 0.999f, 1e-8f, 0, n->wf.p, n->wd.p);
+        LCK(cudaGetLastError());
+        LCK(cudaStreamSynchronize(st));
+    });
+}
+
+int pg_learned_create(pg_plan* plan, pg_net* net, const int32_t* node_pixel, pg_learned** out) {
+    if (out) *out = nullptr;
+    if (!plan || !net) return PG_EINVAL;
+    pg_ctx* c = pgi::plan_ctx(plan);
+    if (c != net->ctx) return PG_EINVAL;
+    return lguarded(c, [&] {
+        if (!out || !node_pixel) throw LFail{PG_EINVAL, "out / node_pixel is NULL"};
+        auto L = std::make_unique<pg_learned>();
+        L->plan = plan;
+        L->net = net;
+        L->ctx = c;
+        std::string e = pgi::plan_operator(plan, &L->ov);
+        if (!e.empty()) throw LFail{PG_ECUDA, e};
+        if (L->ov.npe != 4 && L->ov.npe != 3) throw LFail{PG_EINVAL, "unsupported element type"};
+        L->op = make_op(L->ov);
+        L->HW = net->H * net->W;
+        const int Nn = L->ov.Nn;
+        std::vector<char> seen(L->HW, 0);
+        for (int i = 0; i < Nn; i++) {
+            const int px = node_pixel[i];
+            if (px < 0 || px >= L->HW || seen[px])
+                throw LFail{PG_EINVAL, "node_pixel must map every node to a distinct pixel of the grid"};
+            seen[px] = 1;
+        }
+        cudaStream_t st = pgi::ctx_stream(c);
+        L->node_pixel.alloc(Nn);
+        LCK(cudaMemcpyAsync(L->node_pixel.p, node_pixel, Nn * sizeof(int), cudaMemcpyHostToDevice, st));
+        const size_t n3 = 3 * (size_t)Nn;
+        for (Buf<float>* b : {&L->F, &L->r, &L->r_prev, &L->r1, &L->y, &L->r2, &L->z, &L->p0, &L->p1, &L->q}) {
+            b->alloc(n3);
+            b->zero(st);
+        }
+        L->x.alloc(n3);
+        L->parts.alloc(14 * (size_t)grid_nodes(Nn));
+        L->st.alloc(1);
+        L->stats.alloc(6);
+        LCK(cudaStreamCreateWithFlags(&L->cap, cudaStreamNonBlocking));
+        LCK(cudaStreamSynchronize(st));
+        *out = L.release();
+    });
+}
+
+void pg_learned_destroy(pg_learned* L) {
+    if (!L) return;
+    {
+        std::lock_guard<std::mutex> lk(pgi::ctx_mutex(L->ctx));
+        cudaSetDevice(pgi::ctx_device(L->ctx));
+        cudaStreamSynchronize(pgi::ctx_stream(L->ctx));
+    }
+    delete L;
+}
+
+int pg_learned_make_pairs(pg_learned* L, int count, const float* F_dev, const double* xstar_dev,
+                          const double* xk_dev, float* R_out, float* E_out) {
+    if (!L) return PG_EINVAL;
+    return lguarded(L->ctx, [&] {
+        if (count < 0 || (count > 0 && (!F_dev || !xstar_dev || !R_out || !E_out)))
+            throw LFail{PG_EINVAL, "NULL buffer"};
+        if (count == 0) return;
+        cudaStream_t st = pgi::ctx_stream(L->ctx);
+        dim3 grid(grid_nodes(L->op.Nn), count);
+        if (L->ov.npe == 4)
+            make_pairs_kernel<4><<<grid, 256, 0, st>>>(L->op, count, F_dev, xstar_dev, xk_dev, R_out, E_out);
+        else
+            make_pairs_kernel<3><<<grid, 256, 0, st>>>(L->op, count, F_dev, xstar_dev, xk_dev, R_out, E_out);
+        LCK(cudaGetLastError());
+        LCK(cudaStreamSynchronize(st));
+    });
+}
+
+namespace {
+
+// Pre-smooths `count` pairs into the training set (replacing it).  With
+// set_scales, the network's input / output scales become 1 / rms(r1_c)
+// and rms(e1_c) over the pairs.
+void load_pairs(pg_learned* L, int count, const float* R, const float* E, bool set_scales) {
+    pg_net* n = L->net;
+    cudaStream_t st = pgi::ctx_stream(L->ctx);
+    dim3 grid(grid_nodes(L->op.Nn), count);
+    if (set_scales) {
+        L->stats.zero(st);
+        if (L->ov.npe == 4)
+            prep_pairs_kernel<4><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 0, 1, 1, 1,
+                                                        L->stats.p, nullptr, nullptr, nullptr);
+        else
+            prep_pairs_kernel<3><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 0, 1, 1, 1,
+                                                        L->stats.p, nullptr, nullptr, nullptr);
+        LCK(cudaGetLastError());
+        double s[6];
+        LCK(cudaMemcpyAsync(s, L->stats.p, sizeof s, cudaMemcpyDeviceToHost, st));
+        LCK(cudaStreamSynchronize(st));
+        const double cnt = (double)count * L->op.Nn;
+        for (int d = 0; d < 3; d++) {
+            const double ri = std::sqrt(s[d] / cnt), eo = std::sqrt(s[3 + d] / cnt);
+            n->scale[d] = ri > 0 && std::isfinite(ri) ? (float)(1.0 / ri) : 1.f;
+            n->scale[3 + d] = eo > 0 && std::isfinite(eo) ? (float)eo : 1.f;
+        }
+        n->version++;
+    }
+    L->P = count;
+    L->img.alloc((size_t)count * L->HW * 4);
+    L->img.zero(st);
+    L->E1.alloc((size_t)count * 3 * L->op.Nn);
+    L->den.alloc(count);
+    L->den.zero(st);
+    if (L->ov.npe == 4)
+        prep_pairs_kernel<4><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 1, n->scale[0],
+                                                    n->scale[1], n->scale[2], nullptr, L->img.p, L->E1.p, L->den.p);
+    else
+        prep_pairs_kernel<3><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 1, n->scale[0],
+                                                    n->scale[1], n->scale[2], nullptr, L->img.p, L->E1.p, L->den.p);
+    LCK(cudaGetLastError());
+    LCK(cudaStreamSynchronize(st));
+}
+
+// Mean loss of pairs [first, first + count) of the training set (forward
+// passes of up to `batch` pairs, no gradient); per-pair losses into per
+// (host, optional).
+double eval_loss(pg_learned* L, int first, int count, int batch, double* per) {
+    pg_net* n = L->net;
+    cudaStream_t st = pgi::ctx_stream(L->ctx);
+    Workspace* w = workspace(n, batch, false);
+    Buf<int> idx;
+    idx.alloc(batch);
+    Buf<double> acc;
+    acc.alloc(1);
+    double total = 0.0;
+    std::vector<int> ids(batch);
+    for (int s = 0; s < count; s += batch) {
+        const int b = std::min(batch, count - s);
+        for (int i = 0; i < batch; i++) ids[i] = first + s + std::min(i, b - 1);
+        LCK(cudaMemcpyAsync(idx.p, ids.data(), batch * sizeof(int), cudaMemcpyHostToDevice, st));
+        gather_batch_kernel<<<ew_grid((long)batch * L->HW), 256, 0, st>>>(batch, L->HW, L->img.p, idx.p, nullptr,
+                                                                        w->in.p);
+        net_forward(n, w, st, nullptr);
+        for (int i = 0; i < b; i++) {
+            // one pair at a time so each pair's loss is separate (B = 1 scaling)
+            acc.zero(st);
+            dim3 grid(grid_nodes(L->op.Nn), 1);
+            const float* outb = w->out.p + (size_t)i * L->HW * 4;
+            const int* idb = idx.p + i;
+            if (L->ov.npe == 4)
+                loss_kernel<4><<<grid, 256, 0, st>>>(L->op, 1, L->HW, L->node_pixel.p, outb, L->E1.p, L->den.p, idb,
+                                                     nullptr, n->scale[3], n->scale[4], n->scale[5], acc.p, nullptr);
+            else
+                loss_kernel<3><<<grid, 256, 0, st>>>(L->op, 1, L->HW, L->node_pixel.p, outb, L->E1.p, L->den.p, idb,
+                                                     nullptr, n->scale[3], n->scale[4], n->scale[5], acc.p, nullptr);
+            LCK(cudaGetLastError());
+            double v = 0;
+            LCK(cudaMemcpyAsync(&v, acc.p, sizeof v, cudaMemcpyDeviceToHost, st));
+            LCK(cudaStreamSynchronize(st));
+            if (per) per[s + i] = v;
+            total += v;
+        }
+    }
+    return count > 0 ? total / count : 0.0;
+}
+
+void build_train_graph(pg_learned* L, int B, int total_steps, float lr, bool cosine) {
+    pg_net* n = L->net;
+    Workspace* w = workspace(n, B, true);
+    cudaStream_t cs = L->cap;
+    if (L->train_exec) {
+        cudaGraphExecDestroy(L->train_exec);
+        L->train_exec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    LCK(cudaGraphCreate(&g, 0));
+    try {
+        cudaGraphConditionalHandle h;
+        LCK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t loop;
+        LCK(cudaGraphAddNode(&loop, g, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        LCK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        step_begin_kernel<<<1, 1, 0, cs>>>(n->step.p);
+        cudaMemsetAsync(n->g.p, 0, n->g.n * sizeof(float), cs);
+        gather_batch_kernel<<<ew_grid((long)B * L->HW), 256, 0, cs>>>(B, L->HW, L->img.p, L->perm.p, n->step.p,
+                                                                    w->in.p);
+        net_forward(n, w, cs, nullptr);
+        dim3 grid(grid_nodes(L->op.Nn), B);
+        if (L->ov.npe == 4)
+            loss_kernel<4><<<grid, 256, 0, cs>>>(L->op, B, L->HW, L->node_pixel.p, w->out.p, L->E1.p, L->den.p,
+                                                 L->perm.p, n->step.p, n->scale[3], n->scale[4], n->scale[5],
+                                                 L->loss_hist.p, w->gout.p);
+        else
+            loss_kernel<3><<<grid, 256, 0, cs>>>(L->op, B, L->HW, L->node_pixel.p, w->out.p, L->E1.p, L->den.p,
+                                                 L->perm.p, n->step.p, n->scale[3], n->scale[4], n->scale[5],
+                                                 L->loss_hist.p, w->gout.p);
+        net_backward(n, w, cs, false);
+        pgn::adam_kernel<<<ew_grid(n->T.total), 256, 0, cs>>>(n->T, n->w.p, n->m.p, n->v.p, n->g.p, n->step.p, lr,
+                                                              0.9f, 0.999f, 1e-8f, cosine ? total_steps : 0,
+                                                              n->wf.p, n->wd.p);
+        train_tick_kernel<<<1, 1, 0, cs>>>(h, n->step.p, L->stop_step.p);
+        cudaError_t ce = cudaGetLastError();
+        cudaGraph_t got = nullptr;
+        cudaError_t ee = cudaStreamEndCapture(cs, &got);
+        LCK(ce);
+        LCK(ee);
+        LCK(cudaGraphInstantiate(&L->train_exec, g, 0));
+    } catch (...) {
+        cudaGraphDestroy(g);
+        throw;
+    }
+    cudaGraphDestroy(g);
+    L->train_B = B;
+}
+
+}  // namespace
+
+void pg_train_options_default(pg_train_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof *o);
+    o->struct_size = sizeof *o;
+    o->epochs = 20;
+    o->batch = 32;
+    o->lr = 1e-3f;
+    o->cosine = 1;
+    o->seed = 1;
+    o->val_count = 0;
+    o->set_scales = 1;
+}
+
+int pg_learned_train(pg_learned* L, int count, const float* R_dev, const float* E_dev,
+                     const pg_train_options* opt, pg_train_info* info) {
+    if (!L) return PG_EINVAL;
+    if (info) std::memset(info, 0, sizeof *info);
+    return lguarded(L->ctx, [&] {
+        pg_train_options o;
+        pg_train_options_default(&o);
+        if (opt) {
+            if (opt->struct_size != sizeof(pg_train_options)) throw LFail{PG_EINVAL, "pg_train_options size mismatch"};
+            o = *opt;
+        }
+        if (count < 2 || !R_dev || !E_dev) throw LFail{PG_EINVAL, "need at least 2 pairs"};
+        if (o.batch < 1 || o.epochs < 0 || !(o.lr > 0) || o.val_count < 0 || o.val_count >= count)
+            throw LFail{PG_EINVAL, "bad training options"};
+        if (o.epochs > PG_TRAIN_MAX_EPOCHS) throw LFail{PG_EINVAL, "too many epochs"};
+        pg_net* n = L->net;
+        cudaStream_t st = pgi::ctx_stream(L->ctx);
+        auto t0 = std::chrono::steady_clock::now();
+        load_pairs(L, count, R_dev, E_dev, o.set_scales != 0);
+        const int ntrain = count - o.val_count;
+        const int B = std::min(o.batch, ntrain);
+        const int spe = ntrain / B;  // steps per epoch (the remainder of a shuffle is left out)
+        const int total = spe * o.epochs;
+        // one shuffle of the training pairs per epoch, all uploaded at once
+        std::mt19937_64 rng(o.seed);
+        std::vector<int> perm((size_t)std::max(1, total) * B), ids(ntrain);
+        for (int e = 0; e < o.epochs; e++) {
+            for (int i = 0; i < ntrain; i++) ids[i] = i;
+            std::shuffle(ids.begin(), ids.end(), rng);
+            std::copy(ids.begin(), ids.begin() + (size_t)spe * B, perm.begin() + (size_t)e * spe * B);
+        }
+        L->perm.alloc(perm.size());
+        LCK(cudaMemcpyAsync(L->perm.p, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        L->loss_hist.alloc(std::max(1, total));
+        L->loss_hist.zero(st);
+        L->stop_step.alloc(1);
+        n->step.zero(st);
+        n->m.zero(st);
+        n->v.zero(st);
+        const int vb = std::min(64, std::max(1, o.val_count));
+        if (info) {
+            info->val_loss_before = o.val_count ? eval_loss(L, ntrain, o.val_count, vb, nullptr) : 0.0;
+            info->steps = total;
+            info->batch = B;
+        }
+        if (total > 0) {
+            build_train_graph(L, B, total, o.lr, o.cosine != 0);
+            double tms = 0.0;
+            cudaEvent_t e0, e1;
+            LCK(cudaEventCreate(&e0));
+            LCK(cudaEventCreate(&e1));
+            for (int e = 0; e < o.epochs; e++) {
+                const int stop = (e + 1) * spe;
+                LCK(cudaMemcpyAsync(L->stop_step.p, &stop, sizeof stop, cudaMemcpyHostToDevice, st));
+                LCK(cudaEventRecord(e0, st));
+                LCK(cudaGraphLaunch(L->train_exec, st));
+                LCK(cudaEventRecord(e1, st));
+                LCK(cudaStreamSynchronize(st));
+                float ms = 0;
+                LCK(cudaEventElapsedTime(&ms, e0, e1));
+                tms += ms;
+                if (info) {
+                    std::vector<double> h(spe);
+                    LCK(cudaMemcpy(h.data(), L->loss_hist.p + (size_t)e * spe, spe * sizeof(double),
+                                   cudaMemcpyDeviceToHost));
+                    double s = 0;
+                    for (double v : h) s += v;
+                    info->epoch_loss[e] = s / spe;
+                    info->epoch_val_loss[e] = o.val_count ? eval_loss(L, ntrain, o.val_count, vb, nullptr) : 0.0;
+                }
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            int steps_done = 0;
+            LCK(cudaMemcpy(&steps_done, n->step.p, sizeof(int), cudaMemcpyDeviceToHost));
+            if (steps_done != total) throw LFail{PG_ECUDA, "training graph ran an unexpected number of steps"};
+            if (info) {
+                info->train_ms = tms;
+                double first = 0, last = 0;
+                LCK(cudaMemcpy(&first, L->loss_hist.p, sizeof(double), cudaMemcpyDeviceToHost));
+                LCK(cudaMemcpy(&last, L->loss_hist.p + total - 1, sizeof(double), cudaMemcpyDeviceToHost));
+                info->loss_first_step = first;
+                info->loss_last_step = last;
+            }
+        }
+        if (info) {
+            info->val_loss = o.val_count ? eval_loss(L, ntrain, o.val_count, vb, nullptr) : 0.0;
+            info->total_ms =
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
+    });
+}
+
+int pg_learned_loss(pg_learned* L, int count, const float* R_dev, const float* E_dev, double* loss_out) {
+    if (!L) return PG_EINVAL;
+    return lguarded(L->ctx, [&] {
+        if (count < 1 || !R_dev || !E_dev || !loss_out) throw LFail{PG_EINVAL, "NULL buffer or count < 1"};
+        load_pairs(L, count, R_dev, E_dev, false);
+        eval_loss(L, 0, count, std::min(count, 16), loss_out);
+    });
+}
+
+namespace {
+
+void learned_solve(pg_learned* L, const pg_options* opt, int mode, const float* F, bool host, double* x_out,
+                   pg_info* info, pg_learned_stats* ls) {
+    pg_options o;
+    pg_options_default(&o);
+    if (opt) {
+        if (opt->struct_size != sizeof(pg_options)) throw LFail{PG_EINVAL, "pg_options size mismatch"};
+        o = *opt;
+    }
+    if (!(o.tolerance >= 0) || o.max_iterations < 0) throw LFail{PG_EINVAL, "bad tolerance / max_iterations"};
+    if (mode < 0 || mode > 2) throw LFail{PG_EINVAL, "mode must be 0, 1 or 2"};
+    if (!F || !x_out) throw LFail{PG_EINVAL, "F / x is NULL"};
+    cudaStream_t st = pgi::ctx_stream(L->ctx);
+    const size_t n3 = 3 * (size_t)L->op.Nn;
+    auto t0 = std::chrono::steady_clock::now();
+    if (!L->solve_exec || L->solve_mode != mode || L->solve_maxit != o.max_iterations ||
+        L->solve_rule != o.stop_rule || L->solve_tol != o.tolerance || L->solve_version != L->net->version)
+        build_solve_graph(L, o, mode, 3, 50);
+    if (host) {
+        for (size_t i = 0; i < n3; i++)
+            if (!std::isfinite(F[i])) throw LFail{PG_ENONFINITE, "F contains NaN or Inf"};
+    }
+    LCK(cudaMemcpyAsync(L->F.p, F, n3 * sizeof(float), host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                        st));
+    cudaEvent_t e0, e1;
+    LCK(cudaEventCreate(&e0));
+    LCK(cudaEventCreate(&e1));
+    LCK(cudaEventRecord(e0, st));
+    LCK(cudaGraphLaunch(L->solve_exec, st));
+    LCK(cudaEventRecord(e1, st));
+    LCK(cudaMemcpyAsync(x_out, L->x.p, n3 * sizeof(double), host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                        st));
+    FState s{};
+    LCK(cudaMemcpyAsync(&s, L->st.p, sizeof s, cudaMemcpyDeviceToHost, st));
+    LCK(cudaStreamSynchronize(st));
+    float ms = 0;
+    LCK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s.error) throw LFail{PG_ENONFINITE, "non-finite value in the flexible PCG iteration"};
+    if (info) {
+        info->iterations = s.iterations;
+        info->converged = s.converged;
+        info->stop_reason = s.stop_reason;
+        info->b_norm = std::sqrt(s.bnorm2);
+        info->final_residual = std::sqrt(s.true_rr);
+        info->true_rel_residual = s.bnorm2 > 0 ? std::sqrt(s.true_rr / s.bnorm2) : 0.0;
+        info->solve_ms = ms;
+        info->reliable_updates = s.replacements;
+        info->reductions = s.iterations;
+        info->plan_cached = 1;
+        info->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    if (ls) {
+        ls->network_iterations = s.net_iters;
+        ls->network_off_at = s.net_off ? s.net_off_at : -1;
+        ls->replacements = s.replacements;
+        ls->mode = mode;
+    }
+}
+
+}  // namespace
+
+int pg_learned_solve_device(pg_learned* L, const pg_options* opt, int mode, const float* F_dev, double* x_dev,
+                            pg_info* info, pg_learned_stats* stats) {
+    if (info) std::memset(info, 0, sizeof *info);
+    if (!L) return PG_EINVAL;
+    const int st = lguarded(L->ctx, [&] { learned_solve(L, opt, mode, F_dev, false, x_dev, info, stats); });
+    if (info) info->status = st;
+    return st;
+}
+
+int pg_learned_solve(pg_learned* L, const pg_options* opt, int mode, const float* F, double* x_out,
+                     pg_info* info, pg_learned_stats* stats) {
+    if (info) std::memset(info, 0, sizeof *info);
+    if (!L) return PG_EINVAL;
+    const int st = lguarded(L->ctx, [&] { learned_solve(L, opt, mode, F, true, x_out, info, stats); });
+    if (info) info->status = st;
+    return st;
+}
+
+}  // extern "C"

@@ -31,7 +31,16 @@ EXPORTED = ("pg_options_default", "pg_is_available", "pg_create", "pg_destroy", 
             "pg_plan_destroy", "pg_apply_k", "pg_apply_k_static",
             "pg_block_jacobi", "pg_element_stiffness", "pg_plan_inspect",
             "pg_plan_inspect_halo", "pg_batch_create", "pg_batch_solve", "pg_batch_destroy",
-            "pg_solve_batch", "pg_batch_schedule", "pg_moments", "pg_plan_moments_device", "pg_solve_load_cases")
+            "pg_solve_batch", "pg_batch_schedule", "pg_moments", "pg_plan_moments_device", "pg_solve_load_cases",
+            "pg_net_create", "pg_net_destroy", "pg_net_param_count", "pg_net_set_params",
+            "pg_net_get_params", "pg_net_forward", "pg_net_backward", "pg_net_adam_step",
+            "pg_learned_create", "pg_learned_destroy", "pg_learned_make_pairs",
+            "pg_train_options_default", "pg_learned_train", "pg_learned_loss",
+            "pg_learned_solve_device", "pg_learned_solve")
+
+PG_TRAIN_MAX_EPOCHS = 256
+# pg_learned_solve modes
+LEARNED_BLOCK_JACOBI, LEARNED_NETWORK, LEARNED_SMOOTHING_ONLY = 0, 1, 2
 
 
 class PgProblem(C.Structure):
@@ -132,6 +141,46 @@ class PgInfo(C.Structure):
         return d
 
 
+class PgTrainOptions(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("epochs", C.c_int32),
+        ("batch", C.c_int32),
+        ("lr", C.c_float),
+        ("cosine", C.c_int32),
+        ("seed", C.c_uint64),
+        ("val_count", C.c_int32),
+        ("set_scales", C.c_int32),
+    ]
+
+
+class PgTrainInfo(C.Structure):
+    _fields_ = [
+        ("steps", C.c_int32),
+        ("batch", C.c_int32),
+        ("loss_first_step", C.c_double),
+        ("loss_last_step", C.c_double),
+        ("val_loss_before", C.c_double),
+        ("val_loss", C.c_double),
+        ("train_ms", C.c_double),
+        ("total_ms", C.c_double),
+        ("epoch_loss", C.c_double * PG_TRAIN_MAX_EPOCHS),
+        ("epoch_val_loss", C.c_double * PG_TRAIN_MAX_EPOCHS),
+    ]
+
+
+class PgLearnedStats(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int32),
+        ("network_iterations", C.c_int32),
+        ("network_off_at", C.c_int32),
+        ("replacements", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class PlateGPUError(RuntimeError):
     """A non-OK pg_status; ``status`` holds the code name."""
 
@@ -204,6 +253,40 @@ def load() -> C.CDLL:
     L.pg_moments.restype = I
     L.pg_plan_moments_device.argtypes = [P, P, P]
     L.pg_plan_moments_device.restype = I
+    L.pg_net_create.argtypes = [P, I, I, C.c_uint64, C.POINTER(P)]
+    L.pg_net_create.restype = I
+    L.pg_net_destroy.argtypes = [P]
+    L.pg_net_destroy.restype = None
+    L.pg_net_param_count.argtypes = [P]
+    L.pg_net_param_count.restype = C.c_int64
+    L.pg_net_set_params.argtypes = [P, P, P]
+    L.pg_net_set_params.restype = I
+    L.pg_net_get_params.argtypes = [P, P, P]
+    L.pg_net_get_params.restype = I
+    L.pg_net_forward.argtypes = [P, I, P, P]
+    L.pg_net_forward.restype = I
+    L.pg_net_backward.argtypes = [P, I, P, P, P]
+    L.pg_net_backward.restype = I
+    L.pg_net_adam_step.argtypes = [P, P, C.c_float]
+    L.pg_net_adam_step.restype = I
+    L.pg_learned_create.argtypes = [P, P, P, C.POINTER(P)]
+    L.pg_learned_create.restype = I
+    L.pg_learned_destroy.argtypes = [P]
+    L.pg_learned_destroy.restype = None
+    L.pg_learned_make_pairs.argtypes = [P, I, P, P, P, P, P]
+    L.pg_learned_make_pairs.restype = I
+    L.pg_train_options_default.argtypes = [C.POINTER(PgTrainOptions)]
+    L.pg_train_options_default.restype = None
+    L.pg_learned_train.argtypes = [P, I, P, P, C.POINTER(PgTrainOptions), C.POINTER(PgTrainInfo)]
+    L.pg_learned_train.restype = I
+    L.pg_learned_loss.argtypes = [P, I, P, P, P]
+    L.pg_learned_loss.restype = I
+    L.pg_learned_solve_device.argtypes = [P, C.POINTER(PgOptions), I, P, P, C.POINTER(PgInfo),
+                                          C.POINTER(PgLearnedStats)]
+    L.pg_learned_solve_device.restype = I
+    L.pg_learned_solve.argtypes = [P, C.POINTER(PgOptions), I, P, P, C.POINTER(PgInfo),
+                                   C.POINTER(PgLearnedStats)]
+    L.pg_learned_solve.restype = I
     _lib = L
     return L
 
@@ -479,6 +562,125 @@ class DevicePlan:
     def close(self):
         if getattr(self, "h", None):
             self.ctx.L.pg_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Net:
+    """A pg_net: the learned preconditioner's U-Net on a height x width grid."""
+
+    def __init__(self, ctx: Context, height: int, width: int, seed: int = 1):
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx._check(ctx.L.pg_net_create(ctx.h, int(height), int(width), C.c_uint64(int(seed)), C.byref(h)))
+        self.h = h
+        self.height, self.width = int(height), int(width)
+
+    @property
+    def param_count(self) -> int:
+        return int(self.ctx.L.pg_net_param_count(self.h))
+
+    def set_params(self, params=None, scales=None):
+        p = None if params is None else np.ascontiguousarray(params, np.float32)
+        if p is not None and p.size != self.param_count:
+            raise ValueError(f"expected {self.param_count} parameters, got {p.size}")
+        s = None if scales is None else np.ascontiguousarray(scales, np.float32)
+        if s is not None and s.size != 6:
+            raise ValueError("scales: 6 values")
+        self.ctx._check(self.ctx.L.pg_net_set_params(self.h, _ptr(p), _ptr(s)))
+
+    def get_params(self):
+        p = np.zeros(self.param_count, np.float32)
+        s = np.zeros(6, np.float32)
+        self.ctx._check(self.ctx.L.pg_net_get_params(self.h, _ptr(p), _ptr(s)))
+        return p, s
+
+    def forward(self, batch: int, in_dev: int, out_dev: int):
+        self.ctx._check(self.ctx.L.pg_net_forward(self.h, int(batch), C.c_void_p(in_dev), C.c_void_p(out_dev)))
+
+    def backward(self, batch: int, gout_dev: int, gin_dev=None, want_params: bool = True):
+        g = np.zeros(self.param_count, np.float32) if want_params else None
+        self.ctx._check(self.ctx.L.pg_net_backward(self.h, int(batch), C.c_void_p(gout_dev),
+                                                   None if gin_dev is None else C.c_void_p(gin_dev), _ptr(g)))
+        return g
+
+    def adam_step(self, grads, lr: float):
+        g = np.ascontiguousarray(grads, np.float32)
+        self.ctx._check(self.ctx.L.pg_net_adam_step(self.h, _ptr(g), C.c_float(lr)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.pg_net_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def train_options(epochs=20, batch=32, lr=1e-3, cosine=True, seed=1, val_count=0,
+                  set_scales=True) -> PgTrainOptions:
+    o = PgTrainOptions()
+    load().pg_train_options_default(C.byref(o))
+    o.epochs, o.batch, o.lr = int(epochs), int(batch), float(lr)
+    o.cosine, o.seed, o.val_count = int(bool(cosine)), int(seed), int(val_count)
+    o.set_scales = int(bool(set_scales))
+    return o
+
+
+class Learned:
+    """A pg_learned: flexible PCG with the network as the coarse correction
+    of a two-level preconditioner, on one plan."""
+
+    def __init__(self, plan: "DevicePlan", net: Net, node_pixel):
+        self.ctx, self.plan, self.net = plan.ctx, plan, net
+        npx = np.ascontiguousarray(node_pixel, np.int32)
+        h = C.c_void_p()
+        self.ctx._check(self.ctx.L.pg_learned_create(plan.h, net.h, _ptr(npx), C.byref(h)))
+        self.h = h
+        self.n = 3 * int(plan.prob.struct.node_count)
+
+    def make_pairs(self, count, F_dev, xstar_dev, xk_dev, R_dev, E_dev):
+        self.ctx._check(self.ctx.L.pg_learned_make_pairs(
+            self.h, int(count), C.c_void_p(F_dev), C.c_void_p(xstar_dev),
+            None if xk_dev is None else C.c_void_p(xk_dev), C.c_void_p(R_dev), C.c_void_p(E_dev)))
+
+    def train(self, count, R_dev, E_dev, opts: PgTrainOptions):
+        info = PgTrainInfo()
+        self.ctx._check(self.ctx.L.pg_learned_train(self.h, int(count), C.c_void_p(R_dev), C.c_void_p(E_dev),
+                                                    C.byref(opts), C.byref(info)))
+        return info
+
+    def loss(self, count, R_dev, E_dev):
+        out = np.zeros(int(count), np.float64)
+        self.ctx._check(self.ctx.L.pg_learned_loss(self.h, int(count), C.c_void_p(R_dev), C.c_void_p(E_dev),
+                                                   _ptr(out)))
+        return out
+
+    def solve_device(self, opts: PgOptions, F_dev: int, x_dev: int, mode: int = LEARNED_NETWORK):
+        info, stats = PgInfo(), PgLearnedStats()
+        self.ctx._check(self.ctx.L.pg_learned_solve_device(self.h, C.byref(opts), int(mode), C.c_void_p(F_dev),
+                                                           C.c_void_p(x_dev), C.byref(info), C.byref(stats)))
+        return info, stats
+
+    def solve(self, opts: PgOptions, F, mode: int = LEARNED_NETWORK):
+        F = np.ascontiguousarray(F, np.float32)
+        x = np.zeros(self.n, np.float64)
+        info, stats = PgInfo(), PgLearnedStats()
+        self.ctx._check(self.ctx.L.pg_learned_solve(self.h, C.byref(opts), int(mode), _ptr(F), _ptr(x),
+                                                    C.byref(info), C.byref(stats)))
+        return x, info, stats
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.L.pg_learned_destroy(self.h)
             self.h = None
 
     def __del__(self):

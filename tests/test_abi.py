@@ -151,3 +151,36 @@ def test_dkt_plan_invariants_two_ring_halo():
     assert _lib.plan_inspect(pr, 37, rings=2)["violations"] == 0
     with pytest.raises(_lib.PlateGPUError, match="rings"):
         _lib.plan_inspect(pr, 37, rings=3)
+
+
+def test_learned_struct_layouts_match_header():
+    prog = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "plategpu.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(pg_train_options), offsetof(pg_train_options, seed),
+         sizeof(pg_train_info), offsetof(pg_train_info, epoch_val_loss), sizeof(pg_learned_stats),
+         offsetof(pg_learned_stats, replacements));
+  return 0;
+}
+"""
+    import ctypes as C
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(c, "w").write(prog)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        vals = [int(v) for v in subprocess.run([exe], capture_output=True, text=True,
+                                               check=True).stdout.split()]
+    assert vals == [C.sizeof(_lib.PgTrainOptions), _lib.PgTrainOptions.seed.offset,
+                    C.sizeof(_lib.PgTrainInfo), _lib.PgTrainInfo.epoch_val_loss.offset,
+                    C.sizeof(_lib.PgLearnedStats), _lib.PgLearnedStats.replacements.offset]
+
+
+def test_train_options_defaults():
+    import ctypes as C
+    o = _lib.PgTrainOptions()
+    _lib.load().pg_train_options_default(C.byref(o))
+    assert o.struct_size == C.sizeof(_lib.PgTrainOptions)
+    assert o.epochs == 20 and o.batch == 32 and abs(o.lr - 1e-3) < 1e-9 and o.cosine == 1

@@ -1,0 +1,238 @@
+"""Learned two-level preconditioner on the GPU against the CPU oracle
+(oracle/unet_oracle.py) and the FP64 truth.
+
+- The U-Net's forward and backward passes (BF16 tensor-core convolutions,
+  FP32 accumulation) against the oracle with the same bfloat16 rounding:
+  output and input gradient within 2e-2 relative L2, every layer's weight
+  gradient within 5e-2 (accumulation order and rare rounding flips differ).
+- Adam against the oracle's float64 step (1e-5 relative).
+- Residual/error pairs, the pre-smoothing and the energy-norm loss against
+  the oracle's operator.
+- Training on the GPU lowers the held-out loss; the trained network cuts
+  the iterations of flexible PCG against the same method without it
+  (smoothing steps only, and plain block Jacobi), and every solve reaches
+  the FP64 error bar; a network whose correction does not help is switched
+  off and the solve still converges.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from plategpu import _lib, learned, workloads
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.fixture(scope="module")
+def U():
+    import unet_oracle
+    return unet_oracle
+
+
+@pytest.mark.parametrize("shape", [(2, 16, 24), (1, 40, 32)])
+def test_forward_backward_match_oracle(gpu_ctx, U, shape):
+    B, H, W = shape
+    rng = np.random.default_rng(7)
+    params = U.init_params(11)
+    net = _lib.Net(gpu_ctx, H, W)
+    net.set_params(U.flatten(params).astype(np.float32))
+    x = rng.standard_normal((B, H, W, 3)).astype(np.float32)
+    out = torch.zeros((B, H, W, 3), dtype=torch.float32, device="cuda")
+    net.forward(B, dev(x).data_ptr(), out.data_ptr())
+    ref, cache = U.forward(params, x.astype(np.float64), bf=True)
+    assert rel_err(out.cpu().numpy(), ref) < 2e-2
+    g = rng.standard_normal((B, H, W, 3)).astype(np.float32)
+    gin = torch.zeros_like(out)
+    gW = net.backward(B, dev(g).data_ptr(), gin.data_ptr())
+    rW, rx = U.backward(cache, g.astype(np.float64))
+    assert rel_err(gin.cpu().numpy(), rx) < 2e-2
+    k = 0
+    for li, (name, ci, co, _relu) in enumerate(U.LAYERS):
+        m = 9 * ci * co
+        assert rel_err(gW[k:k + m], rW[li].reshape(-1)) < 5e-2, name
+        k += m
+    net.close()
+
+
+def test_forward_is_positively_homogeneous(gpu_ctx, U):
+    """No biases and ReLU: N(c x) = c N(x) for c > 0 (up to BF16 rounding,
+    exactly for powers of two)."""
+    rng = np.random.default_rng(3)
+    net = _lib.Net(gpu_ctx, 16, 16, seed=5)
+    x = rng.standard_normal((1, 16, 16, 3)).astype(np.float32)
+    a = torch.zeros((1, 16, 16, 3), dtype=torch.float32, device="cuda")
+    b = torch.zeros_like(a)
+    net.forward(1, dev(x).data_ptr(), a.data_ptr())
+    net.forward(1, dev(x * np.float32(2.0 ** -20)).data_ptr(), b.data_ptr())
+    assert np.array_equal(b.cpu().numpy(), a.cpu().numpy() * np.float32(2.0 ** -20))
+    net.close()
+
+
+def test_adam_matches_oracle(gpu_ctx, U):
+    rng = np.random.default_rng(9)
+    params = U.init_params(2)
+    net = _lib.Net(gpu_ctx, 8, 8)
+    flat = U.flatten(params)
+    net.set_params(flat.astype(np.float32))
+    P = [p.copy() for p in params]
+    M = [np.zeros_like(p) for p in params]
+    V = [np.zeros_like(p) for p in params]
+    for t in (1, 2, 3):
+        g = [rng.standard_normal(p.shape) * 1e-2 for p in params]
+        gf = U.flatten(g).astype(np.float32)
+        net.adam_step(gf, 1e-3)
+        P, M, V = U.adam(P, [gg.astype(np.float32).astype(np.float64) for gg in g], M, V, t, lr=1e-3)
+    got, _ = net.get_params()
+    assert np.allclose(got, U.flatten(P), rtol=1e-5, atol=1e-7)
+    net.close()
+
+
+@pytest.fixture(scope="module")
+def small():
+    return workloads.plate_q4(32, seed=3, edges="fixed", pressure=2e3, n_point_loads=4, name="plate_q4_32_learned")
+
+
+def oracle_operator(oracle, wl):
+    m, mat = wl.mesh, wl.material
+    ke = oracle.all_ke(m.nodes, m.elements, 4, mat.E, mat.nu, mat.t, mode=oracle.FP64)
+    A = oracle.assemble(m.nodeCount, m.elements, 4, ke, wl.cons_mask)
+    bd = oracle.invert_block_diag(oracle.block_diag(m.nodeCount, m.elements, 4, ke, oracle.FP64),
+                                  wl.cons_mask, oracle.FP64)
+    return A, bd
+
+
+def test_pairs_and_loss_match_oracle(gpu_ctx, oracle, U, small):
+    wl = small
+    ls = learned.LearnedSolver(gpu_ctx, wl, seed=4)
+    A, bd = oracle_operator(oracle, wl)
+    n = wl.n_dof
+    rng = np.random.default_rng(5)
+    F = workloads.random_field_loads(wl, 3, 17)
+    xs = np.stack([np.linalg.solve(A.toarray(), np.where(wl.cons_mask != 0, 0.0, f.astype(np.float64)))
+                   for f in F])
+    xk = xs * rng.uniform(0.2, 0.9, size=(3, 1))
+    R = torch.zeros((3, n), dtype=torch.float32, device="cuda")
+    E = torch.zeros_like(R)
+    ls.learned.make_pairs(3, dev(F).data_ptr(), dev(xs).data_ptr(), dev(xk).data_ptr(), R.data_ptr(),
+                          E.data_ptr())
+    Rh, Eh = R.cpu().numpy(), E.cpu().numpy()
+    for i in range(3):
+        r_ref = np.where(wl.cons_mask != 0, 0.0, F[i].astype(np.float64)) - A @ xk[i]
+        assert rel_err(Rh[i], r_ref) < 1e-5
+        assert rel_err(Eh[i], xs[i] - xk[i]) < 1e-6
+    # the loss of each pair through the network, against the oracle's
+    scales = np.array([2.0, 0.5, 0.25, 1e-3, 4e-4, 3e-4], np.float32)
+    ls.net.set_params(None, scales)
+    got = ls.learned.loss(3, R.data_ptr(), E.data_ptr())
+    p, _ = ls.net.get_params()
+    params = U.unflatten(p.astype(np.float64))
+    H, W = ls.net.height, ls.net.width
+    for i in range(3):
+        r1, e1 = U.training_pair(A, bd.astype(np.float32).astype(np.float64), Rh[i].astype(np.float64),
+                                 Eh[i].astype(np.float64))
+        img = U.to_image(r1, ls.node_pixel, H, W, scales[:3])[None]
+        out, _ = U.forward(params, img, bf=True)
+        y = U.from_image(out[0], ls.node_pixel, scales[3:], wl.cons_mask)
+        want, _ = U.energy_loss(A, e1, y)
+        assert abs(got[i] - want) < 2e-2 * max(1.0, abs(want)), (got[i], want)
+    ls.close()
+
+
+@pytest.fixture(scope="module")
+def trained(gpu_ctx, small):
+    """A network trained on the GPU for the 32 x 32 plate (512 pairs)."""
+    ls, info = learned.train_plate(torch, gpu_ctx, small, loads=512, epochs=12, batch=16, val=64,
+                                   k_max=120, seed=21, log=lambda *_: None)
+    yield ls, info
+    ls.close()
+
+
+def test_training_lowers_the_held_out_loss(trained):
+    ls, info = trained
+    assert info["steps"] == 12 * (448 // 16)
+    assert info["val_loss"] < 0.5 * info["val_loss_before"], info
+    assert info["loss_last_step"] < info["loss_first_step"]
+    assert all(np.isfinite(info["epoch_loss"]))
+
+
+def truth_of(oracle, wl, F):
+    m, mat = wl.mesh, wl.material
+    ke = oracle.all_ke(m.nodes, m.elements, 4, mat.E, mat.nu, mat.t, mode=oracle.FP64)
+    solve = oracle.truth_factor(m.nodeCount, m.elements, 4, ke, wl.cons_mask)
+    return np.stack([solve(f)[0] for f in F])
+
+
+def test_trained_network_cuts_iterations_and_meets_the_error_bar(oracle, trained, small):
+    ls, _info = trained
+    wl = small
+    F = workloads.random_field_loads(wl, 4, 99)  # loads the network never saw
+    xt = truth_of(oracle, wl, F)
+    rows = {m: learned.evaluate(torch, ls, F, tolerance=1e-8, mode=m, truth=xt)
+            for m in (_lib.LEARNED_NETWORK, _lib.LEARNED_SMOOTHING_ONLY, _lib.LEARNED_BLOCK_JACOBI)}
+    for m, rs in rows.items():
+        for r in rs:
+            assert r["converged"] and r["rel_l2"] < 1e-6, (m, r)
+    it_net = np.mean([r["iterations"] for r in rows[_lib.LEARNED_NETWORK]])
+    it_smooth = np.mean([r["iterations"] for r in rows[_lib.LEARNED_SMOOTHING_ONLY]])
+    it_bj = np.mean([r["iterations"] for r in rows[_lib.LEARNED_BLOCK_JACOBI]])
+    assert it_net < 0.7 * it_smooth and it_smooth < it_bj, (it_net, it_smooth, it_bj)
+    assert all(r["network_iterations"] > 0 for r in rows[_lib.LEARNED_NETWORK])
+
+
+def test_block_jacobi_mode_matches_plain_pcg(gpu_ctx, oracle, small):
+    wl = small
+    ls = learned.LearnedSolver(gpu_ctx, wl)
+    xt = truth_of(oracle, wl, [wl.F])[0]
+    x, info, st = ls.learned.solve(learned.solve_options(1e-8), wl.F, mode=_lib.LEARNED_BLOCK_JACOBI)
+    assert info.converged and rel_err(x, xt) < 1e-6
+    pr = _lib.Problem(wl.mesh, wl.material, wl.coloring, wl.F, wl.cons_mask)
+    _x1, one = gpu_ctx.solve(pr, _lib.make_options(tolerance=1e-8, max_iterations=20000,
+                                                   stop_rule=_lib.PG_STOP_RELATIVE))
+    assert abs(info.iterations - one.iterations) <= max(3, 0.03 * one.iterations)
+    assert st.network_iterations == 0
+    ls.close()
+
+
+def test_unhelpful_network_is_switched_off(gpu_ctx, oracle, U, small):
+    """A network whose correction points away from the error (its output
+    layer negated and scaled up) stops being used after three iterations
+    that do not reduce the residual; the solve finishes as block-Jacobi PCG
+    and meets the error bar."""
+    wl = small
+    ls = learned.LearnedSolver(gpu_ctx, wl, seed=8)
+    p, s = ls.net.get_params()
+    k = sum(9 * ci * co for _n, ci, co, _r in U.LAYERS[:-1])
+    p[k:] *= -1e3
+    ls.net.set_params(p, s)
+    xt = truth_of(oracle, wl, [wl.F])[0]
+    x, info, st = ls.learned.solve(learned.solve_options(1e-8), wl.F, mode=_lib.LEARNED_NETWORK)
+    assert info.converged and rel_err(x, xt) < 1e-6
+    assert 0 <= st.network_off_at <= 4 and st.network_iterations == 0
+    ls.close()
+
+
+def test_host_and_device_solves_agree(trained, small):
+    ls, _ = trained
+    wl = small
+    opts = learned.solve_options(1e-8)
+    x, info, _st = ls.learned.solve(opts, wl.F)
+    xd = torch.zeros(wl.n_dof, dtype=torch.float64, device="cuda")
+    info2, _ = ls.learned.solve_device(opts, dev(wl.F).data_ptr(), xd.data_ptr())
+    assert info.iterations == info2.iterations
+    assert np.array_equal(x, xd.cpu().numpy())
+
+
+def test_zero_load_and_iteration_limit(trained, small):
+    ls, _ = trained
+    wl = small
+    x, info, _ = ls.learned.solve(learned.solve_options(1e-8), np.zeros(wl.n_dof, np.float32))
+    assert info.converged and info.iterations == 0 and not np.any(x)
+    x, info, _ = ls.learned.solve(learned.solve_options(1e-14, max_iterations=5), wl.F)
+    assert not info.converged and info.iterations == 5
+    assert info.stop_reason == _lib.PG_STOP_MAX_ITER
