@@ -81,17 +81,24 @@ napi_status napi_create_array_with_length(napi_env, size_t, napi_value*);
 napi_status napi_set_element(napi_env, napi_value, uint32_t, napi_value);
 #define NAPI_AUTO_LENGTH ((size_t)-1)
 
-/* ---- one solver context per process, created on first use ---- */
+/* ---- one solver context per CUDA device, created on first use ---- */
+#define MAX_DEVICES 16
 static pthread_mutex_t g_ctx_mu = PTHREAD_MUTEX_INITIALIZER;
-static pg_ctx* g_ctx = NULL;
-static int g_ctx_status = PG_OK;
+static pg_ctx* g_ctx[MAX_DEVICES];
+static int g_ctx_status[MAX_DEVICES];
 
-static pg_ctx* shared_ctx(int* status) {
+static pg_ctx* shared_ctx(int device, int* status) {
+    if (device < 0 || device >= MAX_DEVICES) {
+        *status = PG_EINVAL;
+        return NULL;
+    }
     pthread_mutex_lock(&g_ctx_mu);
-    if (!g_ctx && g_ctx_status == PG_OK) g_ctx_status = pg_create(0, &g_ctx);
-    *status = g_ctx ? PG_OK : g_ctx_status;
+    if (!g_ctx[device] && g_ctx_status[device] == PG_OK)
+        g_ctx_status[device] = pg_create(device, &g_ctx[device]);
+    *status = g_ctx[device] ? PG_OK : g_ctx_status[device];
+    pg_ctx* c = g_ctx[device];
     pthread_mutex_unlock(&g_ctx_mu);
-    return g_ctx;
+    return c;
 }
 
 static const char* status_name(int st) {
@@ -109,6 +116,7 @@ typedef struct {
     void* owned[7]; /* copies of the input arrays */
     double* x;
     int cases;       /* > 0: a load-case job (pg_solve_load_cases), F holds `cases` loads */
+    int device;      /* CUDA device of the job's context */
     pg_info* infos;  /* [cases] */
     int status;
     char error[512];
@@ -160,10 +168,11 @@ static void solve_execute(napi_env env, void* data) {
     (void)env;
     SolveJob* j = (SolveJob*)data;
     int st = PG_OK;
-    pg_ctx* ctx = shared_ctx(&st);
+    pg_ctx* ctx = shared_ctx(j->device, &st);
     if (!ctx) {
         j->status = st;
-        strncpy(j->error, pg_last_error(NULL), sizeof j->error - 1);
+        strncpy(j->error, st == PG_EINVAL ? "device index out of range" : pg_last_error(NULL),
+                sizeof j->error - 1);
         return;
     }
     if (j->cases > 0)
@@ -237,7 +246,7 @@ static napi_value start_job(napi_env env, napi_callback_info info, int load_case
         napi_throw_error(env, "PG_ENOMEM", "out of memory");
         return NULL;
     }
-    double nn, ne, npe, E, nu, t, tol, maxit, prec, pre, smo, stop, cases;
+    double nn, ne, npe, E, nu, t, tol, maxit, prec, pre, smo, stop, cases, device;
     napi_value o = argv[0];
     int bad = get_number(env, o, "nodeCount", -1, &nn) | get_number(env, o, "elementCount", -1, &ne) |
               get_number(env, o, "nodesPerElement", 4, &npe) | get_number(env, o, "E", 0, &E) |
@@ -248,9 +257,10 @@ static napi_value start_job(napi_env env, napi_callback_info info, int load_case
               get_number(env, o, "preconditioner", PG_PRECOND_BLOCK_JACOBI, &pre) |
               get_number(env, o, "smoother", PG_SMOOTHER_BLOCK_JACOBI, &smo) |
               get_number(env, o, "stopRule", PG_STOP_REFERENCE, &stop) |
-              get_number(env, o, "cases", 1, &cases);
+              get_number(env, o, "cases", 1, &cases) | get_number(env, o, "device", 0, &device);
     if (!load_cases) cases = 1;
-    if (bad || nn < 0 || ne < 0 || nn > 67108864.0 || ne > 67108864.0 || cases < 1 || cases > 65536.0) {
+    if (bad || nn < 0 || ne < 0 || nn > 67108864.0 || ne > 67108864.0 || cases < 1 || cases > 65536.0 ||
+        !(device >= 0 && device < MAX_DEVICES) || device != (double)(int)device) {
         job_free(j);
         napi_throw_error(env, "PG_EINVAL", "problem needs nodeCount, elementCount, E, nu, t");
         return NULL;
@@ -279,6 +289,7 @@ static napi_value start_job(napi_env env, napi_callback_info info, int load_case
         return NULL;
     }
     j->cases = load_cases ? (int)cases : 0;
+    j->device = (int)device;
     j->x = (double*)malloc(3 * Nn * (size_t)cases * sizeof(double) + 8);
     if (load_cases) j->infos = (pg_info*)calloc((size_t)cases, sizeof(pg_info));
     if (!j->x || (load_cases && !j->infos)) {
@@ -333,9 +344,11 @@ static napi_value js_is_available(napi_env env, napi_callback_info info) {
 
 static napi_value js_clear_cache(napi_env env, napi_callback_info info) {
     (void)info;
-    int st = PG_OK;
-    pg_ctx* ctx = shared_ctx(&st);
-    if (ctx) pg_clear_cache(ctx);
+    /* every context created so far */
+    pthread_mutex_lock(&g_ctx_mu);
+    for (int d = 0; d < MAX_DEVICES; d++)
+        if (g_ctx[d]) pg_clear_cache(g_ctx[d]);
+    pthread_mutex_unlock(&g_ctx_mu);
     napi_value u;
     napi_get_undefined(env, &u);
     return u;

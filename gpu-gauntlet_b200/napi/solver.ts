@@ -29,6 +29,8 @@ export interface GPUSolverOptions {
   smoother?: 'block-jacobi' | 'chebyshev';
   /** 'reference' (default: ||r|| < tol or ||r||/||b|| < tol) or 'relative' (||r||/||b|| < tol) */
   stopRule?: 'reference' | 'relative';
+  /** CUDA device index (default 0); each device gets its own solver context */
+  device?: number;
 }
 
 export interface GPUSolveResult {
@@ -129,6 +131,7 @@ function addonProblem(
     preconditioner: options.preconditioner === 'two-level' ? 1 : 0,
     smoother: options.smoother === 'chebyshev' ? 1 : 0,
     stopRule: options.stopRule === 'relative' ? 1 : 0,
+    device: options.device ?? 0,
   };
 }
 
