@@ -39,5 +39,20 @@ pg_ctx* plan_ctx(const pg_plan* h);
 // the caller holds the context's mutex.  Returns an empty message on
 // success.
 std::string plan_operator(pg_plan* h, OperatorView* out);
+// lambda_max(D^-1 K) of the plan's operator (30 power steps on the device,
+// cached in the plan); the caller holds the context's mutex.
+double plan_lambda_max(pg_plan* h);
+
+// Flexible PCG on global memory (learned.cu): the solve of a plate whose
+// partition does not fit the persistent kernel's shared memory.  FP32
+// vectors, FP64 x, dot products and true-residual stop; mode 0 block
+// Jacobi, mode 2 damped block-Jacobi smoothing steps (damping from
+// lambda_max).  The caller holds the context's mutex and has set the
+// device.  Failures return a pg_status and a message.
+struct GlobalPcg;
+GlobalPcg* global_pcg_create(pg_ctx* c, const OperatorView& ov, double lambda_max, std::string* err);
+void global_pcg_destroy(GlobalPcg* g);
+int global_pcg_solve(GlobalPcg* g, const pg_options& o, int mode, const float* F_dev, void* x_dst, bool x_host,
+                     pg_info* info, std::string* err);
 
 }  // namespace pgi

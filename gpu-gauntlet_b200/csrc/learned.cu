@@ -527,14 +527,14 @@ __global__ void make_pairs_kernel(Op op, int count, const float* __restrict__ F,
     }
 }
 
-// Pre-smoothed pairs: t = D^-1 r, r1 = r - K t, e1 = e - t.  mode 0 sums
+// Pre-smoothed pairs: t = omega D^-1 r, r1 = r - K t, e1 = e - t.  mode 0 sums
 // r1_c^2 and e1_c^2 (stats[6]); mode 1 writes the scaled r1 into the
 // compact image set img[p][pixel][4] (BF16, channels 0..2), e1 into E1, and
 // e1^T K e1 into den[p].
 template <int NPE>
 __global__ void prep_pairs_kernel(Op op, int count, const float* __restrict__ R, const float* __restrict__ E,
-                                  const int* __restrict__ node_pixel, int HW, int mode, float s0, float s1,
-                                  float s2, double* __restrict__ stats, bf16* __restrict__ img,
+                                  const int* __restrict__ node_pixel, int HW, int mode, float omega, float s0,
+                                  float s1, float s2, double* __restrict__ stats, bf16* __restrict__ img,
                                   float* __restrict__ E1, double* __restrict__ den) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x, p = blockIdx.y;
     const bool live = n < op.Nn;
@@ -543,7 +543,7 @@ __global__ void prep_pairs_kernel(Op op, int count, const float* __restrict__ R,
     const float* e = E + base;
     auto tv = [&](int m, int d) {
         const float* B9 = op.binv32 + 9 * m;
-        return binv_row(B9, d, r[3 * m], r[3 * m + 1], r[3 * m + 2]);
+        return omega * binv_row(B9, d, r[3 * m], r[3 * m + 1], r[3 * m + 2]);
     };
     auto e1v = [&](int m, int d) { return e[3 * m + d] - tv(m, d); };
     double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -676,6 +676,7 @@ struct FArgs {
     bf16* img_in;        // [HW][16]
     const float* img_out;  // [HW][4]
     float si0, si1, si2, so0, so1, so2;
+    float omega;  // damping of the block-Jacobi smoothing steps
     const float* F;
     double* x;
     float *r, *r_prev, *r1, *y, *r2, *z, *p0, *p1, *q;
@@ -804,8 +805,8 @@ __global__ void fp_true_res_kernel(FArgs a) {
     block_partials<1>(acc, a.pTR);
 }
 
-// A: stop decision on the true residual; then r1 = r - K D^-1 r and the
-// network input image (s_in r1).
+// A: stop decision on the true residual; then r1 = r - K t, t = omega D^-1 r,
+// and the network input image (s_in r1).
 template <int NPE>
 __global__ void fp_prep_kernel(FArgs a) {
     FState* st = a.st;
@@ -837,8 +838,9 @@ __global__ void fp_prep_kernel(FArgs a) {
     double acc[1] = {0.0};
     if (n < a.op.Nn) {
         const float* r = a.r;
+        const float om = a.omega;
         auto tv = [&](int m, int d) {
-            return binv_row(a.op.binv32 + 9 * m, d, r[3 * m], r[3 * m + 1], r[3 * m + 2]);
+            return om * binv_row(a.op.binv32 + 9 * m, d, r[3 * m], r[3 * m + 1], r[3 * m + 2]);
         };
         float u[3];
         kv_node<NPE>(a.op, n, tv, u);
@@ -879,8 +881,10 @@ __global__ void fp_net_kernel(FArgs a) {
     block_partials<1>(acc, a.pB);
 }
 
-// C: z = D^-1 r (+ y + D^-1 r2 when the network's correction reduced the
-// residual; mode 2: + D^-1 r1, the smoothing steps without the network).
+// C: z = t + y + omega D^-1 r2 (t = omega D^-1 r) when the network's
+// correction reduced the residual; mode 2 (the smoothing steps without the
+// network): z = t + omega D^-1 r1; otherwise (mode 0, or an iteration whose
+// correction did not help) plain block Jacobi z = D^-1 r.
 __global__ void fp_prec_kernel(FArgs a) {
     FState* st = a.st;
     if (st->done) return;
@@ -898,14 +902,15 @@ __global__ void fp_prec_kernel(FArgs a) {
         const float* B9 = a.op.binv32 + 9 * n;
         const int i = 3 * n;
         const float r0 = a.r[i], r1_ = a.r[i + 1], r2_ = a.r[i + 2];
+        const float om = a.omega;
         float z[3];
         for (int d = 0; d < 3; d++) z[d] = binv_row(B9, d, r0, r1_, r2_);
         if (use) {
             const float q0 = a.r2[i], q1 = a.r2[i + 1], q2 = a.r2[i + 2];
-            for (int d = 0; d < 3; d++) z[d] += a.y[i + d] + binv_row(B9, d, q0, q1, q2);
+            for (int d = 0; d < 3; d++) z[d] = om * z[d] + a.y[i + d] + om * binv_row(B9, d, q0, q1, q2);
         } else if (smooth2) {
             const float q0 = a.r1[i], q1 = a.r1[i + 1], q2 = a.r1[i + 2];
-            for (int d = 0; d < 3; d++) z[d] += binv_row(B9, d, q0, q1, q2);
+            for (int d = 0; d < 3; d++) z[d] = om * z[d] + om * binv_row(B9, d, q0, q1, q2);
         }
         for (int d = 0; d < 3; d++) {
             a.z[i + d] = z[d];
@@ -992,8 +997,29 @@ int lguarded(pg_ctx* c, F&& body) {
 
 }  // namespace
 
-// The learned solver of one plan: the node -> pixel map, the training set,
-// the solve's vectors and its graph.
+// Flexible-PCG solver state on one operator: its vectors, reduction
+// partials, device state record and the solve graph (the learned solver's,
+// and the global-memory path's for plates past shared-memory capacity).
+struct FpcgSolver {
+    pg_ctx* ctx = nullptr;
+    Op op{};
+    int npe = 4;
+    float omega = 1.f;
+    Buf<float> F, r, r_prev, r1, y, r2, z, p0, p1, q;
+    Buf<double> x, parts;
+    Buf<FState> st;
+    cudaStream_t cap = nullptr;  // capture stream
+    cudaGraphExec_t exec = nullptr;
+    int mode = -1, maxit = -1, rule = -1, version = -1;
+    double tol = -1;
+    ~FpcgSolver() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (cap) cudaStreamDestroy(cap);
+    }
+};
+
+// The learned solver of one plan: the node -> pixel map, the training set
+// and the flexible-PCG solver.
 struct pg_learned {
     pg_plan* plan = nullptr;
     pg_net* net = nullptr;
@@ -1001,6 +1027,7 @@ struct pg_learned {
     pgi::OperatorView ov{};
     Op op{};
     int HW = 0;
+    float omega = 1.f;  // damping of the smoothing steps (training and solve)
     Buf<int> node_pixel;
     // training set
     int P = 0;
@@ -1008,20 +1035,11 @@ struct pg_learned {
     Buf<float> E1;
     Buf<double> den, stats, loss_hist;
     Buf<int> perm, stop_step;
-    // solve
-    Buf<float> F, r, r_prev, r1, y, r2, z, p0, p1, q;
-    Buf<double> x, parts;
-    Buf<FState> st;
-    cudaGraphExec_t solve_exec = nullptr;
-    int solve_mode = -1, solve_maxit = -1, solve_rule = -1, solve_version = -1;
-    double solve_tol = -1;
+    FpcgSolver S;
     cudaGraphExec_t train_exec = nullptr;
     int train_B = 0;
-    cudaStream_t cap = nullptr;  // capture stream
     ~pg_learned() {
-        if (solve_exec) cudaGraphExecDestroy(solve_exec);
         if (train_exec) cudaGraphExecDestroy(train_exec);
-        if (cap) cudaStreamDestroy(cap);
     }
 };
 
@@ -1078,35 +1096,60 @@ __global__ void unpack_din_kernel(long P, const bf16* __restrict__ src, float* _
 
 int grid_nodes(int Nn) { return (Nn + 255) / 256; }
 
-void build_solve_graph(pg_learned* L, const pg_options& o, int mode, int fallback_after, int replace_every) {
-    pg_net* n = L->net;
-    cudaStream_t cs = L->cap;
-    Workspace* w = workspace(n, 1, false);
-    const int G = grid_nodes(L->op.Nn);
+// Buffers of a flexible-PCG solver for an operator with Nn nodes.
+void fpcg_init(FpcgSolver* S, pg_ctx* c, const Op& op, int npe, float omega) {
+    S->ctx = c;
+    S->op = op;
+    S->npe = npe;
+    S->omega = omega;
+    cudaStream_t st = pgi::ctx_stream(c);
+    const size_t n3 = 3 * (size_t)op.Nn;
+    for (Buf<float>* b : {&S->F, &S->r, &S->r_prev, &S->r1, &S->y, &S->r2, &S->z, &S->p0, &S->p1, &S->q}) {
+        b->alloc(n3);
+        b->zero(st);
+    }
+    S->x.alloc(n3);
+    S->parts.alloc(14 * (size_t)grid_nodes(op.Nn));
+    S->st.alloc(1);
+    LCK(cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
+    LCK(cudaStreamSynchronize(st));
+}
+
+// Builds the solve graph of S: an init node, then a conditional WHILE node
+// whose body is one flexible-PCG iteration (mode 1 includes the network
+// forward pass on net's batch-1 workspace).
+void fpcg_build(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const int* node_pixel, int HW,
+                int fallback_after, int replace_every) {
+    cudaStream_t cs = S->cap;
+    Workspace* w = mode == 1 ? workspace(n, 1, false) : nullptr;
+    const int G = grid_nodes(S->op.Nn);
     FArgs a{};
-    a.op = L->op;
-    a.HW = L->HW;
-    a.node_pixel = L->node_pixel.p;
-    a.img_in = w->in.p;
-    a.img_out = w->out.p;
-    a.si0 = n->scale[0];
-    a.si1 = n->scale[1];
-    a.si2 = n->scale[2];
-    a.so0 = n->scale[3];
-    a.so1 = n->scale[4];
-    a.so2 = n->scale[5];
-    a.F = L->F.p;
-    a.x = L->x.p;
-    a.r = L->r.p;
-    a.r_prev = L->r_prev.p;
-    a.r1 = L->r1.p;
-    a.y = L->y.p;
-    a.r2 = L->r2.p;
-    a.z = L->z.p;
-    a.p0 = L->p0.p;
-    a.p1 = L->p1.p;
-    a.q = L->q.p;
-    double* P = L->parts.p;
+    a.op = S->op;
+    a.HW = HW;
+    a.node_pixel = node_pixel;
+    a.img_in = w ? w->in.p : nullptr;
+    a.img_out = w ? w->out.p : nullptr;
+    const float one[6] = {1, 1, 1, 1, 1, 1};
+    const float* sc = n ? n->scale : one;
+    a.si0 = sc[0];
+    a.si1 = sc[1];
+    a.si2 = sc[2];
+    a.so0 = sc[3];
+    a.so1 = sc[4];
+    a.so2 = sc[5];
+    a.omega = S->omega;
+    a.F = S->F.p;
+    a.x = S->x.p;
+    a.r = S->r.p;
+    a.r_prev = S->r_prev.p;
+    a.r1 = S->r1.p;
+    a.y = S->y.p;
+    a.r2 = S->r2.p;
+    a.z = S->z.p;
+    a.p0 = S->p0.p;
+    a.p1 = S->p1.p;
+    a.q = S->q.p;
+    double* P = S->parts.p;
     a.pU = P;
     a.pTR = P + 2 * G;
     a.pA = P + 4 * G;
@@ -1114,7 +1157,7 @@ void build_solve_graph(pg_learned* L, const pg_options& o, int mode, int fallbac
     a.pC = P + 8 * G;
     a.pD = P + 10 * G;
     a.pI = P + 12 * G;
-    a.st = L->st.p;
+    a.st = S->st.p;
     a.G = G;
     a.tol2 = o.tolerance * o.tolerance;
     a.stop_rule = o.stop_rule;
@@ -1123,16 +1166,16 @@ void build_solve_graph(pg_learned* L, const pg_options& o, int mode, int fallbac
     a.mode = mode;
     a.fallback_after = fallback_after;
 
-    if (L->solve_exec) {
-        cudaGraphExecDestroy(L->solve_exec);
-        L->solve_exec = nullptr;
+    if (S->exec) {
+        cudaGraphExecDestroy(S->exec);
+        S->exec = nullptr;
     }
     cudaGraph_t g = nullptr;
     LCK(cudaGraphCreate(&g, 0));
     try {
         cudaGraphConditionalHandle h;
         LCK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
-        // the body's init runs as the first node of the graph, before the loop
+        // the state and vectors are reset by the first node, before the loop
         cudaGraphNode_t init_node, loop;
         cudaKernelNodeParams kp{};
         void* init_args[] = {&a};
@@ -1149,7 +1192,7 @@ void build_solve_graph(pg_learned* L, const pg_options& o, int mode, int fallbac
         LCK(cudaGraphAddNode(&loop, g, &init_node, 1, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         LCK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-        const bool q4 = L->op.inc_ptr && L->ov.npe == 4;
+        const bool q4 = S->npe == 4;
         fp_update_kernel<<<G, 256, 0, cs>>>(a);
         if (q4) {
             fp_true_res_kernel<4><<<G, 256, 0, cs>>>(a);
@@ -1159,7 +1202,7 @@ void build_solve_graph(pg_learned* L, const pg_options& o, int mode, int fallbac
             fp_prep_kernel<3><<<G, 256, 0, cs>>>(a);
         }
         if (mode == 1) {
-            net_forward(n, w, cs, &L->st.p->skip_net);
+            net_forward(n, w, cs, &S->st.p->skip_net);
             if (q4)
                 fp_net_kernel<4><<<G, 256, 0, cs>>>(a);
             else
@@ -1176,17 +1219,72 @@ void build_solve_graph(pg_learned* L, const pg_options& o, int mode, int fallbac
         cudaError_t ee = cudaStreamEndCapture(cs, &got);
         LCK(ce);
         LCK(ee);
-        LCK(cudaGraphInstantiate(&L->solve_exec, g, 0));
+        LCK(cudaGraphInstantiate(&S->exec, g, 0));
     } catch (...) {
         cudaGraphDestroy(g);
         throw;
     }
     cudaGraphDestroy(g);
-    L->solve_mode = mode;
-    L->solve_version = n->version;
-    L->solve_maxit = o.max_iterations;
-    L->solve_rule = o.stop_rule;
-    L->solve_tol = o.tolerance;
+    S->mode = mode;
+    S->version = n ? n->version : 0;
+    S->maxit = o.max_iterations;
+    S->rule = o.stop_rule;
+    S->tol = o.tolerance;
+}
+
+// One solve with S (graph rebuilt when the options, the mode or the
+// network's scales changed).  F and x on the host or the device.
+void fpcg_run(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const int* node_pixel, int HW,
+              const float* F, bool host_F, double* x_out, bool host_x, pg_info* info, pg_learned_stats* ls) {
+    if (!(o.tolerance >= 0) || o.max_iterations < 0) throw LFail{PG_EINVAL, "bad tolerance / max_iterations"};
+    if (!F || !x_out) throw LFail{PG_EINVAL, "F / x is NULL"};
+    cudaStream_t st = pgi::ctx_stream(S->ctx);
+    const size_t n3 = 3 * (size_t)S->op.Nn;
+    auto t0 = std::chrono::steady_clock::now();
+    if (!S->exec || S->mode != mode || S->maxit != o.max_iterations || S->rule != o.stop_rule ||
+        S->tol != o.tolerance || S->version != (n ? n->version : 0))
+        fpcg_build(S, o, mode, n, node_pixel, HW, 3, 50);
+    if (host_F) {
+        for (size_t i = 0; i < n3; i++)
+            if (!std::isfinite(F[i])) throw LFail{PG_ENONFINITE, "F contains NaN or Inf"};
+    }
+    LCK(cudaMemcpyAsync(S->F.p, F, n3 * sizeof(float), host_F ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                        st));
+    cudaEvent_t e0, e1;
+    LCK(cudaEventCreate(&e0));
+    LCK(cudaEventCreate(&e1));
+    LCK(cudaEventRecord(e0, st));
+    LCK(cudaGraphLaunch(S->exec, st));
+    LCK(cudaEventRecord(e1, st));
+    LCK(cudaMemcpyAsync(x_out, S->x.p, n3 * sizeof(double),
+                        host_x ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st));
+    FState s{};
+    LCK(cudaMemcpyAsync(&s, S->st.p, sizeof s, cudaMemcpyDeviceToHost, st));
+    LCK(cudaStreamSynchronize(st));
+    float ms = 0;
+    LCK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s.error) throw LFail{PG_ENONFINITE, "non-finite value in the flexible PCG iteration"};
+    if (info) {
+        info->iterations = s.iterations;
+        info->converged = s.converged;
+        info->stop_reason = s.stop_reason;
+        info->b_norm = std::sqrt(s.bnorm2);
+        info->final_residual = std::sqrt(s.true_rr);
+        info->true_rel_residual = s.bnorm2 > 0 ? std::sqrt(s.true_rr / s.bnorm2) : 0.0;
+        info->solve_ms = ms;
+        info->reliable_updates = s.replacements;
+        info->reductions = s.iterations;
+        info->plan_cached = 1;
+        info->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    if (ls) {
+        ls->network_iterations = s.net_iters;
+        ls->network_off_at = s.net_off ? s.net_off_at : -1;
+        ls->replacements = s.replacements;
+        ls->mode = mode;
+    }
 }
 
 }  // namespace
@@ -1371,17 +1469,13 @@ int pg_learned_create(pg_plan* plan, pg_net* net, const int32_t* node_pixel, pg_
         cudaStream_t st = pgi::ctx_stream(c);
         L->node_pixel.alloc(Nn);
         LCK(cudaMemcpyAsync(L->node_pixel.p, node_pixel, Nn * sizeof(int), cudaMemcpyHostToDevice, st));
-        const size_t n3 = 3 * (size_t)Nn;
-        for (Buf<float>* b : {&L->F, &L->r, &L->r_prev, &L->r1, &L->y, &L->r2, &L->z, &L->p0, &L->p1, &L->q}) {
-            b->alloc(n3);
-            b->zero(st);
-        }
-        L->x.alloc(n3);
-        L->parts.alloc(14 * (size_t)grid_nodes(Nn));
-        L->st.alloc(1);
         L->stats.alloc(6);
-        LCK(cudaStreamCreateWithFlags(&L->cap, cudaStreamNonBlocking));
-        LCK(cudaStreamSynchronize(st));
+        // damped smoothing steps: omega lambda_max(D^-1 K) <= 1.5 keeps the
+        // pre-/post-smoothing pair positive definite (plates have lambda_max
+        // just above 2)
+        const double lam = pgi::plan_lambda_max(plan);
+        L->omega = (float)std::min(1.0, 1.5 / std::max(lam, 1e-30));
+        fpcg_init(&L->S, c, L->op, L->ov.npe, L->omega);
         *out = L.release();
     });
 }
@@ -1426,10 +1520,10 @@ void load_pairs(pg_learned* L, int count, const float* R, const float* E, bool s
     if (set_scales) {
         L->stats.zero(st);
         if (L->ov.npe == 4)
-            prep_pairs_kernel<4><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 0, 1, 1, 1,
+            prep_pairs_kernel<4><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 0, L->omega, 1, 1, 1,
                                                         L->stats.p, nullptr, nullptr, nullptr);
         else
-            prep_pairs_kernel<3><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 0, 1, 1, 1,
+            prep_pairs_kernel<3><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 0, L->omega, 1, 1, 1,
                                                         L->stats.p, nullptr, nullptr, nullptr);
         LCK(cudaGetLastError());
         double s[6];
@@ -1450,10 +1544,10 @@ void load_pairs(pg_learned* L, int count, const float* R, const float* E, bool s
     L->den.alloc(count);
     L->den.zero(st);
     if (L->ov.npe == 4)
-        prep_pairs_kernel<4><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 1, n->scale[0],
+        prep_pairs_kernel<4><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 1, L->omega, n->scale[0],
                                                     n->scale[1], n->scale[2], nullptr, L->img.p, L->E1.p, L->den.p);
     else
-        prep_pairs_kernel<3><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 1, n->scale[0],
+        prep_pairs_kernel<3><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 1, L->omega, n->scale[0],
                                                     n->scale[1], n->scale[2], nullptr, L->img.p, L->E1.p, L->den.p);
     LCK(cudaGetLastError());
     LCK(cudaStreamSynchronize(st));
@@ -1505,7 +1599,7 @@ double eval_loss(pg_learned* L, int first, int count, int batch, double* per) {
 void build_train_graph(pg_learned* L, int B, int total_steps, float lr, bool cosine) {
     pg_net* n = L->net;
     Workspace* w = workspace(n, B, true);
-    cudaStream_t cs = L->cap;
+    cudaStream_t cs = L->S.cap;
     if (L->train_exec) {
         cudaGraphExecDestroy(L->train_exec);
         L->train_exec = nullptr;
@@ -1684,56 +1778,8 @@ void learned_solve(pg_learned* L, const pg_options* opt, int mode, const float* 
         if (opt->struct_size != sizeof(pg_options)) throw LFail{PG_EINVAL, "pg_options size mismatch"};
         o = *opt;
     }
-    if (!(o.tolerance >= 0) || o.max_iterations < 0) throw LFail{PG_EINVAL, "bad tolerance / max_iterations"};
     if (mode < 0 || mode > 2) throw LFail{PG_EINVAL, "mode must be 0, 1 or 2"};
-    if (!F || !x_out) throw LFail{PG_EINVAL, "F / x is NULL"};
-    cudaStream_t st = pgi::ctx_stream(L->ctx);
-    const size_t n3 = 3 * (size_t)L->op.Nn;
-    auto t0 = std::chrono::steady_clock::now();
-    if (!L->solve_exec || L->solve_mode != mode || L->solve_maxit != o.max_iterations ||
-        L->solve_rule != o.stop_rule || L->solve_tol != o.tolerance || L->solve_version != L->net->version)
-        build_solve_graph(L, o, mode, 3, 50);
-    if (host) {
-        for (size_t i = 0; i < n3; i++)
-            if (!std::isfinite(F[i])) throw LFail{PG_ENONFINITE, "F contains NaN or Inf"};
-    }
-    LCK(cudaMemcpyAsync(L->F.p, F, n3 * sizeof(float), host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
-                        st));
-    cudaEvent_t e0, e1;
-    LCK(cudaEventCreate(&e0));
-    LCK(cudaEventCreate(&e1));
-    LCK(cudaEventRecord(e0, st));
-    LCK(cudaGraphLaunch(L->solve_exec, st));
-    LCK(cudaEventRecord(e1, st));
-    LCK(cudaMemcpyAsync(x_out, L->x.p, n3 * sizeof(double), host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
-                        st));
-    FState s{};
-    LCK(cudaMemcpyAsync(&s, L->st.p, sizeof s, cudaMemcpyDeviceToHost, st));
-    LCK(cudaStreamSynchronize(st));
-    float ms = 0;
-    LCK(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (s.error) throw LFail{PG_ENONFINITE, "non-finite value in the flexible PCG iteration"};
-    if (info) {
-        info->iterations = s.iterations;
-        info->converged = s.converged;
-        info->stop_reason = s.stop_reason;
-        info->b_norm = std::sqrt(s.bnorm2);
-        info->final_residual = std::sqrt(s.true_rr);
-        info->true_rel_residual = s.bnorm2 > 0 ? std::sqrt(s.true_rr / s.bnorm2) : 0.0;
-        info->solve_ms = ms;
-        info->reliable_updates = s.replacements;
-        info->reductions = s.iterations;
-        info->plan_cached = 1;
-        info->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    }
-    if (ls) {
-        ls->network_iterations = s.net_iters;
-        ls->network_off_at = s.net_off ? s.net_off_at : -1;
-        ls->replacements = s.replacements;
-        ls->mode = mode;
-    }
+    fpcg_run(&L->S, o, mode, L->net, L->node_pixel.p, L->HW, F, host, x_out, host, info, ls);
 }
 
 }  // namespace
@@ -1757,3 +1803,41 @@ int pg_learned_solve(pg_learned* L, const pg_options* opt, int mode, const float
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// global-memory path of plategpu.cu (plates past shared-memory capacity)
+// ---------------------------------------------------------------------------
+
+struct pgi::GlobalPcg {
+    FpcgSolver S;
+};
+
+namespace pgi {
+
+GlobalPcg* global_pcg_create(pg_ctx* c, const OperatorView& ov, double lambda_max, std::string* err) {
+    try {
+        auto g = std::make_unique<GlobalPcg>();
+        const float omega = (float)std::min(1.0, 1.5 / std::max(lambda_max, 1e-30));
+        fpcg_init(&g->S, c, make_op(ov), ov.npe, omega);
+        return g.release();
+    } catch (const LFail& f) {
+        *err = f.msg;
+        return nullptr;
+    }
+}
+
+void global_pcg_destroy(GlobalPcg* g) { delete g; }
+
+int global_pcg_solve(GlobalPcg* g, const pg_options& o, int mode, const float* F_dev, void* x_dst, bool x_host,
+                     pg_info* info, std::string* err) {
+    try {
+        fpcg_run(&g->S, o, mode, nullptr, nullptr, 0, F_dev, false, static_cast<double*>(x_dst), x_host, info,
+                 nullptr);
+        return PG_OK;
+    } catch (const LFail& f) {
+        *err = f.msg;
+        return f.status;
+    }
+}
+
+}  // namespace pgi

@@ -112,6 +112,12 @@ struct Plan {
     // the FP32 residual
     DevBuf<double> xw, kx, nrm, pw;
     DevBuf<float> rf;
+    // global-memory flexible PCG of a plate too large for the persistent
+    // kernel's shared memory (created on first use)
+    pgi::GlobalPcg* gpcg = nullptr;
+    ~Plan() {
+        if (gpcg) pgi::global_pcg_destroy(gpcg);
+    }
 };
 
 }  // namespace
@@ -924,10 +930,66 @@ void fp64_correction(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* mi, void
     mi->solve_ms += mixed_ms;
 }
 
+pgi::OperatorView operator_view(Plan* pl) {
+    const pg::HostPlan& hp = pl->hp;
+    pgi::OperatorView v;
+    v.Nn = hp.Nn;
+    v.Ne = hp.Ne;
+    v.npe = hp.npe;
+    v.inc_ptr = pl->inc_ptr.p;
+    v.inc_idx = pl->inc_idx.p;
+    v.elements = pl->mesh_elements.p;
+    v.ke32 = pl->ke32.p;
+    v.ke64 = pl->ke64.p;
+    v.binv32 = pl->binv32.p;
+    v.binv64 = pl->binv64.p;
+    v.cons = pl->cons.p;
+    return v;
+}
+
+// Whether the smallest layout of the persistent kernel (element blocks and
+// coarse rows in L2) fits one block's shared memory for this plan's parts.
+bool persistent_fits(const pg_ctx* c, const Plan* pl, const pg_options& o) {
+    const pg::SmemLayout L = make_layout(pl->hp, o.precision == PG_PREC_MIXED, 0, false, false);
+    return L.total <= c->max_smem;
+}
+
+// A plate whose parts do not fit shared memory even with one part per SM:
+// flexible PCG over global memory (FP32 vectors in L2/HBM, FP64 x, dot
+// products and true-residual stop), block Jacobi, or damped block-Jacobi
+// smoothing steps when a faster preconditioner was asked for.  F is in
+// pl->F.
+void global_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_dst, cudaMemcpyKind kind) {
+    run_setup(c, pl);
+    if (!pl->gpcg) {
+        if (!(pl->lambda_max > 0)) pl->lambda_max = device_lambda_max(c, pl, 30);
+        std::string err;
+        pl->gpcg = pgi::global_pcg_create(c, operator_view(pl), pl->lambda_max, &err);
+        if (!pl->gpcg) throw Fail{PG_ECUDA, err};
+    }
+    if (!x_dst) {
+        if (pl->x.n != 3 * (size_t)pl->hp.Nn) pl->x.alloc(3 * (size_t)pl->hp.Nn);
+        x_dst = pl->x.p;
+        kind = cudaMemcpyDeviceToDevice;
+    }
+    const int mode = (o.preconditioner == PG_PRECOND_TWO_LEVEL || o.smoother == PG_SMOOTHER_CHEBYSHEV) ? 2 : 0;
+    std::string err;
+    pg_info local{};
+    pg_info* fi = info ? info : &local;
+    const int st = pgi::global_pcg_solve(pl->gpcg, o, mode, pl->F.p, x_dst, kind == cudaMemcpyDeviceToHost, fi, &err);
+    if (st != PG_OK) throw Fail{st, err};
+    fi->ctas = pl->G;
+    fi->global_path = 1;
+}
+
 void solve_with_fallback(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_dst = nullptr,
                          cudaMemcpyKind kind = cudaMemcpyDeviceToDevice) {
     pg_info local{};
     pg_info* fi = info ? info : &local;
+    if (!persistent_fits(c, pl, o)) {
+        global_solve(c, pl, o, fi, x_dst, kind);
+        return;
+    }
     run_solve(c, pl, o, fi, x_dst, kind);
     if (o.precision != PG_PREC_MIXED || !o.fallback || fi->stop_reason != PG_STOP_STAGNATED) return;
     fp64_correction(c, pl, o, fi, x_dst, kind);
@@ -1491,22 +1553,21 @@ std::string plan_operator(pg_plan* h, OperatorView* out) {
     try {
         Plan* pl = h->plan.get();
         run_setup(h->ctx, pl);
-        const pg::HostPlan& hp = pl->hp;
-        out->Nn = hp.Nn;
-        out->Ne = hp.Ne;
-        out->npe = hp.npe;
-        out->inc_ptr = pl->inc_ptr.p;
-        out->inc_idx = pl->inc_idx.p;
-        out->elements = pl->mesh_elements.p;
-        out->ke32 = pl->ke32.p;
-        out->ke64 = pl->ke64.p;
-        out->binv32 = pl->binv32.p;
-        out->binv64 = pl->binv64.p;
-        out->cons = pl->cons.p;
+        *out = operator_view(pl);
         return std::string();
     } catch (const Fail& f) {
         return f.msg;
     }
+}
+
+double plan_lambda_max(pg_plan* h) {
+    Plan* pl = h->plan.get();
+    try {
+        if (!(pl->lambda_max > 0)) pl->lambda_max = device_lambda_max(h->ctx, pl, 30);
+    } catch (const Fail&) {
+        return 2.0;
+    }
+    return pl->lambda_max;
 }
 
 }  // namespace pgi

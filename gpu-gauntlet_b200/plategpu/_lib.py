@@ -131,6 +131,7 @@ class PgInfo(C.Structure):
         ("phase_us", C.c_double * 8),
         ("trace_ns", C.c_double * 6),
         ("smoother_lambda_max", C.c_double),
+        ("global_path", C.c_int32),
     ]
 
     def as_dict(self) -> dict:

@@ -1,9 +1,11 @@
 """Element colouring (host side), mirroring src/lib/plate/coloring.ts.
 
 Two elements conflict when they share a node; elements of one colour can be
-applied in parallel with no scatter conflict.  The CUDA solver consumes the
-caller's colouring to order the element work inside each thread block
-(colour by colour, so the scatter into shared memory needs no atomics).
+applied in parallel with no scatter conflict.  The CUDA solver validates the
+caller's colouring (recolouring greedily when two node-sharing elements
+share a colour) and uses it in the colour-ordered K.x of pg_apply_k; the
+persistent PCG kernel does not need it, because every (element, node)
+task writes its own slot and each node sums its slots in a fixed order.
 """
 from __future__ import annotations
 

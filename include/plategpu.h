@@ -179,6 +179,12 @@ typedef struct pg_info {
                                      to the first block holding every partial; spread
                                      of exchange completion; whole iteration */
     double smoother_lambda_max;   /* Chebyshev smoother: the lambda_max(D^-1 K) estimate used */
+    int32_t global_path;          /* 1 when the plate's parts did not fit one block's shared
+                                     memory and the solve ran as flexible PCG over global
+                                     memory: FP32 vectors, FP64 x, dot products and true-
+                                     residual stop; block Jacobi, or damped block-Jacobi
+                                     smoothing steps when the two-level preconditioner or
+                                     the Chebyshev smoother was asked for */
 } pg_info;
 
 typedef struct pg_ctx pg_ctx;
