@@ -286,12 +286,13 @@ static double dot4(const double* a, const double* b, int k0, int k1) {
     return (s0 + s1) + (s2 + s3);
 }
 
-std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, HostPlan& plan) {
-    const int G = plan.G, Nn = plan.Nn, npe = plan.npe, nd = 3 * npe;
+std::string build_coarse_meta(const pg_problem& p, HostPlan& plan) {
+    const int G = plan.G, Nn = plan.Nn;
     const int C = 3 * G;
     plan.C = C;
-    std::vector<int> owner(Nn, 0);
-    std::vector<double> cx(G, 0.0), cy(G, 0.0), ih(G, 1.0);
+    plan.coarse_owner.assign(Nn, 0);
+    plan.coarse_geom.assign(3 * (size_t)G, 0.0);
+    std::vector<int>& owner = plan.coarse_owner;
     for (int g = 0; g < G; g++) {
         const int n0 = plan.node_off[g], no = plan.nown[g];
         double sx = 0, sy = 0, lo[2] = {INFINITY, INFINITY}, hi[2] = {-INFINITY, -INFINITY};
@@ -304,18 +305,72 @@ std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, H
             lo[0] = std::min(lo[0], x); hi[0] = std::max(hi[0], x);
             lo[1] = std::min(lo[1], y); hi[1] = std::max(hi[1], y);
         }
+        double cx = 0, cy = 0, ih = 1.0;
         if (no > 0) {
-            cx[g] = sx / no;
-            cy[g] = sy / no;
+            cx = sx / no;
+            cy = sy / no;
             const double h = std::max(hi[0] - lo[0], hi[1] - lo[1]);
-            ih[g] = h > 0 ? 1.0 / h : 1.0;
+            ih = h > 0 ? 1.0 / h : 1.0;
         }
+        plan.coarse_geom[3 * g] = cx;
+        plan.coarse_geom[3 * g + 1] = cy;
+        plan.coarse_geom[3 * g + 2] = ih;
     }
+    // per part: aggregates of its local nodes, node slots and basis data
+    plan.node_basis.assign(3 * plan.nodes.size(), 0.0);
+    plan.node_slot.assign(plan.nodes.size(), 0);
+    plan.cagg_off.assign(G + 1, 0);
+    plan.cagg.clear();
+    plan.ainv_off.assign(G + 1, 0);
+    plan.ainv_src.clear();
+    plan.ainv.clear();
+    plan.max_kagg = 0;
+    std::vector<int> slot_of(G, -1);
+    for (int g = 0; g < G; g++) {
+        // aggregates of the nodes where the part forms u: owned and ring 1
+        // (ring-2 nodes, rings = 2, carry only r, s and w: slot 0, unused)
+        const int n0 = plan.node_off[g], nl = plan.node_off[g + 1] - n0;
+        const int nu = plan.rings == 2 ? plan.n1[g] : nl;
+        std::vector<int> list = {g};
+        slot_of[g] = 0;
+        for (int k = 0; k < nu; k++) {
+            const int a = owner[plan.nodes[n0 + k]];
+            if (slot_of[a] < 0) { slot_of[a] = (int)list.size(); list.push_back(a); }
+        }
+        for (int k = 0; k < nl; k++) {
+            const int n = plan.nodes[n0 + k], a = owner[n];
+            const double* ge = plan.coarse_geom.data() + 3 * a;
+            plan.node_slot[n0 + k] = k < nu ? slot_of[a] : 0;
+            plan.node_basis[3 * (n0 + k)] = (p.nodes[2 * n] - ge[0]) * ge[2];
+            plan.node_basis[3 * (n0 + k) + 1] = (p.nodes[2 * n + 1] - ge[1]) * ge[2];
+            plan.node_basis[3 * (n0 + k) + 2] = ge[2];
+        }
+        plan.ainv_off[g] = (int)plan.ainv_src.size();
+        for (int a : list)
+            for (int m = 0; m < 3; m++) plan.ainv_src.push_back(3 * a + m);
+        plan.cagg.insert(plan.cagg.end(), list.begin(), list.end());
+        plan.cagg_off[g + 1] = (int)plan.cagg.size();
+        plan.max_kagg = std::max(plan.max_kagg, (int)list.size());
+        for (int a : list) slot_of[a] = -1;
+    }
+    plan.ainv_off[G] = (int)plan.ainv_src.size();
+    return "";
+}
+
+std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, HostPlan& plan) {
+    std::string e = build_coarse_meta(p, plan);
+    if (!e.empty()) return e;
+    const int Nn = plan.Nn, npe = plan.npe, nd = 3 * npe;
+    const int C = plan.C;
+    const std::vector<int>& owner = plan.coarse_owner;
+    const std::vector<double>& geom = plan.coarse_geom;
+    (void)Nn;
     // basis of node n in mode m, DOF d (masked by constraints); Phi[d][m]
     auto phi = [&](int n, double Phi[3][3]) {
         const int a = owner[n];
-        const double dx = (p.nodes[2 * n] - cx[a]) * ih[a], dy = (p.nodes[2 * n + 1] - cy[a]) * ih[a];
-        const double v[3][3] = {{1.0, dy, dx}, {0.0, ih[a], 0.0}, {0.0, 0.0, -ih[a]}};
+        const double ih = geom[3 * a + 2];
+        const double dx = (p.nodes[2 * n] - geom[3 * a]) * ih, dy = (p.nodes[2 * n + 1] - geom[3 * a + 1]) * ih;
+        const double v[3][3] = {{1.0, dy, dx}, {0.0, ih, 0.0}, {0.0, 0.0, -ih}};
         for (int d = 0; d < 3; d++)
             for (int m = 0; m < 3; m++) Phi[d][m] = p.constrained[3 * n + d] ? 0.0 : v[d][m];
     };
@@ -389,45 +444,11 @@ std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, H
             Ainv[(size_t)i * C + j] = s;
             Ainv[(size_t)j * C + i] = s;
         }
-    // per part: aggregates of its local nodes, node slots and basis data
-    plan.node_basis.assign(3 * plan.nodes.size(), 0.0);
-    plan.node_slot.assign(plan.nodes.size(), 0);
-    plan.cagg_off.assign(G + 1, 0);
-    plan.cagg.clear();
-    plan.ainv_off.assign(G + 1, 0);
-    plan.ainv.clear();
-    plan.ainv.reserve((size_t)G * 3 * 10 * C);  // about 9 aggregates per part; grows if needed
-    plan.max_kagg = 0;
-    std::vector<int> slot_of(G, -1);
-    for (int g = 0; g < G; g++) {
-        // aggregates of the nodes where the part forms u: owned and ring 1
-        // (ring-2 nodes, rings = 2, carry only r, s and w: slot 0, unused)
-        const int n0 = plan.node_off[g], nl = plan.node_off[g + 1] - n0;
-        const int nu = plan.rings == 2 ? plan.n1[g] : nl;
-        std::vector<int> list = {g};
-        slot_of[g] = 0;
-        for (int k = 0; k < nu; k++) {
-            const int a = owner[plan.nodes[n0 + k]];
-            if (slot_of[a] < 0) { slot_of[a] = (int)list.size(); list.push_back(a); }
-        }
-        for (int k = 0; k < nl; k++) {
-            const int n = plan.nodes[n0 + k], a = owner[n];
-            plan.node_slot[n0 + k] = k < nu ? slot_of[a] : 0;
-            plan.node_basis[3 * (n0 + k)] = (p.nodes[2 * n] - cx[a]) * ih[a];
-            plan.node_basis[3 * (n0 + k) + 1] = (p.nodes[2 * n + 1] - cy[a]) * ih[a];
-            plan.node_basis[3 * (n0 + k) + 2] = ih[a];
-        }
-        plan.ainv_off[g] = (int)(plan.ainv.size() / C);
-        for (int a : list)
-            for (int m = 0; m < 3; m++)
-                plan.ainv.insert(plan.ainv.end(), Ainv.begin() + (size_t)(3 * a + m) * C,
-                                 Ainv.begin() + (size_t)(3 * a + m + 1) * C);
-        plan.cagg.insert(plan.cagg.end(), list.begin(), list.end());
-        plan.cagg_off[g + 1] = (int)plan.cagg.size();
-        plan.max_kagg = std::max(plan.max_kagg, (int)list.size());
-        for (int a : list) slot_of[a] = -1;
-    }
-    plan.ainv_off[G] = (int)(plan.ainv.size() / C);
+    // each part's rows of A_c^-1 (3 per aggregate of its list)
+    plan.ainv.resize(plan.ainv_src.size() * (size_t)C);
+    for (size_t r = 0; r < plan.ainv_src.size(); r++)
+        std::copy(Ainv.begin() + (size_t)plan.ainv_src[r] * C, Ainv.begin() + (size_t)(plan.ainv_src[r] + 1) * C,
+                  plan.ainv.begin() + r * C);
     plan.coarse = true;
     return "";
 }

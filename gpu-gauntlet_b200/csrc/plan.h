@@ -56,7 +56,10 @@ struct HostPlan {
     std::vector<int> node_slot;      // per part-local node: index in the part's aggregate list
     std::vector<int> cagg_off, cagg; // per part: aggregates touching its local nodes (own first)
     std::vector<int> ainv_off;       // per part: first row of its A_c^-1 rows (3 per aggregate)
-    std::vector<double> ainv;        // rows of A_c^-1, [rows][C]
+    std::vector<int> ainv_src;       // [rows]: the A_c^-1 row each part row copies (3 a + m)
+    std::vector<double> ainv;        // rows of A_c^-1, [rows][C] (host set-up only)
+    std::vector<int> coarse_owner;   // [Nn] aggregate (part) owning each node
+    std::vector<double> coarse_geom; // [G][3] aggregate centre x, y and 1/size
     int dropped_modes = 0;           // coarse modes dropped as numerically dependent
 };
 
@@ -74,6 +77,11 @@ std::string build_partition(const pg_problem& p, int G, int rings, HostPlan& pla
 // ke64 ([Ne][(3 npe)^2], FP64): per-node basis data, per-part aggregate
 // lists, and the rows of A_c^-1 = (P^T A P)^-1 each part needs.
 std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, HostPlan& plan);
+// The part of build_coarse that needs no element matrices: aggregate owners
+// and geometry, per-node basis data, per-part aggregate lists and the
+// source row of each part row of A_c^-1 (ainv_src); plan.ainv stays empty
+// and plan.coarse false (the dense steps then run on the device).
+std::string build_coarse_meta(const pg_problem& p, HostPlan& plan);
 
 // Team schedule of a batch of independent plates.  A plate of n nodes gets
 // a team of d blocks: a power of two, or every block of the device for the

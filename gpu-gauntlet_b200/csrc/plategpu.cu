@@ -16,6 +16,7 @@
 #include <thread>
 #include <vector>
 
+#include "coarse.cuh"
 #include "internal.h"
 #include "kernels.cuh"
 #include "multi.cuh"
@@ -520,38 +521,80 @@ void fill_options(const pg_options* in, pg_options* o) {
 // polynomial smoother, else 1.
 int halo_rings(const pg_options& o) { return o.smoother == PG_SMOOTHER_CHEBYSHEV ? 2 : 1; }
 
-// Coarse data of the two-level preconditioner, built once per plan: the
-// element matrices come from the device, A_c = P^T K P and its inverse are
-// formed on the host, and each part's A_c^-1 rows go back to the device.
+// Coarse data of the two-level preconditioner, built once per plan.  One
+// plate: the aggregate lists and basis data on the host (build_coarse_meta),
+// A_c = P^T K P, its factorisation and inverse, and each part's A_c^-1 rows
+// on the device (coarse.cuh), from the element matrices already there.
+// Batches build the dense part on host threads (prepare_many, build_coarse).
 void upload_coarse(pg_ctx* c, Plan* pl);
+void upload_coarse_meta(pg_ctx* c, Plan* pl);
 
 void ensure_coarse(pg_ctx* c, Plan* pl) {
     pg::HostPlan& hp = pl->hp;
     if (hp.coarse) return;
     run_setup(c, pl);
-    const size_t kk = 9 * (size_t)hp.npe * hp.npe;
-    std::vector<double> ke(std::max<size_t>(1, (size_t)hp.Ne * kk));
-    if (hp.Ne > 0)
-        CK(cudaMemcpyAsync(ke.data(), pl->ke64.p, (size_t)hp.Ne * kk * sizeof(double),
-                           cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    std::string e = pg::build_coarse(pl->prob_view, ke, hp);
+    std::string e = pg::build_coarse_meta(pl->prob_view, hp);
     if (!e.empty()) throw Fail{PG_EINVAL, e};
-    upload_coarse(c, pl);
+    cudaStream_t st = c->stream;
+    const int C = hp.C;
+    const size_t CC = (size_t)C * C;
+    DevBuf<int> owner, src, keep, dropped;
+    DevBuf<double> geom, Ac, L, Lt, Ainv;
+    owner.upload(hp.coarse_owner.data(), hp.coarse_owner.size(), st);
+    geom.upload(hp.coarse_geom.data(), hp.coarse_geom.size(), st);
+    src.upload(hp.ainv_src.data(), hp.ainv_src.size(), st);
+    for (DevBuf<double>* b : {&Ac, &L, &Lt, &Ainv}) {
+        b->alloc(CC);
+        CK(cudaMemsetAsync(b->p, 0, CC * sizeof(double), st));
+    }
+    keep.alloc(C);
+    dropped.alloc(1);
+    if (hp.Ne > 0) {
+        if (hp.npe == 4)
+            pg::coarse_assemble_kernel<4><<<(hp.Ne + 127) / 128, 128, 0, st>>>(
+                hp.Ne, C, pl->mesh_nodes.p, pl->mesh_elements.p, pl->cons.p, owner.p, geom.p, pl->ke64.p, Ac.p);
+        else
+            pg::coarse_assemble_kernel<3><<<(hp.Ne + 127) / 128, 128, 0, st>>>(
+                hp.Ne, C, pl->mesh_nodes.p, pl->mesh_elements.p, pl->cons.p, owner.p, geom.p, pl->ke64.p, Ac.p);
+        CK(cudaGetLastError());
+    }
+    pg::coarse_factor_kernel<<<1, pg::kCoarseThreads, 0, st>>>(C, Ac.p, L.p, Lt.p, Ainv.p, keep.p, dropped.p);
+    CK(cudaGetLastError());
+    const int rows = (int)hp.ainv_src.size();
+    pl->ainv64.alloc((size_t)rows * C);
+    pl->ainv32.alloc((size_t)rows * C);
+    if (rows > 0) {
+        const long tot = (long)rows * C;
+        pg::coarse_rows_kernel<<<(int)std::min<long>((tot + 255) / 256, 4096), 256, 0, st>>>(
+            rows, C, src.p, Ainv.p, pl->ainv64.p, pl->ainv32.p);
+        CK(cudaGetLastError());
+    }
+    int nd = 0;
+    CK(cudaMemcpyAsync(&nd, dropped.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    upload_coarse_meta(c, pl);  // synchronises the stream
+    hp.dropped_modes = nd;
+    hp.coarse = true;
 }
 
-// Device copies of a plan's coarse data (after build_coarse).
-void upload_coarse(pg_ctx* c, Plan* pl) {
+// Device copies of a plan's aggregate lists and node basis data.
+void upload_coarse_meta(pg_ctx* c, Plan* pl) {
     const pg::HostPlan& hp = pl->hp;
     cudaStream_t st = c->stream;
     pl->cagg_off.upload(hp.cagg_off.data(), hp.cagg_off.size(), st);
     pl->node_slot.upload(hp.node_slot.data(), hp.node_slot.size(), st);
     pl->node_basis.upload(hp.node_basis.data(), hp.node_basis.size(), st);
     pl->ainv_off.upload(hp.ainv_off.data(), hp.ainv_off.size(), st);
+    CK(cudaStreamSynchronize(st));
+}
+
+// Device copies of a plan's coarse data built on the host (build_coarse).
+void upload_coarse(pg_ctx* c, Plan* pl) {
+    const pg::HostPlan& hp = pl->hp;
+    cudaStream_t st = c->stream;
     pl->ainv64.upload(hp.ainv.data(), hp.ainv.size(), st);
     std::vector<float> a32(hp.ainv.begin(), hp.ainv.end());
     pl->ainv32.upload(a32.data(), a32.size(), st);
-    CK(cudaStreamSynchronize(st));
+    upload_coarse_meta(c, pl);
 }
 
 // Largest eigenvalue of D^-1 K for the polynomial smoother, estimated once
