@@ -1009,6 +1009,7 @@ def batch_bench(args, ctx, check, world=1, rank=0, local=0):
         row = {"solves_per_s": len(ALL) / (med * 1e-3), "batch_ms": med, "batch_ms_all": t,
                "plate_ms_p50": bi.plate_ms_p50, "plate_ms_p99": bi.plate_ms_p99,
                "plate_ms_max": bi.plate_ms_max, "phases": bi.phases, "teams": bi.teams,
+               "cuda_graph": int(bi.graph),
                "fallbacks_rank0": bi.fallbacks, "converged_rank0": bi.converged,
                "iterations_median": float(np.median(its)), "iterations_max": int(max(its))}
         if check:

@@ -149,6 +149,14 @@ struct pg_batch {
     std::vector<std::vector<float>> hF;   // each plate's current load (for the FP64 fallback)
     std::unique_ptr<pg_batch> fb;         // FP64 batch of the plates whose mixed solve stagnated
     std::vector<int> fb_ids;              // its plates
+    // the phase launches captured as one CUDA graph (per precision and
+    // shared-memory size); graph_failed: capture not possible, launch directly
+    cudaGraphExec_t graph = nullptr;
+    int graph_precision = 0, graph_smem = 0;
+    bool graph_failed = false;
+    ~pg_batch() {
+        if (graph) cudaGraphExecDestroy(graph);
+    }
 };
 
 struct pg_ctx {
@@ -1421,13 +1429,46 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
         b->ok_precision = mixed ? 1 : 2;  // residency checked for this precision and size
         b->ok_smem = smem;
     }
-    for (auto& ph : b->phases) {  // one persistent launch per phase, back to back
-        const void* fn = kernel_of(ph->kind);
-        pg::BatchArgs ba{b->args.p, ph->block_team.p, ph->team_base.p, ph->queue_off.p, ph->queue.p,
-                         b->times.p};
-        void* args[] = {&ba};
-        CK(cudaLaunchCooperativeKernel(fn, dim3(ph->grid), dim3(pg::kMaxThreads), args, smem, st));
+    // one persistent launch per phase, back to back, captured once per batch
+    // (and precision / shared-memory size) into a CUDA graph
+    auto launch_phases = [&](cudaStream_t s) -> cudaError_t {
+        for (auto& ph : b->phases) {
+            const void* fn = kernel_of(ph->kind);
+            pg::BatchArgs ba{b->args.p, ph->block_team.p, ph->team_base.p, ph->queue_off.p, ph->queue.p,
+                             b->times.p};
+            void* args[] = {&ba};
+            cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(ph->grid), dim3(pg::kMaxThreads), args, smem, s);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+    const int prec_key = mixed ? 1 : 2;
+    if (!b->graph_failed && (!b->graph || b->graph_precision != prec_key || b->graph_smem != smem)) {
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            const cudaError_t el = launch_phases(st);
+            e = cudaStreamEndCapture(st, &g);
+            if (el != cudaSuccess) e = el;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            b->graph = nullptr;
+            b->graph_failed = true;
+        }
+        b->graph_precision = prec_key;
+        b->graph_smem = smem;
     }
+    if (b->graph)
+        CK(cudaGraphLaunch(b->graph, st));
+    else
+        CK(launch_phases(st));
     CK(cudaEventRecord(c->ev[2], st));
     if (x_out)
         for (int i = 0; i < count; i++)
@@ -1472,6 +1513,7 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
         bi->plate_ms_max = percentile(plate_ms, 1.0);
         bi->solves_per_s = ms_solve > 0 ? count / (ms_solve * 1e-3) : 0.0;
         bi->shared_bytes = smem;
+        bi->graph = b->graph != nullptr;
     }
     for (int i = 0; i < count; i++) throw_on_failure(r[i]);
     // plates whose mixed solve stagnated: an FP64 correction K d = F - K x_m

@@ -100,6 +100,7 @@ class PgBatchInfo(C.Structure):
         ("plate_ms_p99", C.c_double),
         ("plate_ms_max", C.c_double),
         ("solves_per_s", C.c_double),
+        ("graph", C.c_int32),
     ]
 
     def as_dict(self) -> dict:

@@ -285,6 +285,7 @@ typedef struct pg_batch_info {
     double plate_ms_p99;          /*   99th percentile */
     double plate_ms_max;          /*   and largest */
     double solves_per_s;          /* count / solve_ms */
+    int32_t graph;                /* 1 when the phase launches ran as one captured CUDA graph */
 } pg_batch_info;
 
 typedef struct pg_batch pg_batch;

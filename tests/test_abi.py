@@ -184,3 +184,26 @@ def test_train_options_defaults():
     _lib.load().pg_train_options_default(C.byref(o))
     assert o.struct_size == C.sizeof(_lib.PgTrainOptions)
     assert o.epochs == 20 and o.batch == 32 and abs(o.lr - 1e-3) < 1e-9 and o.cosine == 1
+
+
+def test_batch_info_layout_matches_header():
+    prog = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "plategpu.h"
+int main(void) {
+  printf("%zu %zu %zu %zu\n", sizeof(pg_batch_info), offsetof(pg_batch_info, graph), sizeof(pg_info),
+         offsetof(pg_info, global_path));
+  return 0;
+}
+"""
+    import ctypes as C
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(c, "w").write(prog)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        vals = [int(v) for v in subprocess.run([exe], capture_output=True, text=True,
+                                               check=True).stdout.split()]
+    assert vals == [C.sizeof(_lib.PgBatchInfo), _lib.PgBatchInfo.graph.offset, C.sizeof(_lib.PgInfo),
+                    _lib.PgInfo.global_path.offset]

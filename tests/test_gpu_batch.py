@@ -43,6 +43,7 @@ def test_batch_matches_truth_and_single_solves(gpu_ctx, oracle, small_batch, kw)
     xs, infos, bi = gpu_ctx.solve_batch(probs, opts)
     assert bi.count == len(small_batch) and bi.converged == len(small_batch)
     assert bi.fallbacks >= 0 and bi.phases >= 1
+    assert bi.graph == 1  # the phase launches ran as one captured CUDA graph
     assert 0 < bi.grid <= 148 and bi.solve_ms > 0 and bi.plate_ms_p50 > 0
     assert bi.plate_ms_p50 <= bi.plate_ms_p99 <= bi.plate_ms_max <= bi.solve_ms * 1.01
     for wl, pr, x, info in zip(small_batch, probs, xs, infos):
