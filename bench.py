@@ -930,16 +930,17 @@ def cases_bench(args, ctx, wl, prob, H, method, check, world=1, local=0):
 BATCH_METHODS = ("mixed_two_level", "fp64_two_level", "fp64_two_level_cheb", "fp64_block_jacobi")
 
 
-def batch_options(name):
+def batch_options(name, part_nodes=0):
     """Options of one batch method: the stop is ||r||/||b|| < 2e-7 for all
-    (the DKT plates need a tighter residual than the Q4 ones for 1e-6 error)."""
+    (the DKT plates need a tighter residual than the Q4 ones for 1e-6 error);
+    part_nodes: the team-size target (0 = the library's default)."""
     from plategpu import _lib
 
     prec = _lib.PG_PREC_MIXED if name.startswith("mixed") else _lib.PG_PREC_FP64
     pre = _lib.PG_PRECOND_BLOCK_JACOBI if name.endswith("block_jacobi") else _lib.PG_PRECOND_TWO_LEVEL
     smo = _lib.PG_SMOOTHER_CHEBYSHEV if name.endswith("cheb") else _lib.PG_SMOOTHER_BLOCK_JACOBI
     return _lib.make_options(tolerance=2e-7, max_iterations=50000, stop_rule=_lib.PG_STOP_RELATIVE,
-                             precision=prec, preconditioner=pre, smoother=smo)
+                             precision=prec, preconditioner=pre, smoother=smo, batch_part_nodes=part_nodes)
 
 
 def batch_bench(args, ctx, check, world=1, rank=0, local=0):
@@ -981,8 +982,15 @@ def batch_bench(args, ctx, check, world=1, rank=0, local=0):
                                         mat.E, mat.nu, mat.t, mat.elem_t, w.cons_mask, w.F)
     methods = BATCH_METHODS if args.batch_fp64 else BATCH_METHODS[:1]
     rows, per_plate, fallback_plates, truth_note = {}, {}, [], None
+    # the team-size target, tuned on this GPU for this batch (FP64 two-level)
+    # by plategpu.autotune and cached per GPU name and batch
+    import torch
+    from plategpu import autotune
+    part_nodes, tune = autotune.tune_batch(
+        ctx, probs, batch_options("fp64_two_level"), torch.cuda.get_device_name(local),
+        candidates=(250, 400, 640), cache_path=os.path.join(tempfile.gettempdir(), "plategpu_autotune.json"))
     for name in methods:
-        opts = batch_options(name)
+        opts = batch_options(name, part_nodes)
         steps = 1 if name == "fp64_block_jacobi" else max(1, args.batch_steps)
         ms, last, err = [], None, None
         try:  # every rank reaches the collectives below whatever happens here
@@ -1059,7 +1067,9 @@ def batch_bench(args, ctx, check, world=1, rank=0, local=0):
                         "30%% DKT, random material, supports and random-field loads" % len(ALL)),
            "dof_total": int(sum(3 * w.mesh.nodeCount for w in ALL)),
            "ranks": world, "plates_per_rank": [len(sh) for sh in shards],
-           "method": head, "stop": "||r||/||b|| < 2e-7"}
+           "method": head, "stop": "||r||/||b|| < 2e-7",
+           "autotune": {"batch_part_nodes": part_nodes, "times_ms": tune["times_ms"],
+                        "cached": tune["cached"]}}
     out.update(rows[head])
     out["methods"] = rows
     if check:

@@ -454,7 +454,8 @@ std::string build_coarse(const pg_problem& p, const std::vector<double>& ke64, H
 }
 
 std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>& caps,
-                           const std::vector<int>& kinds, int sms, BatchSchedule& out) {
+                           const std::vector<int>& kinds, int sms, BatchSchedule& out, int part_nodes) {
+    const double target = part_nodes > 0 ? part_nodes : 400.0;
     out = BatchSchedule{};
     const int count = (int)nodes.size();
     if (count == 0) return "empty batch";
@@ -472,7 +473,7 @@ std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>
             if ((double)sms * cap < n) return "a plate of the batch needs more blocks than the device has";
             need = sms;
         }
-        const int pref = std::max(1, (int)std::lround(std::exp2(std::round(std::log2(std::max(1.0, n / 400.0))))));
+        const int pref = std::max(1, (int)std::lround(std::exp2(std::round(std::log2(std::max(1.0, n / target))))));
         d[i] = std::max(need, std::min(top, pref));
         w[i] = std::sqrt(n) * (n + 300.0 * d[i]);
     }

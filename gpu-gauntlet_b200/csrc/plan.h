@@ -86,7 +86,7 @@ std::string build_coarse_meta(const pg_problem& p, HostPlan& plan);
 // Team schedule of a batch of independent plates.  A plate of n nodes gets
 // a team of d blocks: a power of two, or every block of the device for the
 // largest plates, with at most caps[i] nodes per block (so its parts fit in
-// shared memory) and about n / 400 nodes per block otherwise (fewer blocks
+// shared memory) and about part_nodes (default 400) nodes per block otherwise (fewer blocks
 // per plate cost less block time, since an iteration's latency hardly
 // depends on the part size).  Team sizes that fit side by side form a
 // phase, one persistent launch; inside a phase the blocks are shared out
@@ -107,6 +107,6 @@ struct BatchSchedule {
     std::vector<int> plate_phase, plate_team, plate_size;  // [count]; team index within its phase
 };
 std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>& caps,
-                           const std::vector<int>& kinds, int sms, BatchSchedule& out);
+                           const std::vector<int>& kinds, int sms, BatchSchedule& out, int part_nodes = 400);
 
 }  // namespace pg

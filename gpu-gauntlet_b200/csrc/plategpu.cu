@@ -517,6 +517,8 @@ void fill_options(const pg_options* in, pg_options* o) {
     if (o->threads < 0 || o->threads > pg::kMaxThreads || (o->threads % 32) != 0)
         throw Fail{PG_EINVAL, "threads must be a multiple of 32 in [32, 576] (0 = automatic)"};
     if (o->ctas < 0) throw Fail{PG_EINVAL, "ctas must be >= 0"};
+    if (o->batch_part_nodes < 0 || o->batch_part_nodes > 100000)
+        throw Fail{PG_EINVAL, "batch_part_nodes must be in [0, 100000]"};
     if (!(o->wait_timeout_ms >= 0) || !std::isfinite(o->wait_timeout_ms) || o->wait_timeout_ms > 600000.0)
         throw Fail{PG_EINVAL, "wait_timeout_ms must be finite and in [0, 600000]"};
     if (o->preconditioner != PG_PRECOND_BLOCK_JACOBI && o->preconditioner != PG_PRECOND_TWO_LEVEL)
@@ -1284,7 +1286,7 @@ std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int co
         caps[i] = std::max(caps[i], (nodes[i] + c->sms - 1) / c->sms);
     }
     for (int attempt = 0;; attempt++) {
-        std::string e = pg::schedule_batch(nodes, caps, kinds, c->sms, b->sched);
+        std::string e = pg::schedule_batch(nodes, caps, kinds, c->sms, b->sched, o.batch_part_nodes);
         if (!e.empty() && attempt > 0)
             throw Fail{PG_EUNSUPPORTED, "a plate of the batch does not fit in shared memory even on the whole "
                                         "device with these options"};

@@ -80,6 +80,7 @@ class PgOptions(C.Structure):
         ("trace_iteration", C.c_int32),
         ("smoother", C.c_int32),
         ("fallback", C.c_int32),
+        ("batch_part_nodes", C.c_int32),
     ]
 
 
@@ -364,7 +365,7 @@ def make_options(tolerance=1e-6, max_iterations=1000, precision=PG_PREC_FP64,
                  reliable_interval=0, reliable_delta=0.0, phase_timing=False,
                  test_stall=False, preconditioner=PG_PRECOND_BLOCK_JACOBI,
                  trace_iteration=0, smoother=PG_SMOOTHER_BLOCK_JACOBI,
-                 fallback=True) -> PgOptions:
+                 fallback=True, batch_part_nodes=0) -> PgOptions:
     o = PgOptions()
     load().pg_options_default(C.byref(o))
     o.tolerance = float(tolerance)
@@ -383,6 +384,7 @@ def make_options(tolerance=1e-6, max_iterations=1000, precision=PG_PREC_FP64,
     o.trace_iteration = int(trace_iteration)
     o.smoother = int(smoother)
     o.fallback = 1 if fallback else 0
+    o.batch_part_nodes = int(batch_part_nodes)
     return o
 
 

@@ -140,6 +140,9 @@ typedef struct pg_options {
                                      of the correction K d = F - K x_m from the stagnated x_m,
                                      stopped by the same rule on x_m + d; 0 returns the
                                      stagnated result */
+    int32_t batch_part_nodes;     /* batches: preferred nodes per block of a plate's team
+                                     (0 = automatic, 400); plategpu.autotune picks it per
+                                     GPU and batch */
 } pg_options;
 
 /* Per-solve result (GPUSolveResult plus extended statistics). */

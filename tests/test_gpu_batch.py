@@ -208,3 +208,27 @@ def test_plate_too_large_for_the_smoother_halo_runs_with_block_jacobi(gpu_ctx, s
     x1, one = gpu_ctx.solve(probs[2], _lib.make_options(ctas=148, **kw))
     assert abs(infos[2].iterations - one.iterations) <= 1
     assert rel_err(xs[2], x1) < 1e-9
+
+
+def test_autotuner_times_candidates_and_the_schedule_follows(gpu_ctx, small_batch, tmp_path):
+    """The autotuner times the batch at each part-size target on the GPU and
+    caches the fastest; a larger target gives a plate fewer blocks."""
+    import torch
+
+    from plategpu import autotune
+
+    probs = probs_of(small_batch)
+    opts = _lib.make_options(tolerance=1e-9, max_iterations=20000, stop_rule=_lib.PG_STOP_RELATIVE,
+                             precision=_lib.PG_PREC_FP64, preconditioner=_lib.PG_PRECOND_TWO_LEVEL)
+    path = str(tmp_path / "tune.json")
+    name = torch.cuda.get_device_name(0)
+    best, rec = autotune.tune_batch(gpu_ctx, probs, opts, name, candidates=(64, 400), cache_path=path)
+    assert best in (64, 400) and not rec["cached"] and all(v > 0 for v in rec["times_ms"].values())
+    assert autotune.tune_batch(gpu_ctx, probs, opts, name, candidates=(64, 400), cache_path=path)[1]["cached"]
+    few = gpu_ctx.solve_batch(probs, _lib.make_options(**{**dict(tolerance=1e-9, max_iterations=20000,
+                                                                stop_rule=_lib.PG_STOP_RELATIVE),
+                                                             "batch_part_nodes": 4000}))
+    many = gpu_ctx.solve_batch(probs, _lib.make_options(tolerance=1e-9, max_iterations=20000,
+                                                        stop_rule=_lib.PG_STOP_RELATIVE, batch_part_nodes=16))
+    assert sum(i.ctas for i in few[1]) < sum(i.ctas for i in many[1])
+    assert few[2].converged == many[2].converged == len(small_batch)
