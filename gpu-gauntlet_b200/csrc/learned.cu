@@ -7,19 +7,20 @@
 // 190-553).  This file adds, at that point of the iteration, a two-level
 // preconditioner for plates on a structured node grid:
 //
-//   t  = D^-1 r                       block-Jacobi pre-smoothing
+//   t  = S r                          damped block-Jacobi pre-smoothing,
+//                                     S = omega D^-1
 //   r1 = r - K t                      residual after smoothing
 //   y  = N(r1)                        network correction (coarse level)
-//   r2 = r1 - K y
-//   z  = t + y + D^-1 r2              block-Jacobi post-smoothing
+//   c  = y.r1 / y.K y                 energy-optimal step along y
+//   z  = t + c y + S (r1 - c K y)     post-smoothing
 //
 // N maps the residual, laid out as a 3-channel image over the node grid
 // (w, theta_x, theta_y per node), to an approximation of K^-1 r1.  It is a
 // 4-level U-Net (unet.cuh) without biases, so N(c r) = c N(r) for c > 0 and
-// its correction scales with the residual.  Whenever the correction does
-// not reduce the residual (|r2| >= |r1|) that iteration uses z = D^-1 r
-// (plain block Jacobi), and after `fallback_after` such iterations in a
-// row the rest of the solve is plain block-Jacobi PCG.  Because N is
+// its correction scales with the residual.  Whenever the correction cannot
+// reduce the energy norm of the error (y.r1 <= 0) that iteration uses
+// z = D^-1 r (plain block Jacobi), and after `fallback_after` such
+// iterations in a row the rest of the solve is plain block-Jacobi PCG.  Because N is
 // nonlinear the outer iteration is flexible PCG with the Polak-Ribiere
 // beta = z_k+1 . (r_k+1 - r_k) / (z_k . r_k) and alpha = p.r / p.Kp.
 //
@@ -210,6 +211,14 @@ pgn::ConvArgs cargs(int B, int H, int W, const bf16* in, int in_cs, const bf16* 
     return a;
 }
 
+// The encoder's second convolution of a level also writes the pooled
+// input of the next level (2 x 2 average in its epilogue).
+pgn::ConvArgs pooled(pgn::ConvArgs a, bf16* pool_out, int pool_cs) {
+    a.pool_out = pool_out;
+    a.pool_cs = pool_cs;
+    return a;
+}
+
 int ew_grid(long items) { return (int)std::min<long>((items + 255) / 256, 148L * 16); }
 
 // The workspace of batch size B, created on first use; gradient buffers
@@ -288,14 +297,11 @@ void net_forward(pg_net* n, Workspace* w, cudaStream_t st, const int* skip) {
     auto wf = [&](int k) { return n->wf.p + T.l[k].off_f; };
     using namespace pgn;
     conv(OUT_BF16_RELU, 16, 16, cargs(B, H0, W0, w->in.p, 16, wf(E0A), 16, w->e0a.p, 16, 0, 16, skip), st);
-    conv(OUT_BF16_RELU, 16, 16, cargs(B, H0, W0, w->e0a.p, 16, wf(E0B), 16, w->cat0.p, 48, 0, 16, skip), st);
-    pool2_kernel<<<ew_grid((long)B * H1 * W1 * 2), 256, 0, st>>>(B, H1, W1, w->cat0.p, 48, 16, w->p1.p, 16, skip);
+    conv(OUT_BF16_RELU, 16, 16, pooled(cargs(B, H0, W0, w->e0a.p, 16, wf(E0B), 16, w->cat0.p, 48, 0, 16, skip), w->p1.p, 16), st);
     conv(OUT_BF16_RELU, 16, 32, cargs(B, H1, W1, w->p1.p, 16, wf(E1A), 32, w->e1a.p, 32, 0, 32, skip), st);
-    conv(OUT_BF16_RELU, 32, 32, cargs(B, H1, W1, w->e1a.p, 32, wf(E1B), 32, w->cat1.p, 96, 0, 32, skip), st);
-    pool2_kernel<<<ew_grid((long)B * H2 * W2 * 4), 256, 0, st>>>(B, H2, W2, w->cat1.p, 96, 32, w->p2.p, 32, skip);
+    conv(OUT_BF16_RELU, 32, 32, pooled(cargs(B, H1, W1, w->e1a.p, 32, wf(E1B), 32, w->cat1.p, 96, 0, 32, skip), w->p2.p, 32), st);
     conv(OUT_BF16_RELU, 32, 64, cargs(B, H2, W2, w->p2.p, 32, wf(E2A), 64, w->e2a.p, 64, 0, 64, skip), st);
-    conv(OUT_BF16_RELU, 64, 64, cargs(B, H2, W2, w->e2a.p, 64, wf(E2B), 64, w->cat2.p, 192, 0, 64, skip), st);
-    pool2_kernel<<<ew_grid((long)B * H3 * W3 * 8), 256, 0, st>>>(B, H3, W3, w->cat2.p, 192, 64, w->p3.p, 64, skip);
+    conv(OUT_BF16_RELU, 64, 64, pooled(cargs(B, H2, W2, w->e2a.p, 64, wf(E2B), 64, w->cat2.p, 192, 0, 64, skip), w->p3.p, 64), st);
     conv(OUT_BF16_RELU, 64, 128, cargs(B, H3, W3, w->p3.p, 64, wf(E3A), 128, w->e3a.p, 128, 0, 128, skip), st);
     conv(OUT_BF16_RELU, 128, 128, cargs(B, H3, W3, w->e3a.p, 128, wf(E3B), 128, w->e3.p, 128, 0, 128, skip), st);
     up2_kernel<<<ew_grid((long)B * H2 * W2 * 16), 256, 0, st>>>(B, H2, W2, w->e3.p, 128, 128, w->cat2.p, 192, 64, skip);
@@ -529,13 +535,14 @@ __global__ void make_pairs_kernel(Op op, int count, const float* __restrict__ F,
 
 // Pre-smoothed pairs: t = omega D^-1 r, r1 = r - K t, e1 = e - t.  mode 0 sums
 // r1_c^2 and e1_c^2 (stats[6]); mode 1 writes the scaled r1 into the
-// compact image set img[p][pixel][4] (BF16, channels 0..2), e1 into E1, and
-// e1^T K e1 into den[p].
+// compact image set img[p][pixel][4] (BF16, channels 0..2), e1 into E1,
+// e1^T K e1 into den[p] and sum_c (e1_c / s_out_c)^2 into den2[p].
 template <int NPE>
 __global__ void prep_pairs_kernel(Op op, int count, const float* __restrict__ R, const float* __restrict__ E,
                                   const int* __restrict__ node_pixel, int HW, int mode, float omega, float s0,
-                                  float s1, float s2, double* __restrict__ stats, bf16* __restrict__ img,
-                                  float* __restrict__ E1, double* __restrict__ den) {
+                                  float s1, float s2, float so0, float so1, float so2, double* __restrict__ stats,
+                                  bf16* __restrict__ img, float* __restrict__ E1, double* __restrict__ den,
+                                  double* __restrict__ den2) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x, p = blockIdx.y;
     const bool live = n < op.Nn;
     const size_t base = (size_t)p * 3 * op.Nn;
@@ -569,6 +576,8 @@ __global__ void prep_pairs_kernel(Op op, int count, const float* __restrict__ R,
             float ke1[3];
             kv_node<NPE>(op, n, e1v, ke1);
             acc[0] = (double)e1[0] * ke1[0] + (double)e1[1] * ke1[1] + (double)e1[2] * ke1[2];
+            const float so[3] = {so0, so1, so2};
+            for (int d = 0; d < 3; d++) acc[1] += (double)(e1[d] / so[d]) * (e1[d] / so[d]);
         }
     }
     __shared__ double red[6][32];
@@ -587,9 +596,13 @@ __global__ void prep_pairs_kernel(Op op, int count, const float* __restrict__ R,
                 atomicAdd(stats + k, s);
             }
         } else {
-            double s = 0;
-            for (int i = 0; i < nw; i++) s += red[0][i];
+            double s = 0, s2 = 0;
+            for (int i = 0; i < nw; i++) {
+                s += red[0][i];
+                s2 += red[1][i];
+            }
             atomicAdd(den + p, s);
+            atomicAdd(den2 + p, s2);
         }
     }
 }
@@ -614,14 +627,19 @@ __global__ void gather_batch_kernel(int B, int HW, const bf16* __restrict__ img,
     }
 }
 
-// Energy-norm loss of a batch: d = e1 - y, y = s_out * N(r1) (0 on
-// constrained DOFs), loss += (d^T K d) / (B e1^T K e1) into *loss; with
-// gout, dL/d(out) = -2 s_out (K d) / (B e1^T K e1) into gout[b][pixel][0..2].
+// Loss of a batch, d = e1 - y with y = s_out * N(r1) (0 on constrained
+// DOFs).  kind PG_LOSS_ENERGY: the energy norm of the error after the
+// correction, loss += (d^T K d) / (B e1^T K e1), dL/d(out) = -2 s_out (K d) /
+// (B e1^T K e1); kind PG_LOSS_SCALED_L2: the error in the network's output
+// units, loss += sum (d / s_out)^2 / (B sum (e1 / s_out)^2), dL/d(out) =
+// -2 (d / s_out) / (B sum (e1 / s_out)^2).  The gradient goes to
+// gout[b][pixel][0..2] when gout is given.
 template <int NPE>
 __global__ void loss_kernel(Op op, int B, int HW, const int* __restrict__ node_pixel, const float* __restrict__ out,
                             const float* __restrict__ E1, const double* __restrict__ den,
-                            const int* __restrict__ perm, const int* __restrict__ step, float so0, float so1,
-                            float so2, double* __restrict__ loss_hist, bf16* __restrict__ gout) {
+                            const double* __restrict__ den2, int kind, const int* __restrict__ perm,
+                            const int* __restrict__ step, float so0, float so1, float so2,
+                            double* __restrict__ loss_hist, bf16* __restrict__ gout) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
     const int idx = step ? perm[(size_t)(*step - 1) * B + b] : perm[b];
     const float so[3] = {so0, so1, so2};
@@ -631,9 +649,18 @@ __global__ void loss_kernel(Op op, int B, int HW, const int* __restrict__ node_p
         const float y = op.cons[3 * m + d] ? 0.f : so[d] * ob[(size_t)node_pixel[m] * 4 + d];
         return e1[3 * m + d] - y;
     };
-    const double sc = 1.0 / ((double)B * den[idx]);
     double acc[1] = {0.0};
-    if (n < op.Nn) {
+    if (n < op.Nn && kind == PG_LOSS_SCALED_L2) {
+        const double sc = 1.0 / ((double)B * den2[idx]);
+        float q[3];
+        for (int d = 0; d < 3; d++) q[d] = op.cons[3 * n + d] ? 0.f : dv(n, d) / so[d];
+        acc[0] = ((double)q[0] * q[0] + (double)q[1] * q[1] + (double)q[2] * q[2]) * sc;
+        if (gout) {
+            bf16* g = gout + ((size_t)b * HW + node_pixel[n]) * 16;
+            for (int d = 0; d < 3; d++) g[d] = __float2bfloat16_rn((float)(-2.0 * sc * q[d]));
+        }
+    } else if (n < op.Nn) {
+        const double sc = 1.0 / ((double)B * den[idx]);
         float kd[3];
         kv_node<NPE>(op, n, dv, kd);
         acc[0] = ((double)dv(n, 0) * kd[0] + (double)dv(n, 1) * kd[1] + (double)dv(n, 2) * kd[2]) * sc;
@@ -666,6 +693,7 @@ __global__ void train_tick_kernel(cudaGraphConditionalHandle h, const int* step,
 struct FState {
     int it, done, converged, stop_reason, tr_ran, net_off, net_off_at, bad_count, use_net, skip_net;
     int iterations, net_iters, replacements, error;
+    float net_step;  // the last iteration's step c along the network's correction
     double bnorm2, rr, true_rr, alpha, beta, gamma_prev, gamma_next;
 };
 
@@ -857,7 +885,8 @@ __global__ void fp_prep_kernel(FArgs a) {
     block_partials<1>(acc, a.pA);
 }
 
-// B: y = s_out N(r1) (0 on constrained DOFs), r2 = r1 - K y.
+// B: y = s_out N(r1) (0 on constrained DOFs) and v = K y (kept in a.r2);
+// partial sums of y.r1 and y.v for the correction's step.
 template <int NPE>
 __global__ void fp_net_kernel(FArgs a) {
     FState* st = a.st;
@@ -867,34 +896,41 @@ __global__ void fp_net_kernel(FArgs a) {
     auto yv = [&](int m, int d) {
         return a.op.cons[3 * m + d] ? 0.f : so[d] * a.img_out[(size_t)a.node_pixel[m] * 4 + d];
     };
-    double acc[1] = {0.0};
+    double acc[2] = {0.0, 0.0};
     if (n < a.op.Nn) {
         float v[3];
         kv_node<NPE>(a.op, n, yv, v);
         for (int d = 0; d < 3; d++) {
             const int i = 3 * n + d;
-            const float r2 = a.r1[i] - v[d];
-            a.y[i] = yv(n, d);
-            a.r2[i] = r2;
-            acc[0] += (double)r2 * r2;
+            const float y = yv(n, d);
+            a.y[i] = y;
+            a.r2[i] = v[d];
+            acc[0] += (double)y * a.r1[i];
+            acc[1] += (double)y * v[d];
         }
     }
-    block_partials<1>(acc, a.pB);
+    block_partials<2>(acc, a.pB);
 }
 
-// C: z = t + y + omega D^-1 r2 (t = omega D^-1 r) when the network's
-// correction reduced the residual; mode 2 (the smoothing steps without the
-// network): z = t + omega D^-1 r1; otherwise (mode 0, or an iteration whose
-// correction did not help) plain block Jacobi z = D^-1 r.
+// C: with the network's correction y (mode 1), its energy-optimal step
+// c = y.r1 / y.K y (the multiple of y that most reduces the energy norm of
+// the error e1 = K^-1 r1: by (y.r1)^2 / y.K y) and
+// z = t + c y + omega D^-1 (r1 - c K y), t = omega D^-1 r; the correction is
+// used only when y.r1 > 0 and y.K y > 0 (otherwise it cannot reduce the
+// error) and the iteration falls back to plain block Jacobi z = D^-1 r.
+// Mode 2 (the smoothing steps without the network): z = t + omega D^-1 r1.
+// Mode 0: z = D^-1 r.
 __global__ void fp_prec_kernel(FArgs a) {
     FState* st = a.st;
     if (st->done) return;
     bool use = false;
+    float c = 0.f;
     if (a.mode == 1 && !st->skip_net) {
-        double s1[1], s2[1];
-        reduce_parts<1>(a.pA, a.G, s1);
-        reduce_parts<1>(a.pB, a.G, s2);
-        use = s2[0] < s1[0];
+        double s[2];
+        reduce_parts<2>(a.pB, a.G, s);
+        const double cd = s[0] / s[1];
+        use = s[0] > 0.0 && s[1] > 0.0 && isfinite(cd);
+        c = use ? (float)cd : 0.f;
     }
     const bool smooth2 = a.mode == 2;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -907,8 +943,9 @@ __global__ void fp_prec_kernel(FArgs a) {
         float z[3];
         for (int d = 0; d < 3; d++) z[d] = binv_row(B9, d, r0, r1_, r2_);
         if (use) {
-            const float q0 = a.r2[i], q1 = a.r2[i + 1], q2 = a.r2[i + 2];
-            for (int d = 0; d < 3; d++) z[d] = om * z[d] + a.y[i + d] + om * binv_row(B9, d, q0, q1, q2);
+            const float q0 = a.r1[i] - c * a.r2[i], q1 = a.r1[i + 1] - c * a.r2[i + 1],
+                        q2 = a.r1[i + 2] - c * a.r2[i + 2];
+            for (int d = 0; d < 3; d++) z[d] = om * z[d] + c * a.y[i + d] + om * binv_row(B9, d, q0, q1, q2);
         } else if (smooth2) {
             const float q0 = a.r1[i], q1 = a.r1[i + 1], q2 = a.r1[i + 2];
             for (int d = 0; d < 3; d++) z[d] = om * z[d] + om * binv_row(B9, d, q0, q1, q2);
@@ -925,6 +962,7 @@ __global__ void fp_prec_kernel(FArgs a) {
         if (a.mode == 1 && !st->skip_net) {
             st->bad_count = use ? 0 : st->bad_count + 1;
             st->net_iters += use;
+            st->net_step = c;
         }
     }
 }
@@ -1034,7 +1072,7 @@ struct pg_learned {
     int P = 0;
     Buf<bf16> img;
     Buf<float> E1;
-    Buf<double> den, stats, loss_hist;
+    Buf<double> den, den2, stats, loss_hist;
     Buf<int> perm, stop_step;
     FpcgSolver S;
     cudaGraphExec_t train_exec = nullptr;
@@ -1522,10 +1560,10 @@ void load_pairs(pg_learned* L, int count, const float* R, const float* E, bool s
         L->stats.zero(st);
         if (L->ov.npe == 4)
             prep_pairs_kernel<4><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 0, L->omega, 1, 1, 1,
-                                                        L->stats.p, nullptr, nullptr, nullptr);
+                                                        1, 1, 1, L->stats.p, nullptr, nullptr, nullptr, nullptr);
         else
             prep_pairs_kernel<3><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 0, L->omega, 1, 1, 1,
-                                                        L->stats.p, nullptr, nullptr, nullptr);
+                                                        1, 1, 1, L->stats.p, nullptr, nullptr, nullptr, nullptr);
         LCK(cudaGetLastError());
         double s[6];
         LCK(cudaMemcpyAsync(s, L->stats.p, sizeof s, cudaMemcpyDeviceToHost, st));
@@ -1544,12 +1582,16 @@ void load_pairs(pg_learned* L, int count, const float* R, const float* E, bool s
     L->E1.alloc((size_t)count * 3 * L->op.Nn);
     L->den.alloc(count);
     L->den.zero(st);
+    L->den2.alloc(count);
+    L->den2.zero(st);
     if (L->ov.npe == 4)
         prep_pairs_kernel<4><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 1, L->omega, n->scale[0],
-                                                    n->scale[1], n->scale[2], nullptr, L->img.p, L->E1.p, L->den.p);
+                                                    n->scale[1], n->scale[2], n->scale[3], n->scale[4], n->scale[5],
+                                                    nullptr, L->img.p, L->E1.p, L->den.p, L->den2.p);
     else
         prep_pairs_kernel<3><<<grid, 256, 0, st>>>(L->op, count, R, E, L->node_pixel.p, L->HW, 1, L->omega, n->scale[0],
-                                                    n->scale[1], n->scale[2], nullptr, L->img.p, L->E1.p, L->den.p);
+                                                    n->scale[1], n->scale[2], n->scale[3], n->scale[4], n->scale[5],
+                                                    nullptr, L->img.p, L->E1.p, L->den.p, L->den2.p);
     LCK(cudaGetLastError());
     LCK(cudaStreamSynchronize(st));
 }
@@ -1581,10 +1623,12 @@ double eval_loss(pg_learned* L, int first, int count, int batch, double* per) {
             const float* outb = w->out.p + (size_t)i * L->HW * 4;
             const int* idb = idx.p + i;
             if (L->ov.npe == 4)
-                loss_kernel<4><<<grid, 256, 0, st>>>(L->op, 1, L->HW, L->node_pixel.p, outb, L->E1.p, L->den.p, idb,
+                loss_kernel<4><<<grid, 256, 0, st>>>(L->op, 1, L->HW, L->node_pixel.p, outb, L->E1.p, L->den.p,
+                                                     L->den2.p, PG_LOSS_ENERGY, idb,
                                                      nullptr, n->scale[3], n->scale[4], n->scale[5], acc.p, nullptr);
             else
-                loss_kernel<3><<<grid, 256, 0, st>>>(L->op, 1, L->HW, L->node_pixel.p, outb, L->E1.p, L->den.p, idb,
+                loss_kernel<3><<<grid, 256, 0, st>>>(L->op, 1, L->HW, L->node_pixel.p, outb, L->E1.p, L->den.p,
+                                                     L->den2.p, PG_LOSS_ENERGY, idb,
                                                      nullptr, n->scale[3], n->scale[4], n->scale[5], acc.p, nullptr);
             LCK(cudaGetLastError());
             double v = 0;
@@ -1597,7 +1641,7 @@ double eval_loss(pg_learned* L, int first, int count, int batch, double* per) {
     return count > 0 ? total / count : 0.0;
 }
 
-void build_train_graph(pg_learned* L, int B, int total_steps, float lr, bool cosine) {
+void build_train_graph(pg_learned* L, int B, int total_steps, float lr, bool cosine, int loss_kind) {
     pg_net* n = L->net;
     Workspace* w = workspace(n, B, true);
     cudaStream_t cs = L->S.cap;
@@ -1627,11 +1671,11 @@ void build_train_graph(pg_learned* L, int B, int total_steps, float lr, bool cos
         dim3 grid(grid_nodes(L->op.Nn), B);
         if (L->ov.npe == 4)
             loss_kernel<4><<<grid, 256, 0, cs>>>(L->op, B, L->HW, L->node_pixel.p, w->out.p, L->E1.p, L->den.p,
-                                                 L->perm.p, n->step.p, n->scale[3], n->scale[4], n->scale[5],
+                                                 L->den2.p, loss_kind, L->perm.p, n->step.p, n->scale[3], n->scale[4], n->scale[5],
                                                  L->loss_hist.p, w->gout.p);
         else
             loss_kernel<3><<<grid, 256, 0, cs>>>(L->op, B, L->HW, L->node_pixel.p, w->out.p, L->E1.p, L->den.p,
-                                                 L->perm.p, n->step.p, n->scale[3], n->scale[4], n->scale[5],
+                                                 L->den2.p, loss_kind, L->perm.p, n->step.p, n->scale[3], n->scale[4], n->scale[5],
                                                  L->loss_hist.p, w->gout.p);
         net_backward(n, w, cs, false);
         pgn::adam_kernel<<<ew_grid(n->T.total), 256, 0, cs>>>(n->T, n->w.p, n->m.p, n->v.p, n->g.p, n->step.p, lr,
@@ -1665,6 +1709,7 @@ void pg_train_options_default(pg_train_options* o) {
     o->seed = 1;
     o->val_count = 0;
     o->set_scales = 1;
+    o->loss = PG_LOSS_ENERGY;
 }
 
 int pg_learned_train(pg_learned* L, int count, const float* R_dev, const float* E_dev,
@@ -1682,6 +1727,7 @@ int pg_learned_train(pg_learned* L, int count, const float* R_dev, const float* 
         if (o.batch < 1 || o.epochs < 0 || !(o.lr > 0) || o.val_count < 0 || o.val_count >= count)
             throw LFail{PG_EINVAL, "bad training options"};
         if (o.epochs > PG_TRAIN_MAX_EPOCHS) throw LFail{PG_EINVAL, "too many epochs"};
+        if (o.loss != PG_LOSS_ENERGY && o.loss != PG_LOSS_SCALED_L2) throw LFail{PG_EINVAL, "unknown loss"};
         pg_net* n = L->net;
         cudaStream_t st = pgi::ctx_stream(L->ctx);
         auto t0 = std::chrono::steady_clock::now();
@@ -1713,7 +1759,7 @@ int pg_learned_train(pg_learned* L, int count, const float* R_dev, const float* 
             info->batch = B;
         }
         if (total > 0) {
-            build_train_graph(L, B, total, o.lr, o.cosine != 0);
+            build_train_graph(L, B, total, o.lr, o.cosine != 0, o.loss);
             double tms = 0.0;
             cudaEvent_t e0, e1;
             LCK(cudaEventCreate(&e0));

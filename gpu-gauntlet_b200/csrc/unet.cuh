@@ -84,6 +84,8 @@ struct ConvArgs {
     const bf16* mask;  // OUT_BF16_MASKED: [B][H][W][mask_cs], channel co
     int mask_cs;
     const int* skip;   // non-NULL and *skip != 0: the launch does nothing
+    bf16* pool_out;    // OUT_BF16_RELU, non-NULL: also the 2 x 2 average of the outputs,
+    int pool_cs;       //   [B][H/2][W/2][pool_cs], channel co (H and W even)
 };
 
 constexpr int kConvThreads = 128;
@@ -187,6 +189,28 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(ConvArgs a) {
             }
         }
     }
+    if constexpr (MODE == OUT_BF16_RELU) {
+        if (a.pool_out) {
+            // 2 x 2 average pooling of the tile's stored (BF16) outputs: a thread
+            // holds rows 2w and 2w+1 of column g, and lane ^ 4 holds column g ^ 1
+            // (the tile is 8-aligned and H, W are even, so a window never
+            // straddles the image edge)
+            const int Hp = a.H >> 1, Wp = a.W >> 1;
+            const int py = (ty0 >> 1) + warp, px = (tx0 >> 1) + (g >> 1);
+            auto bfr = [](float v) { return __bfloat162float(__float2bfloat16_rn(fmaxf(v, 0.f))); };
+#pragma unroll
+            for (int nt = 0; nt < COT / 8; nt++) {
+                float s0 = bfr(acc[nt][0]) + bfr(acc[nt][2]);
+                float s1 = bfr(acc[nt][1]) + bfr(acc[nt][3]);
+                s0 += __shfl_xor_sync(0xffffffffu, s0, 4);
+                s1 += __shfl_xor_sync(0xffffffffu, s1, 4);
+                const int co = co0 + nt * 8 + 2 * q4;
+                if ((g & 1) == 0 && py < Hp && px < Wp && co < a.cout_real)
+                    *reinterpret_cast<bf162*>(a.pool_out + (((size_t)b * Hp + py) * Wp + px) * a.pool_cs + co) =
+                        __floats2bfloat162_rn(0.25f * s0, 0.25f * s1);
+            }
+        }
+    }
 }
 
 struct WgradArgs {
@@ -279,36 +303,6 @@ __global__ void __launch_bounds__((COT / 16) * (CIT / 16) * 32) wgrad_kernel(Wgr
                 atomicAdd(d, acc[tap][n][2 * h]);
                 atomicAdd(d + 1, acc[tap][n][2 * h + 1]);
             }
-}
-
-// 2 x 2 average pooling: out[b][y][x][c] = mean of in[b][2y+i][2x+j][c] for
-// c < C (C a multiple of 8).  One thread per 8 channels.
-__global__ void pool2_kernel(int B, int Ho, int Wo, const bf16* __restrict__ in, int in_cs, int C,
-                             bf16* __restrict__ out, int out_cs, const int* skip) {
-    if (skip && *skip) return;
-    const int C8 = C / 8;
-    const long total = (long)B * Ho * Wo * C8;
-    for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
-        const int c8 = (int)(q % C8);
-        const long p = q / C8;
-        const int x = (int)(p % Wo), y = (int)((p / Wo) % Ho), b = (int)(p / ((long)Wo * Ho));
-        float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int i = 0; i < 2; i++)
-            for (int k = 0; k < 2; k++) {
-                const uint4 v = *reinterpret_cast<const uint4*>(
-                    in + (((size_t)b * 2 * Ho + 2 * y + i) * 2 * Wo + 2 * x + k) * in_cs + c8 * 8);
-                const bf162* h = reinterpret_cast<const bf162*>(&v);
-                for (int e = 0; e < 4; e++) {
-                    const float2 f = __bfloat1622float2(h[e]);
-                    s[2 * e] += f.x;
-                    s[2 * e + 1] += f.y;
-                }
-            }
-        uint4 o;
-        bf162* ho = reinterpret_cast<bf162*>(&o);
-        for (int e = 0; e < 4; e++) ho[e] = __floats2bfloat162_rn(0.25f * s[2 * e], 0.25f * s[2 * e + 1]);
-        *reinterpret_cast<uint4*>(out + (((size_t)b * Ho + y) * Wo + x) * out_cs + c8 * 8) = o;
-    }
 }
 
 // Nearest 2x upsampling into a concatenation buffer:

@@ -154,6 +154,7 @@ class PgTrainOptions(C.Structure):
         ("seed", C.c_uint64),
         ("val_count", C.c_int32),
         ("set_scales", C.c_int32),
+        ("loss", C.c_int32),
     ]
 
 
@@ -629,13 +630,17 @@ class Net:
             pass
 
 
+PG_LOSS_ENERGY, PG_LOSS_SCALED_L2 = 0, 1
+
+
 def train_options(epochs=20, batch=32, lr=1e-3, cosine=True, seed=1, val_count=0,
-                  set_scales=True) -> PgTrainOptions:
+                  set_scales=True, loss=PG_LOSS_ENERGY) -> PgTrainOptions:
     o = PgTrainOptions()
     load().pg_train_options_default(C.byref(o))
     o.epochs, o.batch, o.lr = int(epochs), int(batch), float(lr)
     o.cosine, o.seed, o.val_count = int(bool(cosine)), int(seed), int(val_count)
     o.set_scales = int(bool(set_scales))
+    o.loss = int(loss)
     return o
 
 

@@ -187,10 +187,47 @@ def tight_solutions(torch, ctx, ls: LearnedSolver, loads, tol=1e-12):
     return out
 
 
-def train_plate(torch, ctx, wl, loads=8192, epochs=20, batch=32, lr=1e-3, k_max=300, val=256,
-                seed=TRAIN_SEED, log=print):
+def train_net(ls: LearnedSolver, count, R, E, epochs=20, energy_epochs=None, batch=32, lr=1e-3, val=256,
+              seed=TRAIN_SEED):
+    """Trains ls's network on `count` pairs (device tensors R, E): first
+    with the scaled-L2 loss of the error (well-conditioned gradients: the
+    network learns the smooth bulk of the error), then `energy_epochs`
+    (default a quarter of `epochs`) with the energy-norm loss of the error
+    after the correction, the quantity the preconditioner needs.  Returns
+    one info dict for the run."""
+    if energy_epochs is None:
+        energy_epochs = epochs // 4
+    stages = [(_lib.PG_LOSS_SCALED_L2, epochs - energy_epochs), (_lib.PG_LOSS_ENERGY, energy_epochs)]
+    out = {"stages": [], "epoch_loss": [], "epoch_val_loss": [], "train_ms": 0.0, "steps": 0}
+    first = True
+    for loss, ep in stages:
+        if ep <= 0:
+            continue
+        opts = _lib.train_options(epochs=ep, batch=batch, lr=lr, seed=seed, val_count=val,
+                                  set_scales=first, loss=loss)
+        info = ls.learned.train(count, R.data_ptr(), E.data_ptr(), opts)
+        if first:
+            out["val_loss_before"] = info.val_loss_before
+            out["loss_first_step"] = info.loss_first_step
+            out["batch"] = int(info.batch)
+        first = False
+        out["stages"].append({"loss": "scaled_l2" if loss == _lib.PG_LOSS_SCALED_L2 else "energy",
+                              "epochs": ep, "steps": int(info.steps), "val_loss": info.val_loss,
+                              "loss_last_step": info.loss_last_step})
+        out["epoch_loss"] += list(info.epoch_loss)[:ep]
+        out["epoch_val_loss"] += list(info.epoch_val_loss)[:ep]
+        out["train_ms"] += info.train_ms
+        out["steps"] += int(info.steps)
+        out["val_loss"] = info.val_loss
+        out["loss_last_step"] = info.loss_last_step
+    return out
+
+
+def train_plate(torch, ctx, wl, loads=8192, epochs=20, energy_epochs=None, batch=32, lr=1e-3, k_max=300,
+                val=256, seed=TRAIN_SEED, log=print):
     """The full pipeline for one plate: seeded random-field loads, plain
-    solves, pairs, training.  Returns (LearnedSolver, info dict)."""
+    solves, pairs, training (train_net).  Returns (LearnedSolver, info
+    dict); the validation losses are energy-norm losses (1 = no gain)."""
     t0 = time.time()
     ls = LearnedSolver(ctx, wl, seed=seed)
     F = workloads.random_field_loads(wl, loads, seed)
@@ -199,19 +236,15 @@ def train_plate(torch, ctx, wl, loads=8192, epochs=20, batch=32, lr=1e-3, k_max=
     torch.cuda.synchronize()
     t2 = time.time()
     log(f"pairs: {loads} loads in {t1 - t0:.1f} s (host), solved in {t2 - t1:.1f} s")
-    opts = _lib.train_options(epochs=epochs, batch=batch, lr=lr, seed=seed, val_count=val)
-    info = ls.learned.train(loads, R.data_ptr(), E.data_ptr(), opts)
+    tr = train_net(ls, loads, R, E, epochs=epochs, energy_epochs=energy_epochs, batch=batch, lr=lr, val=val,
+                   seed=seed)
     del R, E
     torch.cuda.synchronize()
-    out = {"loads": loads, "epochs": epochs, "batch": int(info.batch), "steps": int(info.steps),
-           "lr": lr, "k_max": k_max, "val_pairs": val, "seed": seed,
-           "loss_first_step": info.loss_first_step, "loss_last_step": info.loss_last_step,
-           "val_loss_before": info.val_loss_before, "val_loss": info.val_loss,
-           "train_ms": info.train_ms, "train_total_ms": info.total_ms,
-           "epoch_loss": list(info.epoch_loss)[:epochs], "epoch_val_loss": list(info.epoch_val_loss)[:epochs],
+    out = {"loads": loads, "epochs": epochs, "lr": lr, "k_max": k_max, "val_pairs": val, "seed": seed,
            "load_gen_s": t1 - t0, "pair_solve_s": t2 - t1, "params": ls.net.param_count}
-    log(f"trained {info.steps} steps in {info.train_ms / 1e3:.1f} s: val loss {info.val_loss_before:.4f} -> "
-        f"{info.val_loss:.4f}")
+    out.update(tr)
+    log(f"trained {out['steps']} steps in {out['train_ms'] / 1e3:.1f} s: validation energy loss "
+        f"{out['val_loss_before']:.4f} -> {out['val_loss']:.4f}")
     return ls, out
 
 
@@ -222,6 +255,8 @@ def main(argv=None):
     t.add_argument("--out", default=DEFAULT_WEIGHTS)
     t.add_argument("--loads", type=int, default=8192)
     t.add_argument("--epochs", type=int, default=20)
+    t.add_argument("--energy-epochs", type=int, default=None,
+                   help="final epochs with the energy-norm loss (default a quarter of --epochs)")
     t.add_argument("--batch", type=int, default=32)
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--k-max", type=int, default=300)
@@ -232,8 +267,8 @@ def main(argv=None):
 
     wl = workloads.plate_q4_141()
     ctx = _lib.Context(0)
-    ls, info = train_plate(torch, ctx, wl, loads=a.loads, epochs=a.epochs, batch=a.batch, lr=a.lr,
-                           k_max=a.k_max)
+    ls, info = train_plate(torch, ctx, wl, loads=a.loads, epochs=a.epochs, energy_epochs=a.energy_epochs,
+                           batch=a.batch, lr=a.lr, k_max=a.k_max)
     if a.eval:
         H = workloads.random_field_loads(wl, a.eval, HELD_OUT_SEED)
         xt = tight_solutions(torch, ctx, ls, H)

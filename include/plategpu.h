@@ -430,6 +430,14 @@ int pg_learned_make_pairs(pg_learned* learned, int count, const float* F_dev, co
                           const double* xk_dev, float* R_out, float* E_out);
 
 #define PG_TRAIN_MAX_EPOCHS 256
+typedef enum pg_loss {
+    PG_LOSS_ENERGY = 0,    /* energy norm of the error after the correction:
+                              (e1 - y)^T K (e1 - y) / e1^T K e1 */
+    PG_LOSS_SCALED_L2 = 1  /* the same error in the network's output units:
+                              |(e1 - y) / s_out|^2 / |e1 / s_out|^2 (its gradient is not
+                              weighted by K, whose condition number makes the energy
+                              loss's gradient descent slow on smooth errors) */
+} pg_loss;
 typedef struct pg_train_options {
     uint32_t struct_size;   /* sizeof(pg_train_options); set by pg_train_options_default */
     int32_t epochs;         /* default 20 */
@@ -439,6 +447,8 @@ typedef struct pg_train_options {
     uint64_t seed;          /* shuffles */
     int32_t val_count;      /* the last val_count pairs are held out for the validation loss */
     int32_t set_scales;     /* 1 (default): set the network's scales from the pairs */
+    int32_t loss;           /* pg_loss of the training steps, default PG_LOSS_ENERGY (the
+                               validation loss is always the energy loss) */
 } pg_train_options;
 
 typedef struct pg_train_info {
@@ -472,12 +482,14 @@ typedef struct pg_learned_stats {
 } pg_learned_stats;
 
 /* Flexible PCG (Polak-Ribiere) with the two-level preconditioner
- * z = t + y + D^-1 (r1 - K y), t = D^-1 r, r1 = r - K t, y = N(r1)
- * (mode 1); an iteration whose network correction does not reduce the
- * residual uses z = D^-1 r, and after three such iterations in a row the
- * solve continues as plain block-Jacobi PCG.  mode 0: plain block-Jacobi
- * PCG in the same loop; mode 2: the smoothing steps without the network
- * (z = t + D^-1 r1).  FP32 vectors and BF16 network, FP64 x, dot products
+ * z = t + c y + S (r1 - c K y), t = S r, r1 = r - K t, y = N(r1),
+ * S = omega D^-1 (omega = min(1, 1.5 / lambda_max(D^-1 K))) and
+ * c = y.r1 / y.K y the step along the correction that most reduces the
+ * energy norm of the error (mode 1); an iteration whose correction cannot
+ * reduce it (y.r1 <= 0) uses z = D^-1 r, and after three such iterations in
+ * a row the solve continues as plain block-Jacobi PCG.  mode 0: plain
+ * block-Jacobi PCG in the same loop; mode 2: the smoothing steps without
+ * the network (z = t + S r1).  FP32 vectors and BF16 network, FP64 x, dot products
  * and alpha/beta; the stop test (opt: tolerance, max_iterations,
  * stop_rule) is made on the FP64 true residual F - K x, which also
  * replaces the recursive residual every 50 iterations.  The whole solve is
