@@ -427,6 +427,11 @@ struct Op {
     const double* ke64;
     const float* binv32;
     const uint8_t* cons;
+    // floats between element matrices in the FP32 K products: (3 npe)^2, or 0
+    // when every element matrix equals the first to FP32 precision (a
+    // uniform structured mesh), so that one matrix serves all elements from
+    // L1; the FP64 products (true residual, pairs) always use each element's
+    int ke_stride;
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -483,7 +488,7 @@ __device__ __forceinline__ void kv_node(const Op& op, int n, GetV getv, float (&
     float s0 = 0.f, s1 = 0.f, s2 = 0.f;
     for (int q = op.inc_ptr[n]; q < op.inc_ptr[n + 1]; q++) {
         const int e = op.inc_idx[q] >> 2, k = op.inc_idx[q] & 3;
-        const float* Ke = op.ke32 + (size_t)e * ND * ND + 3 * k * ND;
+        const float* Ke = op.ke32 + (size_t)e * op.ke_stride + 3 * k * ND;
 #pragma unroll
         for (int b = 0; b < NPE; b++) {
             const int m = (int)op.el[(size_t)e * NPE + b];
@@ -1084,8 +1089,40 @@ struct pg_learned {
 
 namespace {
 
-Op make_op(const pgi::OperatorView& v) {
-    return Op{v.Nn, v.inc_ptr, v.inc_idx, v.elements, v.ke32, v.ke64, v.binv32, v.cons};
+// Largest |Ke_e - Ke_0| and |Ke_0| entries (FP32 element matrices) as
+// float bit patterns (non-negative floats order like their bits).
+__global__ void ke_spread_kernel(long total, int kk, const float* __restrict__ ke, unsigned* out) {
+    unsigned md = 0, m0 = 0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const float a = ke[i], b = ke[i % kk];
+        md = max(md, __float_as_uint(fabsf(a - b)));
+        if (i < kk) m0 = max(m0, __float_as_uint(fabsf(a)));
+    }
+    atomicMax(out, md);
+    atomicMax(out + 1, m0);
+}
+
+// The operator of a plan for the flexible-PCG kernels: one shared FP32
+// element matrix when all agree with the first within 1e-6 of its largest
+// entry (FP32's own rounding is 6e-8), else each element's own.
+Op make_op(const pgi::OperatorView& v, cudaStream_t st) {
+    Op op{v.Nn, v.inc_ptr, v.inc_idx, v.elements, v.ke32, v.ke64, v.binv32, v.cons, 9 * v.npe * v.npe};
+    if (v.Ne <= 1) return op;
+    Buf<unsigned> mx;
+    mx.alloc(2);
+    mx.zero(st);
+    const int kk = 9 * v.npe * v.npe;
+    const long total = (long)v.Ne * kk;
+    ke_spread_kernel<<<(int)std::min<long>((total + 255) / 256, 2048), 256, 0, st>>>(total, kk, v.ke32, mx.p);
+    LCK(cudaGetLastError());
+    unsigned h[2];
+    LCK(cudaMemcpyAsync(h, mx.p, sizeof h, cudaMemcpyDeviceToHost, st));
+    LCK(cudaStreamSynchronize(st));
+    float d, m;
+    std::memcpy(&d, &h[0], 4);
+    std::memcpy(&m, &h[1], 4);
+    if (m > 0 && d <= 1e-6f * m) op.ke_stride = 0;
+    return op;
 }
 
 // Real (unpadded, oracle-order) parameters <-> padded master layout.
@@ -1495,7 +1532,7 @@ int pg_learned_create(pg_plan* plan, pg_net* net, const int32_t* node_pixel, pg_
         std::string e = pgi::plan_operator(plan, &L->ov);
         if (!e.empty()) throw LFail{PG_ECUDA, e};
         if (L->ov.npe != 4 && L->ov.npe != 3) throw LFail{PG_EINVAL, "unsupported element type"};
-        L->op = make_op(L->ov);
+        L->op = make_op(L->ov, pgi::ctx_stream(c));
         L->HW = net->H * net->W;
         const int Nn = L->ov.Nn;
         std::vector<char> seen(L->HW, 0);
@@ -1865,7 +1902,7 @@ GlobalPcg* global_pcg_create(pg_ctx* c, const OperatorView& ov, double lambda_ma
     try {
         auto g = std::make_unique<GlobalPcg>();
         const float omega = (float)std::min(1.0, 1.5 / std::max(lambda_max, 1e-30));
-        fpcg_init(&g->S, c, make_op(ov), ov.npe, omega);
+        fpcg_init(&g->S, c, make_op(ov, pgi::ctx_stream(c)), ov.npe, omega);
         return g.release();
     } catch (const LFail& f) {
         *err = f.msg;
