@@ -161,23 +161,45 @@ int pick_cot(int rows) {
     return 16;
 }
 
+// Launches kernel<<<grid, block, smem, st>>>(args...), with programmatic
+// stream serialisation when pdl is set (the kernel then starts while its
+// predecessor finishes and waits in pdl_wait before reading its results).
+template <typename... K, typename... A>
+void launch(bool pdl, void (*kernel)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args) {
+    if (!pdl) {
+        kernel<<<grid, block, smem, st>>>(std::forward<A>(args)...);
+        LCK(cudaGetLastError());
+        return;
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    LCK(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
+}
+
 template <int CIN, int COT, int MODE>
-void conv_launch(const pgn::ConvArgs& a, int rows, cudaStream_t st) {
+void conv_launch(const pgn::ConvArgs& a, int rows, cudaStream_t st, bool pdl) {
     const int smem = pgn::conv_smem_bytes(CIN, COT);
     const void* fn = (const void*)pgn::conv3x3_kernel<CIN, COT, MODE>;
     LCK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     dim3 grid((a.W + 7) / 8, ((a.H + 7) / 8) * a.B, rows / COT);
-    pgn::conv3x3_kernel<CIN, COT, MODE><<<grid, pgn::kConvThreads, smem, st>>>(a);
-    LCK(cudaGetLastError());
+    launch(pdl, pgn::conv3x3_kernel<CIN, COT, MODE>, grid, dim3(pgn::kConvThreads), smem, st, a);
 }
 
 // Dispatches the (input channels, output tile, epilogue) combinations the
 // network uses.
-void conv(int mode, int cin, int rows, const pgn::ConvArgs& a, cudaStream_t st) {
+void conv(int mode, int cin, int rows, const pgn::ConvArgs& a, cudaStream_t st, bool pdl = false) {
     const int cot = pick_cot(rows);
 #define PG_CONV(C, T, M)                                   \
     if (cin == C && cot == T && mode == M) {               \
-        conv_launch<C, T, M>(a, rows, st);                 \
+        conv_launch<C, T, M>(a, rows, st, pdl);            \
         return;                                            \
     }
     using namespace pgn;
@@ -290,30 +312,30 @@ Workspace* workspace(pg_net* n, int B, bool grads) {
 }
 
 // U-Net forward of ws->in ([B][H][W][16], channels 0..2 used) into ws->out.
-void net_forward(pg_net* n, Workspace* w, cudaStream_t st, const int* skip) {
+void net_forward(pg_net* n, Workspace* w, cudaStream_t st, const int* skip, bool pdl = false) {
     const int B = w->B;
     const int H0 = n->H, W0 = n->W, H1 = H0 / 2, W1 = W0 / 2, H2 = H1 / 2, W2 = W1 / 2, H3 = H2 / 2, W3 = W2 / 2;
     const pgn::LayerTable& T = n->T;
     auto wf = [&](int k) { return n->wf.p + T.l[k].off_f; };
     using namespace pgn;
-    conv(OUT_BF16_RELU, 16, 16, cargs(B, H0, W0, w->in.p, 16, wf(E0A), 16, w->e0a.p, 16, 0, 16, skip), st);
-    conv(OUT_BF16_RELU, 16, 16, pooled(cargs(B, H0, W0, w->e0a.p, 16, wf(E0B), 16, w->cat0.p, 48, 0, 16, skip), w->p1.p, 16), st);
-    conv(OUT_BF16_RELU, 16, 32, cargs(B, H1, W1, w->p1.p, 16, wf(E1A), 32, w->e1a.p, 32, 0, 32, skip), st);
-    conv(OUT_BF16_RELU, 32, 32, pooled(cargs(B, H1, W1, w->e1a.p, 32, wf(E1B), 32, w->cat1.p, 96, 0, 32, skip), w->p2.p, 32), st);
-    conv(OUT_BF16_RELU, 32, 64, cargs(B, H2, W2, w->p2.p, 32, wf(E2A), 64, w->e2a.p, 64, 0, 64, skip), st);
-    conv(OUT_BF16_RELU, 64, 64, pooled(cargs(B, H2, W2, w->e2a.p, 64, wf(E2B), 64, w->cat2.p, 192, 0, 64, skip), w->p3.p, 64), st);
-    conv(OUT_BF16_RELU, 64, 128, cargs(B, H3, W3, w->p3.p, 64, wf(E3A), 128, w->e3a.p, 128, 0, 128, skip), st);
-    conv(OUT_BF16_RELU, 128, 128, cargs(B, H3, W3, w->e3a.p, 128, wf(E3B), 128, w->e3.p, 128, 0, 128, skip), st);
-    up2_kernel<<<ew_grid((long)B * H2 * W2 * 16), 256, 0, st>>>(B, H2, W2, w->e3.p, 128, 128, w->cat2.p, 192, 64, skip);
-    conv(OUT_BF16_RELU, 192, 64, cargs(B, H2, W2, w->cat2.p, 192, wf(D2A), 64, w->d2a.p, 64, 0, 64, skip), st);
-    conv(OUT_BF16_RELU, 64, 64, cargs(B, H2, W2, w->d2a.p, 64, wf(D2B), 64, w->d2.p, 64, 0, 64, skip), st);
-    up2_kernel<<<ew_grid((long)B * H1 * W1 * 8), 256, 0, st>>>(B, H1, W1, w->d2.p, 64, 64, w->cat1.p, 96, 32, skip);
-    conv(OUT_BF16_RELU, 96, 32, cargs(B, H1, W1, w->cat1.p, 96, wf(D1A), 32, w->d1a.p, 32, 0, 32, skip), st);
-    conv(OUT_BF16_RELU, 32, 32, cargs(B, H1, W1, w->d1a.p, 32, wf(D1B), 32, w->d1.p, 32, 0, 32, skip), st);
-    up2_kernel<<<ew_grid((long)B * H0 * W0 * 4), 256, 0, st>>>(B, H0, W0, w->d1.p, 32, 32, w->cat0.p, 48, 16, skip);
-    conv(OUT_BF16_RELU, 48, 16, cargs(B, H0, W0, w->cat0.p, 48, wf(D0A), 16, w->d0a.p, 16, 0, 16, skip), st);
-    conv(OUT_BF16_RELU, 16, 16, cargs(B, H0, W0, w->d0a.p, 16, wf(D0B), 16, w->d0.p, 16, 0, 16, skip), st);
-    conv(OUT_F32, 16, 16, cargs(B, H0, W0, w->d0.p, 16, wf(OUTL), 16, w->out.p, 4, 0, 3, skip), st);
+    conv(OUT_BF16_RELU, 16, 16, cargs(B, H0, W0, w->in.p, 16, wf(E0A), 16, w->e0a.p, 16, 0, 16, skip), st, pdl);
+    conv(OUT_BF16_RELU, 16, 16, pooled(cargs(B, H0, W0, w->e0a.p, 16, wf(E0B), 16, w->cat0.p, 48, 0, 16, skip), w->p1.p, 16), st, pdl);
+    conv(OUT_BF16_RELU, 16, 32, cargs(B, H1, W1, w->p1.p, 16, wf(E1A), 32, w->e1a.p, 32, 0, 32, skip), st, pdl);
+    conv(OUT_BF16_RELU, 32, 32, pooled(cargs(B, H1, W1, w->e1a.p, 32, wf(E1B), 32, w->cat1.p, 96, 0, 32, skip), w->p2.p, 32), st, pdl);
+    conv(OUT_BF16_RELU, 32, 64, cargs(B, H2, W2, w->p2.p, 32, wf(E2A), 64, w->e2a.p, 64, 0, 64, skip), st, pdl);
+    conv(OUT_BF16_RELU, 64, 64, pooled(cargs(B, H2, W2, w->e2a.p, 64, wf(E2B), 64, w->cat2.p, 192, 0, 64, skip), w->p3.p, 64), st, pdl);
+    conv(OUT_BF16_RELU, 64, 128, cargs(B, H3, W3, w->p3.p, 64, wf(E3A), 128, w->e3a.p, 128, 0, 128, skip), st, pdl);
+    conv(OUT_BF16_RELU, 128, 128, cargs(B, H3, W3, w->e3a.p, 128, wf(E3B), 128, w->e3.p, 128, 0, 128, skip), st, pdl);
+    launch(pdl, up2_kernel, dim3(ew_grid((long)B * H2 * W2 * 16)), dim3(256), 0, st, B, H2, W2, w->e3.p, 128, 128, w->cat2.p, 192, 64, skip);
+    conv(OUT_BF16_RELU, 192, 64, cargs(B, H2, W2, w->cat2.p, 192, wf(D2A), 64, w->d2a.p, 64, 0, 64, skip), st, pdl);
+    conv(OUT_BF16_RELU, 64, 64, cargs(B, H2, W2, w->d2a.p, 64, wf(D2B), 64, w->d2.p, 64, 0, 64, skip), st, pdl);
+    launch(pdl, up2_kernel, dim3(ew_grid((long)B * H1 * W1 * 8)), dim3(256), 0, st, B, H1, W1, w->d2.p, 64, 64, w->cat1.p, 96, 32, skip);
+    conv(OUT_BF16_RELU, 96, 32, cargs(B, H1, W1, w->cat1.p, 96, wf(D1A), 32, w->d1a.p, 32, 0, 32, skip), st, pdl);
+    conv(OUT_BF16_RELU, 32, 32, cargs(B, H1, W1, w->d1a.p, 32, wf(D1B), 32, w->d1.p, 32, 0, 32, skip), st, pdl);
+    launch(pdl, up2_kernel, dim3(ew_grid((long)B * H0 * W0 * 4)), dim3(256), 0, st, B, H0, W0, w->d1.p, 32, 32, w->cat0.p, 48, 16, skip);
+    conv(OUT_BF16_RELU, 48, 16, cargs(B, H0, W0, w->cat0.p, 48, wf(D0A), 16, w->d0a.p, 16, 0, 16, skip), st, pdl);
+    conv(OUT_BF16_RELU, 16, 16, cargs(B, H0, W0, w->d0a.p, 16, wf(D0B), 16, w->d0.p, 16, 0, 16, skip), st, pdl);
+    conv(OUT_F32, 16, 16, cargs(B, H0, W0, w->d0.p, 16, wf(OUTL), 16, w->out.p, 4, 0, 3, skip), st, pdl);
     LCK(cudaGetLastError());
 }
 
@@ -749,6 +771,7 @@ __global__ void fp_init_kernel(FArgs a) {
 // U: x += alpha p, r -= alpha q with alpha = p.r / p.Kp of the last
 // direction (0 at the first iteration).
 __global__ void fp_update_kernel(FArgs a) {
+    pgn::pdl_wait();
     FState* st = a.st;
     const int it = st->it;
     double alpha = 0.0, bn2 = 0.0;
@@ -800,6 +823,7 @@ __global__ void fp_update_kernel(FArgs a) {
 // and |F - K x|^2 for the stop test.
 template <int NPE>
 __global__ void fp_true_res_kernel(FArgs a) {
+    pgn::pdl_wait();
     constexpr int ND = 3 * NPE;
     FState* st = a.st;
     if (st->done) return;
@@ -842,6 +866,7 @@ __global__ void fp_true_res_kernel(FArgs a) {
 // and the network input image (s_in r1).
 template <int NPE>
 __global__ void fp_prep_kernel(FArgs a) {
+    pgn::pdl_wait();
     FState* st = a.st;
     if (st->done) return;
     const int it = st->it;
@@ -894,6 +919,7 @@ __global__ void fp_prep_kernel(FArgs a) {
 // partial sums of y.r1 and y.v for the correction's step.
 template <int NPE>
 __global__ void fp_net_kernel(FArgs a) {
+    pgn::pdl_wait();
     FState* st = a.st;
     if (st->done || st->skip_net) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -926,6 +952,7 @@ __global__ void fp_net_kernel(FArgs a) {
 // Mode 2 (the smoothing steps without the network): z = t + omega D^-1 r1.
 // Mode 0: z = D^-1 r.
 __global__ void fp_prec_kernel(FArgs a) {
+    pgn::pdl_wait();
     FState* st = a.st;
     if (st->done) return;
     bool use = false;
@@ -975,6 +1002,7 @@ __global__ void fp_prec_kernel(FArgs a) {
 // D: beta (Polak-Ribiere), p = z + beta p_old, q = K p.
 template <int NPE>
 __global__ void fp_dir_kernel(FArgs a) {
+    pgn::pdl_wait();
     FState* st = a.st;
     if (st->done) return;
     const int it = st->it;
@@ -1008,6 +1036,7 @@ __global__ void fp_dir_kernel(FArgs a) {
 }
 
 __global__ void fp_tick_kernel(FArgs a, cudaGraphConditionalHandle h) {
+    pgn::pdl_wait();
     FState* st = a.st;
     st->gamma_prev = st->gamma_next;
     if (a.mode == 1 && !st->net_off && st->bad_count >= a.fallback_after) {
@@ -1054,6 +1083,7 @@ struct FpcgSolver {
     Buf<FState> st;
     cudaStream_t cap = nullptr;  // capture stream
     cudaGraphExec_t exec = nullptr;
+    bool pdl = false, pdl_refused = false;  // graph built with programmatic dependent launch
     int mode = -1, maxit = -1, rule = -1, version = -1;
     double tol = -1;
     ~FpcgSolver() {
@@ -1195,7 +1225,7 @@ void fpcg_init(FpcgSolver* S, pg_ctx* c, const Op& op, int npe, float omega) {
 // whose body is one flexible-PCG iteration (mode 1 includes the network
 // forward pass on net's batch-1 workspace).
 void fpcg_build(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const int* node_pixel, int HW,
-                int fallback_after, int replace_every) {
+                int fallback_after, int replace_every, bool pdl) {
     cudaStream_t cs = S->cap;
     Workspace* w = mode == 1 ? workspace(n, 1, false) : nullptr;
     const int G = grid_nodes(S->op.Nn);
@@ -1269,28 +1299,27 @@ void fpcg_build(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const i
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         LCK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         const bool q4 = S->npe == 4;
-        fp_update_kernel<<<G, 256, 0, cs>>>(a);
-        if (q4) {
-            fp_true_res_kernel<4><<<G, 256, 0, cs>>>(a);
-            fp_prep_kernel<4><<<G, 256, 0, cs>>>(a);
-        } else {
-            fp_true_res_kernel<3><<<G, 256, 0, cs>>>(a);
-            fp_prep_kernel<3><<<G, 256, 0, cs>>>(a);
+        // every kernel after the body's first may start while its predecessor
+        // finishes (pdl); each waits in pdl_wait before reading
+        cudaError_t ce = cudaSuccess;
+        try {
+            fp_update_kernel<<<G, 256, 0, cs>>>(a);
+            launch(pdl, q4 ? fp_true_res_kernel<4> : fp_true_res_kernel<3>, dim3(G), dim3(256), 0, cs, a);
+            launch(pdl, q4 ? fp_prep_kernel<4> : fp_prep_kernel<3>, dim3(G), dim3(256), 0, cs, a);
+            if (mode == 1) {
+                net_forward(n, w, cs, &S->st.p->skip_net, pdl);
+                launch(pdl, q4 ? fp_net_kernel<4> : fp_net_kernel<3>, dim3(G), dim3(256), 0, cs, a);
+            }
+            launch(pdl, fp_prec_kernel, dim3(G), dim3(256), 0, cs, a);
+            launch(pdl, q4 ? fp_dir_kernel<4> : fp_dir_kernel<3>, dim3(G), dim3(256), 0, cs, a);
+            launch(pdl, fp_tick_kernel, dim3(1), dim3(1), 0, cs, a, h);
+            ce = cudaGetLastError();
+        } catch (const LFail&) {
+            cudaGraph_t got = nullptr;
+            cudaStreamEndCapture(cs, &got);
+            cudaGetLastError();
+            throw;
         }
-        if (mode == 1) {
-            net_forward(n, w, cs, &S->st.p->skip_net);
-            if (q4)
-                fp_net_kernel<4><<<G, 256, 0, cs>>>(a);
-            else
-                fp_net_kernel<3><<<G, 256, 0, cs>>>(a);
-        }
-        fp_prec_kernel<<<G, 256, 0, cs>>>(a);
-        if (q4)
-            fp_dir_kernel<4><<<G, 256, 0, cs>>>(a);
-        else
-            fp_dir_kernel<3><<<G, 256, 0, cs>>>(a);
-        fp_tick_kernel<<<1, 1, 0, cs>>>(a, h);
-        cudaError_t ce = cudaGetLastError();
         cudaGraph_t got = nullptr;
         cudaError_t ee = cudaStreamEndCapture(cs, &got);
         LCK(ce);
@@ -1300,6 +1329,7 @@ void fpcg_build(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const i
         cudaGraphDestroy(g);
         throw;
     }
+    S->pdl = pdl;
     cudaGraphDestroy(g);
     S->mode = mode;
     S->version = n ? n->version : 0;
@@ -1318,8 +1348,17 @@ void fpcg_run(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const int
     const size_t n3 = 3 * (size_t)S->op.Nn;
     auto t0 = std::chrono::steady_clock::now();
     if (!S->exec || S->mode != mode || S->maxit != o.max_iterations || S->rule != o.stop_rule ||
-        S->tol != o.tolerance || S->version != (n ? n->version : 0))
-        fpcg_build(S, o, mode, n, node_pixel, HW, 3, 50);
+        S->tol != o.tolerance || S->version != (n ? n->version : 0)) {
+        // with programmatic dependent launch where the driver takes it in a
+        // captured conditional body, else without
+        try {
+            fpcg_build(S, o, mode, n, node_pixel, HW, 3, 50, !S->pdl_refused);
+        } catch (const LFail&) {
+            if (S->pdl_refused) throw;
+            S->pdl_refused = true;
+            fpcg_build(S, o, mode, n, node_pixel, HW, 3, 50, false);
+        }
+    }
     if (host_F) {
         for (size_t i = 0; i < n3; i++)
             if (!std::isfinite(F[i])) throw LFail{PG_ENONFINITE, "F contains NaN or Inf"};
@@ -1360,6 +1399,7 @@ void fpcg_run(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const int
         ls->network_off_at = s.net_off ? s.net_off_at : -1;
         ls->replacements = s.replacements;
         ls->mode = mode;
+        ls->pdl = S->pdl;
     }
 }
 

@@ -29,6 +29,12 @@ namespace pgn {
 using bf16 = __nv_bfloat16;
 using bf162 = __nv_bfloat162;
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialisation may start before its predecessor in the stream has
+// finished; it waits here, before reading anything the predecessor wrote
+// (a no-op for an ordinary launch).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
@@ -102,6 +108,7 @@ __host__ __device__ constexpr int conv_smem_bytes(int cin, int cot) {
 template <int CIN, int COT, int MODE>
 __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(ConvArgs a) {
     static_assert(CIN % 16 == 0 && COT % 16 == 0, "channels in multiples of 16");
+    pdl_wait();
     if (a.skip && *a.skip) return;
     constexpr int SP = CIN + 8;  // padded pixel / weight-row stride in shared memory
     constexpr int C8 = CIN / 8;
@@ -309,6 +316,7 @@ __global__ void __launch_bounds__((COT / 16) * (CIT / 16) * 32) wgrad_kernel(Wgr
 // out[b][y][x][coff + c] = in[b][y/2][x/2][c], c < C.
 __global__ void up2_kernel(int B, int H, int W, const bf16* __restrict__ in, int in_cs, int C,
                            bf16* __restrict__ out, int out_cs, int coff, const int* skip) {
+    pdl_wait();
     if (skip && *skip) return;
     const int C8 = C / 8;
     const long total = (long)B * H * W * C8;

@@ -179,6 +179,7 @@ class PgLearnedStats(C.Structure):
         ("network_iterations", C.c_int32),
         ("network_off_at", C.c_int32),
         ("replacements", C.c_int32),
+        ("pdl", C.c_int32),
     ]
 
     def as_dict(self) -> dict:

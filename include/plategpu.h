@@ -479,6 +479,8 @@ typedef struct pg_learned_stats {
     int32_t network_iterations;  /* iterations whose network correction was used */
     int32_t network_off_at;      /* iteration after which the network was switched off, or -1 */
     int32_t replacements;        /* FP64 true-residual recomputations */
+    int32_t pdl;                 /* 1 when the solve graph's kernels use programmatic dependent
+                                    launch (each starts while its predecessor finishes) */
 } pg_learned_stats;
 
 /* Flexible PCG (Polak-Ribiere) with the two-level preconditioner
