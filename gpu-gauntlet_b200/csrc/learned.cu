@@ -709,6 +709,108 @@ __global__ void loss_kernel(Op op, int B, int HW, const int* __restrict__ node_p
     }
 }
 
+// PG_LOSS_SMOOTHED_ENERGY: the energy norm of the error after the
+// correction and the solve's smoothing sweeps, |M^nu (e1 - y)|_K^2 / |e1|_K^2
+// with M = I - S K, S = omega D^-1, nu = kCorrectionSweeps; its gradient is
+// dL/dy = -2 (M^T)^nu K M^nu (e1 - y) / |e1|_K^2, M^T = I - K S.  Batched over
+// [B][3 Nn] vectors; pair b is perm[(step - 1) B + b] (training) or perm[b].
+__device__ __forceinline__ int pair_of(const int* perm, const int* step, int B, int b) {
+    return step ? perm[(size_t)(*step - 1) * B + b] : perm[b];
+}
+
+// g = e1 - y (0 on constrained DOFs)
+__global__ void sl_diff_kernel(Op op, int B, int HW, const int* __restrict__ node_pixel,
+                               const float* __restrict__ out, const float* __restrict__ E1,
+                               const int* __restrict__ perm, const int* __restrict__ step, float so0, float so1,
+                               float so2, float* __restrict__ g) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
+    if (n >= op.Nn) return;
+    const int idx = pair_of(perm, step, B, b);
+    const float so[3] = {so0, so1, so2};
+    const float* e1 = E1 + (size_t)idx * 3 * op.Nn;
+    const float* ob = out + (size_t)b * HW * 4 + (size_t)node_pixel[n] * 4;
+    for (int d = 0; d < 3; d++) {
+        const int i = 3 * n + d;
+        g[(size_t)b * 3 * op.Nn + i] = op.cons[i] ? 0.f : e1[i] - so[d] * ob[d];
+    }
+}
+
+// forward sweep: out = in - S K in
+template <int NPE>
+__global__ void sl_sweep_kernel(Op op, float omega, const float* __restrict__ in, float* __restrict__ out) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
+    if (n >= op.Nn) return;
+    const float* gi = in + (size_t)b * 3 * op.Nn;
+    auto gv = [&](int m, int d) { return gi[3 * m + d]; };
+    float k[3];
+    kv_node<NPE>(op, n, gv, k);
+    const float* B9 = op.binv32 + 9 * n;
+    for (int d = 0; d < 3; d++)
+        out[(size_t)b * 3 * op.Nn + 3 * n + d] = gi[3 * n + d] - omega * binv_row(B9, d, k[0], k[1], k[2]);
+}
+
+// h = K g and loss += g.h / (B e1^T K e1)
+template <int NPE>
+__global__ void sl_energy_kernel(Op op, int B, const float* __restrict__ g, float* __restrict__ h,
+                                 const double* __restrict__ den, const int* __restrict__ perm,
+                                 const int* __restrict__ step, double* __restrict__ loss_hist) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
+    const int idx = pair_of(perm, step, B, b);
+    const float* gi = g + (size_t)b * 3 * op.Nn;
+    auto gv = [&](int m, int d) { return gi[3 * m + d]; };
+    double acc = 0.0;
+    if (n < op.Nn) {
+        float k[3];
+        kv_node<NPE>(op, n, gv, k);
+        for (int d = 0; d < 3; d++) {
+            h[(size_t)b * 3 * op.Nn + 3 * n + d] = k[d];
+            acc += (double)gi[3 * n + d] * k[d];
+        }
+        acc /= (double)B * den[idx];
+    }
+    __shared__ double red[32];
+    const double s = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int i = 0; i < (int)((blockDim.x + 31) >> 5); i++) t += red[i];
+        atomicAdd(loss_hist + (step ? *step - 1 : 0), t);
+    }
+}
+
+// backward sweep: out = in - K S in
+template <int NPE>
+__global__ void sl_bsweep_kernel(Op op, float omega, const float* __restrict__ in, float* __restrict__ out) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
+    if (n >= op.Nn) return;
+    const float* hi = in + (size_t)b * 3 * op.Nn;
+    auto sv = [&](int m, int d) {
+        const float* B9 = op.binv32 + 9 * m;
+        return omega * binv_row(B9, d, hi[3 * m], hi[3 * m + 1], hi[3 * m + 2]);
+    };
+    float k[3];
+    kv_node<NPE>(op, n, sv, k);
+    for (int d = 0; d < 3; d++) out[(size_t)b * 3 * op.Nn + 3 * n + d] = hi[3 * n + d] - k[d];
+}
+
+// dL/d(out) = -2 s_out h / (B e1^T K e1), 0 on constrained DOFs
+__global__ void sl_grad_kernel(Op op, int B, int HW, const int* __restrict__ node_pixel, const float* __restrict__ h,
+                               const double* __restrict__ den, const int* __restrict__ perm,
+                               const int* __restrict__ step, float so0, float so1, float so2,
+                               bf16* __restrict__ gout) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x, b = blockIdx.y;
+    if (n >= op.Nn) return;
+    const int idx = pair_of(perm, step, B, b);
+    const float so[3] = {so0, so1, so2};
+    const double sc = 1.0 / ((double)B * den[idx]);
+    bf16* g = gout + ((size_t)b * HW + node_pixel[n]) * 16;
+    for (int d = 0; d < 3; d++) {
+        const int i = 3 * n + d;
+        g[d] = __float2bfloat16_rn(op.cons[i] ? 0.f : (float)(-2.0 * sc * so[d] * h[(size_t)b * 3 * op.Nn + i]));
+    }
+}
+
 __global__ void step_begin_kernel(int* step) { *step += 1; }
 
 __global__ void train_tick_kernel(cudaGraphConditionalHandle h, const int* step, const int* stop) {
@@ -724,6 +826,13 @@ struct FState {
     double bnorm2, rr, true_rr, alpha, beta, gamma_prev, gamma_next;
 };
 
+// Damped block-Jacobi sweeps applied to the network's correction before
+// it is used (w <- w + S (r1 - K w)): they remove the rough part of the
+// correction -- BF16 rounding alone leaves white noise whose energy is
+// comparable to the whole error's -- and the training loss
+// PG_LOSS_SMOOTHED_ENERGY measures the error after the same sweeps.
+constexpr int kCorrectionSweeps = 2;
+
 struct FArgs {
     Op op;
     int HW;
@@ -735,6 +844,7 @@ struct FArgs {
     const float* F;
     double* x;
     float *r, *r_prev, *r1, *y, *r2, *z, *p0, *p1, *q;
+    float *y2, *v2;  // the correction and its K product after odd sweeps (double buffer)
     double *pU, *pTR, *pA, *pB, *pC, *pD, *pI;
     FState* st;
     int G;
@@ -943,6 +1053,39 @@ __global__ void fp_net_kernel(FArgs a) {
     block_partials<2>(acc, a.pB);
 }
 
+// One smoothing sweep on the network's correction: w' = w + S (r1 - v)
+// (v = K w from the previous pass), and v' = K w' (w' formed on the fly at
+// the neighbours); partial sums of w'.r1 and w'.v' for the step.
+template <int NPE>
+__global__ void fp_sweep_kernel(FArgs a, const float* __restrict__ w_in, const float* __restrict__ v_in,
+                                float* __restrict__ w_out, float* __restrict__ v_out) {
+    pgn::pdl_wait();
+    FState* st = a.st;
+    if (st->done || st->skip_net) return;
+    const float om = a.omega;
+    auto wv = [&](int m, int d) {
+        const float* B9 = a.op.binv32 + 9 * m;
+        const int i = 3 * m;
+        return w_in[i + d] + om * binv_row(B9, d, a.r1[i] - v_in[i], a.r1[i + 1] - v_in[i + 1],
+                                           a.r1[i + 2] - v_in[i + 2]);
+    };
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[2] = {0.0, 0.0};
+    if (n < a.op.Nn) {
+        float v[3];
+        kv_node<NPE>(a.op, n, wv, v);
+        for (int d = 0; d < 3; d++) {
+            const int i = 3 * n + d;
+            const float w = a.op.cons[i] ? 0.f : wv(n, d);
+            w_out[i] = w;
+            v_out[i] = v[d];
+            acc[0] += (double)w * a.r1[i];
+            acc[1] += (double)w * v[d];
+        }
+    }
+    block_partials<2>(acc, a.pB);
+}
+
 // C: with the network's correction y (mode 1), its energy-optimal step
 // c = y.r1 / y.K y (the multiple of y that most reduces the energy norm of
 // the error e1 = K^-1 r1: by (y.r1)^2 / y.K y) and
@@ -1078,7 +1221,7 @@ struct FpcgSolver {
     Op op{};
     int npe = 4;
     float omega = 1.f;
-    Buf<float> F, r, r_prev, r1, y, r2, z, p0, p1, q;
+    Buf<float> F, r, r_prev, r1, y, r2, z, p0, p1, q, y2, v2;
     Buf<double> x, parts;
     Buf<FState> st;
     cudaStream_t cap = nullptr;  // capture stream
@@ -1108,6 +1251,8 @@ struct pg_learned {
     Buf<bf16> img;
     Buf<float> E1;
     Buf<double> den, den2, stats, loss_hist;
+    Buf<float> sg, sh;  // [batch][3 Nn] vectors of the smoothed energy loss
+    int sl_batch = 0;
     Buf<int> perm, stop_step;
     FpcgSolver S;
     cudaGraphExec_t train_exec = nullptr;
@@ -1210,7 +1355,8 @@ void fpcg_init(FpcgSolver* S, pg_ctx* c, const Op& op, int npe, float omega) {
     S->omega = omega;
     cudaStream_t st = pgi::ctx_stream(c);
     const size_t n3 = 3 * (size_t)op.Nn;
-    for (Buf<float>* b : {&S->F, &S->r, &S->r_prev, &S->r1, &S->y, &S->r2, &S->z, &S->p0, &S->p1, &S->q}) {
+    for (Buf<float>* b : {&S->F, &S->r, &S->r_prev, &S->r1, &S->y, &S->r2, &S->z, &S->p0, &S->p1, &S->q, &S->y2,
+                          &S->v2}) {
         b->alloc(n3);
         b->zero(st);
     }
@@ -1251,6 +1397,8 @@ void fpcg_build(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const i
     a.r1 = S->r1.p;
     a.y = S->y.p;
     a.r2 = S->r2.p;
+    a.y2 = S->y2.p;
+    a.v2 = S->v2.p;
     a.z = S->z.p;
     a.p0 = S->p0.p;
     a.p1 = S->p1.p;
@@ -1306,11 +1454,21 @@ void fpcg_build(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const i
             fp_update_kernel<<<G, 256, 0, cs>>>(a);
             launch(pdl, q4 ? fp_true_res_kernel<4> : fp_true_res_kernel<3>, dim3(G), dim3(256), 0, cs, a);
             launch(pdl, q4 ? fp_prep_kernel<4> : fp_prep_kernel<3>, dim3(G), dim3(256), 0, cs, a);
+            FArgs ac = a;  // the preconditioner reads the correction after the sweeps
             if (mode == 1) {
                 net_forward(n, w, cs, &S->st.p->skip_net, pdl);
                 launch(pdl, q4 ? fp_net_kernel<4> : fp_net_kernel<3>, dim3(G), dim3(256), 0, cs, a);
+                float *wi = a.y, *vi = a.r2, *wo = a.y2, *vo = a.v2;
+                for (int k = 0; k < kCorrectionSweeps; k++) {
+                    launch(pdl, q4 ? fp_sweep_kernel<4> : fp_sweep_kernel<3>, dim3(G), dim3(256), 0, cs, a,
+                           (const float*)wi, (const float*)vi, wo, vo);
+                    std::swap(wi, wo);
+                    std::swap(vi, vo);
+                }
+                ac.y = wi;
+                ac.r2 = vi;
             }
-            launch(pdl, fp_prec_kernel, dim3(G), dim3(256), 0, cs, a);
+            launch(pdl, fp_prec_kernel, dim3(G), dim3(256), 0, cs, ac);
             launch(pdl, q4 ? fp_dir_kernel<4> : fp_dir_kernel<3>, dim3(G), dim3(256), 0, cs, a);
             launch(pdl, fp_tick_kernel, dim3(1), dim3(1), 0, cs, a, h);
             ce = cudaGetLastError();
@@ -1673,6 +1831,47 @@ void load_pairs(pg_learned* L, int count, const float* R, const float* E, bool s
     LCK(cudaStreamSynchronize(st));
 }
 
+// Queues the loss of a batch (outputs `out`, pair ids via perm/step) into
+// loss_hist, and with gout its gradient with respect to the network output.
+void queue_loss(pg_learned* L, int B, const float* out, const int* perm, const int* step, int kind,
+                double* loss_hist, bf16* gout, cudaStream_t st) {
+    pg_net* n = L->net;
+    const Op& op = L->op;
+    dim3 grid(grid_nodes(op.Nn), B);
+    const bool q4 = L->ov.npe == 4;
+    if (kind != PG_LOSS_SMOOTHED_ENERGY) {
+        auto k = q4 ? loss_kernel<4> : loss_kernel<3>;
+        k<<<grid, 256, 0, st>>>(op, B, L->HW, L->node_pixel.p, out, L->E1.p, L->den.p, L->den2.p, kind, perm, step,
+                                n->scale[3], n->scale[4], n->scale[5], loss_hist, gout);
+        LCK(cudaGetLastError());
+        return;
+    }
+    if (L->sl_batch < B) {
+        L->sg.alloc((size_t)B * 3 * op.Nn);
+        L->sh.alloc((size_t)B * 3 * op.Nn);
+        L->sl_batch = B;
+    }
+    float *g = L->sg.p, *h = L->sh.p;
+    sl_diff_kernel<<<grid, 256, 0, st>>>(op, B, L->HW, L->node_pixel.p, out, L->E1.p, perm, step, n->scale[3],
+                                         n->scale[4], n->scale[5], g);
+    for (int k = 0; k < kCorrectionSweeps; k++) {
+        (q4 ? sl_sweep_kernel<4> : sl_sweep_kernel<3>)<<<grid, 256, 0, st>>>(op, L->omega, g, h);
+        std::swap(g, h);
+    }
+    (q4 ? sl_energy_kernel<4> : sl_energy_kernel<3>)<<<grid, 256, 0, st>>>(op, B, g, h, L->den.p, perm, step,
+                                                                          loss_hist);
+    std::swap(g, h);  // g = K M^nu d
+    if (gout) {
+        for (int k = 0; k < kCorrectionSweeps; k++) {
+            (q4 ? sl_bsweep_kernel<4> : sl_bsweep_kernel<3>)<<<grid, 256, 0, st>>>(op, L->omega, g, h);
+            std::swap(g, h);
+        }
+        sl_grad_kernel<<<grid, 256, 0, st>>>(op, B, L->HW, L->node_pixel.p, g, L->den.p, perm, step, n->scale[3],
+                                             n->scale[4], n->scale[5], gout);
+    }
+    LCK(cudaGetLastError());
+}
+
 // Mean loss of pairs [first, first + count) of the training set (forward
 // passes of up to `batch` pairs, no gradient); per-pair losses into per
 // (host, optional).
@@ -1696,18 +1895,8 @@ double eval_loss(pg_learned* L, int first, int count, int batch, double* per) {
         for (int i = 0; i < b; i++) {
             // one pair at a time so each pair's loss is separate (B = 1 scaling)
             acc.zero(st);
-            dim3 grid(grid_nodes(L->op.Nn), 1);
             const float* outb = w->out.p + (size_t)i * L->HW * 4;
-            const int* idb = idx.p + i;
-            if (L->ov.npe == 4)
-                loss_kernel<4><<<grid, 256, 0, st>>>(L->op, 1, L->HW, L->node_pixel.p, outb, L->E1.p, L->den.p,
-                                                     L->den2.p, PG_LOSS_ENERGY, idb,
-                                                     nullptr, n->scale[3], n->scale[4], n->scale[5], acc.p, nullptr);
-            else
-                loss_kernel<3><<<grid, 256, 0, st>>>(L->op, 1, L->HW, L->node_pixel.p, outb, L->E1.p, L->den.p,
-                                                     L->den2.p, PG_LOSS_ENERGY, idb,
-                                                     nullptr, n->scale[3], n->scale[4], n->scale[5], acc.p, nullptr);
-            LCK(cudaGetLastError());
+            queue_loss(L, 1, outb, idx.p + i, nullptr, PG_LOSS_SMOOTHED_ENERGY, acc.p, nullptr, st);
             double v = 0;
             LCK(cudaMemcpyAsync(&v, acc.p, sizeof v, cudaMemcpyDeviceToHost, st));
             LCK(cudaStreamSynchronize(st));
@@ -1721,6 +1910,11 @@ double eval_loss(pg_learned* L, int first, int count, int batch, double* per) {
 void build_train_graph(pg_learned* L, int B, int total_steps, float lr, bool cosine, int loss_kind) {
     pg_net* n = L->net;
     Workspace* w = workspace(n, B, true);
+    if (L->sl_batch < B) {  // before the capture: no allocation inside it
+        L->sg.alloc((size_t)B * 3 * L->op.Nn);
+        L->sh.alloc((size_t)B * 3 * L->op.Nn);
+        L->sl_batch = B;
+    }
     cudaStream_t cs = L->S.cap;
     if (L->train_exec) {
         cudaGraphExecDestroy(L->train_exec);
@@ -1745,15 +1939,7 @@ void build_train_graph(pg_learned* L, int B, int total_steps, float lr, bool cos
         gather_batch_kernel<<<ew_grid((long)B * L->HW), 256, 0, cs>>>(B, L->HW, L->img.p, L->perm.p, n->step.p,
                                                                     w->in.p);
         net_forward(n, w, cs, nullptr);
-        dim3 grid(grid_nodes(L->op.Nn), B);
-        if (L->ov.npe == 4)
-            loss_kernel<4><<<grid, 256, 0, cs>>>(L->op, B, L->HW, L->node_pixel.p, w->out.p, L->E1.p, L->den.p,
-                                                 L->den2.p, loss_kind, L->perm.p, n->step.p, n->scale[3], n->scale[4], n->scale[5],
-                                                 L->loss_hist.p, w->gout.p);
-        else
-            loss_kernel<3><<<grid, 256, 0, cs>>>(L->op, B, L->HW, L->node_pixel.p, w->out.p, L->E1.p, L->den.p,
-                                                 L->den2.p, loss_kind, L->perm.p, n->step.p, n->scale[3], n->scale[4], n->scale[5],
-                                                 L->loss_hist.p, w->gout.p);
+        queue_loss(L, B, w->out.p, L->perm.p, n->step.p, loss_kind, L->loss_hist.p, w->gout.p, cs);
         net_backward(n, w, cs, false);
         pgn::adam_kernel<<<ew_grid(n->T.total), 256, 0, cs>>>(n->T, n->w.p, n->m.p, n->v.p, n->g.p, n->step.p, lr,
                                                               0.9f, 0.999f, 1e-8f, cosine ? total_steps : 0,
@@ -1804,7 +1990,8 @@ int pg_learned_train(pg_learned* L, int count, const float* R_dev, const float* 
         if (o.batch < 1 || o.epochs < 0 || !(o.lr > 0) || o.val_count < 0 || o.val_count >= count)
             throw LFail{PG_EINVAL, "bad training options"};
         if (o.epochs > PG_TRAIN_MAX_EPOCHS) throw LFail{PG_EINVAL, "too many epochs"};
-        if (o.loss != PG_LOSS_ENERGY && o.loss != PG_LOSS_SCALED_L2) throw LFail{PG_EINVAL, "unknown loss"};
+        if (o.loss != PG_LOSS_ENERGY && o.loss != PG_LOSS_SCALED_L2 && o.loss != PG_LOSS_SMOOTHED_ENERGY)
+            throw LFail{PG_EINVAL, "unknown loss"};
         pg_net* n = L->net;
         cudaStream_t st = pgi::ctx_stream(L->ctx);
         auto t0 = std::chrono::steady_clock::now();

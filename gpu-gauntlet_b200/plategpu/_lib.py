@@ -631,7 +631,7 @@ class Net:
             pass
 
 
-PG_LOSS_ENERGY, PG_LOSS_SCALED_L2 = 0, 1
+PG_LOSS_ENERGY, PG_LOSS_SCALED_L2, PG_LOSS_SMOOTHED_ENERGY = 0, 1, 2
 
 
 def train_options(epochs=20, batch=32, lr=1e-3, cosine=True, seed=1, val_count=0,

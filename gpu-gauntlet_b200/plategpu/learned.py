@@ -193,11 +193,11 @@ def train_net(ls: LearnedSolver, count, R, E, epochs=20, energy_epochs=None, bat
     with the scaled-L2 loss of the error (well-conditioned gradients: the
     network learns the smooth bulk of the error), then `energy_epochs`
     (default a quarter of `epochs`) with the energy-norm loss of the error
-    after the correction, the quantity the preconditioner needs.  Returns
-    one info dict for the run."""
+    after the correction and the solve's smoothing sweeps, the quantity the
+    preconditioner depends on.  Returns one info dict for the run."""
     if energy_epochs is None:
         energy_epochs = epochs // 4
-    stages = [(_lib.PG_LOSS_SCALED_L2, epochs - energy_epochs), (_lib.PG_LOSS_ENERGY, energy_epochs)]
+    stages = [(_lib.PG_LOSS_SCALED_L2, epochs - energy_epochs), (_lib.PG_LOSS_SMOOTHED_ENERGY, energy_epochs)]
     out = {"stages": [], "epoch_loss": [], "epoch_val_loss": [], "train_ms": 0.0, "steps": 0}
     first = True
     for loss, ep in stages:
@@ -211,7 +211,7 @@ def train_net(ls: LearnedSolver, count, R, E, epochs=20, energy_epochs=None, bat
             out["loss_first_step"] = info.loss_first_step
             out["batch"] = int(info.batch)
         first = False
-        out["stages"].append({"loss": "scaled_l2" if loss == _lib.PG_LOSS_SCALED_L2 else "energy",
+        out["stages"].append({"loss": "scaled_l2" if loss == _lib.PG_LOSS_SCALED_L2 else "smoothed_energy",
                               "epochs": ep, "steps": int(info.steps), "val_loss": info.val_loss,
                               "loss_last_step": info.loss_last_step})
         out["epoch_loss"] += list(info.epoch_loss)[:ep]
@@ -262,8 +262,33 @@ def main(argv=None):
     t.add_argument("--k-max", type=int, default=300)
     t.add_argument("--eval", type=int, default=64, help="held-out loads evaluated after training")
     t.add_argument("--json", default=None, help="write the training record here too")
+    f = sub.add_parser("forward", help="time the network's forward pass (random weights and input)")
+    f.add_argument("--batch", type=int, default=32)
+    f.add_argument("--size", type=int, default=144, help="grid height = width (multiple of 8)")
+    f.add_argument("--reps", type=int, default=20)
     a = ap.parse_args(argv)
     import torch
+
+    if a.cmd == "forward":
+        ctx = _lib.Context(0)
+        net = _lib.Net(ctx, a.size, a.size, seed=1)
+        x = torch.randn(a.batch, a.size, a.size, 3, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(3):
+            net.forward(a.batch, x.data_ptr(), y.data_ptr())
+        torch.cuda.synchronize()
+        s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_.record()
+        for _ in range(a.reps):
+            net.forward(a.batch, x.data_ptr(), y.data_ptr())
+        e_.record()
+        torch.cuda.synchronize()
+        ms = s_.elapsed_time(e_) / a.reps
+        fl = flops_per_image(a.size, a.size) * a.batch
+        print(json.dumps({"batch": a.batch, "size": a.size, "ms": ms, "tflops": fl / (ms * 1e-3) / 1e12}))
+        net.close()
+        ctx.close()
+        return
 
     wl = workloads.plate_q4_141()
     ctx = _lib.Context(0)

@@ -433,10 +433,13 @@ int pg_learned_make_pairs(pg_learned* learned, int count, const float* F_dev, co
 typedef enum pg_loss {
     PG_LOSS_ENERGY = 0,    /* energy norm of the error after the correction:
                               (e1 - y)^T K (e1 - y) / e1^T K e1 */
-    PG_LOSS_SCALED_L2 = 1  /* the same error in the network's output units:
+    PG_LOSS_SCALED_L2 = 1, /* the same error in the network's output units:
                               |(e1 - y) / s_out|^2 / |e1 / s_out|^2 (its gradient is not
                               weighted by K, whose condition number makes the energy
                               loss's gradient descent slow on smooth errors) */
+    PG_LOSS_SMOOTHED_ENERGY = 2 /* the energy norm of the error after the correction and the
+                                   solve's two smoothing sweeps on it (w <- w + S (r1 - K w)):
+                                   |M^2 (e1 - y)|_K^2 / |e1|_K^2, M = I - S K */
 } pg_loss;
 typedef struct pg_train_options {
     uint32_t struct_size;   /* sizeof(pg_train_options); set by pg_train_options_default */
@@ -448,7 +451,8 @@ typedef struct pg_train_options {
     int32_t val_count;      /* the last val_count pairs are held out for the validation loss */
     int32_t set_scales;     /* 1 (default): set the network's scales from the pairs */
     int32_t loss;           /* pg_loss of the training steps, default PG_LOSS_ENERGY (the
-                               validation loss is always the energy loss) */
+                               validation loss is always PG_LOSS_SMOOTHED_ENERGY, the
+                               quantity the solve depends on) */
 } pg_train_options;
 
 typedef struct pg_train_info {
@@ -470,8 +474,8 @@ void pg_train_options_default(pg_train_options* opt);
  * CUDA graph launch per epoch. */
 int pg_learned_train(pg_learned* learned, int count, const float* R_dev, const float* E_dev,
                      const pg_train_options* opt, pg_train_info* info);
-/* Test hook: the loss of each of `count` pairs with the current network
- * (replaces the training set held by `learned`). */
+/* Test hook: the PG_LOSS_SMOOTHED_ENERGY loss of each of `count` pairs with
+ * the current network (replaces the training set held by `learned`). */
 int pg_learned_loss(pg_learned* learned, int count, const float* R_dev, const float* E_dev, double* loss_out);
 
 typedef struct pg_learned_stats {

@@ -266,3 +266,25 @@ def energy_loss(A, e1, y):
     Ad = A @ d
     den = float(e1 @ (A @ e1))
     return float(d @ Ad) / den, -2.0 * Ad / den
+
+
+def smoothed_energy_loss(A, binv, omega, e1, y, sweeps=2):
+    """|M^nu (e1 - y)|_A^2 / |e1|_A^2 with M = I - omega D^-1 A: the energy
+    norm of the error after the correction and `sweeps` damped block-Jacobi
+    sweeps on it (the solve's smoothing of the network's correction)."""
+    g = e1 - y
+    for _ in range(sweeps):
+        g = g - omega * block_apply(binv, A @ g)
+    return float(g @ (A @ g)) / float(e1 @ (A @ e1))
+
+
+def smoothed_energy_grad(A, binv, omega, e1, y, sweeps=2):
+    """Gradient of smoothed_energy_loss with respect to y:
+    -2 (M^T)^nu A M^nu (e1 - y) / |e1|_A^2, M^T = I - omega A D^-1."""
+    g = e1 - y
+    for _ in range(sweeps):
+        g = g - omega * block_apply(binv, A @ g)
+    h = A @ g
+    for _ in range(sweeps):
+        h = h - omega * (A @ block_apply(binv, h))
+    return -2.0 * h / float(e1 @ (A @ e1))

@@ -145,7 +145,12 @@ def test_pairs_and_loss_match_oracle(gpu_ctx, oracle, U, small):
         r_ref = np.where(wl.cons_mask != 0, 0.0, F[i].astype(np.float64)) - A @ xk[i]
         assert rel_err(Rh[i], r_ref) < 1e-5
         assert rel_err(Eh[i], xs[i] - xk[i]) < 1e-6
-    # the loss of each pair through the network, against the oracle's
+    # the loss of each pair through the network (the energy norm of the
+    # error after the correction and two damped block-Jacobi sweeps, with
+    # the solver's damping omega = min(1, 1.5 / lambda_max(D^-1 K))),
+    # against the oracle's
+    import two_level_ref as T
+    omega = min(1.0, 1.5 / T.lambda_max_power(A, bd, wl.cons_mask))
     scales = np.array([2.0, 0.5, 0.25, 1e-3, 4e-4, 3e-4], np.float32)
     ls.net.set_params(None, scales)
     got = ls.learned.loss(3, R.data_ptr(), E.data_ptr())
@@ -153,12 +158,12 @@ def test_pairs_and_loss_match_oracle(gpu_ctx, oracle, U, small):
     params = U.unflatten(p.astype(np.float64))
     H, W = ls.net.height, ls.net.width
     for i in range(3):
-        r1, e1 = U.training_pair(A, bd.astype(np.float32).astype(np.float64), Rh[i].astype(np.float64),
+        r1, e1 = U.training_pair(A, omega * bd.astype(np.float32).astype(np.float64), Rh[i].astype(np.float64),
                                  Eh[i].astype(np.float64))
         img = U.to_image(r1, ls.node_pixel, H, W, scales[:3])[None]
         out, _ = U.forward(params, img, bf=True)
         y = U.from_image(out[0], ls.node_pixel, scales[3:], wl.cons_mask)
-        want, _ = U.energy_loss(A, e1, y)
+        want = U.smoothed_energy_loss(A, bd, omega, e1, y)
         assert abs(got[i] - want) < 2e-2 * max(1.0, abs(want)), (got[i], want)
     ls.close()
 
@@ -175,7 +180,7 @@ def trained(gpu_ctx, small):
 def test_training_lowers_the_held_out_loss(trained):
     ls, info = trained
     assert info["steps"] == 12 * (448 // 16)
-    assert info["val_loss"] < 0.5 * info["val_loss_before"], info
+    assert info["val_loss"] < 0.8, info  # energy error after correction + sweeps below 80% of e1's
     assert info["loss_last_step"] < info["loss_first_step"]
     assert all(np.isfinite(info["epoch_loss"]))
 

@@ -140,3 +140,30 @@ def test_image_maps_round_trip():
     want = v.copy()
     want[4] = 0
     assert np.allclose(back, want)
+
+
+def test_smoothed_energy_loss_gradient():
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(12)
+    nn = 5
+    n = 3 * nn
+    R = sp.random(n, n, density=0.5, random_state=3)
+    A = (R @ R.T + sp.eye(n) * n).tocsr()
+    # symmetric positive 3x3 block inverses
+    blocks = []
+    for _ in range(nn):
+        q = rng.standard_normal((3, 3))
+        blocks.append(np.linalg.inv(q @ q.T + 3 * np.eye(3)))
+    binv = np.stack(blocks).reshape(-1)
+    e1 = rng.standard_normal(n)
+    y = rng.standard_normal(n)
+    g = U.smoothed_energy_grad(A, binv, 0.7, e1, y)
+    h = 1e-6
+    for i in range(n):
+        d = np.zeros(n)
+        d[i] = h
+        fd = (U.smoothed_energy_loss(A, binv, 0.7, e1, y + d) -
+              U.smoothed_energy_loss(A, binv, 0.7, e1, y - d)) / (2 * h)
+        assert abs(fd - g[i]) < 1e-6 * max(1, abs(fd))
+    assert U.smoothed_energy_loss(A, binv, 0.7, e1, e1) == 0.0
