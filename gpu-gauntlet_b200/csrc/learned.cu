@@ -823,6 +823,8 @@ struct FState {
     int it, done, converged, stop_reason, tr_ran, net_off, net_off_at, bad_count, use_net, skip_net;
     int iterations, net_iters, replacements, error;
     float net_step;  // the last iteration's step c along the network's correction
+    int stall;       // set by the stall guard, folded into net_off by the tick
+    double tr_prev;  // true residual^2 at the last periodic replacement
     double bnorm2, rr, true_rr, alpha, beta, gamma_prev, gamma_next;
 };
 
@@ -997,7 +999,16 @@ __global__ void fp_prep_kernel(FArgs a) {
             }
             return;
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0) st->true_rr = s[0];
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            // stall guard: with the network on, a replacement interval that did
+            // not cut the true residual norm by 20% switches it off (a weak
+            // network can keep y.r1 > 0 while flexible PCG stagnates); the
+            // first interval compares with |F|
+            const double prev = st->tr_prev > 0 ? st->tr_prev : st->bnorm2;
+            if (a.mode == 1 && !st->net_off && it % a.replace_every == 0 && s[0] > 0.64 * prev) st->stall = 1;
+            if (it % a.replace_every == 0) st->tr_prev = s[0];
+            st->true_rr = s[0];
+        }
     }
     const bool skip = a.mode != 1 || st->net_off;
     if (blockIdx.x == 0 && threadIdx.x == 0) st->skip_net = skip;
@@ -1182,7 +1193,7 @@ __global__ void fp_tick_kernel(FArgs a, cudaGraphConditionalHandle h) {
     pgn::pdl_wait();
     FState* st = a.st;
     st->gamma_prev = st->gamma_next;
-    if (a.mode == 1 && !st->net_off && st->bad_count >= a.fallback_after) {
+    if (a.mode == 1 && !st->net_off && (st->bad_count >= a.fallback_after || st->stall)) {
         st->net_off = 1;
         st->net_off_at = st->it;
     }

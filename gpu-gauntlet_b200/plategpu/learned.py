@@ -11,7 +11,10 @@ with x_k an early iterate of plain block-Jacobi PCG); everything here runs
 on the GPU through the library (torch provides the device buffers).
 
 Command line (trains the plate_q4_141 network and writes its weight file):
-    python -m plategpu.learned train --out <file.npz> [--loads 8192] [--epochs 20]
+    python -m plategpu.learned train --out <file.npz> [--loads 8192] [--epochs 40]
+Timing (and profiling) entry points:
+    python -m plategpu.learned forward --batch 32     the network's forward pass
+    python -m plategpu.learned solve --count 4        learned solves of plate_q4_141
 """
 from __future__ import annotations
 
@@ -160,7 +163,7 @@ def evaluate(torch, ls: LearnedSolver, loads, tolerance=1e-6, mode=_lib.LEARNED_
     rows = []
     for i in range(loads.shape[0]):
         info, st = ls.learned.solve_device(opts, F[i].data_ptr(), x.data_ptr(), mode)
-        row = {"iterations": int(info.iterations), "ms": float(info.solve_ms),
+        row = {"iterations": int(info.iterations), "ms": float(info.solve_ms), "pdl": int(st.pdl),
                "converged": int(info.converged), "network_iterations": int(st.network_iterations),
                "network_off_at": int(st.network_off_at)}
         if truth is not None:
@@ -187,7 +190,7 @@ def tight_solutions(torch, ctx, ls: LearnedSolver, loads, tol=1e-12):
     return out
 
 
-def train_net(ls: LearnedSolver, count, R, E, epochs=20, energy_epochs=None, batch=32, lr=1e-3, val=256,
+def train_net(ls: LearnedSolver, count, R, E, epochs=40, energy_epochs=None, batch=32, lr=3e-3, val=256,
               seed=TRAIN_SEED):
     """Trains ls's network on `count` pairs (device tensors R, E): first
     with the scaled-L2 loss of the error (well-conditioned gradients: the
@@ -223,7 +226,7 @@ def train_net(ls: LearnedSolver, count, R, E, epochs=20, energy_epochs=None, bat
     return out
 
 
-def train_plate(torch, ctx, wl, loads=8192, epochs=20, energy_epochs=None, batch=32, lr=1e-3, k_max=300,
+def train_plate(torch, ctx, wl, loads=8192, epochs=40, energy_epochs=None, batch=32, lr=3e-3, k_max=300,
                 val=256, seed=TRAIN_SEED, log=print):
     """The full pipeline for one plate: seeded random-field loads, plain
     solves, pairs, training (train_net).  Returns (LearnedSolver, info
@@ -254,11 +257,11 @@ def main(argv=None):
     t = sub.add_parser("train", help="train the plate_q4_141 network and write its weight file")
     t.add_argument("--out", default=DEFAULT_WEIGHTS)
     t.add_argument("--loads", type=int, default=8192)
-    t.add_argument("--epochs", type=int, default=20)
+    t.add_argument("--epochs", type=int, default=40)
     t.add_argument("--energy-epochs", type=int, default=None,
                    help="final epochs with the energy-norm loss (default a quarter of --epochs)")
     t.add_argument("--batch", type=int, default=32)
-    t.add_argument("--lr", type=float, default=1e-3)
+    t.add_argument("--lr", type=float, default=3e-3)
     t.add_argument("--k-max", type=int, default=300)
     t.add_argument("--eval", type=int, default=64, help="held-out loads evaluated after training")
     t.add_argument("--json", default=None, help="write the training record here too")
@@ -266,8 +269,24 @@ def main(argv=None):
     f.add_argument("--batch", type=int, default=32)
     f.add_argument("--size", type=int, default=144, help="grid height = width (multiple of 8)")
     f.add_argument("--reps", type=int, default=20)
+    v = sub.add_parser("solve", help="learned solves of plate_q4_141 held-out loads")
+    v.add_argument("--weights", default=DEFAULT_WEIGHTS)
+    v.add_argument("--count", type=int, default=4)
+    v.add_argument("--mode", type=int, default=_lib.LEARNED_NETWORK)
+    v.add_argument("--tolerance", type=float, default=1e-6)
     a = ap.parse_args(argv)
     import torch
+
+    if a.cmd == "solve":
+        ctx = _lib.Context(0)
+        wl = workloads.plate_q4_141()
+        ls = LearnedSolver(ctx, wl, weights=a.weights)
+        H = workloads.random_field_loads(wl, a.count, HELD_OUT_SEED)
+        for r in evaluate(torch, ls, H, tolerance=a.tolerance, mode=a.mode):
+            print(json.dumps(r))
+        ls.close()
+        ctx.close()
+        return
 
     if a.cmd == "forward":
         ctx = _lib.Context(0)
