@@ -155,9 +155,12 @@ namespace {
 // launches
 // ---------------------------------------------------------------------------
 
-int pick_cot(int rows) {
+// Output channels per block: the largest of 64, 48, 32, 16 that divides
+// the layer's rows and keeps the halo and all nine taps' weights within
+// 160 KB of shared memory.
+int pick_cot(int rows, int cin) {
     for (int c : {64, 48, 32, 16})
-        if (rows % c == 0) return c;
+        if (rows % c == 0 && pgn::conv_smem_bytes(cin, c) <= 160 * 1024) return c;
     return 16;
 }
 
@@ -196,7 +199,7 @@ void conv_launch(const pgn::ConvArgs& a, int rows, cudaStream_t st, bool pdl) {
 // Dispatches the (input channels, output tile, epilogue) combinations the
 // network uses.
 void conv(int mode, int cin, int rows, const pgn::ConvArgs& a, cudaStream_t st, bool pdl = false) {
-    const int cot = pick_cot(rows);
+    const int cot = pick_cot(rows, cin);
 #define PG_CONV(C, T, M)                                   \
     if (cin == C && cot == T && mode == M) {               \
         conv_launch<C, T, M>(a, rows, st, pdl);            \
@@ -204,12 +207,12 @@ void conv(int mode, int cin, int rows, const pgn::ConvArgs& a, cudaStream_t st, 
     }
     using namespace pgn;
     PG_CONV(16, 16, OUT_BF16_RELU) PG_CONV(16, 32, OUT_BF16_RELU) PG_CONV(32, 32, OUT_BF16_RELU)
-    PG_CONV(32, 64, OUT_BF16_RELU) PG_CONV(64, 64, OUT_BF16_RELU) PG_CONV(128, 64, OUT_BF16_RELU)
-    PG_CONV(192, 64, OUT_BF16_RELU) PG_CONV(96, 32, OUT_BF16_RELU) PG_CONV(48, 16, OUT_BF16_RELU)
+    PG_CONV(32, 64, OUT_BF16_RELU) PG_CONV(64, 64, OUT_BF16_RELU) PG_CONV(128, 32, OUT_BF16_RELU)
+    PG_CONV(192, 32, OUT_BF16_RELU) PG_CONV(96, 32, OUT_BF16_RELU) PG_CONV(48, 16, OUT_BF16_RELU)
     PG_CONV(16, 16, OUT_F32)
     PG_CONV(16, 16, OUT_BF16_MASKED) PG_CONV(16, 48, OUT_BF16_MASKED) PG_CONV(32, 32, OUT_BF16_MASKED)
-    PG_CONV(32, 48, OUT_BF16_MASKED) PG_CONV(64, 64, OUT_BF16_MASKED) PG_CONV(128, 64, OUT_BF16_MASKED)
-    PG_CONV(128, 64, OUT_BF16) PG_CONV(64, 32, OUT_BF16) PG_CONV(32, 16, OUT_BF16) PG_CONV(16, 16, OUT_BF16)
+    PG_CONV(32, 48, OUT_BF16_MASKED) PG_CONV(64, 64, OUT_BF16_MASKED) PG_CONV(128, 32, OUT_BF16_MASKED)
+    PG_CONV(128, 32, OUT_BF16) PG_CONV(64, 32, OUT_BF16) PG_CONV(32, 16, OUT_BF16) PG_CONV(16, 16, OUT_BF16)
 #undef PG_CONV
     throw LFail{PG_EUNSUPPORTED, "no convolution kernel for cin " + std::to_string(cin) + ", tile " +
                                      std::to_string(cot) + ", mode " + std::to_string(mode)};

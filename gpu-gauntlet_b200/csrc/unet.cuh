@@ -97,13 +97,16 @@ struct ConvArgs {
 constexpr int kConvThreads = 128;
 
 __host__ __device__ constexpr int conv_smem_bytes(int cin, int cot) {
-    return (100 + 2 * cot) * (cin + 8) * 2;
+    return (100 + 9 * cot) * (cin + 8) * 2;
 }
 
 // 3 x 3 convolution, zero padding, no bias.  A block computes an 8 x 8
 // pixel tile (four warps, each a 2-row x 8-column m16 tile) for COT output
-// channels: the 10 x 10 input halo (CIN channels) stays in shared memory
-// and the weights stream in tap by tap, double buffered.
+// channels.  The 10 x 10 input halo (CIN channels) and all nine taps'
+// COT x CIN weights are staged in shared memory by one cp.async group, so
+// the block pays one L2 round trip before its MMAs (streaming the taps one
+// by one left each small layer waiting nine times); COT is chosen so the
+// weights fit (conv_smem_bytes).
 // Grid: (ceil(W/8), ceil(H/8) * B, w_rows / COT).
 template <int CIN, int COT, int MODE>
 __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(ConvArgs a) {
@@ -114,7 +117,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(ConvArgs a) {
     constexpr int C8 = CIN / 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     bf16* sIn = reinterpret_cast<bf16*>(smem_raw);
-    bf16* sW = sIn + 100 * SP;
+    bf16* sW = sIn + 100 * SP;  // [9][COT][SP]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles_y = (a.H + 7) >> 3;
     const int b = blockIdx.y / tiles_y;
@@ -127,26 +130,22 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(ConvArgs a) {
         const bf16* src = ok ? a.in + (((size_t)b * a.H + gy) * a.W + gx) * a.in_cs + c8 * 8 : a.in;
         cp_async16(sIn + pix * SP + c8 * 8, src, ok);
     }
-    auto load_w = [&](int tap, int buf) {
-        for (int q = tid; q < COT * C8; q += kConvThreads) {
-            const int co = q / C8, c8 = q - co * C8;
-            cp_async16(sW + (buf * COT + co) * SP + c8 * 8,
-                       a.w + ((size_t)tap * a.w_rows + co0 + co) * CIN + c8 * 8, true);
-        }
-    };
-    load_w(0, 0);
+    for (int q = tid; q < 9 * COT * C8; q += kConvThreads) {
+        const int row = q / C8, c8 = q - row * C8;  // row = tap * COT + co
+        const int tap = row / COT, co = row - tap * COT;
+        cp_async16(sW + row * SP + c8 * 8, a.w + ((size_t)tap * a.w_rows + co0 + co) * CIN + c8 * 8, true);
+    }
     cp_async_commit();
     float acc[COT / 8][4];
 #pragma unroll
     for (int i = 0; i < COT / 8; i++) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
     const int j = lane >> 3, i8 = lane & 7;
+    cp_async_wait<0>();
+    __syncthreads();
+#pragma unroll 1
     for (int tap = 0; tap < 9; tap++) {
-        if (tap + 1 < 9) load_w(tap + 1, (tap + 1) & 1);
-        cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();
         const int dy = tap / 3, dx = tap - 3 * (tap / 3);
-        const bf16* sWt = sW + (tap & 1) * COT * SP;
+        const bf16* sWt = sW + tap * COT * SP;
         // A rows: matrix j covers m rows (j & 1) * 8 .. +7 (tile row 2*warp + (j & 1),
         // columns 0..7) and k half j >> 1
         const bf16* aRow = sIn + ((2 * warp + (j & 1) + dy) * 10 + i8 + dx) * SP + (j >> 1) * 8;
@@ -163,7 +162,6 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_kernel(ConvArgs a) {
                 mma_bf16(acc[2 * np + 1], af, bw[2], bw[3]);
             }
         }
-        __syncthreads();
     }
     const int g = lane >> 2, q4 = lane & 3;
 #pragma unroll

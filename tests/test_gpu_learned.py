@@ -168,18 +168,27 @@ def test_pairs_and_loss_match_oracle(gpu_ctx, oracle, U, small):
 
 
 @pytest.fixture(scope="module")
-def trained(gpu_ctx, small):
-    """A network trained on the GPU for the 32 x 32 plate (512 pairs)."""
-    ls, info = learned.train_plate(torch, gpu_ctx, small, loads=512, epochs=40, energy_epochs=10, batch=16,
-                                   lr=3e-3, val=64, k_max=120, seed=21, log=lambda *_: None)
+def c2():
+    return workloads.plate_q4_141()
+
+
+@pytest.fixture(scope="module")
+def trained(gpu_ctx, c2):
+    """A network trained on the GPU for the 60k-DOF plate: 2,048 seeded
+    random-field loads, 30 epochs of the scaled-L2 loss then 10 of the
+    smoothed energy loss (about half a minute)."""
+    ls, info = learned.train_plate(torch, gpu_ctx, c2, loads=2048, epochs=40, energy_epochs=10, batch=32,
+                                   lr=3e-3, val=256, k_max=300, seed=21, log=lambda *_: None)
     yield ls, info
     ls.close()
 
 
 def test_training_lowers_the_held_out_loss(trained):
     ls, info = trained
-    assert info["steps"] == 40 * (448 // 16)
-    assert info["val_loss"] < 0.8, info  # energy error after correction + sweeps below 80% of e1's
+    assert info["steps"] == 40 * ((2048 - 256) // 32)
+    # the energy norm of the error after the correction and its sweeps, on
+    # held-out pairs: below half of the error's own (1 = no gain)
+    assert info["val_loss"] < 0.5, info
     assert info["loss_last_step"] < info["loss_first_step"]
     assert all(np.isfinite(info["epoch_loss"]))
 
@@ -191,21 +200,36 @@ def truth_of(oracle, wl, F):
     return np.stack([solve(f)[0] for f in F])
 
 
-def test_trained_network_cuts_iterations_and_meets_the_error_bar(oracle, trained, small):
-    ls, _info = trained
-    wl = small
-    F = workloads.random_field_loads(wl, 4, 99)  # loads the network never saw
+def gain(oracle, ls, wl, F):
     xt = truth_of(oracle, wl, F)
-    rows = {m: learned.evaluate(torch, ls, F, tolerance=1e-8, mode=m, truth=xt)
+    rows = {m: learned.evaluate(torch, ls, F, tolerance=1e-6, mode=m, truth=xt)
             for m in (_lib.LEARNED_NETWORK, _lib.LEARNED_SMOOTHING_ONLY, _lib.LEARNED_BLOCK_JACOBI)}
     for m, rs in rows.items():
         for r in rs:
-            assert r["converged"] and r["rel_l2"] < 1e-6, (m, r)
-    it_net = np.mean([r["iterations"] for r in rows[_lib.LEARNED_NETWORK]])
-    it_smooth = np.mean([r["iterations"] for r in rows[_lib.LEARNED_SMOOTHING_ONLY]])
-    it_bj = np.mean([r["iterations"] for r in rows[_lib.LEARNED_BLOCK_JACOBI]])
-    assert it_net < 0.7 * it_smooth and it_smooth < it_bj, (it_net, it_smooth, it_bj)
-    assert all(r["network_iterations"] > 0 for r in rows[_lib.LEARNED_NETWORK])
+            assert r["converged"] and r["rel_l2"] <= 1e-6, (m, r)
+    its = {m: np.mean([r["iterations"] for r in rs]) for m, rs in rows.items()}
+    return its, rows
+
+
+def test_trained_network_cuts_iterations_and_meets_the_error_bar(oracle, trained, c2):
+    """On loads the network never saw, flexible PCG with the trained network
+    needs well under 60% of the iterations of the same method without it
+    (its smoothing steps only), which in turn beats plain block Jacobi; every
+    solve meets FP64 error 1e-6."""
+    ls, _info = trained
+    its, rows = gain(oracle, ls, c2, workloads.random_field_loads(c2, 4, 99))
+    net, smooth, bj = its[_lib.LEARNED_NETWORK], its[_lib.LEARNED_SMOOTHING_ONLY], its[_lib.LEARNED_BLOCK_JACOBI]
+    assert net < 0.6 * smooth and smooth < bj, its
+    assert all(r["network_iterations"] > 0 and r["network_off_at"] < 0 for r in rows[_lib.LEARNED_NETWORK])
+
+
+def test_committed_network_on_held_out_loads(gpu_ctx, oracle, c2):
+    """The network that ships with the package (plategpu/weights, trained by
+    python -m plategpu.learned train on 8,192 loads) on 8 held-out loads."""
+    ls = learned.LearnedSolver(gpu_ctx, c2, weights=learned.DEFAULT_WEIGHTS)
+    its, _rows = gain(oracle, ls, c2, workloads.random_field_loads(c2, 8, learned.HELD_OUT_SEED))
+    assert its[_lib.LEARNED_NETWORK] < 0.6 * its[_lib.LEARNED_SMOOTHING_ONLY], its
+    ls.close()
 
 
 def test_block_jacobi_mode_matches_plain_pcg(gpu_ctx, oracle, small):
@@ -243,11 +267,11 @@ def test_unhelpful_network_is_switched_off(gpu_ctx, oracle, U, small):
     ls.close()
 
 
-def test_host_and_device_solves_agree(trained, small):
+def test_host_and_device_solves_agree(trained, c2):
     ls, _ = trained
-    wl = small
-    opts = learned.solve_options(1e-8)
-    x, info, _st = ls.learned.solve(opts, wl.F)
+    wl = c2
+    opts = learned.solve_options(1e-6)
+    x, info, st = ls.learned.solve(opts, wl.F)
     xd = torch.zeros(wl.n_dof, dtype=torch.float64, device="cuda")
     Fd = dev(wl.F)
     info2, _ = ls.learned.solve_device(opts, Fd.data_ptr(), xd.data_ptr())
@@ -255,9 +279,9 @@ def test_host_and_device_solves_agree(trained, small):
     assert np.array_equal(x, xd.cpu().numpy())
 
 
-def test_zero_load_and_iteration_limit(trained, small):
+def test_zero_load_and_iteration_limit(trained, c2):
     ls, _ = trained
-    wl = small
+    wl = c2
     x, info, _ = ls.learned.solve(learned.solve_options(1e-8), np.zeros(wl.n_dof, np.float32))
     assert info.converged and info.iterations == 0 and not np.any(x)
     x, info, _ = ls.learned.solve(learned.solve_options(1e-14, max_iterations=5), wl.F)
