@@ -257,6 +257,36 @@ __global__ void binv_apply_kernel(int Nn, const double* __restrict__ binv, const
     for (int d = 0; d < 3; d++) z[3 * k + d] = B[3 * d] * y0 + B[3 * d + 1] * y1 + B[3 * d + 2] * y2;
 }
 
+// One power step z = D^-1 K x, node by node: (K x)_n gathered from the
+// node's incident elements (FP64 element matrices, constrained rows the
+// identity), then the node's 3x3 block inverse.  One launch per step in
+// place of the colour-ordered K x, the identity rows and the block apply.
+template <int NPE>
+__global__ void power_step_kernel(int Nn, const int* __restrict__ inc_ptr, const int* __restrict__ inc_idx,
+                                  const uint32_t* __restrict__ elements, const double* __restrict__ ke64,
+                                  const uint8_t* __restrict__ cons, const double* __restrict__ binv,
+                                  const double* __restrict__ x, double* __restrict__ z) {
+    constexpr int ND = 3 * NPE;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= Nn) return;
+    double y[3] = {0.0, 0.0, 0.0};
+    for (int q = inc_ptr[n]; q < inc_ptr[n + 1]; q++) {
+        const int e = inc_idx[q] >> 2, k = inc_idx[q] & 3;
+        const double* K = ke64 + (size_t)e * ND * ND + 3 * k * ND;
+        for (int b = 0; b < NPE; b++) {
+            const int m = (int)elements[(size_t)e * NPE + b];
+            const double x0 = x[3 * m], x1 = x[3 * m + 1], x2 = x[3 * m + 2];
+            for (int d = 0; d < 3; d++)
+                y[d] += K[d * ND + 3 * b] * x0 + K[d * ND + 3 * b + 1] * x1 + K[d * ND + 3 * b + 2] * x2;
+        }
+    }
+    for (int d = 0; d < 3; d++)
+        if (cons[3 * n + d]) y[d] = x[3 * n + d];
+    const double* B = binv + 9 * (size_t)n;
+#pragma unroll
+    for (int d = 0; d < 3; d++) z[3 * n + d] = B[3 * d] * y[0] + B[3 * d + 1] * y[1] + B[3 * d + 2] * y[2];
+}
+
 // r = F - y narrowed to FP32, 0 on constrained rows (y = K x): the load of
 // an FP64 correction solve K d = F - K x.  r may be F itself.
 __global__ void residual_f32_kernel(int n, const uint8_t* cons, const float* F, const double* y, float* r) {

@@ -472,8 +472,12 @@ void queue_power_steps(pg_ctx* c, Plan* pl, int iters) {
     pg::power_start_kernel<<<((int)n + 255) / 256, 256, 0, st>>>((int)n, pl->cons.p, a);
     CK(cudaGetLastError());
     for (int it = 0; it < iters; it++) {
-        queue_apply_k(c, pl, a, pl->kx.p);
-        pg::binv_apply_kernel<<<(hp.Nn + 255) / 256, 256, 0, st>>>(hp.Nn, pl->binv64.p, pl->kx.p, b);
+        if (hp.npe == 4)
+            pg::power_step_kernel<4><<<(hp.Nn + 255) / 256, 256, 0, st>>>(
+                hp.Nn, pl->inc_ptr.p, pl->inc_idx.p, pl->mesh_elements.p, pl->ke64.p, pl->cons.p, pl->binv64.p, a, b);
+        else
+            pg::power_step_kernel<3><<<(hp.Nn + 255) / 256, 256, 0, st>>>(
+                hp.Nn, pl->inc_ptr.p, pl->inc_idx.p, pl->mesh_elements.p, pl->ke64.p, pl->cons.p, pl->binv64.p, a, b);
         CK(cudaGetLastError());
         std::swap(a, b);
     }
