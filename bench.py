@@ -16,13 +16,25 @@ step is timed with CUDA events on the solver's stream.  ``roofline``
 compares the PCG kernel's algorithmic bytes per second with the measured
 HBM copy peak and with an in-run L2-resident copy.
 
-Further sections of the line: ``load_cases`` (four loads of the plate
-through pg_solve_load_cases against the same loads one by one),
-``other_configs`` (plate_q4_32, plate_dkt_200 and the unstructured
-plate_holes_dkt, four methods each), ``batch`` (a 256-plate uneven batch,
-Q4 and DKT, sides 16-256, four methods, the fastest that meets the error
-bar reported) and ``cpu_baseline`` (the reference-precision CPU solver,
-one core).  --cases 0, --other-configs 0, --batch 0 skip sections.
+Every variant's FP64 error is checked on the plate's own load and 16
+seeded random-field loads; only a variant whose largest error is <= 1e-6
+can be the headline.
+
+Further sections of the line: ``learned`` (the learned two-level
+preconditioner: flexible PCG with the trained U-Net, one CUDA graph per
+solve; timed like the variants, checked on the same loads, evaluated on
+512 held-out loads, compared with the same loop without the network, and
+the network's forward pass against the BF16 tensor-core peak),
+``load_cases`` (four loads of the plate through pg_solve_load_cases
+against the same loads one by one), ``other_configs`` (plate_q4_32,
+plate_dkt_200, the unstructured plate_holes_dkt and plate_q4_400, which
+runs on the global-memory path; four methods each), ``batch`` (a 256-plate
+uneven batch, Q4 and DKT, sides 16-256, team-size target autotuned, four
+methods, the fastest that meets the error bar reported; errors on the 5
+largest plates and 5% of the others against sparse LU and on every plate
+against an FP64 1e-12 solve) and ``cpu_baseline`` (the reference-precision
+CPU solver, one core).  --learned 0, --cases 0, --other-configs 0,
+--batch 0 skip sections.
 
 Multi-GPU: a single plate does not shard (the solve is bound by the
 latency of the exchange between blocks), so --gpus N runs N independent
