@@ -1192,7 +1192,7 @@ __global__ void fp_dir_kernel(FArgs a) {
     }
 }
 
-__global__ void fp_tick_kernel(FArgs a, cudaGraphConditionalHandle h) {
+__global__ void fp_tick_kernel(FArgs a, cudaGraphConditionalHandle h, int in_graph) {
     pgn::pdl_wait();
     FState* st = a.st;
     st->gamma_prev = st->gamma_next;
@@ -1201,7 +1201,7 @@ __global__ void fp_tick_kernel(FArgs a, cudaGraphConditionalHandle h) {
         st->net_off_at = st->it;
     }
     st->it += 1;
-    cudaGraphSetConditional(h, (!st->done && st->it <= a.maxit + 1) ? 1u : 0u);
+    if (in_graph) cudaGraphSetConditional(h, (!st->done && st->it <= a.maxit + 1) ? 1u : 0u);
 }
 
 // ---------------------------------------------------------------------------
@@ -1381,13 +1381,58 @@ void fpcg_init(FpcgSolver* S, pg_ctx* c, const Op& op, int npe, float omega) {
     LCK(cudaStreamSynchronize(st));
 }
 
+// The kernels of one flexible-PCG iteration, on cs.  in_graph: the tick
+// sets the WHILE node's condition.  ev (9 events, optional) brackets the
+// groups update, true residual, smoothing + network input, network, K y +
+// sweeps, preconditioner, direction + K p, tick for timing.
+void queue_body(FpcgSolver* S, const FArgs& a, int mode, pg_net* n, Workspace* w, cudaStream_t cs, bool pdl,
+                cudaGraphConditionalHandle h, bool in_graph, cudaEvent_t* ev) {
+    const int G = a.G;
+    const bool q4 = S->npe == 4;
+    auto mark = [&](int k) {
+        if (ev) LCK(cudaEventRecord(ev[k], cs));
+    };
+    mark(0);
+    fp_update_kernel<<<G, 256, 0, cs>>>(a);
+    LCK(cudaGetLastError());
+    mark(1);
+    launch(pdl, q4 ? fp_true_res_kernel<4> : fp_true_res_kernel<3>, dim3(G), dim3(256), 0, cs, a);
+    mark(2);
+    launch(pdl, q4 ? fp_prep_kernel<4> : fp_prep_kernel<3>, dim3(G), dim3(256), 0, cs, a);
+    mark(3);
+    FArgs ac = a;  // the preconditioner reads the correction after the sweeps
+    if (mode == 1) {
+        net_forward(n, w, cs, &S->st.p->skip_net, pdl);
+        mark(4);
+        launch(pdl, q4 ? fp_net_kernel<4> : fp_net_kernel<3>, dim3(G), dim3(256), 0, cs, a);
+        float *wi = a.y, *vi = a.r2, *wo = a.y2, *vo = a.v2;
+        for (int k = 0; k < kCorrectionSweeps; k++) {
+            launch(pdl, q4 ? fp_sweep_kernel<4> : fp_sweep_kernel<3>, dim3(G), dim3(256), 0, cs, a,
+                   (const float*)wi, (const float*)vi, wo, vo);
+            std::swap(wi, wo);
+            std::swap(vi, vo);
+        }
+        ac.y = wi;
+        ac.r2 = vi;
+    } else {
+        mark(4);
+    }
+    mark(5);
+    launch(pdl, fp_prec_kernel, dim3(G), dim3(256), 0, cs, ac);
+    mark(6);
+    launch(pdl, q4 ? fp_dir_kernel<4> : fp_dir_kernel<3>, dim3(G), dim3(256), 0, cs, a);
+    mark(7);
+    launch(pdl, fp_tick_kernel, dim3(1), dim3(1), 0, cs, a, h, in_graph ? 1 : 0);
+    mark(8);
+}
+
 // Builds the solve graph of S: an init node, then a conditional WHILE node
 // whose body is one flexible-PCG iteration (mode 1 includes the network
 // forward pass on net's batch-1 workspace).
-void fpcg_build(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const int* node_pixel, int HW,
-                int fallback_after, int replace_every, bool pdl) {
-    cudaStream_t cs = S->cap;
-    Workspace* w = mode == 1 ? workspace(n, 1, false) : nullptr;
+// The kernel arguments of S's iteration for these options and mode (w: the
+// network's batch-1 workspace in mode 1).
+FArgs make_fargs(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, Workspace* w, const int* node_pixel,
+                 int HW, int fallback_after, int replace_every) {
     const int G = grid_nodes(S->op.Nn);
     FArgs a{};
     a.op = S->op;
@@ -1433,6 +1478,15 @@ void fpcg_build(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const i
     a.replace_every = replace_every;
     a.mode = mode;
     a.fallback_after = fallback_after;
+    return a;
+}
+
+void fpcg_build(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const int* node_pixel, int HW,
+                int fallback_after, int replace_every, bool pdl) {
+    cudaStream_t cs = S->cap;
+    Workspace* w = mode == 1 ? workspace(n, 1, false) : nullptr;
+    const int G = grid_nodes(S->op.Nn);
+    FArgs a = make_fargs(S, o, mode, n, w, node_pixel, HW, fallback_after, replace_every);
 
     if (S->exec) {
         cudaGraphExecDestroy(S->exec);
@@ -1460,31 +1514,11 @@ void fpcg_build(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const i
         LCK(cudaGraphAddNode(&loop, g, &init_node, 1, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         LCK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-        const bool q4 = S->npe == 4;
         // every kernel after the body's first may start while its predecessor
         // finishes (pdl); each waits in pdl_wait before reading
         cudaError_t ce = cudaSuccess;
         try {
-            fp_update_kernel<<<G, 256, 0, cs>>>(a);
-            launch(pdl, q4 ? fp_true_res_kernel<4> : fp_true_res_kernel<3>, dim3(G), dim3(256), 0, cs, a);
-            launch(pdl, q4 ? fp_prep_kernel<4> : fp_prep_kernel<3>, dim3(G), dim3(256), 0, cs, a);
-            FArgs ac = a;  // the preconditioner reads the correction after the sweeps
-            if (mode == 1) {
-                net_forward(n, w, cs, &S->st.p->skip_net, pdl);
-                launch(pdl, q4 ? fp_net_kernel<4> : fp_net_kernel<3>, dim3(G), dim3(256), 0, cs, a);
-                float *wi = a.y, *vi = a.r2, *wo = a.y2, *vo = a.v2;
-                for (int k = 0; k < kCorrectionSweeps; k++) {
-                    launch(pdl, q4 ? fp_sweep_kernel<4> : fp_sweep_kernel<3>, dim3(G), dim3(256), 0, cs, a,
-                           (const float*)wi, (const float*)vi, wo, vo);
-                    std::swap(wi, wo);
-                    std::swap(vi, vo);
-                }
-                ac.y = wi;
-                ac.r2 = vi;
-            }
-            launch(pdl, fp_prec_kernel, dim3(G), dim3(256), 0, cs, ac);
-            launch(pdl, q4 ? fp_dir_kernel<4> : fp_dir_kernel<3>, dim3(G), dim3(256), 0, cs, a);
-            launch(pdl, fp_tick_kernel, dim3(1), dim3(1), 0, cs, a, h);
+            queue_body(S, a, mode, n, w, cs, pdl, h, true, nullptr);
             ce = cudaGetLastError();
         } catch (const LFail&) {
             cudaGraph_t got = nullptr;
@@ -1540,8 +1574,37 @@ void fpcg_run(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const int
     cudaEvent_t e0, e1;
     LCK(cudaEventCreate(&e0));
     LCK(cudaEventCreate(&e1));
+    double phase[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int timed_its = 0;
     LCK(cudaEventRecord(e0, st));
-    LCK(cudaGraphLaunch(S->exec, st));
+    if (!o.phase_timing) {
+        LCK(cudaGraphLaunch(S->exec, st));
+    } else {
+        // the same kernels without the graph (profilers cannot look inside a
+        // graph with conditional nodes): each iteration's kernel groups timed
+        // with events, and the host reading the stop flag after every
+        // iteration (so solve_ms includes those waits)
+        Workspace* w = mode == 1 ? workspace(n, 1, false) : nullptr;
+        const FArgs a = make_fargs(S, o, mode, n, w, node_pixel, HW, 3, 50);
+        fp_init_kernel<<<a.G, 256, 0, st>>>(a);
+        LCK(cudaGetLastError());
+        cudaEvent_t ev[9];
+        for (auto& e : ev) LCK(cudaEventCreate(&e));
+        for (int it = 0; it <= o.max_iterations + 1; it++) {
+            queue_body(S, a, mode, n, w, st, false, 0, false, ev);
+            int done = 0;
+            LCK(cudaMemcpyAsync(&done, &S->st.p->done, sizeof(int), cudaMemcpyDeviceToHost, st));
+            LCK(cudaStreamSynchronize(st));
+            for (int k = 0; k < 8; k++) {
+                float ms = 0;
+                LCK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+                phase[k] += ms;
+            }
+            timed_its++;
+            if (done) break;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+    }
     LCK(cudaEventRecord(e1, st));
     LCK(cudaMemcpyAsync(x_out, S->x.p, n3 * sizeof(double),
                         host_x ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, st));
@@ -1565,6 +1628,7 @@ void fpcg_run(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const int
         info->reductions = s.iterations;
         info->plan_cached = 1;
         info->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        for (int k = 0; k < 8; k++) info->phase_us[k] = timed_its ? 1e3 * phase[k] / timed_its : 0.0;
     }
     if (ls) {
         ls->network_iterations = s.net_iters;

@@ -274,16 +274,32 @@ def main(argv=None):
     v.add_argument("--count", type=int, default=4)
     v.add_argument("--mode", type=int, default=_lib.LEARNED_NETWORK)
     v.add_argument("--tolerance", type=float, default=1e-6)
+    v.add_argument("--phase-timing", action="store_true",
+                   help="run without the graph and print the average device time per iteration of each "
+                        "kernel group")
+    v.add_argument("--workload", default="plate_q4_141")
     a = ap.parse_args(argv)
     import torch
 
     if a.cmd == "solve":
         ctx = _lib.Context(0)
-        wl = workloads.plate_q4_141()
-        ls = LearnedSolver(ctx, wl, weights=a.weights)
+        wl = workloads.WORKLOADS[a.workload]()
+        ls = LearnedSolver(ctx, wl, weights=a.weights if a.mode == _lib.LEARNED_NETWORK else None)
         H = workloads.random_field_loads(wl, a.count, HELD_OUT_SEED)
-        for r in evaluate(torch, ls, H, tolerance=a.tolerance, mode=a.mode):
-            print(json.dumps(r))
+        if a.phase_timing:
+            opts = solve_options(a.tolerance)
+            opts.phase_timing = 1
+            F = torch.from_numpy(np.ascontiguousarray(H, np.float32)).cuda()
+            x = torch.zeros(wl.n_dof, dtype=torch.float64, device="cuda")
+            names = ("update", "true_residual", "smoothing_input", "network", "Ky_sweeps", "preconditioner",
+                     "direction_Kp", "tick")
+            for i in range(a.count):
+                info, st = ls.learned.solve_device(opts, F[i].data_ptr(), x.data_ptr(), a.mode)
+                print(json.dumps({"iterations": int(info.iterations),
+                                  "us_per_iteration": dict(zip(names, [round(v, 2) for v in info.phase_us]))}))
+        else:
+            for r in evaluate(torch, ls, H, tolerance=a.tolerance, mode=a.mode):
+                print(json.dumps(r))
         ls.close()
         ctx.close()
         return

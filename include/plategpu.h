@@ -501,7 +501,13 @@ typedef struct pg_learned_stats {
  * replaces the recursive residual every 50 iterations.  The whole solve is
  * one CUDA graph launch (a conditional WHILE node).
  * _device: F_dev / x_dev device [3n] float / double; otherwise host buffers
- * (copies included).  info->solve_ms is the graph's device time. */
+ * (copies included).  info->solve_ms is the graph's device time.  With
+ * opt->phase_timing the iterations run without the graph, one launch at a
+ * time with the host checking the stop flag after each, and
+ * info->phase_us[0..7] receives the average device time per iteration of:
+ * update; true residual; smoothing and network input; network; K y and the
+ * sweeps; preconditioner; direction and K p; loop tick (a diagnostic mode:
+ * profilers cannot look inside a graph with conditional nodes). */
 int pg_learned_solve_device(pg_learned* learned, const pg_options* opt, int mode, const float* F_dev,
                             double* x_dev, pg_info* info, pg_learned_stats* stats);
 int pg_learned_solve(pg_learned* learned, const pg_options* opt, int mode, const float* F, double* x_out,
