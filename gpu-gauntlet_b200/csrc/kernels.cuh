@@ -512,73 +512,74 @@ __device__ void block_publish(double (&v)[KM], double* red, unsigned long long* 
 
 // One exchange round, all threads of the block: waits for the K tagged
 // FP64 partial sums of every block (slots of 16 words; staged to
-// sp[G * K]) and for the tagged
-// values of this block's ghost DOFs in vector buffer vb (written to
-// dst[3 * no .. 3 * nloc)).  Each thread keeps up to IF items in flight, so
-// a round costs about one L2 round trip.  Returns false if a wait gave up.
-template <typename T, int IF = 2>
+// sp[G * K]) and for the tagged values of this block's ghost DOFs in vector
+// buffer vb (written to dst[3 * no .. 3 * nloc)).  Items 0 .. ng - 1 are
+// the ghosts, which their owners publish before their partial sums, then
+// the partials.  Each thread takes items tid, tid + nt, tid + 2 nt, ...
+// with two in flight, and refills a slot with its next item as soon as
+// the slot's item has arrived: a ghost frees its slot after one round
+// trip, so every partial is being polled by the time the partials come
+// in, and the round costs about one L2 round trip after the last block
+// published.  Returns false if a wait gave up.
+template <typename T>
 __device__ bool exchange_round(const unsigned long long* __restrict__ pb, int G, int K,
                                const unsigned long long* __restrict__ vb, T* dst, int no, int nloc,
                                const int* __restrict__ gid, int g, unsigned f, double* sp,
                                Waiter& wt) {
     constexpr int TW = Tag<T>::W;
-    const int np = G * K, n = np + 3 * (nloc - no);
+    const int ng = 3 * (nloc - no), n = ng + G * K, nt = blockDim.x;
     pb += (size_t)(g % kRep) * G * 16;  // the copy of the partials part g reads
-    for (int i0 = threadIdx.x; i0 < n; i0 += IF * blockDim.x) {
-        const unsigned long long* ptr[IF];
-        bool done[IF];
-#pragma unroll
-        for (int j = 0; j < IF; j++) {
-            const int i = i0 + j * (int)blockDim.x;
-            done[j] = i >= n;
-            if (done[j]) {
-                ptr[j] = nullptr;
-            } else if (i < np) {
-                ptr[j] = pb + (size_t)(i / K) * 16 + 2 * (i % K);
-            } else {
-                const int k = 3 * no + i - np;
-                ptr[j] = vb + (size_t)(3 * gid[k / 3] + k % 3) * TW;
-            }
+    auto addr = [&](int i) -> const unsigned long long* {
+        if (i < ng) {
+            const int k = 3 * no + i;
+            return vb + (size_t)(3 * gid[k / 3] + k % 3) * TW;
         }
-        wt.spins = 0;
-        for (;;) {
-            unsigned long long lo[IF], hi[IF];
-#pragma unroll
-            for (int j = 0; j < IF; j++) {
-                if (done[j]) continue;
-                const int i = i0 + j * (int)blockDim.x;
-                if (i < np || TW == 2) {
-                    ld_relaxed2(ptr[j], lo[j], hi[j]);
-                } else {
-                    lo[j] = ld_relaxed(ptr[j]);
-                    hi[j] = lo[j];
-                }
-            }
-            bool all = true;
-#pragma unroll
-            for (int j = 0; j < IF; j++) {
-                if (done[j]) continue;
-                const int i = i0 + j * (int)blockDim.x;
-                if ((unsigned)(lo[j] >> 32) != f || (unsigned)(hi[j] >> 32) != f) {
-                    all = false;
-                    continue;
-                }
-                done[j] = true;
-                const double dv =
-                    __longlong_as_double((long long)((hi[j] << 32) | (lo[j] & 0xffffffffull)));
-                if (i < np) {
-                    sp[i] = dv;
-                } else {
-                    const int k = 3 * no + i - np;
-                    if constexpr (TW == 2)
-                        dst[k] = (T)dv;
-                    else
-                        dst[k] = (T)__uint_as_float((unsigned)lo[j]);
-                }
-            }
-            if (all) break;
-            if (!wt.keep_going()) return false;
+        const int q = i - ng;
+        return pb + (size_t)(q / K) * 16 + 2 * (q % K);
+    };
+    // two slots: item index (>= n when empty) and its address
+    int i0 = threadIdx.x, i1 = threadIdx.x + nt, next = threadIdx.x + 2 * nt;
+    const unsigned long long* p0 = i0 < n ? addr(i0) : nullptr;
+    const unsigned long long* p1 = i1 < n ? addr(i1) : nullptr;
+    auto load = [&](const unsigned long long* p, int i, unsigned long long& lo, unsigned long long& hi) {
+        if (i >= ng || TW == 2) {
+            ld_relaxed2(p, lo, hi);
+        } else {
+            lo = ld_relaxed(p);
+            hi = lo;
         }
+    };
+    // stores the item if its tags match; false if it has not arrived
+    auto take = [&](int i, unsigned long long lo, unsigned long long hi) -> bool {
+        if ((unsigned)(lo >> 32) != f || (unsigned)(hi >> 32) != f) return false;
+        if (i >= ng) {
+            sp[i - ng] = __longlong_as_double((long long)((hi << 32) | (lo & 0xffffffffull)));
+        } else if constexpr (TW == 2) {
+            dst[3 * no + i] = (T)__longlong_as_double((long long)((hi << 32) | (lo & 0xffffffffull)));
+        } else {
+            dst[3 * no + i] = (T)__uint_as_float((unsigned)lo);
+        }
+        return true;
+    };
+    wt.spins = 0;
+    while (i0 < n || i1 < n) {
+        unsigned long long lo0 = 0, hi0 = 0, lo1 = 0, hi1 = 0;
+        if (i0 < n) load(p0, i0, lo0, hi0);
+        if (i1 < n) load(p1, i1, lo1, hi1);
+        bool moved = false;
+        if (i0 < n && take(i0, lo0, hi0)) {
+            i0 = next;
+            next += nt;
+            p0 = i0 < n ? addr(i0) : nullptr;
+            moved = true;
+        }
+        if (i1 < n && take(i1, lo1, hi1)) {
+            i1 = next;
+            next += nt;
+            p1 = i1 < n ? addr(i1) : nullptr;
+            moved = true;
+        }
+        if (!moved && !wt.keep_going()) return false;
     }
     return true;
 }
@@ -773,7 +774,12 @@ enum { STOP_CONVERGED = 0, STOP_MAX_ITER = 1, STOP_BREAKDOWN = 2, STOP_ZERO_RHS 
 enum { ACT_UPDATE = 0, ACT_STOP = 1, ACT_RU = 2, ACT_NONFINITE = 3 };
 enum { ST_OK = 0, ST_TIMEOUT = 4, ST_NONFINITE = 5 };
 
+// Threads per block: at most kMaxThreads (the launch bound of the 96-register
+// build); up to kLeanThreads a build with 128 registers per thread runs
+// instead (no spills); the batch kernel always runs kBatchThreads.
 constexpr int kMaxThreads = 576;
+constexpr int kLeanThreads = 512;
+constexpr int kBatchThreads = 512;
 
 // Per-phase SM cycles of thread 0 of block 0, when timing is requested:
 // 0 K.u, 1 gather + dots + publish w, 2 block reduction, 3 publish partials,
@@ -1452,36 +1458,72 @@ __device__ __forceinline__ void pcg_body(const PcgArgs& a, const int g, unsigned
     }
 }
 
-// One plate on the whole grid: part g = block g.
-template <int NPE, typename T, bool MIXED>
-__global__ void __launch_bounds__(kMaxThreads, 1) pcg_kernel(const __grid_constant__ PcgArgs a) {
+// One plate on the whole grid: part g = block g; MAXT: the launch bound.
+template <int NPE, typename T, bool MIXED, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) pcg_kernel(const __grid_constant__ PcgArgs a) {
     extern __shared__ __align__(16) unsigned char sm[];
     pcg_body<NPE, T, MIXED>(a, blockIdx.x, sm);
 }
 
 // Many independent plates of one element type (NPE) in one launch.  The
-// grid is cut into teams of
-// consecutive blocks; a team solves the plates of its queue one after the
-// other, each plate partitioned into as many parts as the team has blocks,
-// with the plate's own exchange buffers (so teams never wait on each other,
-// and a team starts its next plate as soon as its blocks are done).  Team
-// block 0 stamps each plate's start and end (globaltimer).
+// grid is cut into teams of consecutive blocks; teams of one size form a
+// class with one queue of plates (largest estimated work first).  A free
+// team takes its class's next plate: team block 0 claims a queue position
+// with an atomic counter and logs it in the team's claim slot k (tag
+// k + 1), where the team's other blocks read it.  Each plate is
+// partitioned into as many parts as the team has blocks and has its own
+// exchange buffers, so teams never wait on each other.  Team block 0
+// stamps each plate's start and end (globaltimer).
 struct BatchArgs {
-    const PcgArgs* plates;        // [count], npe 3 or 4, one precision for all
-    const int* block_team;        // [grid] team of each block
-    const int* team_base;         // [teams] first block of each team
-    const int* queue_off;         // [teams + 1] into queue
-    const int* queue;             // plate ids, team by team, in solve order
-    unsigned long long* times;    // [count][2] start / end of each plate
+    const PcgArgs* plates;          // [count], npe 3 or 4, one precision for all
+    const int* block_team;          // [grid] team of each block
+    const int* team_base;           // [teams] first block of each team
+    const int* team_class;          // [teams] class of each team
+    const int* class_off;           // [classes + 1] into class_queue
+    const int* class_queue;         // plate ids, class by class
+    const int* log_off;             // [teams + 1] each team's claim slots
+    int* class_next;                // [classes] next queue position (zero at launch)
+    unsigned long long* claims;     // claim slots (zero at launch)
+    unsigned long long* times;      // [count][2] start / end of each plate
+    int* abort_flag;
+    int* claim_failures;            // waits for a claim that gave up
+    unsigned long long timeout_ns;  // limit of one wait for a claim
 };
 
 template <int NPE, typename T, bool MIXED>
-__global__ void __launch_bounds__(kMaxThreads, 1) pcg_batch_kernel(const __grid_constant__ BatchArgs b) {
+__global__ void __launch_bounds__(kBatchThreads, 1) pcg_batch_kernel(const __grid_constant__ BatchArgs b) {
     extern __shared__ __align__(16) unsigned char sm[];
+    volatile int* s_plate = (volatile int*)sm;  // between plates the shared memory is free
     const int team = b.block_team[blockIdx.x];
     const int g = (int)blockIdx.x - b.team_base[team];
-    for (int q = b.queue_off[team]; q < b.queue_off[team + 1]; q++) {
-        const int pi = b.queue[q];
+    const int cls = b.team_class[team];
+    const int q0 = b.class_off[cls], qn = b.class_off[cls + 1] - q0;
+    unsigned long long* slots = b.claims + b.log_off[team];
+    const int nslots = b.log_off[team + 1] - b.log_off[team];
+    for (int k = 0; k < nslots; k++) {
+        if (threadIdx.x == 0) {
+            unsigned pos = (unsigned)qn;  // past the end: no plate
+            if (g == 0) {
+                pos = (unsigned)atomicAdd(b.class_next + cls, 1);
+                st_relaxed(slots + k, ((unsigned long long)(k + 1) << 32) | pos);
+            } else {
+                Waiter wt;
+                wt.start(b.timeout_ns, b.abort_flag, b.claim_failures);
+                for (;;) {
+                    const unsigned long long v = ld_relaxed(slots + k);
+                    if ((unsigned)(v >> 32) == (unsigned)(k + 1)) {
+                        pos = (unsigned)v;
+                        break;
+                    }
+                    if (!wt.keep_going()) break;
+                }
+            }
+            *s_plate = pos < (unsigned)qn ? b.class_queue[q0 + pos] : -1;
+        }
+        __syncthreads();
+        const int pi = *s_plate;
+        __syncthreads();  // read by all before the plate's data overwrite it
+        if (pi < 0) break;
         const PcgArgs& a = b.plates[pi];
         if (g == 0 && threadIdx.x == 0) b.times[2 * pi] = gtimer();
         // a plate with fewer parts than the team has blocks leaves the rest idle

@@ -556,6 +556,24 @@ std::string schedule_batch(const std::vector<int>& nodes, const std::vector<int>
             P.queue_off[t + 1] = P.queue_off[t] + (int)q[t].size();
             P.queue.insert(P.queue.end(), q[t].begin(), q[t].end());
         }
+        // the dynamic queues: one per class (team size), largest work first
+        std::vector<std::vector<int>> cq(nc);
+        for (int i : order) {
+            if (kinds[i] != kind) continue;
+            const auto it = std::find(pc.begin(), pc.end(), d[i]);
+            if (it != pc.end()) cq[it - pc.begin()].push_back(i);
+        }
+        P.class_off.assign(nc + 1, 0);
+        for (int k = 0; k < nc; k++) {
+            P.class_off[k + 1] = P.class_off[k] + (int)cq[k].size();
+            P.class_queue.insert(P.class_queue.end(), cq[k].begin(), cq[k].end());
+        }
+        P.log_off.assign(T + 1, 0);
+        for (int t = 0; t < T; t++) {
+            const int k = (int)(std::find(pc.begin(), pc.end(), P.team_size[t]) - pc.begin());
+            P.team_class.push_back(k);
+            P.log_off[t + 1] = P.log_off[t] + (int)cq[k].size();
+        }
         out.phases.push_back(std::move(P));
     }
     }

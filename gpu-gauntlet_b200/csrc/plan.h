@@ -95,12 +95,21 @@ std::string build_coarse_meta(const pg_problem& p, HostPlan& plan);
 // and each size's plates go to its teams longest first to the least-loaded
 // team.  Plates of different kinds (element types: the launch's kernel is
 // specialised for one) never share a phase.
+// Teams of one size form a class; a class's plates sit in one queue,
+// largest estimated work first, and each team takes the next plate of its
+// class's queue when it is free (a device-side counter per class), so the
+// estimates only order the queue.  queue_off / queue / team_load keep the
+// static assignment those estimates predict (each plate to the least
+// loaded team of its size), for reporting.
 struct BatchPhase {
     int kind = 4;                         // nodes per element of all its plates
     int grid = 0;                         // blocks of the launch
     std::vector<int> team_base, team_size;
-    std::vector<int> queue_off, queue;    // per team, plates in solve order
-    std::vector<double> team_load;        // estimated work per team
+    std::vector<int> team_class;          // [teams] class of each team
+    std::vector<int> class_off, class_queue;  // [classes + 1]; plates, class by class
+    std::vector<int> log_off;             // [teams + 1] each team's claim slots (its class's plates)
+    std::vector<int> queue_off, queue;    // per team, the predicted plates in solve order
+    std::vector<double> team_load;        // estimated work per team (predicted assignment)
 };
 struct BatchSchedule {
     std::vector<BatchPhase> phases;

@@ -133,7 +133,9 @@ struct pg_plan {
 // launch per phase).
 struct BatchPhaseDev {
     int grid = 0, kind = 4;
-    DevBuf<int> block_team, team_base, queue_off, queue;
+    DevBuf<int> block_team, team_base, team_class, class_off, class_queue, log_off;
+    DevBuf<int> class_next;               // zeroed before each launch
+    DevBuf<unsigned long long> claims;    // zeroed before each launch
 };
 struct pg_batch {
     pg_ctx* ctx = nullptr;
@@ -141,7 +143,7 @@ struct pg_batch {
     std::vector<std::unique_ptr<Plan>> plans;
     pg::BatchSchedule sched;
     std::vector<std::unique_ptr<BatchPhaseDev>> phases;
-    DevBuf<int> abort_flag;
+    DevBuf<int> abort_flag, claim_failures;
     DevBuf<pg::PcgArgs> args;
     DevBuf<pg::PcgResult> res;
     DevBuf<unsigned long long> times;
@@ -153,6 +155,7 @@ struct pg_batch {
     // shared-memory size); graph_failed: capture not possible, launch directly
     cudaGraphExec_t graph = nullptr;
     int graph_precision = 0, graph_smem = 0;
+    unsigned long long graph_timeout_ns = 0;
     bool graph_failed = false;
     ~pg_batch() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -851,7 +854,16 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_
     const pg::HostPlan& hp = pl->hp;
     const bool mixed = o.precision == PG_PREC_MIXED;
     int threads = o.threads;
-    if (!threads) threads = std::min(pg::kMaxThreads, std::max(128, (hp.max_ntask + 31) / 32 * 32));
+    if (!threads) {
+        // one thread per task of the largest part, within the launch bound:
+        // up to 512 threads the kernel has 128 registers (576: 96), which
+        // measured faster for FP32 inner iterations and for FP64 block
+        // Jacobi; FP64 with the Chebyshev smoother keeps 576 threads (its
+        // split task passes: fewer of them)
+        const bool wide = !mixed && o.smoother == PG_SMOOTHER_CHEBYSHEV;
+        threads = std::min(wide ? pg::kMaxThreads : pg::kLeanThreads, std::max(128, (hp.max_ntask + 31) / 32 * 32));
+    }
+    const bool lean = threads <= pg::kLeanThreads;
     prepare_plan_data(c, pl, o);
     int ke_mode = 0;
     bool ainv_smem = false;
@@ -867,10 +879,15 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_
         CK(cudaMemsetAsync(pl->trace.p, 0, pl->trace.n * sizeof(unsigned long long), c->stream));
 
     const void* fn;
+    constexpr int LT = pg::kLeanThreads, MT = pg::kMaxThreads;
     if (hp.npe == 4)
-        fn = mixed ? (const void*)pg::pcg_kernel<4, float, true> : (const void*)pg::pcg_kernel<4, double, false>;
+        fn = mixed ? (lean ? (const void*)pg::pcg_kernel<4, float, true, LT> : (const void*)pg::pcg_kernel<4, float, true, MT>)
+                   : (lean ? (const void*)pg::pcg_kernel<4, double, false, LT>
+                           : (const void*)pg::pcg_kernel<4, double, false, MT>);
     else
-        fn = mixed ? (const void*)pg::pcg_kernel<3, float, true> : (const void*)pg::pcg_kernel<3, double, false>;
+        fn = mixed ? (lean ? (const void*)pg::pcg_kernel<3, float, true, LT> : (const void*)pg::pcg_kernel<3, float, true, MT>)
+                   : (lean ? (const void*)pg::pcg_kernel<3, double, false, LT>
+                           : (const void*)pg::pcg_kernel<3, double, false, MT>);
     opt_in_smem(c, fn);
     if (pl->ok_fn != fn || pl->ok_threads != threads || pl->ok_smem != L.total) {
         int nb = 0;
@@ -1337,12 +1354,17 @@ std::unique_ptr<pg_batch> build_batch(pg_ctx* c, const pg_problem* probs, int co
         d->kind = P.kind;
         d->block_team.upload(bt.data(), bt.size(), st);
         d->team_base.upload(P.team_base.data(), P.team_base.size(), st);
-        d->queue_off.upload(P.queue_off.data(), P.queue_off.size(), st);
-        d->queue.upload(P.queue.data(), P.queue.size(), st);
+        d->team_class.upload(P.team_class.data(), P.team_class.size(), st);
+        d->class_off.upload(P.class_off.data(), P.class_off.size(), st);
+        d->class_queue.upload(P.class_queue.data(), P.class_queue.size(), st);
+        d->log_off.upload(P.log_off.data(), P.log_off.size(), st);
+        d->class_next.alloc(std::max<size_t>(1, P.class_off.size() - 1));
+        d->claims.alloc(std::max(1, P.log_off.back()));
         CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
         b->phases.push_back(std::move(d));
     }
     b->abort_flag.alloc(1);
+    b->claim_failures.alloc(1);
     b->args.alloc(count);
     b->res.alloc(count);
     b->times.alloc(2 * (size_t)count);
@@ -1412,7 +1434,9 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
     }
     CK(cudaMemcpyAsync(b->args.p, a.data(), count * sizeof(pg::PcgArgs), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(b->abort_flag.p, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(b->claim_failures.p, 0, sizeof(int), st));
     CK(cudaMemsetAsync(b->times.p, 0, b->times.n * sizeof(unsigned long long), st));
+    const unsigned long long claim_timeout_ns = (unsigned long long)(o.wait_timeout_ms * 1e6);
     const bool mixed = o.precision == PG_PREC_MIXED;
     auto kernel_of = [&](int kind) {
         if (kind == 4)
@@ -1428,28 +1452,39 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
             const void* fk = kernel_of(kind);
             opt_in_smem(c, fk);
             int nb = 0;
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fk, pg::kMaxThreads, smem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fk, pg::kBatchThreads, smem));
             if (nb < 1 || nb * c->sms < grid_max)
                 throw Fail{PG_EUNSUPPORTED, "batch grid does not fit on the device"};
         }
         b->ok_precision = mixed ? 1 : 2;  // residency checked for this precision and size
         b->ok_smem = smem;
     }
-    // one persistent launch per phase, back to back, captured once per batch
-    // (and precision / shared-memory size) into a CUDA graph
+    // one persistent launch per phase, back to back (each after zeroing its
+    // queue counters and claim slots), captured once per batch (and
+    // precision / shared-memory size / time limit) into a CUDA graph
     auto launch_phases = [&](cudaStream_t s) -> cudaError_t {
         for (auto& ph : b->phases) {
             const void* fn = kernel_of(ph->kind);
-            pg::BatchArgs ba{b->args.p, ph->block_team.p, ph->team_base.p, ph->queue_off.p, ph->queue.p,
-                             b->times.p};
+            cudaError_t e = cudaMemsetAsync(ph->class_next.p, 0, ph->class_next.n * sizeof(int), s);
+            if (e == cudaSuccess)
+                e = cudaMemsetAsync(ph->claims.p, 0, ph->claims.n * sizeof(unsigned long long), s);
+            if (e != cudaSuccess) return e;
+            pg::BatchArgs ba{b->args.p,          ph->block_team.p,
+                             ph->team_base.p,    ph->team_class.p,
+                             ph->class_off.p,    ph->class_queue.p,
+                             ph->log_off.p,      ph->class_next.p,
+                             ph->claims.p,       b->times.p,
+                             b->abort_flag.p,    b->claim_failures.p,
+                             claim_timeout_ns};
             void* args[] = {&ba};
-            cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(ph->grid), dim3(pg::kMaxThreads), args, smem, s);
+            e = cudaLaunchCooperativeKernel(fn, dim3(ph->grid), dim3(pg::kBatchThreads), args, smem, s);
             if (e != cudaSuccess) return e;
         }
         return cudaSuccess;
     };
     const int prec_key = mixed ? 1 : 2;
-    if (!b->graph_failed && (!b->graph || b->graph_precision != prec_key || b->graph_smem != smem)) {
+    if (!b->graph_failed && (!b->graph || b->graph_precision != prec_key || b->graph_smem != smem ||
+                             b->graph_timeout_ns != claim_timeout_ns)) {
         if (b->graph) {
             cudaGraphExecDestroy(b->graph);
             b->graph = nullptr;
@@ -1470,6 +1505,7 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
         }
         b->graph_precision = prec_key;
         b->graph_smem = smem;
+        b->graph_timeout_ns = claim_timeout_ns;
     }
     if (b->graph)
         CK(cudaGraphLaunch(b->graph, st));
@@ -1485,7 +1521,11 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
     std::vector<unsigned long long> tm(2 * (size_t)count);
     CK(cudaMemcpyAsync(r.data(), b->res.p, count * sizeof(pg::PcgResult), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(tm.data(), b->times.p, tm.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    int claim_failures = 0;
+    CK(cudaMemcpyAsync(&claim_failures, b->claim_failures.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    if (claim_failures)
+        throw Fail{PG_ETIMEOUT, "a batch team's wait for its next plate ran out of time"};
     float ms_setup = 0, ms_solve = 0;
     CK(cudaEventElapsedTime(&ms_setup, c->ev[0], c->ev[1]));
     CK(cudaEventElapsedTime(&ms_solve, c->ev[1], c->ev[2]));
@@ -1498,7 +1538,7 @@ void run_batch(pg_batch* b, const pg_options& o, const float* const* F, double* 
         if (infos) {
             std::memset(&infos[i], 0, sizeof(pg_info));
             fill_info(&infos[i], r[i], b->plans[i].get(), plate_options(o, b->plans[i].get()),
-                      pg::kMaxThreads, a[i].L.total);
+                      pg::kBatchThreads, a[i].L.total);
             infos[i].status = r[i].status;
             infos[i].solve_ms = plate_ms[i];
             infos[i].plan_cached = 1;

@@ -302,8 +302,11 @@ int pg_solve_batch(pg_ctx* ctx, const pg_problem* probs, int count, const pg_opt
                    double* const* x_out, pg_info* infos, pg_batch_info* info);
 /* Host-only: the schedule pg_batch_create uses for plates of these node
  * counts on `sms` blocks with at most `cap` nodes per block: per plate its
- * phase, team size and team (index within the phase) [count each]; per
- * phase its grid [count, the first *phases_out entries used]. */
+ * phase, team size and predicted team (index within the phase) [count
+ * each]; per phase its grid [count, the first *phases_out entries used].
+ * At run time the teams of one size share one queue of their plates
+ * (largest estimated work first) and a free team takes the next one, so
+ * the team that solves a plate can differ from the prediction. */
 int pg_batch_schedule(const uint32_t* node_counts, int count, int sms, int cap, int32_t* plate_phase,
                       int32_t* plate_size, int32_t* plate_team, int32_t* phase_grid,
                       int32_t* phases_out);
