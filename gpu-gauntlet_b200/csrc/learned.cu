@@ -457,6 +457,15 @@ struct Op {
     // uniform structured mesh), so that one matrix serves all elements from
     // L1; the FP64 products (true residual, pairs) always use each element's
     int ke_stride;
+    // optional node-block form of the FP32 operator (sliced ELL): nodes in
+    // slices of 32, slice s owning slots [nm_off[s], nm_off[s + 1]); slot j
+    // holds, for each lane (node 32 s + lane), a neighbour column
+    // nm_col[32 j + lane] and the assembled 3x3 block K_(node, column) in
+    // nm_val[(9 j + q) 32 + lane] (row-major q), summed over the shared
+    // elements in FP64 and rounded once; padding slots have zero blocks.
+    const int* nm_off = nullptr;
+    const int* nm_col = nullptr;
+    const float* nm_val = nullptr;
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -485,18 +494,32 @@ __device__ void block_partials(double (&v)[K], double* parts) {
     }
 }
 
-// Sum of nb blocks' partials, the same fixed order in every block; every
-// thread of the block receives the K sums.
+// Sum of nb blocks' partials, the same fixed order in every block (thread
+// t adds partials t, t + blockDim.x, ..., then a fixed tree over lanes and
+// warps); every thread of the block receives the K sums.  All threads load
+// at once, so a grid of hundreds of blocks costs about one L2 round trip.
 template <int K>
 __device__ void reduce_parts(const double* parts, int nb, double (&out)[K]) {
+    __shared__ double red[K][32];
     __shared__ double res[K];
-    if (threadIdx.x < 32) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    double v[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = 0.0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < K; k++) v[k] += parts[i * K + k];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const double t = warp_sum(v[k]);
+        if (lane == 0) red[k][warp] = t;
+    }
+    __syncthreads();
+    if (warp == 0) {
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            double s = 0.0;
-            for (int i = threadIdx.x; i < nb; i += 32) s += parts[i * K + k];
-            s = warp_sum(s);
-            if (threadIdx.x == 0) res[k] = s;
+            const double t = warp_sum(lane < nw ? red[k][lane] : 0.0);
+            if (lane == 0) res[k] = t;
         }
     }
     __syncthreads();
@@ -527,6 +550,113 @@ __device__ __forceinline__ void kv_node(const Op& op, int n, GetV getv, float (&
     out[0] = op.cons[3 * n] ? getv(n, 0) : s0;
     out[1] = op.cons[3 * n + 1] ? getv(n, 1) : s1;
     out[2] = op.cons[3 * n + 2] ? getv(n, 2) : s2;
+}
+
+// (K v)_n from the node-block form (op.nm_* set): one pass over the node's
+// slots, all loads of a slot coalesced across the warp's 32 nodes.
+template <typename GetV>
+__device__ __forceinline__ void kv_block(const Op& op, int n, GetV getv, float (&out)[3]) {
+    const int s = n >> 5, lane = n & 31;
+    const int j1 = op.nm_off[s + 1];
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+#pragma unroll 3
+    for (int j = op.nm_off[s]; j < j1; j++) {
+        const int m = op.nm_col[32 * j + lane];
+        const float* B = op.nm_val + (size_t)288 * j + lane;
+        const float v0 = getv(m, 0), v1 = getv(m, 1), v2 = getv(m, 2);
+        s0 += B[0] * v0 + B[32] * v1 + B[64] * v2;
+        s1 += B[96] * v0 + B[128] * v1 + B[160] * v2;
+        s2 += B[192] * v0 + B[224] * v1 + B[256] * v2;
+    }
+    out[0] = op.cons[3 * n] ? getv(n, 0) : s0;
+    out[1] = op.cons[3 * n + 1] ? getv(n, 1) : s1;
+    out[2] = op.cons[3 * n + 2] ? getv(n, 2) : s2;
+}
+
+// (K v)_n by the node-block form when the operator has one, else by the
+// element gather.
+template <int NPE, typename GetV>
+__device__ __forceinline__ void kv(const Op& op, int n, GetV getv, float (&out)[3]) {
+    if (op.nm_off)
+        kv_block(op, n, getv, out);
+    else
+        kv_node<NPE>(op, n, getv, out);
+}
+
+constexpr int kMaxNbr = 32;  // node-block form: largest neighbour count
+
+// The distinct nodes of the elements around node n (n included), in
+// increasing order, into nb; their count, or -1 past kMaxNbr.
+template <int NPE>
+__device__ int node_nbrs(const Op& op, int n, int (&nb)[kMaxNbr]) {
+    int c = 0;
+    for (int q = op.inc_ptr[n]; q < op.inc_ptr[n + 1]; q++) {
+        const int e = op.inc_idx[q] >> 2;
+        for (int b = 0; b < NPE; b++) {
+            const int m = (int)op.el[(size_t)e * NPE + b];
+            int i = 0;
+            while (i < c && nb[i] < m) i++;
+            if (i < c && nb[i] == m) continue;
+            if (c == kMaxNbr) return -1;
+            for (int k = c; k > i; k--) nb[k] = nb[k - 1];
+            nb[i] = m;
+            c++;
+        }
+    }
+    return c;
+}
+
+// Node-block form, pass 1: the widest neighbour count of each slice of 32
+// nodes (the grid covers exactly Ns * 32 threads in blocks of whole warps);
+// *bad = 1 when some node has more than kMaxNbr neighbours.
+template <int NPE>
+__global__ void nm_width_kernel(Op op, int Ns, int* __restrict__ width, int* __restrict__ bad) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    int c = 0;
+    if (n < op.Nn) {
+        int nb[kMaxNbr];
+        c = node_nbrs<NPE>(op, n, nb);
+        if (c < 0) {
+            atomicOr(bad, 1);
+            c = 0;
+        }
+    }
+    c = __reduce_max_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0 && (n >> 5) < Ns) width[n >> 5] = c;
+}
+
+// Pass 2: columns and FP64-assembled blocks of every slot (padding slots:
+// column n, or 0 past the last node, and a zero block).
+template <int NPE>
+__global__ void nm_fill_kernel(Op op, int Ns, const int* __restrict__ off, int* __restrict__ col,
+                               float* __restrict__ val) {
+    constexpr int ND = 3 * NPE;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = n >> 5, lane = n & 31;
+    if (s >= Ns) return;
+    const int j0 = off[s], w = off[s + 1] - j0;
+    int nb[kMaxNbr];
+    int c = n < op.Nn ? node_nbrs<NPE>(op, n, nb) : 0;
+    if (c < 0) c = 0;
+    for (int j = 0; j < w; j++) {
+        double blk[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        int m = n < op.Nn ? n : 0;
+        if (j < c) {
+            m = nb[j];
+            for (int q = op.inc_ptr[n]; q < op.inc_ptr[n + 1]; q++) {
+                const int e = op.inc_idx[q] >> 2, k = op.inc_idx[q] & 3;
+                const double* Ke = op.ke64 + (size_t)e * ND * ND;
+                for (int b = 0; b < NPE; b++) {
+                    if ((int)op.el[(size_t)e * NPE + b] != m) continue;
+                    for (int r = 0; r < 3; r++)
+                        for (int cc = 0; cc < 3; cc++) blk[3 * r + cc] += Ke[(3 * k + r) * ND + 3 * b + cc];
+                }
+            }
+        }
+        const size_t slot = (size_t)(j0 + j);
+        col[32 * slot + lane] = m;
+        for (int q = 0; q < 9; q++) val[(9 * slot + q) * 32 + lane] = (float)blk[q];
+    }
 }
 
 __device__ __forceinline__ float binv_row(const float* B9, int d, float a, float b, float c) {
@@ -850,6 +980,7 @@ struct FArgs {
     double* x;
     float *r, *r_prev, *r1, *y, *r2, *z, *p0, *p1, *q;
     float *y2, *v2;  // the correction and its K product after odd sweeps (double buffer)
+    float* t;        // omega D^-1 r (modes 1 and 2), written with r
     double *pU, *pTR, *pA, *pB, *pC, *pD, *pI;
     FState* st;
     int G;
@@ -859,6 +990,13 @@ struct FArgs {
 
 __device__ __forceinline__ bool stop_test(const FArgs& a, double rr, double bn2) {
     return a.stop_rule == PG_STOP_RELATIVE ? rr < a.tol2 * bn2 : (rr < a.tol2 || rr < a.tol2 * bn2);
+}
+
+// t_n = omega D_n^-1 r_n, the first smoothing step, for the gathers of the
+// smoothing input (modes 1 and 2)
+__device__ __forceinline__ void write_t(const FArgs& a, int n, const float (&rv)[3]) {
+    const float* B9 = a.op.binv32 + 9 * n;
+    for (int d = 0; d < 3; d++) a.t[3 * n + d] = a.omega * binv_row(B9, d, rv[0], rv[1], rv[2]);
 }
 
 __global__ void fp_init_kernel(FArgs a) {
@@ -908,6 +1046,7 @@ __global__ void fp_update_kernel(FArgs a) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[1] = {0.0};
     if (n < a.op.Nn && !stop) {
+        float rv[3];
         for (int d = 0; d < 3; d++) {
             const int i = 3 * n + d;
             const float ri = a.r[i];
@@ -915,8 +1054,10 @@ __global__ void fp_update_kernel(FArgs a) {
             a.r_prev[i] = ri;
             const float rn = (float)((double)ri - alpha * (double)a.q[i]);
             a.r[i] = rn;
+            rv[d] = rn;
             acc[0] += (double)rn * rn;
         }
+        if (a.mode != 0) write_t(a, n, rv);
     }
     block_partials<1>(acc, a.pU);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -967,12 +1108,15 @@ __global__ void fp_true_res_kernel(FArgs a) {
                                                      Ke[d * ND + 3 * b + 2] * x2;
             }
         }
+        float rv[3];
         for (int d = 0; d < 3; d++) {
             const int i = 3 * n + d;
             const double rt = (double)a.F[i] - (a.op.cons[i] ? a.x[i] : kx[d]);
-            a.r[i] = (float)rt;
+            rv[d] = (float)rt;
+            a.r[i] = rv[d];
             acc[0] += rt * rt;
         }
+        if (a.mode != 0) write_t(a, n, rv);
     }
     block_partials<1>(acc, a.pTR);
 }
@@ -1020,12 +1164,10 @@ __global__ void fp_prep_kernel(FArgs a) {
     double acc[1] = {0.0};
     if (n < a.op.Nn) {
         const float* r = a.r;
-        const float om = a.omega;
-        auto tv = [&](int m, int d) {
-            return om * binv_row(a.op.binv32 + 9 * m, d, r[3 * m], r[3 * m + 1], r[3 * m + 2]);
-        };
+        const float* t = a.t;
+        auto tv = [&](int m, int d) { return t[3 * m + d]; };
         float u[3];
-        kv_node<NPE>(a.op, n, tv, u);
+        kv<NPE>(a.op, n, tv, u);
         const float sc[3] = {a.si0, a.si1, a.si2};
         // only mode 1 has a network (and its input image and pixel map)
         bf16* px = a.mode == 1 ? a.img_in + (size_t)a.node_pixel[n] * 16 : nullptr;
@@ -1039,10 +1181,22 @@ __global__ void fp_prep_kernel(FArgs a) {
     block_partials<1>(acc, a.pA);
 }
 
-// B: y = s_out N(r1) (0 on constrained DOFs) and v = K y (kept in a.r2);
-// partial sums of y.r1 and y.v for the correction's step.
+// The next smoothing sweep's correction at node n: w' = w + omega D^-1
+// (r1 - v), v = K w (0 on constrained DOFs).
+__device__ __forceinline__ void write_sweep(const FArgs& a, int n, const float (&w)[3], const float (&v)[3],
+                                            float* __restrict__ w_next) {
+    const int i = 3 * n;
+    const float* B9 = a.op.binv32 + 9 * n;
+    const float d0 = a.r1[i] - v[0], d1 = a.r1[i + 1] - v[1], d2 = a.r1[i + 2] - v[2];
+    for (int d = 0; d < 3; d++)
+        w_next[i + d] = a.op.cons[i + d] ? 0.f : w[d] + a.omega * binv_row(B9, d, d0, d1, d2);
+}
+
+// B: y = s_out N(r1) (0 on constrained DOFs) into a.y and v = K y into
+// a.r2; partial sums of y.r1 and y.v for the correction's step; w_next
+// (when the correction gets smoothing sweeps): the first sweep's w.
 template <int NPE>
-__global__ void fp_net_kernel(FArgs a) {
+__global__ void fp_net_kernel(FArgs a, float* __restrict__ w_next) {
     pgn::pdl_wait();
     FState* st = a.st;
     if (st->done || st->skip_net) return;
@@ -1053,49 +1207,44 @@ __global__ void fp_net_kernel(FArgs a) {
     };
     double acc[2] = {0.0, 0.0};
     if (n < a.op.Nn) {
-        float v[3];
-        kv_node<NPE>(a.op, n, yv, v);
+        float v[3], y[3];
+        kv<NPE>(a.op, n, yv, v);
         for (int d = 0; d < 3; d++) {
             const int i = 3 * n + d;
-            const float y = yv(n, d);
-            a.y[i] = y;
+            y[d] = yv(n, d);
+            a.y[i] = y[d];
             a.r2[i] = v[d];
-            acc[0] += (double)y * a.r1[i];
-            acc[1] += (double)y * v[d];
+            acc[0] += (double)y[d] * a.r1[i];
+            acc[1] += (double)y[d] * v[d];
         }
+        if (w_next) write_sweep(a, n, y, v, w_next);
     }
     block_partials<2>(acc, a.pB);
 }
 
-// One smoothing sweep on the network's correction: w' = w + S (r1 - v)
-// (v = K w from the previous pass), and v' = K w' (w' formed on the fly at
-// the neighbours); partial sums of w'.r1 and w'.v' for the step.
+// One smoothing sweep on the network's correction: v = K w for the w the
+// previous kernel formed (w = w_prev + omega D^-1 (r1 - K w_prev)), partial
+// sums of w.r1 and w.v for the step, and (w_next) the next sweep's w.
 template <int NPE>
-__global__ void fp_sweep_kernel(FArgs a, const float* __restrict__ w_in, const float* __restrict__ v_in,
-                                float* __restrict__ w_out, float* __restrict__ v_out) {
+__global__ void fp_sweep_kernel(FArgs a, const float* __restrict__ w_in, float* __restrict__ v_out,
+                                float* __restrict__ w_next) {
     pgn::pdl_wait();
     FState* st = a.st;
     if (st->done || st->skip_net) return;
-    const float om = a.omega;
-    auto wv = [&](int m, int d) {
-        const float* B9 = a.op.binv32 + 9 * m;
-        const int i = 3 * m;
-        return w_in[i + d] + om * binv_row(B9, d, a.r1[i] - v_in[i], a.r1[i + 1] - v_in[i + 1],
-                                           a.r1[i + 2] - v_in[i + 2]);
-    };
+    auto wv = [&](int m, int d) { return w_in[3 * m + d]; };
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     double acc[2] = {0.0, 0.0};
     if (n < a.op.Nn) {
-        float v[3];
-        kv_node<NPE>(a.op, n, wv, v);
+        float v[3], w[3];
+        kv<NPE>(a.op, n, wv, v);
         for (int d = 0; d < 3; d++) {
             const int i = 3 * n + d;
-            const float w = a.op.cons[i] ? 0.f : wv(n, d);
-            w_out[i] = w;
+            w[d] = w_in[i];
             v_out[i] = v[d];
-            acc[0] += (double)w * a.r1[i];
-            acc[1] += (double)w * v[d];
+            acc[0] += (double)w[d] * a.r1[i];
+            acc[1] += (double)w[d] * v[d];
         }
+        if (w_next) write_sweep(a, n, w, v, w_next);
     }
     block_partials<2>(acc, a.pB);
 }
@@ -1175,7 +1324,7 @@ __global__ void fp_dir_kernel(FArgs a) {
     double acc[2] = {0.0, 0.0};
     if (n < a.op.Nn) {
         float qv[3];
-        kv_node<NPE>(a.op, n, pv, qv);
+        kv<NPE>(a.op, n, pv, qv);
         for (int d = 0; d < 3; d++) {
             const int i = 3 * n + d;
             const float pi = pv(n, d);
@@ -1235,8 +1384,10 @@ struct FpcgSolver {
     Op op{};
     int npe = 4;
     float omega = 1.f;
-    Buf<float> F, r, r_prev, r1, y, r2, z, p0, p1, q, y2, v2;
+    Buf<float> F, r, r_prev, r1, y, r2, z, p0, p1, q, y2, v2, t;
     Buf<double> x, parts;
+    Buf<int> nm_off, nm_col;  // node-block form of the operator (op.nm_*)
+    Buf<float> nm_val;
     Buf<FState> st;
     cudaStream_t cap = nullptr;  // capture stream
     cudaGraphExec_t exec = nullptr;
@@ -1362,6 +1513,41 @@ __global__ void unpack_din_kernel(long P, const bf16* __restrict__ src, float* _
 int grid_nodes(int Nn) { return (Nn + 255) / 256; }
 
 // Buffers of a flexible-PCG solver for an operator with Nn nodes.
+// The node-block form of S's operator (Op::nm_*): slice widths on the
+// device, their offsets on the host, then the columns and blocks.  A mesh
+// with a node of more than kMaxNbr neighbours keeps the element gather.
+void build_node_blocks(FpcgSolver* S, cudaStream_t st) {
+    const int Nn = S->op.Nn;
+    if (Nn < 1 || !S->op.ke64) return;
+    const int Ns = (Nn + 31) / 32;
+    const int grid = (int)(((long)Ns * 32 + 255) / 256);
+    Buf<int> width, bad;
+    width.alloc(Ns);
+    bad.alloc(1);
+    bad.zero(st);
+    (S->npe == 4 ? nm_width_kernel<4> : nm_width_kernel<3>)<<<grid, 256, 0, st>>>(S->op, Ns, width.p, bad.p);
+    LCK(cudaGetLastError());
+    std::vector<int> w(Ns);
+    int hb = 0;
+    LCK(cudaMemcpyAsync(w.data(), width.p, Ns * sizeof(int), cudaMemcpyDeviceToHost, st));
+    LCK(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    LCK(cudaStreamSynchronize(st));
+    if (hb) return;
+    std::vector<int> off(Ns + 1, 0);
+    for (int k = 0; k < Ns; k++) off[k + 1] = off[k] + w[k];
+    S->nm_off.alloc(Ns + 1);
+    S->nm_col.alloc(32 * (size_t)std::max(1, off[Ns]));
+    S->nm_val.alloc(288 * (size_t)std::max(1, off[Ns]));
+    LCK(cudaMemcpyAsync(S->nm_off.p, off.data(), (Ns + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
+    (S->npe == 4 ? nm_fill_kernel<4> : nm_fill_kernel<3>)<<<grid, 256, 0, st>>>(S->op, Ns, S->nm_off.p,
+                                                                              S->nm_col.p, S->nm_val.p);
+    LCK(cudaGetLastError());
+    LCK(cudaStreamSynchronize(st));  // off leaves scope
+    S->op.nm_off = S->nm_off.p;
+    S->op.nm_col = S->nm_col.p;
+    S->op.nm_val = S->nm_val.p;
+}
+
 void fpcg_init(FpcgSolver* S, pg_ctx* c, const Op& op, int npe, float omega) {
     S->ctx = c;
     S->op = op;
@@ -1370,7 +1556,7 @@ void fpcg_init(FpcgSolver* S, pg_ctx* c, const Op& op, int npe, float omega) {
     cudaStream_t st = pgi::ctx_stream(c);
     const size_t n3 = 3 * (size_t)op.Nn;
     for (Buf<float>* b : {&S->F, &S->r, &S->r_prev, &S->r1, &S->y, &S->r2, &S->z, &S->p0, &S->p1, &S->q, &S->y2,
-                          &S->v2}) {
+                          &S->v2, &S->t}) {
         b->alloc(n3);
         b->zero(st);
     }
@@ -1378,6 +1564,7 @@ void fpcg_init(FpcgSolver* S, pg_ctx* c, const Op& op, int npe, float omega) {
     S->parts.alloc(14 * (size_t)grid_nodes(op.Nn));
     S->st.alloc(1);
     LCK(cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
+    build_node_blocks(S, st);
     LCK(cudaStreamSynchronize(st));
 }
 
@@ -1404,16 +1591,21 @@ void queue_body(FpcgSolver* S, const FArgs& a, int mode, pg_net* n, Workspace* w
     if (mode == 1) {
         net_forward(n, w, cs, &S->st.p->skip_net, pdl);
         mark(4);
-        launch(pdl, q4 ? fp_net_kernel<4> : fp_net_kernel<3>, dim3(G), dim3(256), 0, cs, a);
-        float *wi = a.y, *vi = a.r2, *wo = a.y2, *vo = a.v2;
-        for (int k = 0; k < kCorrectionSweeps; k++) {
+        // w_0 = y in a.y with v_0 in a.r2; sweep k's w_k alternates between
+        // a.y2 (odd k) and a.y, its v_k between a.v2 and a.r2
+        float* w_cur = a.y;
+        float* v_cur = a.r2;
+        float* w_nxt = kCorrectionSweeps > 0 ? a.y2 : nullptr;
+        launch(pdl, q4 ? fp_net_kernel<4> : fp_net_kernel<3>, dim3(G), dim3(256), 0, cs, a, w_nxt);
+        for (int k = 1; k <= kCorrectionSweeps; k++) {
+            w_cur = w_nxt;
+            v_cur = (k & 1) ? a.v2 : a.r2;
+            w_nxt = k < kCorrectionSweeps ? (w_cur == a.y2 ? a.y : a.y2) : nullptr;
             launch(pdl, q4 ? fp_sweep_kernel<4> : fp_sweep_kernel<3>, dim3(G), dim3(256), 0, cs, a,
-                   (const float*)wi, (const float*)vi, wo, vo);
-            std::swap(wi, wo);
-            std::swap(vi, vo);
+                   (const float*)w_cur, v_cur, w_nxt);
         }
-        ac.y = wi;
-        ac.r2 = vi;
+        ac.y = w_cur;
+        ac.r2 = v_cur;
     } else {
         mark(4);
     }
@@ -1458,6 +1650,7 @@ FArgs make_fargs(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, Worksp
     a.r2 = S->r2.p;
     a.y2 = S->y2.p;
     a.v2 = S->v2.p;
+    a.t = S->t.p;
     a.z = S->z.p;
     a.p0 = S->p0.p;
     a.p1 = S->p1.p;
