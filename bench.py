@@ -11,7 +11,9 @@ coarse set-up ran in the warm-up and is cached).  Seven methods are timed
 solve for the whole job (lower is better).  ``e2e`` is the same through
 the public C ABI (pg_solve) from host buffers, copies included;
 ``first_solve_new_mesh_ms`` a first pg_solve in a new context (the plan's
-set-up included).  L2 is flushed (256 MiB write) between timed steps; each
+set-up included; ``first_solve_new_mesh_phases`` splits it as the library
+times it: partition plan, coarse space, eigenvalue estimate, device set-up
+and solve).  L2 is flushed (256 MiB write) between timed steps; each
 step is timed with CUDA events on the solver's stream.  ``roofline``
 compares the PCG kernel's algorithmic bytes per second with the measured
 HBM copy peak and with an in-run L2-resident copy.
@@ -558,9 +560,14 @@ def run_plategpu(args, world, rank, local):
     cold_ctx = _lib.Context(local)
     prob.set_F(wl.F)
     t0 = time.perf_counter()
-    cold_ctx.solve(prob, H["opts"])
+    _xc, cold_info = cold_ctx.solve(prob, H["opts"])
     cold_ms = max_over_ranks(world, (time.perf_counter() - t0) * 1e3, local)
     cold_ctx.close()
+    # its one-time steps as the library times them (host wall time; the
+    # device set-up and solve by CUDA events)
+    cold_phases = {"partition_plan_ms": cold_info.plan_ms, "coarse_space_ms": cold_info.coarse_ms,
+                   "eigenvalue_estimate_ms": cold_info.eigen_ms, "device_setup_ms": cold_info.setup_ms,
+                   "device_solve_ms": cold_info.solve_ms}
     # the same cold path in two steps: the plan (host partition, device
     # copies) and its first device solve (element matrices, block inverses,
     # coarse space, eigenvalue estimate, then the solve)
@@ -628,6 +635,7 @@ def run_plategpu(args, world, rank, local):
                 "d2h_bytes_per_step": 8 * n + 64},
         "first_solve_new_mesh_ms": cold_ms,
         "first_solve_new_mesh_split": cold_split,
+        "first_solve_new_mesh_phases": cold_phases,
         # one persistent PCG launch per timed solve: the plan's set-up kernels
         # (element matrices, block inverses, task blocks) ran in the warm-up
         "gpu_launches": args.steps,
@@ -654,7 +662,10 @@ def run_plategpu(args, world, rank, local):
     ctx.close()
 
 
-LEARNED_TOL = 1e-6  # relative FP64 true residual of the learned flexible PCG (see learned_bench)
+# relative FP64 true residual of the learned flexible PCG and of the same
+# loop without the network: at 1e-6 one of the 512 held-out loads ended at
+# 1.02e-6 FP64 error; 5e-7 keeps every load under the 1e-6 bar
+LEARNED_TOL = 5e-7
 
 
 def learned_bench(args, ctx, stream, flush, local, wl, chk, extra_F):

@@ -2,7 +2,7 @@
 // steps of build_coarse in plan.cpp, which the host keeps for batches):
 //   coarse_assemble_kernel  A_c = P^T K P from the FP64 element matrices,
 //                           one thread per element, FP64 atomics into A_c
-//   coarse_factor_kernel    one block: left-looking Cholesky of A_c with
+//   coarse_factor_kernel    one block: right-looking Cholesky of A_c with
 //                           numerically dependent modes dropped (pivot <=
 //                           1e-13 max diagonal), the inverse of L, and
 //                           A_c^-1 = L^-T L^-1
@@ -56,104 +56,133 @@ __global__ void coarse_assemble_kernel(int Ne, int C, const float* __restrict__ 
         }
 }
 
-// sum_{k in [k0, k1)} a[k] b[k] in four interleaved partial sums
-__device__ __forceinline__ double cdot4(const double* a, const double* b, int k0, int k1) {
-    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-    int k = k0;
-    for (; k + 4 <= k1; k += 4) {
-        s0 += a[k] * b[k];
-        s1 += a[k + 1] * b[k + 1];
-        s2 += a[k + 2] * b[k + 2];
-        s3 += a[k + 3] * b[k + 3];
-    }
-    for (; k < k1; k++) s0 += a[k] * b[k];
-    return (s0 + s1) + (s2 + s3);
-}
-
 constexpr int kCoarseThreads = 1024;
 
-// One block of kCoarseThreads threads.  L, Lt and Ainv ([C][C]) start
-// zeroed; keep [C] receives 1 for kept modes; *dropped the count of
-// dropped ones.
+// Dynamic shared memory of coarse_factor_kernel: a column of C doubles, and
+// two 32 x 65 tiles for the product of phase 3.
+__host__ __device__ constexpr size_t coarse_factor_smem(int C) {
+    return (size_t)(C > 2 * 32 * 65 ? C : 2 * 32 * 65) * sizeof(double);
+}
+
+// Block-wide maximum of v (every thread receives it).
+__device__ __forceinline__ double block_max(double v, double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmax(m, red[w]);
+    return m;
+}
+
+// One block of kCoarseThreads threads, dynamic shared memory coarse_factor_smem(C).
+// L, Lt and Ainv ([C][C], row-major) start zeroed; keep [C] receives 1 for
+// kept modes; *dropped the count of dropped ones.
+//   1. right-looking Cholesky of A_c in L (lower triangle), column by
+//      column: the pivot, the column scaled below it (staged in shared
+//      memory), then the trailing update row by row (a warp per row,
+//      lanes along the row, so every access is coalesced); a mode whose
+//      pivot is <= 1e-13 max diagonal is dropped (its column zero)
+//   2. Y = L^-1 by forward substitution over all columns at once, kept
+//      transposed (Lt[c][r] = Y[r][c]): at step i row i of Y is scaled by
+//      1 / L_ii and subtracted from the rows below (warps over columns c,
+//      lanes along r); dropped rows are zero
+//   3. A_c^-1 = Y^T Y: entry (i, j), j <= i, is Lt[i] . Lt[j] over k >= i,
+//      in 32 x 32 tiles staged through shared memory
 __global__ void __launch_bounds__(kCoarseThreads) coarse_factor_kernel(int C, const double* __restrict__ Ac,
                                                                        double* L, double* Lt, double* Ainv,
                                                                        int* keep, int* dropped) {
+    extern __shared__ double col[];  // [C] (phases 1, 2), two tiles (phase 3)
     __shared__ double red[kCoarseThreads / 32];
-    __shared__ double s_val;
-    __shared__ int s_keep, s_dropped;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // largest diagonal entry
+    __shared__ double s_inv;
+    __shared__ int s_keep;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
     double mx = 0.0;
     for (int i = tid; i < C; i += blockDim.x) mx = fmax(mx, Ac[(size_t)i * C + i]);
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if (lane == 0) red[warp] = mx;
+    const double dmax = block_max(mx, red);
+    for (int i = warp; i < C; i += nw)
+        for (int k = lane; k <= i; k += 32) L[(size_t)i * C + k] = Ac[(size_t)i * C + k];
+    int nd = 0;
     __syncthreads();
-    if (tid == 0) {
-        double m = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmax(m, red[w]);
-        s_val = m;
-        s_dropped = 0;
-    }
-    __syncthreads();
-    const double dmax = s_val;
-    __syncthreads();
-    // left-looking Cholesky, column by column
+    // 1. Cholesky
     for (int j = 0; j < C; j++) {
-        const double* lj = L + (size_t)j * C;
-        double part = 0.0;
-        for (int k = tid; k < j; k += blockDim.x) part += lj[k] * lj[k];
-        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-        if (lane == 0) red[warp] = part;
-        __syncthreads();
         if (tid == 0) {
-            double s = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
-            const double d = Ac[(size_t)j * C + j] - s;
+            const double d = L[(size_t)j * C + j];
             s_keep = d > 1e-13 * dmax;
             keep[j] = s_keep;
-            if (s_keep) {
-                s_val = sqrt(d);
-                L[(size_t)j * C + j] = s_val;
-            } else {
-                s_dropped++;
-            }
+            const double ljj = s_keep ? sqrt(d) : 0.0;
+            L[(size_t)j * C + j] = ljj;
+            s_inv = s_keep ? 1.0 / ljj : 0.0;
         }
         __syncthreads();
-        if (s_keep) {
-            const double ljj = s_val;
-            for (int i = j + 1 + tid; i < C; i += blockDim.x) {
-                const double* li = L + (size_t)i * C;
-                L[(size_t)i * C + j] = (Ac[(size_t)i * C + j] - cdot4(li, lj, 0, j)) / ljj;
-            }
+        const bool kj = s_keep != 0;
+        nd += kj ? 0 : 1;
+        const double inv = s_inv;
+        for (int i = j + 1 + tid; i < C; i += blockDim.x) {
+            const double v = L[(size_t)i * C + j] * inv;  // 0 for a dropped mode
+            L[(size_t)i * C + j] = v;
+            col[i] = v;
         }
         __syncthreads();
+        if (kj)
+            for (int i = j + 1 + warp; i < C; i += nw) {
+                const double ci = col[i];
+                double* li = L + (size_t)i * C;
+                for (int k = j + 1 + lane; k <= i; k += 32) li[k] -= ci * col[k];
+            }
+        __syncthreads();
     }
-    if (tid == 0) *dropped = s_dropped;
-    // inverse of L, kept transposed (Lt[j][k] = (L^-1)[k][j]): column j of
-    // L^-1 by forward substitution, one thread per column
-    for (int j = tid; j < C; j += blockDim.x) {
-        if (!keep[j]) continue;
-        double* lt = Lt + (size_t)j * C;
-        lt[j] = 1.0 / L[(size_t)j * C + j];
-        for (int i = j + 1; i < C; i++) {
-            if (!keep[i]) continue;
-            const double* li = L + (size_t)i * C;
-            lt[i] = -cdot4(li, lt, j, i) / li[i];
-        }
-    }
+    if (tid == 0) *dropped = nd;
+    // 2. Y = L^-1, transposed into Lt
+    for (int i = tid; i < C; i += blockDim.x) Lt[(size_t)i * C + i] = keep[i] ? 1.0 : 0.0;
     __syncthreads();
-    // A_c^-1 = L^-T L^-1: entry (i, j), j <= i, is Lt[i] . Lt[j] over k >= i
-    const long pairs = (long)C * (C + 1) / 2;
-    for (long q = tid; q < pairs; q += blockDim.x) {
-        // q -> (i, j) with q = i (i + 1) / 2 + j
-        int i = (int)((sqrt(8.0 * (double)q + 1.0) - 1.0) * 0.5);
-        while ((long)i * (i + 1) / 2 > q) i--;
-        while ((long)(i + 1) * (i + 2) / 2 <= q) i++;
-        const int j = (int)(q - (long)i * (i + 1) / 2);
-        const double s = cdot4(Lt + (size_t)i * C, Lt + (size_t)j * C, i, C);
-        Ainv[(size_t)i * C + j] = s;
-        Ainv[(size_t)j * C + i] = s;
+    for (int i = 0; i < C; i++) {
+        const double lii = L[(size_t)i * C + i];
+        const double inv = lii > 0.0 ? 1.0 / lii : 0.0;
+        // row i of Y (column i of Lt, entries c <= i) scaled; below-diagonal
+        // column i of L staged
+        for (int c = tid; c <= i; c += blockDim.x) Lt[(size_t)c * C + i] *= inv;
+        for (int r = i + 1 + tid; r < C; r += blockDim.x) col[r] = L[(size_t)r * C + i];
+        __syncthreads();
+        for (int c = warp; c <= i; c += nw) {
+            double* ltc = Lt + (size_t)c * C;
+            const double yic = ltc[i];
+            if (yic != 0.0)
+                for (int r = i + 1 + lane; r < C; r += 32) ltc[r] -= col[r] * yic;
+        }
+        __syncthreads();
     }
+    // 3. A_c^-1 = L^-T L^-1: entry (i, j), j <= i, is Lt[i] . Lt[j] over
+    //    k >= i; 32 x 32 tiles of entries (a thread each), the rows of Lt
+    //    they need staged in shared memory 64 columns at a time
+    __syncthreads();
+    double* ta = col;                 // [32][65] rows I0 .. I0 + 31 of Lt
+    double* tb = col + 32 * 65;       // [32][65] rows J0 .. J0 + 31
+    const int ty = tid >> 5, tx = tid & 31;  // entry (I0 + ty, J0 + tx)
+    const int nt = (C + 31) / 32;
+    for (int I = 0; I < nt; I++)
+        for (int J = 0; J <= I; J++) {
+            const int I0 = 32 * I, J0 = 32 * J;
+            double acc = 0.0;
+            for (int k0 = I0; k0 < C; k0 += 64) {
+                for (int q = tid; q < 32 * 64; q += blockDim.x) {
+                    const int rr = q >> 6, kk = q & 63, k = k0 + kk;
+                    const int ia = I0 + rr, ib = J0 + rr;
+                    ta[rr * 65 + kk] = (ia < C && k < C) ? Lt[(size_t)ia * C + k] : 0.0;
+                    tb[rr * 65 + kk] = (ib < C && k < C) ? Lt[(size_t)ib * C + k] : 0.0;
+                }
+                __syncthreads();
+#pragma unroll 8
+                for (int kk = 0; kk < 64; kk++) acc += ta[ty * 65 + kk] * tb[tx * 65 + kk];
+                __syncthreads();
+            }
+            const int i = I0 + ty, j = J0 + tx;
+            if (i < C && j <= i) {
+                Ainv[(size_t)i * C + j] = acc;
+                Ainv[(size_t)j * C + i] = acc;
+            }
+        }
 }
 
 // Part rows of A_c^-1: out64/out32[r][k] = Ainv[src[r]][k].

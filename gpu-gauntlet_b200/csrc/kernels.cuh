@@ -782,8 +782,9 @@ constexpr int kLeanThreads = 512;
 constexpr int kBatchThreads = 512;
 
 // Per-phase SM cycles of thread 0 of block 0, when timing is requested:
-// 0 K.u, 1 gather + dots + publish w, 2 block reduction, 3 publish partials,
-// 4 exchange wait, 5 decisions, 6 coarse solve, 7 vector update (and the
+// 0 K.u, 1 gather + dots + publish w, 2 block reduction and publishing the
+// partials, 3 the Chebyshev smoother's K t, 4 exchange wait, 5 the barrier
+// after the decision, 6 thread 0's decision, 7 vector updates (and the
 // residual replacement rounds of the mixed mode).
 struct PhaseClock {
     bool on;
@@ -1494,28 +1495,31 @@ template <int NPE, typename T, bool MIXED>
 __global__ void __launch_bounds__(kBatchThreads, 1) pcg_batch_kernel(const __grid_constant__ BatchArgs b) {
     extern __shared__ __align__(16) unsigned char sm[];
     volatile int* s_plate = (volatile int*)sm;  // between plates the shared memory is free
-    const int team = b.block_team[blockIdx.x];
-    const int g = (int)blockIdx.x - b.team_base[team];
-    const int cls = b.team_class[team];
-    const int q0 = b.class_off[cls], qn = b.class_off[cls + 1] - q0;
-    unsigned long long* slots = b.claims + b.log_off[team];
-    const int nslots = b.log_off[team + 1] - b.log_off[team];
-    for (int k = 0; k < nslots; k++) {
+    const int g = (int)blockIdx.x - b.team_base[b.block_team[blockIdx.x]];
+    for (int k = 0;; k++) {
         if (threadIdx.x == 0) {
+            // the team's class queue and claim slots, re-read each time so
+            // that only g and k stay live across the plate's solve
+            const int team = b.block_team[blockIdx.x], cls = b.team_class[team];
+            const int q0 = b.class_off[cls], qn = b.class_off[cls + 1] - q0;
+            const int lo = b.log_off[team];
             unsigned pos = (unsigned)qn;  // past the end: no plate
-            if (g == 0) {
-                pos = (unsigned)atomicAdd(b.class_next + cls, 1);
-                st_relaxed(slots + k, ((unsigned long long)(k + 1) << 32) | pos);
-            } else {
-                Waiter wt;
-                wt.start(b.timeout_ns, b.abort_flag, b.claim_failures);
-                for (;;) {
-                    const unsigned long long v = ld_relaxed(slots + k);
-                    if ((unsigned)(v >> 32) == (unsigned)(k + 1)) {
-                        pos = (unsigned)v;
-                        break;
+            if (k < b.log_off[team + 1] - lo) {
+                unsigned long long* slot = b.claims + lo + k;
+                if (g == 0) {
+                    pos = (unsigned)atomicAdd(b.class_next + cls, 1);
+                    st_relaxed(slot, ((unsigned long long)(k + 1) << 32) | pos);
+                } else {
+                    Waiter wt;
+                    wt.start(b.timeout_ns, b.abort_flag, b.claim_failures);
+                    for (;;) {
+                        const unsigned long long v = ld_relaxed(slot);
+                        if ((unsigned)(v >> 32) == (unsigned)(k + 1)) {
+                            pos = (unsigned)v;
+                            break;
+                        }
+                        if (!wt.keep_going()) break;
                     }
-                    if (!wt.keep_going()) break;
                 }
             }
             *s_plate = pos < (unsigned)qn ? b.class_queue[q0 + pos] : -1;

@@ -1341,6 +1341,17 @@ __global__ void fp_dir_kernel(FArgs a) {
     }
 }
 
+// y = K x by the flexible PCG's operator (pg_learned_apply_k)
+template <int NPE>
+__global__ void apply_op_kernel(Op op, const float* __restrict__ x, float* __restrict__ y) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= op.Nn) return;
+    auto xv = [&](int m, int d) { return x[3 * m + d]; };
+    float v[3];
+    kv<NPE>(op, n, xv, v);
+    for (int d = 0; d < 3; d++) y[3 * n + d] = v[d];
+}
+
 __global__ void fp_tick_kernel(FArgs a, cudaGraphConditionalHandle h, int in_graph) {
     pgn::pdl_wait();
     FState* st = a.st;
@@ -2382,6 +2393,25 @@ int pg_learned_solve(pg_learned* L, const pg_options* opt, int mode, const float
     const int st = lguarded(L->ctx, [&] { learned_solve(L, opt, mode, F, true, x_out, info, stats); });
     if (info) info->status = st;
     return st;
+}
+
+int pg_learned_apply_k(pg_learned* L, const float* x, float* y) {
+    if (!L) return PG_EINVAL;
+    return lguarded(L->ctx, [&] {
+        if (!x || !y) throw LFail{PG_EINVAL, "x / y is NULL"};
+        const size_t n3 = 3 * (size_t)L->S.op.Nn;
+        if (n3 == 0) return;
+        cudaStream_t st = pgi::ctx_stream(L->ctx);
+        Buf<float> dx, dy;
+        dx.alloc(n3);
+        dy.alloc(n3);
+        LCK(cudaMemcpyAsync(dx.p, x, n3 * sizeof(float), cudaMemcpyHostToDevice, st));
+        const int grid = grid_nodes(L->S.op.Nn);
+        (L->S.npe == 4 ? apply_op_kernel<4> : apply_op_kernel<3>)<<<grid, 256, 0, st>>>(L->S.op, dx.p, dy.p);
+        LCK(cudaGetLastError());
+        LCK(cudaMemcpyAsync(y, dy.p, n3 * sizeof(float), cudaMemcpyDeviceToHost, st));
+        LCK(cudaStreamSynchronize(st));
+    });
 }
 
 }  // extern "C"

@@ -575,7 +575,10 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
                 hp.Ne, C, pl->mesh_nodes.p, pl->mesh_elements.p, pl->cons.p, owner.p, geom.p, pl->ke64.p, Ac.p);
         CK(cudaGetLastError());
     }
-    pg::coarse_factor_kernel<<<1, pg::kCoarseThreads, 0, st>>>(C, Ac.p, L.p, Lt.p, Ainv.p, keep.p, dropped.p);
+    const size_t fsm = pg::coarse_factor_smem(C);
+    if (fsm > 48 * 1024)
+        CK(cudaFuncSetAttribute(pg::coarse_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+    pg::coarse_factor_kernel<<<1, pg::kCoarseThreads, fsm, st>>>(C, Ac.p, L.p, Lt.p, Ainv.p, keep.p, dropped.p);
     CK(cudaGetLastError());
     const int rows = (int)hp.ainv_src.size();
     pl->ainv64.alloc((size_t)rows * C);
@@ -637,11 +640,25 @@ void chebyshev2(double lambda_max, double* a, double* b) {
 // Queues setup + persistent PCG on the context stream, then waits for the
 // result record (one small readback).  F must already be in pl->F.
 // Coarse data and the smoother's eigenvalue, built once per plan on first use.
-void prepare_plan_data(pg_ctx* c, Plan* pl, const pg_options& o) {
+// info (optional) receives the host wall time of the coarse space and of
+// the eigenvalue estimate (0 when the plan already had them).
+void prepare_plan_data(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info = nullptr) {
     if (o.smoother == PG_SMOOTHER_CHEBYSHEV && pl->hp.rings != 2)
         throw Fail{PG_EINVAL, "the Chebyshev smoother needs a plan made with it (2-ring halo)"};
-    if (o.preconditioner == PG_PRECOND_TWO_LEVEL) ensure_coarse(c, pl);
-    if (o.smoother == PG_SMOOTHER_CHEBYSHEV) ensure_smoother(c, pl);
+    using clk = std::chrono::steady_clock;
+    auto ms_since = [](clk::time_point t0) {
+        return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+    };
+    auto t0 = clk::now();
+    if (o.preconditioner == PG_PRECOND_TWO_LEVEL && !pl->hp.coarse) {
+        ensure_coarse(c, pl);
+        if (info) info->coarse_ms = ms_since(t0);
+    }
+    t0 = clk::now();
+    if (o.smoother == PG_SMOOTHER_CHEBYSHEV && !(pl->lambda_max > 0)) {
+        ensure_smoother(c, pl);
+        if (info) info->eigen_ms = ms_since(t0);
+    }
 }
 
 // prepare_plan_data for many plans (a batch): the eigenvalue estimates run on
@@ -864,7 +881,7 @@ void run_solve(pg_ctx* c, Plan* pl, const pg_options& o, pg_info* info, void* x_
         threads = std::min(wide ? pg::kMaxThreads : pg::kLeanThreads, std::max(128, (hp.max_ntask + 31) / 32 * 32));
     }
     const bool lean = threads <= pg::kLeanThreads;
-    prepare_plan_data(c, pl, o);
+    prepare_plan_data(c, pl, o, info);
     int ke_mode = 0;
     bool ainv_smem = false;
     const pg::SmemLayout L = choose_layout(c, hp, o, &ke_mode, &ainv_smem);
@@ -1813,13 +1830,19 @@ int pg_solve(pg_ctx* c, const pg_problem* p, const pg_options* opt, double* x_ou
         }
         const int G = o.ctas ? std::min(o.ctas, (int)p->node_count) : auto_ctas(c, (int)p->node_count);
         bool cached = false;
+        const auto tp = std::chrono::steady_clock::now();
         Plan* pl = get_plan(c, *p, G, halo_rings(o), &cached);
+        const double plan_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp).count();
         ensure_staging(c, n);
         std::memcpy(c->hF, p->F, n * sizeof(float));
         CK(cudaMemcpyAsync(pl->F.p, c->hF, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
         solve_with_fallback(c, pl, o, info, c->hx, cudaMemcpyDeviceToHost);
         std::memcpy(x_out, c->hx, n * sizeof(double));
-        if (info) info->plan_cached = cached ? 1 : 0;
+        if (info) {
+            info->plan_cached = cached ? 1 : 0;
+            info->plan_ms = cached ? 0.0 : plan_ms;
+        }
     });
 }
 

@@ -36,7 +36,7 @@ EXPORTED = ("pg_options_default", "pg_is_available", "pg_create", "pg_destroy", 
             "pg_net_get_params", "pg_net_forward", "pg_net_backward", "pg_net_adam_step",
             "pg_learned_create", "pg_learned_destroy", "pg_learned_make_pairs",
             "pg_train_options_default", "pg_learned_train", "pg_learned_loss",
-            "pg_learned_solve_device", "pg_learned_solve")
+            "pg_learned_solve_device", "pg_learned_solve", "pg_learned_apply_k")
 
 PG_TRAIN_MAX_EPOCHS = 256
 # pg_learned_solve modes
@@ -134,6 +134,10 @@ class PgInfo(C.Structure):
         ("trace_ns", C.c_double * 6),
         ("smoother_lambda_max", C.c_double),
         ("global_path", C.c_int32),
+        ("reserved", C.c_int32),
+        ("plan_ms", C.c_double),
+        ("coarse_ms", C.c_double),
+        ("eigen_ms", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -292,6 +296,8 @@ def load() -> C.CDLL:
     L.pg_learned_solve.argtypes = [P, C.POINTER(PgOptions), I, P, P, C.POINTER(PgInfo),
                                    C.POINTER(PgLearnedStats)]
     L.pg_learned_solve.restype = I
+    L.pg_learned_apply_k.argtypes = [P, P, P]
+    L.pg_learned_apply_k.restype = I
     _lib = L
     return L
 
@@ -687,6 +693,13 @@ class Learned:
         self.ctx._check(self.ctx.L.pg_learned_solve(self.h, C.byref(opts), int(mode), _ptr(F), _ptr(x),
                                                     C.byref(info), C.byref(stats)))
         return x, info, stats
+
+    def apply_k(self, x):
+        """K x (FP32) by the operator the flexible PCG applies."""
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.zeros(self.n, np.float32)
+        self.ctx._check(self.ctx.L.pg_learned_apply_k(self.h, _ptr(x), _ptr(y)))
+        return y
 
     def close(self):
         if getattr(self, "h", None):

@@ -188,6 +188,13 @@ typedef struct pg_info {
                                      residual stop; block Jacobi, or damped block-Jacobi
                                      smoothing steps when the two-level preconditioner or
                                      the Chebyshev smoother was asked for */
+    int32_t reserved;
+    double plan_ms;               /* host wall time in this call of: building the partition
+                                     plan (pg_solve; 0 when the plan was cached), */
+    double coarse_ms;             /* the two-level coarse space (A_c on the device, its
+                                     factorisation and inverse; 0 once done for the plan), */
+    double eigen_ms;              /* the Chebyshev smoother's lambda_max estimate (0 once
+                                     done for the plan) */
 } pg_info;
 
 typedef struct pg_ctx pg_ctx;
@@ -515,6 +522,12 @@ int pg_learned_solve_device(pg_learned* learned, const pg_options* opt, int mode
                             double* x_dev, pg_info* info, pg_learned_stats* stats);
 int pg_learned_solve(pg_learned* learned, const pg_options* opt, int mode, const float* F, double* x_out,
                      pg_info* info, pg_learned_stats* stats);
+
+/* y = K x by the FP32 operator the learned solver's flexible PCG applies
+ * (the node-block form of K, summed in FP64 and rounded once, where every
+ * node has at most 32 neighbours; else the element gather), constrained
+ * rows replaced by the identity.  x, y: host [3n] float. */
+int pg_learned_apply_k(pg_learned* learned, const float* x, float* y);
 
 #ifdef __cplusplus
 }

@@ -236,21 +236,53 @@ def test_committed_network_on_held_out_loads(gpu_ctx, oracle, c2):
     ls.close()
 
 
-def test_block_jacobi_mode_matches_plain_pcg(gpu_ctx, oracle, small):
-    wl = small
-    ls = learned.LearnedSolver(gpu_ctx, wl)
-    xt = truth_of(oracle, wl, [wl.F])[0]
-    x, info, st = ls.learned.solve(learned.solve_options(1e-8), wl.F, mode=_lib.LEARNED_BLOCK_JACOBI)
+def test_block_jacobi_mode_matches_plain_pcg(gpu_ctx, oracle, small, c2):
+    """Mode 0 is block-Jacobi PCG in the flexible loop: it meets the error
+    bar, and on plate_q4_141 its iteration count at ||r||/||b|| < 1e-6 is
+    that of the persistent FP64 PCG within 10%.  (On the 32 x 32 plate FP32
+    rounding sets the count near 1e-6: the persistent kernel's own mixed
+    precision needs 44% more iterations than FP64 there.)"""
+    ls = learned.LearnedSolver(gpu_ctx, small)
+    xt = truth_of(oracle, small, [small.F])[0]
+    x, info, st = ls.learned.solve(learned.solve_options(1e-8), small.F, mode=_lib.LEARNED_BLOCK_JACOBI)
     assert info.converged and rel_err(x, xt) < 1e-6
-    # the iteration count of plain PCG at a stop FP32 vectors resolve easily
-    # (FP32 rounding slows the recursion near 1e-7 and below)
-    x6, info6, _ = ls.learned.solve(learned.solve_options(1e-6), wl.F, mode=_lib.LEARNED_BLOCK_JACOBI)
-    pr = _lib.Problem(wl.mesh, wl.material, wl.coloring, wl.F, wl.cons_mask)
-    _x1, one = gpu_ctx.solve(pr, _lib.make_options(tolerance=1e-6, max_iterations=20000,
-                                                   stop_rule=_lib.PG_STOP_RELATIVE))
-    assert abs(info6.iterations - one.iterations) <= 0.1 * one.iterations
     assert st.network_iterations == 0
     ls.close()
+    ls = learned.LearnedSolver(gpu_ctx, c2)
+    x6, info6, _ = ls.learned.solve(learned.solve_options(1e-6), c2.F, mode=_lib.LEARNED_BLOCK_JACOBI)
+    pr = _lib.Problem(c2.mesh, c2.material, c2.coloring, c2.F, c2.cons_mask)
+    _x1, one = gpu_ctx.solve(pr, _lib.make_options(tolerance=1e-6, max_iterations=20000,
+                                                   stop_rule=_lib.PG_STOP_RELATIVE))
+    assert info6.converged and abs(info6.iterations - one.iterations) <= 0.1 * one.iterations
+    ls.close()
+
+
+def test_flexible_pcg_operator_matches_fp64_k(gpu_ctx, oracle, small):
+    """The FP32 operator the flexible PCG applies (the node-block form,
+    assembled in FP64 and rounded once) against the oracle's FP64 K x to
+    1e-6 relative, on the uniform plate and on the same mesh with an
+    element thickness field (every element matrix differs); constrained
+    rows are the identity."""
+    import dataclasses
+
+    from plategpu.types import PlateMaterial
+    rng = np.random.default_rng(5)
+    mat = small.material
+    et = np.clip(mat.t * (1 + 0.3 * rng.standard_normal(small.mesh.elementCount)), 0.5 * mat.t, 1.5 * mat.t)
+    varied = dataclasses.replace(small, material=PlateMaterial(mat.E, mat.nu, mat.t, elem_t=et.astype(np.float32)))
+    for wl in (small, varied):
+        ls = learned.LearnedSolver(gpu_ctx, wl)
+        m, mt = wl.mesh, wl.material
+        x = rng.standard_normal(wl.n_dof).astype(np.float32)
+        y = ls.learned.apply_k(x)
+        ke = oracle.all_ke(m.nodes, m.elements, 4, mt.E, mt.nu, mt.t, elem_t=mt.elem_t, mode=oracle.FP64)
+        offs, flat = wl.coloring.flat()
+        y64 = oracle.apply_k(m.nodeCount, m.elements, 4, ke, offs, flat, wl.cons_mask, x.astype(np.float64),
+                             oracle.FP64)
+        assert rel_err(y, y64) < 1e-6
+        cons = wl.cons_mask != 0
+        np.testing.assert_array_equal(y[cons], x[cons])
+        ls.close()
 
 
 def test_unhelpful_network_is_switched_off(gpu_ctx, oracle, U, small):
