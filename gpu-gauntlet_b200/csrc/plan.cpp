@@ -2,9 +2,11 @@
 #include "plan.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <thread>
 
 namespace pg {
 
@@ -142,21 +144,20 @@ void strip_partition(const float* xy, int Nn, int G, std::vector<int>& part_of) 
     const double W = std::max(1e-30, (double)hi[0] - lo[0]), H = std::max(1e-30, (double)hi[1] - lo[1]);
     int R = (int)std::lround(std::sqrt((double)G * H / W));
     R = std::max(1, std::min(R, G));
-    std::vector<int> ids(Nn);
-    std::iota(ids.begin(), ids.end(), 0);
-    auto by = [&](int a, int b) {
-        const float ya = xy[2 * a + 1], yb = xy[2 * b + 1];
-        if (ya != yb) return ya < yb;
-        const float xa = xy[2 * a], xb = xy[2 * b];
-        return xa < xb || (xa == xb && a < b);
+    // sort keys held contiguously (primary, secondary coordinate, node id):
+    // first by (y, x, id), then each strip by (x, y, id)
+    struct Key {
+        float a, b;
+        int id;
     };
-    auto bx = [&](int a, int b) {
-        const float xa = xy[2 * a], xb = xy[2 * b];
-        if (xa != xb) return xa < xb;
-        const float ya = xy[2 * a + 1], yb = xy[2 * b + 1];
-        return ya < yb || (ya == yb && a < b);
+    auto less = [](const Key& u, const Key& v) {
+        if (u.a != v.a) return u.a < v.a;
+        if (u.b != v.b) return u.b < v.b;
+        return u.id < v.id;
     };
-    std::sort(ids.begin(), ids.end(), by);
+    std::vector<Key> keys(Nn);
+    for (int n = 0; n < Nn; n++) keys[n] = Key{xy[2 * n + 1], xy[2 * n], n};
+    std::sort(keys.begin(), keys.end(), less);
     int part = 0;
     long long done_blocks = 0;
     int start = 0;
@@ -164,12 +165,13 @@ void strip_partition(const float* xy, int Nn, int G, std::vector<int>& part_of) 
         const int blocks = G / R + (s < G % R ? 1 : 0);
         done_blocks += blocks;
         const int end = (int)((long long)Nn * done_blocks / G);
-        std::sort(ids.begin() + start, ids.begin() + end, bx);
+        for (int i = start; i < end; i++) std::swap(keys[i].a, keys[i].b);
+        std::sort(keys.begin() + start, keys.begin() + end, less);
         const int len = end - start;
         for (int b = 0; b < blocks; b++) {
             const int b0 = start + (int)((long long)len * b / blocks);
             const int b1 = start + (int)((long long)len * (b + 1) / blocks);
-            for (int i = b0; i < b1; i++) part_of[ids[i]] = part;
+            for (int i = b0; i < b1; i++) part_of[keys[i].id] = part;
             part++;
         }
         start = end;
@@ -202,69 +204,112 @@ std::string build_partition(const pg_problem& p, int G, int rings, HostPlan& pla
     plan.n1.assign(G, 0);
     plan.max_nloc = plan.max_nown = plan.max_ntask = plan.max_ntask_own = plan.max_n1 = 0;
 
-    std::vector<int> local(Nn, -1), ghosts, ring2;
-    // fills `out` (sorted) with the nodes of elements around `from` not yet numbered
-    auto next_ring = [&](const std::vector<int>& from, std::vector<int>& out) {
-        out.clear();
-        for (int n : from)
-            for (int q = plan.inc_ptr[n]; q < plan.inc_ptr[n + 1]; q++) {
-                const int e = plan.inc_idx[q] / 4;
-                for (int k = 0; k < npe; k++) {
-                    const int m = (int)p.elements[(size_t)e * npe + k];
-                    if (local[m] == -1) { local[m] = -2; out.push_back(m); }
-                }
-            }
-        std::sort(out.begin(), out.end());
+    // Each part's lists are built independently (host threads over parts,
+    // each with its own node -> local-index map), then concatenated in part
+    // order.
+    struct PartOut {
+        std::vector<int> nodes, tptr, task_elem;
+        std::vector<uint8_t> task_pos;
+        std::vector<uint16_t> task_nodes;
+        int nown = 0, n1 = 0, nloc = 0, ntask_own = 0;
+        bool too_large = false;
     };
-    for (int g = 0; g < G; g++) {
+    std::vector<PartOut> out(G);
+    const bool two = rings == 2;
+    auto build_part = [&](int g, std::vector<int>& local, std::vector<int>& ghosts, std::vector<int>& ring2) {
+        // fills `dst` (sorted) with the nodes of elements around `from` not yet numbered
+        auto next_ring = [&](const std::vector<int>& from, std::vector<int>& dst) {
+            dst.clear();
+            for (int n : from)
+                for (int q = plan.inc_ptr[n]; q < plan.inc_ptr[n + 1]; q++) {
+                    const int e = plan.inc_idx[q] / 4;
+                    for (int k = 0; k < npe; k++) {
+                        const int m = (int)p.elements[(size_t)e * npe + k];
+                        if (local[m] == -1) { local[m] = -2; dst.push_back(m); }
+                    }
+                }
+            std::sort(dst.begin(), dst.end());
+        };
+        PartOut& o = out[g];
         const std::vector<int>& own = owned[g];
         for (size_t i = 0; i < own.size(); i++) local[own[i]] = (int)i;
         next_ring(own, ghosts);
         for (size_t i = 0; i < ghosts.size(); i++) local[ghosts[i]] = (int)(own.size() + i);
         ring2.clear();
-        if (plan.rings == 2) {
+        if (two) {
             next_ring(ghosts, ring2);
-            for (size_t i = 0; i < ring2.size(); i++)
-                local[ring2[i]] = (int)(own.size() + ghosts.size() + i);
+            for (size_t i = 0; i < ring2.size(); i++) local[ring2[i]] = (int)(own.size() + ghosts.size() + i);
         }
-        const int nloc = (int)(own.size() + ghosts.size() + ring2.size());
-        if (nloc > 65535) return "a part has more than 65535 local nodes: use more ctas";
-
-        plan.nown[g] = (int)own.size();
-        plan.n1[g] = plan.rings == 2 ? (int)(own.size() + ghosts.size()) : (int)own.size();
-        plan.nodes.insert(plan.nodes.end(), own.begin(), own.end());
-        plan.nodes.insert(plan.nodes.end(), ghosts.begin(), ghosts.end());
-        plan.nodes.insert(plan.nodes.end(), ring2.begin(), ring2.end());
-        plan.node_off[g + 1] = (int)plan.nodes.size();
-        const int t0 = (int)plan.task_elem.size();
-        plan.tp_off[g] = (int)plan.tptr.size();
-        std::vector<int> task_nodes_of(own);
-        if (plan.rings == 2) task_nodes_of.insert(task_nodes_of.end(), ghosts.begin(), ghosts.end());
-        int ntask_own = 0;
-        for (size_t i = 0; i < task_nodes_of.size(); i++) {
-            const int n = task_nodes_of[i];
-            if (i == own.size()) ntask_own = (int)plan.task_elem.size() - t0;
-            plan.tptr.push_back((int)plan.task_elem.size() - t0);
-            for (int q = plan.inc_ptr[n]; q < plan.inc_ptr[n + 1]; q++) {
-                const int e = plan.inc_idx[q] / 4, k = plan.inc_idx[q] % 4;
-                plan.task_elem.push_back(e);
-                plan.task_pos.push_back((uint8_t)k);
-                for (int j = 0; j < npe; j++)
-                    plan.task_nodes.push_back(
-                        (uint16_t)local[p.elements[(size_t)e * npe + (k + j) % npe]]);
+        o.nloc = (int)(own.size() + ghosts.size() + ring2.size());
+        o.nown = (int)own.size();
+        o.n1 = two ? (int)(own.size() + ghosts.size()) : (int)own.size();
+        o.too_large = o.nloc > 65535;
+        if (!o.too_large) {
+            o.nodes.reserve(o.nloc);
+            o.nodes.insert(o.nodes.end(), own.begin(), own.end());
+            o.nodes.insert(o.nodes.end(), ghosts.begin(), ghosts.end());
+            o.nodes.insert(o.nodes.end(), ring2.begin(), ring2.end());
+            const int ntn = o.n1;
+            for (int i = 0; i < ntn; i++) {
+                const int n = i < (int)own.size() ? own[i] : ghosts[i - own.size()];
+                if (i == (int)own.size()) o.ntask_own = (int)o.task_elem.size();
+                o.tptr.push_back((int)o.task_elem.size());
+                for (int q = plan.inc_ptr[n]; q < plan.inc_ptr[n + 1]; q++) {
+                    const int e = plan.inc_idx[q] / 4, k = plan.inc_idx[q] % 4;
+                    o.task_elem.push_back(e);
+                    o.task_pos.push_back((uint8_t)k);
+                    for (int j = 0; j < npe; j++)
+                        o.task_nodes.push_back((uint16_t)local[p.elements[(size_t)e * npe + (k + j) % npe]]);
+                }
             }
+            if (ntn == (int)own.size()) o.ntask_own = (int)o.task_elem.size();
+            o.tptr.push_back((int)o.task_elem.size());
         }
-        if (task_nodes_of.size() == own.size()) ntask_own = (int)plan.task_elem.size() - t0;
-        plan.tptr.push_back((int)plan.task_elem.size() - t0);
-        plan.task_off[g + 1] = (int)plan.task_elem.size();
-        plan.max_nloc = std::max(plan.max_nloc, nloc);
-        plan.max_nown = std::max(plan.max_nown, (int)own.size());
-        plan.max_n1 = std::max(plan.max_n1, plan.n1[g]);
-        plan.max_ntask = std::max(plan.max_ntask, (int)plan.task_elem.size() - t0);
-        plan.max_ntask_own = std::max(plan.max_ntask_own, ntask_own);
         for (int n : own) local[n] = -1;
         for (int n : ghosts) local[n] = -1;
         for (int n : ring2) local[n] = -1;
+    };
+    const int nth = std::max(1, std::min({(int)std::thread::hardware_concurrency(), 16, G, 1 + Nn / 4096}));
+    std::atomic<int> next{0};
+    auto worker = [&]() {
+        std::vector<int> local(Nn, -1), ghosts, ring2;
+        for (int g; (g = next.fetch_add(1)) < G;) build_part(g, local, ghosts, ring2);
+    };
+    {
+        std::vector<std::thread> th;
+        for (int t = 1; t < nth; t++) th.emplace_back(worker);
+        worker();
+        for (auto& t : th) t.join();
+    }
+    size_t tot_nodes = 0, tot_tasks = 0, tot_tptr = 0;
+    for (int g = 0; g < G; g++) {
+        if (out[g].too_large) return "a part has more than 65535 local nodes: use more ctas";
+        tot_nodes += out[g].nodes.size();
+        tot_tasks += out[g].task_elem.size();
+        tot_tptr += out[g].tptr.size();
+    }
+    plan.nodes.reserve(tot_nodes);
+    plan.task_elem.reserve(tot_tasks);
+    plan.task_pos.reserve(tot_tasks);
+    plan.task_nodes.reserve(tot_tasks * npe);
+    plan.tptr.reserve(tot_tptr);
+    for (int g = 0; g < G; g++) {
+        const PartOut& o = out[g];
+        plan.nown[g] = o.nown;
+        plan.n1[g] = o.n1;
+        plan.nodes.insert(plan.nodes.end(), o.nodes.begin(), o.nodes.end());
+        plan.node_off[g + 1] = (int)plan.nodes.size();
+        plan.tp_off[g] = (int)plan.tptr.size();
+        plan.tptr.insert(plan.tptr.end(), o.tptr.begin(), o.tptr.end());
+        plan.task_elem.insert(plan.task_elem.end(), o.task_elem.begin(), o.task_elem.end());
+        plan.task_pos.insert(plan.task_pos.end(), o.task_pos.begin(), o.task_pos.end());
+        plan.task_nodes.insert(plan.task_nodes.end(), o.task_nodes.begin(), o.task_nodes.end());
+        plan.task_off[g + 1] = (int)plan.task_elem.size();
+        plan.max_nloc = std::max(plan.max_nloc, o.nloc);
+        plan.max_nown = std::max(plan.max_nown, o.nown);
+        plan.max_n1 = std::max(plan.max_n1, o.n1);
+        plan.max_ntask = std::max(plan.max_ntask, (int)o.task_elem.size());
+        plan.max_ntask_own = std::max(plan.max_ntask_own, o.ntask_own);
     }
     plan.tp_off[G] = (int)plan.tptr.size();
     return "";

@@ -575,10 +575,21 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
                 hp.Ne, C, pl->mesh_nodes.p, pl->mesh_elements.p, pl->cons.p, owner.p, geom.p, pl->ke64.p, Ac.p);
         CK(cudaGetLastError());
     }
-    const size_t fsm = pg::coarse_factor_smem(C);
-    if (fsm > 48 * 1024)
-        CK(cudaFuncSetAttribute(pg::coarse_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
-    pg::coarse_factor_kernel<<<1, pg::kCoarseThreads, fsm, st>>>(C, Ac.p, L.p, Lt.p, Ainv.p, keep.p, dropped.p);
+    // the blocked factorisation when its panels fit in shared memory
+    // (1 KB left for the kernel's static shared memory)
+    const size_t smem_cap = (size_t)c->max_smem - 1024;
+    const bool blocked = pg::coarse_factor_blocked_smem(C) <= smem_cap;
+    const size_t fsm = blocked ? pg::coarse_factor_blocked_smem(C) : pg::coarse_factor_smem(C);
+    if (fsm > smem_cap) throw Fail{PG_EUNSUPPORTED, "coarse space too large for its factorisation"};
+    const void* ffn = blocked ? (const void*)pg::coarse_factor_kernel : (const void*)pg::coarse_factor_tiles_kernel;
+    if (fsm > 48 * 1024) CK(cudaFuncSetAttribute(ffn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+    {
+        const double* acp = Ac.p;
+        double *lp = L.p, *ltp = Lt.p, *aip = Ainv.p;
+        int *kp = keep.p, *dp = dropped.p;
+        void* fargs[] = {(void*)&C, (void*)&acp, (void*)&lp, (void*)&ltp, (void*)&aip, (void*)&kp, (void*)&dp};
+        CK(cudaLaunchKernel(ffn, dim3(1), dim3(pg::kCoarseThreads), fargs, fsm, st));
+    }
     CK(cudaGetLastError());
     const int rows = (int)hp.ainv_src.size();
     pl->ainv64.alloc((size_t)rows * C);

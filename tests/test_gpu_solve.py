@@ -284,3 +284,21 @@ def test_plan_cache_compares_every_array(gpu_ctx, c1):
     col2 = ElementColoring(colors, c1.coloring.elementColors, c1.coloring.colorCount)
     _x, info = gpu_ctx.solve(_lib.Problem(m, mat, col2, c1.F, c1.cons_mask), o)
     assert info.plan_cached == 0
+
+
+def test_first_solve_reports_its_set_up_phases(c1):
+    """A solve in a new context times its one-time steps (partition plan,
+    coarse space, eigenvalue estimate); the next solve of the same plate
+    reuses them and reports zeros."""
+    kw = dict(tolerance=1e-8, max_iterations=20000, stop_rule=_lib.PG_STOP_RELATIVE,
+              preconditioner=_lib.PG_PRECOND_TWO_LEVEL, smoother=_lib.PG_SMOOTHER_CHEBYSHEV)
+    ctx = _lib.Context(0)
+    try:
+        _x, first = gsolve(ctx, c1, **kw)
+        assert first.converged and first.plan_cached == 0
+        assert first.plan_ms > 0 and first.coarse_ms > 0 and first.eigen_ms > 0
+        assert first.plan_ms + first.coarse_ms + first.eigen_ms < first.total_ms
+        _x, again = gsolve(ctx, c1, **kw)
+        assert again.plan_cached == 1 and again.plan_ms == 0 and again.coarse_ms == 0 and again.eigen_ms == 0
+    finally:
+        ctx.close()
