@@ -776,10 +776,12 @@ enum { ST_OK = 0, ST_TIMEOUT = 4, ST_NONFINITE = 5 };
 
 // Threads per block: at most kMaxThreads (the launch bound of the 96-register
 // build); up to kLeanThreads a build with 128 registers per thread runs
-// instead (no spills); the batch kernel always runs kBatchThreads.
+// instead (no spills); the batch and load-case kernels always run
+// kBatchThreads / kMultiThreads.
 constexpr int kMaxThreads = 576;
 constexpr int kLeanThreads = 512;
 constexpr int kBatchThreads = 512;
+constexpr int kMultiThreads = 512;  // the load-case kernel (128 registers)
 
 // Per-phase SM cycles of thread 0 of block 0, when timing is requested:
 // 0 K.u, 1 gather + dots + publish w, 2 block reduction and publishing the

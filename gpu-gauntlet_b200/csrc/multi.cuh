@@ -115,69 +115,71 @@ __device__ void block_publish_multi(double (&v)[KP], double* red, unsigned long 
 // One exchange round for NR cases: the K = KP * NR partial sums of every
 // block (staged to sp[G][K]) and case k of each ghost DOF of vector buffer
 // vb (words ((dof * NR + k) * TW), written to dst[dof_local * NR + k] for
-// local DOFs [3 no, 3 nloc)).  Returns false if a wait gave up.
-template <typename T, int NR, int IF = 2>
+// local DOFs [3 no, 3 nloc)).  Items: the ghost values first (their owners
+// publish them before their partial sums), then the partials; each thread
+// takes items tid, tid + nt, ... with S in flight, refilling a slot with
+// its next item as soon as the slot's item has arrived.  Returns false if a
+// wait gave up.
+template <typename T, int NR, int S = 4>
 __device__ bool exchange_round_multi(const unsigned long long* __restrict__ pb, int G, int K,
                                      const unsigned long long* __restrict__ vb, T* dst, int no, int nloc,
                                      const int* __restrict__ gid, int g, unsigned f, double* sp,
                                      Waiter& wt) {
     constexpr int TW = Tag<T>::W, SW = multi_slot_words<NR>();
-    const int np = G * K, n = np + 3 * (nloc - no) * NR;
+    const int ng = 3 * (nloc - no) * NR, n = ng + G * K, nt = blockDim.x;
     pb += (size_t)(g % kRep) * G * SW;
-    for (int i0 = threadIdx.x; i0 < n; i0 += IF * blockDim.x) {
-        const unsigned long long* ptr[IF];
-        bool done[IF];
+    auto addr = [&](int i) -> const unsigned long long* {
+        if (i < ng) {
+            const int k3 = 3 * no + i / NR;
+            return vb + ((size_t)(3 * gid[k3 / 3] + k3 % 3) * NR + i % NR) * TW;
+        }
+        const int q = i - ng;
+        return pb + (size_t)(q / K) * SW + 2 * (q % K);
+    };
+    int it[S];
+    const unsigned long long* pp[S];
 #pragma unroll
-        for (int j = 0; j < IF; j++) {
-            const int i = i0 + j * (int)blockDim.x;
-            done[j] = i >= n;
-            if (done[j]) {
-                ptr[j] = nullptr;
-            } else if (i < np) {
-                ptr[j] = pb + (size_t)(i / K) * SW + 2 * (i % K);
+    for (int s = 0; s < S; s++) {
+        it[s] = threadIdx.x + s * nt;
+        pp[s] = it[s] < n ? addr(it[s]) : nullptr;
+    }
+    int next = threadIdx.x + S * nt;
+    wt.spins = 0;
+    for (;;) {
+        unsigned long long lo[S], hi[S];
+        bool any = false;
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+            lo[s] = hi[s] = 0;
+            if (it[s] >= n) continue;
+            any = true;
+            if (it[s] >= ng || TW == 2) {
+                ld_relaxed2(pp[s], lo[s], hi[s]);
             } else {
-                const int q = i - np, k3 = 3 * no + q / NR;
-                ptr[j] = vb + ((size_t)(3 * gid[k3 / 3] + k3 % 3) * NR + q % NR) * TW;
+                lo[s] = ld_relaxed(pp[s]);
+                hi[s] = lo[s];
             }
         }
-        wt.spins = 0;
-        for (;;) {
-            unsigned long long lo[IF], hi[IF];
+        if (!any) break;
+        bool moved = false;
 #pragma unroll
-            for (int j = 0; j < IF; j++) {
-                if (done[j]) continue;
-                const int i = i0 + j * (int)blockDim.x;
-                if (i < np || TW == 2) {
-                    ld_relaxed2(ptr[j], lo[j], hi[j]);
-                } else {
-                    lo[j] = ld_relaxed(ptr[j]);
-                    hi[j] = lo[j];
-                }
+        for (int s = 0; s < S; s++) {
+            if (it[s] >= n) continue;
+            if ((unsigned)(lo[s] >> 32) != f || (unsigned)(hi[s] >> 32) != f) continue;
+            const int i = it[s];
+            if (i >= ng) {
+                sp[i - ng] = __longlong_as_double((long long)((hi[s] << 32) | (lo[s] & 0xffffffffull)));
+            } else if constexpr (TW == 2) {
+                dst[3 * no * NR + i] = (T)__longlong_as_double((long long)((hi[s] << 32) | (lo[s] & 0xffffffffull)));
+            } else {
+                dst[3 * no * NR + i] = (T)__uint_as_float((unsigned)lo[s]);
             }
-            bool all = true;
-#pragma unroll
-            for (int j = 0; j < IF; j++) {
-                if (done[j]) continue;
-                const int i = i0 + j * (int)blockDim.x;
-                if ((unsigned)(lo[j] >> 32) != f || (unsigned)(hi[j] >> 32) != f) {
-                    all = false;
-                    continue;
-                }
-                done[j] = true;
-                const double dv = __longlong_as_double((long long)((hi[j] << 32) | (lo[j] & 0xffffffffull)));
-                if (i < np) {
-                    sp[i] = dv;
-                } else {
-                    const int q = i - np;
-                    if constexpr (TW == 2)
-                        dst[3 * no * NR + q] = (T)dv;
-                    else
-                        dst[3 * no * NR + q] = (T)__uint_as_float((unsigned)lo[j]);
-                }
-            }
-            if (all) break;
-            if (!wt.keep_going()) return false;
+            it[s] = next;
+            next += nt;
+            pp[s] = it[s] < n ? addr(it[s]) : nullptr;
+            moved = true;
         }
+        if (!moved && !wt.keep_going()) return false;
     }
     return true;
 }
@@ -820,7 +822,7 @@ __device__ __forceinline__ void pcg_multi_body(const PcgArgs& a, const int g, un
 // a.x hold NR vectors of 3 Nn back to back, a.res NR result records, and the
 // exchange buffers are sized for NR cases.
 template <int NPE, typename T, bool MIXED, int NR>
-__global__ void __launch_bounds__(kMaxThreads, 1) pcg_multi_kernel(const __grid_constant__ PcgArgs a) {
+__global__ void __launch_bounds__(kMultiThreads, 1) pcg_multi_kernel(const __grid_constant__ PcgArgs a) {
     extern __shared__ __align__(16) unsigned char sm[];
     pcg_multi_body<NPE, T, MIXED, NR>(a, blockIdx.x, sm);
 }

@@ -1187,14 +1187,14 @@ void run_solve_multi(pg_ctx* c, Plan* pl, const pg_options& o, int NR, int count
     opt_in_smem(c, fn);
     if (pl->m_ok_fn != fn || pl->m_ok_smem != L.total) {
         int nb = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, pg::kMaxThreads, L.total));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, pg::kMultiThreads, L.total));
         if (nb < 1 || nb * c->sms < pl->G)
             throw Fail{PG_EUNSUPPORTED, "load-case grid does not fit on the device"};
         pl->m_ok_fn = fn;
         pl->m_ok_smem = L.total;
     }
     void* args[] = {&a};
-    CK(cudaLaunchCooperativeKernel(fn, dim3(pl->G), dim3(pg::kMaxThreads), args, L.total, st));
+    CK(cudaLaunchCooperativeKernel(fn, dim3(pl->G), dim3(pg::kMultiThreads), args, L.total, st));
     CK(cudaEventRecord(c->ev[2], st));
     std::vector<pg::PcgResult> r(NR);
     if (x) CK(cudaMemcpyAsync(c->hx, pl->mx.p, n * count * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1218,7 +1218,7 @@ void run_solve_multi(pg_ctx* c, Plan* pl, const pg_options& o, int NR, int count
     for (int k = 0; k < count; k++) {
         if (infos) {
             std::memset(&infos[k], 0, sizeof(pg_info));
-            fill_info(&infos[k], r[k], pl, o, pg::kMaxThreads, L.total);
+            fill_info(&infos[k], r[k], pl, o, pg::kMultiThreads, L.total);
             infos[k].status = r[k].status;
             infos[k].setup_ms = ms_setup;
             infos[k].solve_ms = ms_solve;
@@ -1236,7 +1236,7 @@ void run_solve_multi(pg_ctx* c, Plan* pl, const pg_options& o, int NR, int count
         CK(cudaMemcpyAsync(pl->x.p, pl->mx.p + k * n, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(pl->F.p, F[k], n * sizeof(float), cudaMemcpyHostToDevice, st));
         pg_info fi{};
-        fill_info(&fi, r[k], pl, o, pg::kMaxThreads, L.total);
+        fill_info(&fi, r[k], pl, o, pg::kMultiThreads, L.total);
         fi.solve_ms = ms_solve;
         fp64_correction(c, pl, o, &fi, x ? (void*)x[k] : nullptr, cudaMemcpyDeviceToHost);
         if (infos) {
