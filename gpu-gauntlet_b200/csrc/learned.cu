@@ -466,6 +466,10 @@ struct Op {
     const int* nm_off = nullptr;
     const int* nm_col = nullptr;
     const float* nm_val = nullptr;
+    // threads per node of the flexible-PCG kernels (1 or 2): a plate that
+    // fills less than a wave of the device at one thread per node splits
+    // each node's K product between two threads
+    int tpn = 1;
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -530,11 +534,13 @@ __device__ void reduce_parts(const double* parts, int nb, double (&out)[K]) {
 
 // (K v)_n for node n with v read through getv(m, d) (FP32 element matrices),
 // constrained rows replaced by the identity (y_c = v_c).
+// Partial sums of (K v)_n over the node's incident elements h, h + step, ...
+// (FP32 element matrices).
 template <int NPE, typename GetV>
-__device__ __forceinline__ void kv_node(const Op& op, int n, GetV getv, float (&out)[3]) {
+__device__ __forceinline__ void kv_elem_sum(const Op& op, int n, int h, int step, GetV getv, float& s0, float& s1,
+                                            float& s2) {
     constexpr int ND = 3 * NPE;
-    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-    for (int q = op.inc_ptr[n]; q < op.inc_ptr[n + 1]; q++) {
+    for (int q = op.inc_ptr[n] + h; q < op.inc_ptr[n + 1]; q += step) {
         const int e = op.inc_idx[q] >> 2, k = op.inc_idx[q] & 3;
         const float* Ke = op.ke32 + (size_t)e * op.ke_stride + 3 * k * ND;
 #pragma unroll
@@ -547,20 +553,18 @@ __device__ __forceinline__ void kv_node(const Op& op, int n, GetV getv, float (&
             s2 += c0[2 * ND] * v0 + c0[2 * ND + 1] * v1 + c0[2 * ND + 2] * v2;
         }
     }
-    out[0] = op.cons[3 * n] ? getv(n, 0) : s0;
-    out[1] = op.cons[3 * n + 1] ? getv(n, 1) : s1;
-    out[2] = op.cons[3 * n + 2] ? getv(n, 2) : s2;
 }
 
-// (K v)_n from the node-block form (op.nm_* set): one pass over the node's
-// slots, all loads of a slot coalesced across the warp's 32 nodes.
+// Partial sums of (K v)_n over the node's node-block slots h, h + step,
+// ... (op.nm_* set); the loads of a slot are coalesced across the nodes of
+// a slice.
 template <typename GetV>
-__device__ __forceinline__ void kv_block(const Op& op, int n, GetV getv, float (&out)[3]) {
+__device__ __forceinline__ void kv_block_sum(const Op& op, int n, int h, int step, GetV getv, float& s0,
+                                             float& s1, float& s2) {
     const int s = n >> 5, lane = n & 31;
     const int j1 = op.nm_off[s + 1];
-    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
 #pragma unroll 3
-    for (int j = op.nm_off[s]; j < j1; j++) {
+    for (int j = op.nm_off[s] + h; j < j1; j += step) {
         const int m = op.nm_col[32 * j + lane];
         const float* B = op.nm_val + (size_t)288 * j + lane;
         const float v0 = getv(m, 0), v1 = getv(m, 1), v2 = getv(m, 2);
@@ -568,19 +572,45 @@ __device__ __forceinline__ void kv_block(const Op& op, int n, GetV getv, float (
         s1 += B[96] * v0 + B[128] * v1 + B[160] * v2;
         s2 += B[192] * v0 + B[224] * v1 + B[256] * v2;
     }
+}
+
+// (K v)_n for node n with v read through getv(m, d) (FP32 element
+// matrices), constrained rows replaced by the identity (y_c = v_c).
+template <int NPE, typename GetV>
+__device__ __forceinline__ void kv_node(const Op& op, int n, GetV getv, float (&out)[3]) {
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    kv_elem_sum<NPE>(op, n, 0, 1, getv, s0, s1, s2);
     out[0] = op.cons[3 * n] ? getv(n, 0) : s0;
     out[1] = op.cons[3 * n + 1] ? getv(n, 1) : s1;
     out[2] = op.cons[3 * n + 2] ? getv(n, 2) : s2;
 }
 
-// (K v)_n by the node-block form when the operator has one, else by the
-// element gather.
+// (K v)_n by op.tpn threads per node: with two, lanes 2i and 2i + 1 of a
+// warp share node n (h = lane parity), each sums half its slots
+// (node-block form) or half its elements, and they exchange their sums.
+// Every lane of the warp must call it; lanes with n >= Nn take part with
+// zero sums and get zeros.
 template <int NPE, typename GetV>
-__device__ __forceinline__ void kv(const Op& op, int n, GetV getv, float (&out)[3]) {
-    if (op.nm_off)
-        kv_block(op, n, getv, out);
-    else
-        kv_node<NPE>(op, n, getv, out);
+__device__ __forceinline__ void kv2(const Op& op, int n, int h, GetV getv, float (&out)[3]) {
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    const bool live = n < op.Nn;
+    if (live) {
+        if (op.nm_off)
+            kv_block_sum(op, n, h, op.tpn, getv, s0, s1, s2);
+        else
+            kv_elem_sum<NPE>(op, n, h, op.tpn, getv, s0, s1, s2);
+    }
+    if (op.tpn == 2) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, 1);
+    }
+    out[0] = out[1] = out[2] = 0.f;
+    if (live) {
+        out[0] = op.cons[3 * n] ? getv(n, 0) : s0;
+        out[1] = op.cons[3 * n + 1] ? getv(n, 1) : s1;
+        out[2] = op.cons[3 * n + 2] ? getv(n, 2) : s2;
+    }
 }
 
 constexpr int kMaxNbr = 32;  // node-block form: largest neighbour count
@@ -999,10 +1029,20 @@ __device__ __forceinline__ void write_t(const FArgs& a, int n, const float (&rv)
     for (int d = 0; d < 3; d++) a.t[3 * n + d] = a.omega * binv_row(B9, d, rv[0], rv[1], rv[2]);
 }
 
+// op.tpn threads per node in the flexible-PCG kernels: thread t works on
+// node t / tpn (h = t mod tpn); the K products split the node's sums
+// between them (kv2), node-local work runs on the first thread only.
+__device__ __forceinline__ int fp_node(const Op& op, int& h) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    h = op.tpn == 2 ? (t & 1) : 0;
+    return op.tpn == 2 ? (t >> 1) : t;
+}
+
 __global__ void fp_init_kernel(FArgs a) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    int h;
+    const int n = fp_node(a.op, h);
     double acc[1] = {0.0};
-    if (n < a.op.Nn) {
+    if (n < a.op.Nn && h == 0) {
         for (int d = 0; d < 3; d++) {
             const int i = 3 * n + d;
             const float f = a.F[i];
@@ -1043,9 +1083,10 @@ __global__ void fp_update_kernel(FArgs a) {
         else alpha = s[1] / s[0];
     }
     const float* p = (it & 1) ? a.p1 : a.p0;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    int h;
+    const int n = fp_node(a.op, h);
     double acc[1] = {0.0};
-    if (n < a.op.Nn && !stop) {
+    if (n < a.op.Nn && h == 0 && !stop) {
         float rv[3];
         for (int d = 0; d < 3; d++) {
             const int i = 3 * n + d;
@@ -1094,11 +1135,14 @@ __global__ void fp_true_res_kernel(FArgs a) {
         if (trig) st->replacements++;
     }
     if (!trig) return;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    int h;
+    const int n = fp_node(a.op, h);
     double acc[1] = {0.0};
-    if (n < a.op.Nn) {
-        double kx[3] = {0, 0, 0};
-        for (int q = a.op.inc_ptr[n]; q < a.op.inc_ptr[n + 1]; q++) {
+    // the node's FP64 product split between the two threads (every other
+    // incident element), then exchanged
+    double kx[3] = {0, 0, 0};
+    if (n < a.op.Nn)
+        for (int q = a.op.inc_ptr[n] + h; q < a.op.inc_ptr[n + 1]; q += a.op.tpn) {
             const int e = a.op.inc_idx[q] >> 2, k = a.op.inc_idx[q] & 3;
             const double* Ke = a.op.ke64 + (size_t)e * ND * ND + 3 * k * ND;
             for (int b = 0; b < NPE; b++) {
@@ -1108,6 +1152,9 @@ __global__ void fp_true_res_kernel(FArgs a) {
                                                      Ke[d * ND + 3 * b + 2] * x2;
             }
         }
+    if (a.op.tpn == 2)
+        for (int d = 0; d < 3; d++) kx[d] += __shfl_xor_sync(0xffffffffu, kx[d], 1);
+    if (n < a.op.Nn && h == 0) {
         float rv[3];
         for (int d = 0; d < 3; d++) {
             const int i = 3 * n + d;
@@ -1160,14 +1207,15 @@ __global__ void fp_prep_kernel(FArgs a) {
     const bool skip = a.mode != 1 || st->net_off;
     if (blockIdx.x == 0 && threadIdx.x == 0) st->skip_net = skip;
     if (a.mode == 0 || (a.mode == 1 && st->net_off)) return;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    int h;
+    const int n = fp_node(a.op, h);
     double acc[1] = {0.0};
-    if (n < a.op.Nn) {
-        const float* r = a.r;
-        const float* t = a.t;
-        auto tv = [&](int m, int d) { return t[3 * m + d]; };
-        float u[3];
-        kv<NPE>(a.op, n, tv, u);
+    const float* r = a.r;
+    const float* t = a.t;
+    auto tv = [&](int m, int d) { return t[3 * m + d]; };
+    float u[3];
+    kv2<NPE>(a.op, n, h, tv, u);
+    if (n < a.op.Nn && h == 0) {
         const float sc[3] = {a.si0, a.si1, a.si2};
         // only mode 1 has a network (and its input image and pixel map)
         bf16* px = a.mode == 1 ? a.img_in + (size_t)a.node_pixel[n] * 16 : nullptr;
@@ -1200,15 +1248,16 @@ __global__ void fp_net_kernel(FArgs a, float* __restrict__ w_next) {
     pgn::pdl_wait();
     FState* st = a.st;
     if (st->done || st->skip_net) return;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    int h;
+    const int n = fp_node(a.op, h);
     const float so[3] = {a.so0, a.so1, a.so2};
     auto yv = [&](int m, int d) {
         return a.op.cons[3 * m + d] ? 0.f : so[d] * a.img_out[(size_t)a.node_pixel[m] * 4 + d];
     };
     double acc[2] = {0.0, 0.0};
-    if (n < a.op.Nn) {
-        float v[3], y[3];
-        kv<NPE>(a.op, n, yv, v);
+    float v[3], y[3];
+    kv2<NPE>(a.op, n, h, yv, v);
+    if (n < a.op.Nn && h == 0) {
         for (int d = 0; d < 3; d++) {
             const int i = 3 * n + d;
             y[d] = yv(n, d);
@@ -1232,11 +1281,12 @@ __global__ void fp_sweep_kernel(FArgs a, const float* __restrict__ w_in, float* 
     FState* st = a.st;
     if (st->done || st->skip_net) return;
     auto wv = [&](int m, int d) { return w_in[3 * m + d]; };
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    int h;
+    const int n = fp_node(a.op, h);
     double acc[2] = {0.0, 0.0};
-    if (n < a.op.Nn) {
-        float v[3], w[3];
-        kv<NPE>(a.op, n, wv, v);
+    float v[3], w[3];
+    kv2<NPE>(a.op, n, h, wv, v);
+    if (n < a.op.Nn && h == 0) {
         for (int d = 0; d < 3; d++) {
             const int i = 3 * n + d;
             w[d] = w_in[i];
@@ -1271,9 +1321,10 @@ __global__ void fp_prec_kernel(FArgs a) {
         c = use ? (float)cd : 0.f;
     }
     const bool smooth2 = a.mode == 2;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    int h;
+    const int n = fp_node(a.op, h);
     double acc[2] = {0.0, 0.0};
-    if (n < a.op.Nn) {
+    if (n < a.op.Nn && h == 0) {
         const float* B9 = a.op.binv32 + 9 * n;
         const int i = 3 * n;
         const float r0 = a.r[i], r1_ = a.r[i + 1], r2_ = a.r[i + 2];
@@ -1320,11 +1371,12 @@ __global__ void fp_dir_kernel(FArgs a) {
     float* pn = (it & 1) ? a.p0 : a.p1;
     const float bf = (float)beta;
     auto pv = [&](int m, int d) { return a.z[3 * m + d] + bf * po[3 * m + d]; };
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    int h;
+    const int n = fp_node(a.op, h);
     double acc[2] = {0.0, 0.0};
-    if (n < a.op.Nn) {
-        float qv[3];
-        kv<NPE>(a.op, n, pv, qv);
+    float qv[3];
+    kv2<NPE>(a.op, n, h, pv, qv);
+    if (n < a.op.Nn && h == 0) {
         for (int d = 0; d < 3; d++) {
             const int i = 3 * n + d;
             const float pi = pv(n, d);
@@ -1344,12 +1396,13 @@ __global__ void fp_dir_kernel(FArgs a) {
 // y = K x by the flexible PCG's operator (pg_learned_apply_k)
 template <int NPE>
 __global__ void apply_op_kernel(Op op, const float* __restrict__ x, float* __restrict__ y) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= op.Nn) return;
+    int h;
+    const int n = fp_node(op, h);
     auto xv = [&](int m, int d) { return x[3 * m + d]; };
     float v[3];
-    kv<NPE>(op, n, xv, v);
-    for (int d = 0; d < 3; d++) y[3 * n + d] = v[d];
+    kv2<NPE>(op, n, h, xv, v);
+    if (n < op.Nn && h == 0)
+        for (int d = 0; d < 3; d++) y[3 * n + d] = v[d];
 }
 
 __global__ void fp_tick_kernel(FArgs a, cudaGraphConditionalHandle h, int in_graph) {
@@ -1521,7 +1574,15 @@ __global__ void unpack_din_kernel(long P, const bf16* __restrict__ src, float* _
         for (int c = 0; c < 3; c++) dst[i * 3 + c] = __bfloat162float(src[i * 16 + c]);
 }
 
-int grid_nodes(int Nn) { return (Nn + 255) / 256; }
+// blocks of 256 threads: for the flexible-PCG kernels (tpn threads per
+// node), and for the training kernels (one thread per node)
+int grid_nodes(int Nn, int tpn) { return (int)(((long)tpn * Nn + 255) / 256); }
+int grid_nodes1(int Nn) { return (Nn + 255) / 256; }
+
+// Nodes below which the flexible-PCG kernels run two threads per node
+// (measured: plate_q4_141, 20,164 nodes, K products 10-20% faster with two;
+// plate_q4_400, 160,801 nodes, 15% slower)
+constexpr int kTwoThreadNodes = 75000;
 
 // Buffers of a flexible-PCG solver for an operator with Nn nodes.
 // The node-block form of S's operator (Op::nm_*): slice widths on the
@@ -1572,7 +1633,8 @@ void fpcg_init(FpcgSolver* S, pg_ctx* c, const Op& op, int npe, float omega) {
         b->zero(st);
     }
     S->x.alloc(n3);
-    S->parts.alloc(14 * (size_t)grid_nodes(op.Nn));
+    S->op.tpn = op.Nn < kTwoThreadNodes ? 2 : 1;
+    S->parts.alloc(14 * (size_t)grid_nodes(op.Nn, S->op.tpn));
     S->st.alloc(1);
     LCK(cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
     build_node_blocks(S, st);
@@ -1636,7 +1698,7 @@ void queue_body(FpcgSolver* S, const FArgs& a, int mode, pg_net* n, Workspace* w
 // network's batch-1 workspace in mode 1).
 FArgs make_fargs(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, Workspace* w, const int* node_pixel,
                  int HW, int fallback_after, int replace_every) {
-    const int G = grid_nodes(S->op.Nn);
+    const int G = grid_nodes(S->op.Nn, S->op.tpn);
     FArgs a{};
     a.op = S->op;
     a.HW = HW;
@@ -1689,7 +1751,7 @@ void fpcg_build(FpcgSolver* S, const pg_options& o, int mode, pg_net* n, const i
                 int fallback_after, int replace_every, bool pdl) {
     cudaStream_t cs = S->cap;
     Workspace* w = mode == 1 ? workspace(n, 1, false) : nullptr;
-    const int G = grid_nodes(S->op.Nn);
+    const int G = grid_nodes(S->op.Nn, S->op.tpn);
     FArgs a = make_fargs(S, o, mode, n, w, node_pixel, HW, fallback_after, replace_every);
 
     if (S->exec) {
@@ -2054,7 +2116,7 @@ int pg_learned_make_pairs(pg_learned* L, int count, const float* F_dev, const do
             throw LFail{PG_EINVAL, "NULL buffer"};
         if (count == 0) return;
         cudaStream_t st = pgi::ctx_stream(L->ctx);
-        dim3 grid(grid_nodes(L->op.Nn), count);
+        dim3 grid(grid_nodes1(L->op.Nn), count);
         if (L->ov.npe == 4)
             make_pairs_kernel<4><<<grid, 256, 0, st>>>(L->op, count, F_dev, xstar_dev, xk_dev, R_out, E_out);
         else
@@ -2072,7 +2134,7 @@ namespace {
 void load_pairs(pg_learned* L, int count, const float* R, const float* E, bool set_scales) {
     pg_net* n = L->net;
     cudaStream_t st = pgi::ctx_stream(L->ctx);
-    dim3 grid(grid_nodes(L->op.Nn), count);
+    dim3 grid(grid_nodes1(L->op.Nn), count);
     if (set_scales) {
         L->stats.zero(st);
         if (L->ov.npe == 4)
@@ -2119,7 +2181,7 @@ void queue_loss(pg_learned* L, int B, const float* out, const int* perm, const i
                 double* loss_hist, bf16* gout, cudaStream_t st) {
     pg_net* n = L->net;
     const Op& op = L->op;
-    dim3 grid(grid_nodes(op.Nn), B);
+    dim3 grid(grid_nodes1(op.Nn), B);
     const bool q4 = L->ov.npe == 4;
     if (kind != PG_LOSS_SMOOTHED_ENERGY) {
         auto k = q4 ? loss_kernel<4> : loss_kernel<3>;
@@ -2406,7 +2468,7 @@ int pg_learned_apply_k(pg_learned* L, const float* x, float* y) {
         dx.alloc(n3);
         dy.alloc(n3);
         LCK(cudaMemcpyAsync(dx.p, x, n3 * sizeof(float), cudaMemcpyHostToDevice, st));
-        const int grid = grid_nodes(L->S.op.Nn);
+        const int grid = grid_nodes(L->S.op.Nn, L->S.op.tpn);
         (L->S.npe == 4 ? apply_op_kernel<4> : apply_op_kernel<3>)<<<grid, 256, 0, st>>>(L->S.op, dx.p, dy.p);
         LCK(cudaGetLastError());
         LCK(cudaMemcpyAsync(y, dy.p, n3 * sizeof(float), cudaMemcpyDeviceToHost, st));
