@@ -5,6 +5,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <new>
 #include <numeric>
 #include <thread>
 
@@ -271,9 +272,16 @@ std::string build_partition(const pg_problem& p, int G, int rings, HostPlan& pla
     };
     const int nth = std::max(1, std::min({(int)std::thread::hardware_concurrency(), 16, G, 1 + Nn / 4096}));
     std::atomic<int> next{0};
+    std::atomic<bool> failed{false};
     auto worker = [&]() {
-        std::vector<int> local(Nn, -1), ghosts, ring2;
-        for (int g; (g = next.fetch_add(1)) < G;) build_part(g, local, ghosts, ring2);
+        // an exception must not leave a worker thread (std::terminate):
+        // recorded here, raised again on the calling thread
+        try {
+            std::vector<int> local(Nn, -1), ghosts, ring2;
+            for (int g; !failed && (g = next.fetch_add(1)) < G;) build_part(g, local, ghosts, ring2);
+        } catch (...) {
+            failed = true;
+        }
     };
     {
         std::vector<std::thread> th;
@@ -281,6 +289,7 @@ std::string build_partition(const pg_problem& p, int G, int rings, HostPlan& pla
         worker();
         for (auto& t : th) t.join();
     }
+    if (failed) throw std::bad_alloc();
     size_t tot_nodes = 0, tot_tasks = 0, tot_tptr = 0;
     for (int g = 0; g < G; g++) {
         if (out[g].too_large) return "a part has more than 65535 local nodes: use more ctas";
