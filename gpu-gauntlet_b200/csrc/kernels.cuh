@@ -482,10 +482,14 @@ __device__ __forceinline__ double warp_reduce_scatter(double (&v)[KM]) {
 
 // Block-wide totals of the first K (<= KM) of the KM values v, published
 // as this block's partial sums: copy r < kRep goes to slots
-// pb[r][g][2k, 2k+1] (lane r of warp 0 writes copy r).  Every block reads
-// the copy g % kRep, so each slot line has about G / kRep readers
-// instead of G.  All threads call it; it has one barrier, and warp 0 alone
-// works after it, so `red` must not be written again before a later barrier.
+// pb[r][g][2k, 2k+1].  Every block reads the copy g % kRep, so each slot
+// line has about G / kRep readers instead of G.  After the warps' own
+// reduce-scatter, lane l of warp 0 adds value k = l mod KM over warps
+// l / KM, l / KM + 32 / KM, ... and the 32 / KM lanes of one value finish
+// with an xor butterfly: IEEE addition is commutative, so every one of them
+// holds the same bits, and each writes its share of the copies.  All
+// threads call it; it has one barrier, and warp 0 alone works after it, so
+// `red` must not be written again before a later barrier.
 template <int KM>
 __device__ void block_publish(double (&v)[KM], double* red, unsigned long long* pb, int G, int g,
                               int K, unsigned f) {
@@ -495,19 +499,13 @@ __device__ void block_publish(double (&v)[KM], double* red, unsigned long long* 
     if (lane % SH == 0) red[warp * KM + lane / SH] = t;
     __syncthreads();
     if (warp != 0) return;
-    double q[KM];
+    const int k = lane % KM, w0 = lane / KM;
+    double tk = 0.0;
+    for (int w = w0; w < nw; w += SH) tk += red[w * KM + k];
 #pragma unroll
-    for (int k = 0; k < KM; k++) q[k] = lane < nw ? red[lane * KM + k] : 0.0;
-    const double tt = warp_reduce_scatter<KM>(q);
-    double tk[KM];
-#pragma unroll
-    for (int k = 0; k < KM; k++) tk[k] = __shfl_sync(0xffffffffu, tt, k * SH);
-    if (lane < kRep) {
-        unsigned long long* dst = pb + ((size_t)lane * G + g) * 16;
-#pragma unroll
-        for (int k = 0; k < KM; k++)
-            if (k < K) Tag<double>::put(dst + 2 * k, tk[k], f);
-    }
+    for (int o = KM; o < 32; o <<= 1) tk += __shfl_xor_sync(0xffffffffu, tk, o);
+    if (k < K)
+        for (int r = w0; r < kRep; r += SH) Tag<double>::put(pb + ((size_t)r * G + g) * 16 + 2 * k, tk, f);
 }
 
 // One exchange round, all threads of the block: waits for the K tagged
