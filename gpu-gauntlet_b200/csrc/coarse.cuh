@@ -67,7 +67,7 @@ __host__ __device__ constexpr size_t coarse_factor_smem(int C) {
 
 // Panel widths of coarse_factor_kernel (Cholesky, inverse of L) and its
 // dynamic shared memory: a C x 32 panel of L; a 16-row panel of L^-1 and the
-// matching 16 columns of L, C x 17 each; the tiles of the final product.
+// matching 16 columns of L, C x 17 each.
 constexpr int kPanelChol = 32, kPanelInv = 16;
 __host__ __device__ constexpr size_t coarse_factor_blocked_smem(int C) {
     const size_t a = (size_t)C * (kPanelChol + 1), b = 2 * (size_t)C * (kPanelInv + 1), c = 2 * 32 * 65;
@@ -87,43 +87,46 @@ __device__ __forceinline__ double block_max(double v, double* red) {
 }
 
 // A_c^-1 = L^-T L^-1 from Lt (Lt[c][r] = (L^-1)[r][c]): entry (i, j),
-// j <= i, is Lt[i] . Lt[j] over k >= i; 32 x 32 tiles of entries (a thread
-// each, kCoarseThreads threads), the rows of Lt they need staged in shared
-// memory (sm: 2 x 32 x 65 doubles) 64 columns at a time.
-__device__ void coarse_inverse_product(int C, const double* Lt, double* Ainv, double* sm) {
+// j <= i, is Lt[i] . Lt[j] over k >= i; 32 x 32 tiles of entries, one block
+// of kCoarseThreads threads per tile (a thread per entry), the rows of Lt
+// the tile needs staged in shared memory 64 columns at a time.  Grid: the
+// nt (nt + 1) / 2 tiles of the lower triangle, nt = ceil(C / 32).
+__global__ void __launch_bounds__(kCoarseThreads) coarse_inverse_kernel(int C, const double* __restrict__ Lt,
+                                                                        double* __restrict__ Ainv) {
+    __shared__ double ta[32 * 65];  // rows I0 .. I0 + 31 of Lt
+    __shared__ double tb[32 * 65];  // rows J0 .. J0 + 31
     const int tid = threadIdx.x;
-    double* ta = sm;                  // [32][65] rows I0 .. I0 + 31 of Lt
-    double* tb = sm + 32 * 65;        // [32][65] rows J0 .. J0 + 31
     const int ty = tid >> 5, tx = tid & 31;  // entry (I0 + ty, J0 + tx)
-    const int nt = (C + 31) / 32;
-    for (int I = 0; I < nt; I++)
-        for (int J = 0; J <= I; J++) {
-            const int I0 = 32 * I, J0 = 32 * J;
-            double acc = 0.0;
-            for (int k0 = I0; k0 < C; k0 += 64) {
-                for (int q = tid; q < 32 * 64; q += blockDim.x) {
-                    const int rr = q >> 6, kk = q & 63, k = k0 + kk;
-                    const int ia = I0 + rr, ib = J0 + rr;
-                    ta[rr * 65 + kk] = (ia < C && k < C) ? Lt[(size_t)ia * C + k] : 0.0;
-                    tb[rr * 65 + kk] = (ib < C && k < C) ? Lt[(size_t)ib * C + k] : 0.0;
-                }
-                __syncthreads();
-#pragma unroll 8
-                for (int kk = 0; kk < 64; kk++) acc += ta[ty * 65 + kk] * tb[tx * 65 + kk];
-                __syncthreads();
-            }
-            const int i = I0 + ty, j = J0 + tx;
-            if (i < C && j <= i) {
-                Ainv[(size_t)i * C + j] = acc;
-                Ainv[(size_t)j * C + i] = acc;
-            }
+    const int p = blockIdx.x;
+    int I = (int)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+    while (I * (I + 1) / 2 > p) I--;
+    while ((I + 1) * (I + 2) / 2 <= p) I++;
+    const int J = p - I * (I + 1) / 2;
+    const int I0 = 32 * I, J0 = 32 * J;
+    double acc = 0.0;
+    for (int k0 = I0; k0 < C; k0 += 64) {
+        for (int q = tid; q < 32 * 64; q += blockDim.x) {
+            const int rr = q >> 6, kk = q & 63, k = k0 + kk;
+            const int ia = I0 + rr, ib = J0 + rr;
+            ta[rr * 65 + kk] = (ia < C && k < C) ? Lt[(size_t)ia * C + k] : 0.0;
+            tb[rr * 65 + kk] = (ib < C && k < C) ? Lt[(size_t)ib * C + k] : 0.0;
         }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < 64; kk++) acc += ta[ty * 65 + kk] * tb[tx * 65 + kk];
+        __syncthreads();
+    }
+    const int i = I0 + ty, j = J0 + tx;
+    if (i < C && j <= i) {
+        Ainv[(size_t)i * C + j] = acc;
+        Ainv[(size_t)j * C + i] = acc;
+    }
 }
 
 // The unblocked form of coarse_factor_kernel, for a C whose panels do not
 // fit in shared memory.  One block of kCoarseThreads threads, dynamic
 // shared memory coarse_factor_smem(C).
-// L, Lt and Ainv ([C][C], row-major) start zeroed; keep [C] receives 1 for
+// L and Lt ([C][C], row-major) start zeroed; keep [C] receives 1 for
 // kept modes; *dropped the count of dropped ones.
 //   1. right-looking Cholesky of A_c in L (lower triangle), column by
 //      column: the pivot, the column scaled below it (staged in shared
@@ -135,9 +138,7 @@ __device__ void coarse_inverse_product(int C, const double* Lt, double* Ainv, do
 //      transposed (Lt[c][r] = Y[r][c]): at step i row i of Y is scaled by
 //      1 / L_ii (and staged) and subtracted from the rows below; dropped
 //      rows are zero
-//   3. A_c^-1 = Y^T Y: entry (i, j), j <= i, is Lt[i] . Lt[j] over k >= i,
-//      in 32 x 32 tiles staged through shared memory
-// The updates of 1 and 2 run over 32 x 32 tiles of their region (warp w,
+// then A_c^-1 = Y^T Y by coarse_inverse_kernel.  The updates of 1 and 2 run over 32 x 32 tiles of their region (warp w,
 // lane l: entry (32 I + w, 32 K + l), so every access is coalesced), four
 // tiles per round with all loads issued before the stores: the matrices are
 // L2-resident and each round costs one L2 round trip.
@@ -149,8 +150,8 @@ __device__ __forceinline__ void tile_cursor_next(int& I, int& K, int tri, int nK
 }
 
 __global__ void __launch_bounds__(kCoarseThreads) coarse_factor_tiles_kernel(int C, const double* __restrict__ Ac,
-                                                                             double* L, double* Lt, double* Ainv,
-                                                                             int* keep, int* dropped) {
+                                                                             double* L, double* Lt, int* keep,
+                                                                             int* dropped) {
     extern __shared__ double col[];  // [C] col, [C] nxt (phases 1, 2); two tiles (phase 3)
     double* nxt = col + C;
     __shared__ double red[kCoarseThreads / 32];
@@ -266,12 +267,10 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_factor_tiles_kernel(int
         }
         __syncthreads();
     }
-    __syncthreads();
-    coarse_inverse_product(C, Lt, Ainv, col);
 }
 
 // One block of kCoarseThreads threads (32 warps), dynamic shared memory
-// coarse_factor_blocked_smem(C).  L, Lt and Ainv ([C][C], row-major) start
+// coarse_factor_blocked_smem(C).  L and Lt ([C][C], row-major) start
 // zeroed; keep [C] receives 1 for kept modes; *dropped the count of dropped
 // ones.  Blocked, so the O(C^3) work runs from shared memory and each entry
 // of the global matrices is read and written once per panel:
@@ -285,10 +284,10 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_factor_tiles_kernel(int
 //      substitution in 16-row panels: the panel's rows of Y and the
 //      matching columns of L in shared memory, the panel solved there, then
 //      the rank-16 update of the rows below
-//   3. A_c^-1 = Y^T Y (coarse_inverse_product)
+// then A_c^-1 = Y^T Y by coarse_inverse_kernel
 __global__ void __launch_bounds__(kCoarseThreads) coarse_factor_kernel(int C, const double* __restrict__ Ac,
-                                                                       double* L, double* Lt, double* Ainv,
-                                                                       int* keep, int* dropped) {
+                                                                       double* L, double* Lt, int* keep,
+                                                                       int* dropped) {
     extern __shared__ double cf_smem[];
     double* sm = cf_smem;
     __shared__ double red[kCoarseThreads / 32];
@@ -436,8 +435,6 @@ __global__ void __launch_bounds__(kCoarseThreads) coarse_factor_kernel(int C, co
         }
         __syncthreads();
     }
-    // 3. A_c^-1
-    coarse_inverse_product(C, Lt, Ainv, sm);
 }
 
 // Part rows of A_c^-1: out64/out32[r][k] = Ainv[src[r]][k].

@@ -560,10 +560,11 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
     owner.upload(hp.coarse_owner.data(), hp.coarse_owner.size(), st);
     geom.upload(hp.coarse_geom.data(), hp.coarse_geom.size(), st);
     src.upload(hp.ainv_src.data(), hp.ainv_src.size(), st);
-    for (DevBuf<double>* b : {&Ac, &L, &Lt, &Ainv}) {
+    for (DevBuf<double>* b : {&Ac, &L, &Lt}) {
         b->alloc(CC);
         CK(cudaMemsetAsync(b->p, 0, CC * sizeof(double), st));
     }
+    Ainv.alloc(CC);  // every entry written by coarse_inverse_kernel
     keep.alloc(C);
     dropped.alloc(1);
     if (hp.Ne > 0) {
@@ -585,11 +586,15 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
     if (fsm > 48 * 1024) CK(cudaFuncSetAttribute(ffn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
     {
         const double* acp = Ac.p;
-        double *lp = L.p, *ltp = Lt.p, *aip = Ainv.p;
+        double *lp = L.p, *ltp = Lt.p;
         int *kp = keep.p, *dp = dropped.p;
-        void* fargs[] = {(void*)&C, (void*)&acp, (void*)&lp, (void*)&ltp, (void*)&aip, (void*)&kp, (void*)&dp};
+        void* fargs[] = {(void*)&C, (void*)&acp, (void*)&lp, (void*)&ltp, (void*)&kp, (void*)&dp};
         CK(cudaLaunchKernel(ffn, dim3(1), dim3(pg::kCoarseThreads), fargs, fsm, st));
     }
+    CK(cudaGetLastError());
+    // A_c^-1 = L^-T L^-1: one block per 32 x 32 tile of the lower triangle
+    const int ntile = (C + 31) / 32;
+    pg::coarse_inverse_kernel<<<ntile * (ntile + 1) / 2, pg::kCoarseThreads, 0, st>>>(C, Lt.p, Ainv.p);
     CK(cudaGetLastError());
     const int rows = (int)hp.ainv_src.size();
     pl->ainv64.alloc((size_t)rows * C);
