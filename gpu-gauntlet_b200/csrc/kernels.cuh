@@ -514,13 +514,15 @@ __device__ void block_publish(double (&v)[KM], double* red, unsigned long long* 
 // buffer vb (written to dst[3 * no .. 3 * nloc)).  Items 0 .. ng - 1 are
 // the ghosts, which their owners publish before their partial sums, then
 // the partials.  Each thread takes items tid, tid + nt, tid + 2 nt, ...
-// with two in flight, and refills a slot with its next item as soon as
-// the slot's item has arrived: a ghost frees its slot after one round
-// trip, so every partial is being polled by the time the partials come
-// in, and the round costs about one L2 round trip after the last block
-// published.  Returns false if a wait gave up.
-template <typename T>
-__device__ bool exchange_round(const unsigned long long* __restrict__ pb, int G, int K,
+// with S in flight, and refills a slot with its next item as soon as the
+// slot's item has arrived: a ghost frees its slot after one round trip, so
+// every partial is being polled by the time the partials come in, and the
+// round costs about one L2 round trip after the last block published.
+// The block that publishes last finds every other item already there; with
+// S slots per thread it reads them in ceil(items / (S nt)) round trips.
+// Returns false if a wait gave up.
+template <typename T, int S>
+__device__ bool exchange_round_s(const unsigned long long* __restrict__ pb, int G, int K,
                                const unsigned long long* __restrict__ vb, T* dst, int no, int nloc,
                                const int* __restrict__ gid, int g, unsigned f, double* sp,
                                Waiter& wt) {
@@ -535,51 +537,75 @@ __device__ bool exchange_round(const unsigned long long* __restrict__ pb, int G,
         const int q = i - ng;
         return pb + (size_t)(q / K) * 16 + 2 * (q % K);
     };
-    // two slots: item index (>= n when empty) and its address
-    int i0 = threadIdx.x, i1 = threadIdx.x + nt, next = threadIdx.x + 2 * nt;
-    const unsigned long long* p0 = i0 < n ? addr(i0) : nullptr;
-    const unsigned long long* p1 = i1 < n ? addr(i1) : nullptr;
-    auto load = [&](const unsigned long long* p, int i, unsigned long long& lo, unsigned long long& hi) {
-        if (i >= ng || TW == 2) {
-            ld_relaxed2(p, lo, hi);
-        } else {
-            lo = ld_relaxed(p);
-            hi = lo;
-        }
-    };
-    // stores the item if its tags match; false if it has not arrived
-    auto take = [&](int i, unsigned long long lo, unsigned long long hi) -> bool {
-        if ((unsigned)(lo >> 32) != f || (unsigned)(hi >> 32) != f) return false;
-        if (i >= ng) {
-            sp[i - ng] = __longlong_as_double((long long)((hi << 32) | (lo & 0xffffffffull)));
-        } else if constexpr (TW == 2) {
-            dst[3 * no + i] = (T)__longlong_as_double((long long)((hi << 32) | (lo & 0xffffffffull)));
-        } else {
-            dst[3 * no + i] = (T)__uint_as_float((unsigned)lo);
-        }
-        return true;
-    };
+    // S slots: item index (>= n when empty) and its address
+    int it[S];
+    const unsigned long long* pp[S];
+#pragma unroll
+    for (int s = 0; s < S; s++) {
+        it[s] = threadIdx.x + s * nt;
+        pp[s] = it[s] < n ? addr(it[s]) : nullptr;
+    }
+    int next = threadIdx.x + S * nt;
     wt.spins = 0;
-    while (i0 < n || i1 < n) {
-        unsigned long long lo0 = 0, hi0 = 0, lo1 = 0, hi1 = 0;
-        if (i0 < n) load(p0, i0, lo0, hi0);
-        if (i1 < n) load(p1, i1, lo1, hi1);
-        bool moved = false;
-        if (i0 < n && take(i0, lo0, hi0)) {
-            i0 = next;
-            next += nt;
-            p0 = i0 < n ? addr(i0) : nullptr;
-            moved = true;
+    for (;;) {
+        unsigned long long lo[S], hi[S];
+        bool any = false;
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+            lo[s] = hi[s] = 0;
+            if (it[s] >= n) continue;
+            any = true;
+            if (it[s] >= ng || TW == 2) {
+                ld_relaxed2(pp[s], lo[s], hi[s]);
+            } else {
+                lo[s] = ld_relaxed(pp[s]);
+                hi[s] = lo[s];
+            }
         }
-        if (i1 < n && take(i1, lo1, hi1)) {
-            i1 = next;
+        if (!any) break;
+        bool moved = false;
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+            if (it[s] >= n) continue;
+            if ((unsigned)(lo[s] >> 32) != f || (unsigned)(hi[s] >> 32) != f) continue;
+            const int i = it[s];
+            if (i >= ng) {
+                sp[i - ng] = __longlong_as_double((long long)((hi[s] << 32) | (lo[s] & 0xffffffffull)));
+            } else if constexpr (TW == 2) {
+                dst[3 * no + i] = (T)__longlong_as_double((long long)((hi[s] << 32) | (lo[s] & 0xffffffffull)));
+            } else {
+                dst[3 * no + i] = (T)__uint_as_float((unsigned)lo[s]);
+            }
+            it[s] = next;
             next += nt;
-            p1 = i1 < n ? addr(i1) : nullptr;
+            pp[s] = it[s] < n ? addr(it[s]) : nullptr;
             moved = true;
         }
         if (!moved && !wt.keep_going()) return false;
     }
     return true;
+}
+
+// exchange_round_s with two slots per thread while the round's items fit
+// in two per thread (block Jacobi: 3 partials per block), else, when XS
+// allows, three (the two-level preconditioner's 6 partials per block and
+// the ghosts make about 2.5 items per thread on the 60k-DOF plate, and the
+// block that publishes last then reads them in one round trip, not two).
+// Measured on that plate, in A/B runs on one B200: with XS = 3 the mixed-
+// precision two-level solves run 0.9% (Chebyshev) and 1.8% faster, and the
+// mixed block-Jacobi solves, whose rounds keep two slots, 0.9-1.8% slower
+// (the larger kernel); in the FP64 kernels the third slot's code made block
+// Jacobi 2.4% slower, and in the batch kernel it costs spills, so those
+// keep XS = 2.
+template <typename T, int XS = 3>
+__device__ __forceinline__ bool exchange_round(const unsigned long long* __restrict__ pb, int G, int K,
+                                               const unsigned long long* __restrict__ vb, T* dst, int no,
+                                               int nloc, const int* __restrict__ gid, int g, unsigned f,
+                                               double* sp, Waiter& wt) {
+    const int n = 3 * (nloc - no) + G * K;
+    if constexpr (XS >= 3)
+        if (n > 2 * (int)blockDim.x) return exchange_round_s<T, 3>(pb, G, K, vb, dst, no, nloc, gid, g, f, sp, wt);
+    return exchange_round_s<T, 2>(pb, G, K, vb, dst, no, nloc, gid, g, f, sp, wt);
 }
 
 // Warp 0: adds the first K of each block's `stride` staged partials
@@ -915,7 +941,7 @@ __device__ __forceinline__ void coarse_apply(const T* __restrict__ Ai, int G, in
 // A block overwrites buffer [e & 1] only after it has seen every block's
 // round e - 1 partials, and every block reads round e - 2 before it
 // publishes round e - 1, so no reader can still need the old values.
-template <int NPE, typename T, bool MIXED>
+template <int NPE, typename T, bool MIXED, int XS = (MIXED ? 3 : 2)>
 __device__ __forceinline__ void pcg_body(const PcgArgs& a, const int g, unsigned char* sm) {
     constexpr int ND = 3 * NPE, TW = Tag<T>::W;
     const SmemLayout& L = a.L;
@@ -1040,7 +1066,7 @@ __device__ __forceinline__ void pcg_body(const PcgArgs& a, const int g, unsigned
         for (int n = tid; n < no; n += nt) restrict3(r + 3 * n, cm + 3 * n, nb + 3 * n, v0);
         unsigned long long* pb0 = a.llp + (size_t)(e & 1) * kRep * a.G * 16;
         block_publish<4>(v0, red, pb0, a.G, g, 3, e);
-        const bool ok = exchange_round<T>(pb0, a.G, 3, nullptr, w, no, no, gid, g, e, sp, wt);
+        const bool ok = exchange_round<T, XS>(pb0, a.G, 3, nullptr, w, no, no, gid, g, e, sp, wt);
         if (__syncthreads_or(!ok)) {
             status = ST_TIMEOUT;
         } else {
@@ -1114,7 +1140,7 @@ __device__ __forceinline__ void pcg_body(const PcgArgs& a, const int g, unsigned
         clk.lap(2);
         // ---- exchange: every block's partials and this block's ghost w ----
         {
-            bool ok = exchange_round<T>(pb, a.G, KP, vb, w, no, nloc, gid, g, e, sp, wt);
+            bool ok = exchange_round<T, XS>(pb, a.G, KP, vb, w, no, nloc, gid, g, e, sp, wt);
             if (a.test_stall && it == 0 && tid == 0) {
                 double never;  // a tag no block writes: the wait must run out
                 ok = ok && poll<double>(a.llp + (size_t)kRep * a.G * 32, 0xffffffffu, never, wt);
@@ -1226,7 +1252,7 @@ __device__ __forceinline__ void pcg_body(const PcgArgs& a, const int g, unsigned
                 if (a.coarse) restrict3(rtv, cm + 3 * n, nb + 3 * n, vt + 1);
             }
             block_publish<4>(vt, red, qb, a.G, g, KR, e);
-            ok = exchange_round<T>(qb, a.G, KR, rb, r, no, nloc, gid, g, e, sp, wt);
+            ok = exchange_round<T, XS>(qb, a.G, KR, rb, r, no, nloc, gid, g, e, sp, wt);
             if (__syncthreads_or(!ok)) { status = ST_TIMEOUT; break; }
             sum_partials<1>(sp, a.G, KR, scal);
             // c = A_c^-1 P^T r from the true residual (cs is unchanged)
@@ -1433,7 +1459,7 @@ __device__ __forceinline__ void pcg_body(const PcgArgs& a, const int g, unsigned
             unsigned long long* pb = a.llp + (size_t)(e & 1) * kRep * a.G * 16;
             block_publish<2>(v, red, pb, a.G, g, 2, e);
             if (g == 0) {
-                ok = exchange_round<T>(pb, a.G, 2, nullptr, w, no, no, gid, g, e, sp, wt);
+                ok = exchange_round<T, XS>(pb, a.G, 2, nullptr, w, no, no, gid, g, e, sp, wt);
                 if (__syncthreads_or(!ok)) {
                     status = ST_TIMEOUT;
                 } else {
@@ -1531,7 +1557,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1) pcg_batch_kernel(const __gri
         const PcgArgs& a = b.plates[pi];
         if (g == 0 && threadIdx.x == 0) b.times[2 * pi] = gtimer();
         // a plate with fewer parts than the team has blocks leaves the rest idle
-        if (g < a.G) pcg_body<NPE, T, MIXED>(a, g, sm);
+        if (g < a.G) pcg_body<NPE, T, MIXED, 2>(a, g, sm);
         __syncthreads();  // shared memory is reloaded for the next plate
         if (g == 0 && threadIdx.x == 0) b.times[2 * pi + 1] = gtimer();
     }
