@@ -133,6 +133,27 @@ std::string build_structure(const pg_problem& p, HostPlan& plan) {
 namespace {
 
 // Near-square partition of a node cloud into G parts (see plan.h).
+// Order-preserving map of a finite float to an unsigned key (-0 as +0, so
+// keys compare as the values do).
+inline uint32_t float_key(float v) {
+    if (v == 0.0f) v = 0.0f;
+    uint32_t u;
+    std::memcpy(&u, &v, sizeof u);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+struct SortKey {
+    uint64_t k;  // primary coordinate key << 32 | secondary coordinate key
+    int id;
+};
+
+// Stable sort of v[b, e) by k: equal keys keep their incoming order.
+// Meshes numbered row by row arrive sorted by (y, x) already.
+void sort_keys(std::vector<SortKey>& v, size_t b, size_t e) {
+    auto less = [](const SortKey& u, const SortKey& w) { return u.k < w.k; };
+    if (!std::is_sorted(v.begin() + b, v.begin() + e, less)) std::stable_sort(v.begin() + b, v.begin() + e, less);
+}
+
 void strip_partition(const float* xy, int Nn, int G, std::vector<int>& part_of) {
     part_of.assign(Nn, 0);
     if (G <= 1 || Nn == 0) return;
@@ -145,20 +166,17 @@ void strip_partition(const float* xy, int Nn, int G, std::vector<int>& part_of) 
     const double W = std::max(1e-30, (double)hi[0] - lo[0]), H = std::max(1e-30, (double)hi[1] - lo[1]);
     int R = (int)std::lround(std::sqrt((double)G * H / W));
     R = std::max(1, std::min(R, G));
-    // sort keys held contiguously (primary, secondary coordinate, node id):
-    // first by (y, x, id), then each strip by (x, y, id)
-    struct Key {
-        float a, b;
-        int id;
-    };
-    auto less = [](const Key& u, const Key& v) {
-        if (u.a != v.a) return u.a < v.a;
-        if (u.b != v.b) return u.b < v.b;
-        return u.id < v.id;
-    };
-    std::vector<Key> keys(Nn);
-    for (int n = 0; n < Nn; n++) keys[n] = Key{xy[2 * n + 1], xy[2 * n], n};
-    std::sort(keys.begin(), keys.end(), less);
+    // first by (y, x, id), then each strip by (x, y, id): stable sorts of the
+    // packed coordinate keys, the ids entering in increasing order (and a
+    // strip's equal (x, y) pairs keep the id order of the first sort)
+    std::vector<SortKey> keys(Nn);
+    std::vector<uint32_t> kx(Nn), ky(Nn);
+    for (int n = 0; n < Nn; n++) {
+        kx[n] = float_key(xy[2 * n]);
+        ky[n] = float_key(xy[2 * n + 1]);
+        keys[n] = SortKey{(uint64_t)ky[n] << 32 | kx[n], n};
+    }
+    sort_keys(keys, 0, (size_t)Nn);
     int part = 0;
     long long done_blocks = 0;
     int start = 0;
@@ -166,8 +184,11 @@ void strip_partition(const float* xy, int Nn, int G, std::vector<int>& part_of) 
         const int blocks = G / R + (s < G % R ? 1 : 0);
         done_blocks += blocks;
         const int end = (int)((long long)Nn * done_blocks / G);
-        for (int i = start; i < end; i++) std::swap(keys[i].a, keys[i].b);
-        std::sort(keys.begin() + start, keys.begin() + end, less);
+        for (int i = start; i < end; i++) {
+            const int n = keys[i].id;
+            keys[i].k = (uint64_t)kx[n] << 32 | ky[n];
+        }
+        sort_keys(keys, (size_t)start, (size_t)end);
         const int len = end - start;
         for (int b = 0; b < blocks; b++) {
             const int b0 = start + (int)((long long)len * b / blocks);

@@ -556,24 +556,27 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
     const int C = hp.C;
     const size_t CC = (size_t)C * C;
     DevBuf<int> owner, src, keep, dropped;
-    DevBuf<double> geom, Ac, L, Lt, Ainv;
+    DevBuf<double> geom, mats;
     owner.upload(hp.coarse_owner.data(), hp.coarse_owner.size(), st);
     geom.upload(hp.coarse_geom.data(), hp.coarse_geom.size(), st);
     src.upload(hp.ainv_src.data(), hp.ainv_src.size(), st);
-    for (DevBuf<double>* b : {&Ac, &L, &Lt}) {
-        b->alloc(CC);
-        CK(cudaMemsetAsync(b->p, 0, CC * sizeof(double), st));
-    }
-    Ainv.alloc(CC);  // every entry written by coarse_inverse_kernel
+    // A_c, L, Lt and A_c^-1 ([C][C] each) in one allocation; the first three
+    // start zeroed, every entry of A_c^-1 is written by coarse_inverse_kernel
+    mats.alloc(4 * CC);
+    double* const Ac = mats.p;
+    double* const L = mats.p + CC;
+    double* const Lt = mats.p + 2 * CC;
+    double* const Ainv = mats.p + 3 * CC;
+    CK(cudaMemsetAsync(mats.p, 0, 3 * CC * sizeof(double), st));
     keep.alloc(C);
     dropped.alloc(1);
     if (hp.Ne > 0) {
         if (hp.npe == 4)
             pg::coarse_assemble_kernel<4><<<(hp.Ne + 127) / 128, 128, 0, st>>>(
-                hp.Ne, C, pl->mesh_nodes.p, pl->mesh_elements.p, pl->cons.p, owner.p, geom.p, pl->ke64.p, Ac.p);
+                hp.Ne, C, pl->mesh_nodes.p, pl->mesh_elements.p, pl->cons.p, owner.p, geom.p, pl->ke64.p, Ac);
         else
             pg::coarse_assemble_kernel<3><<<(hp.Ne + 127) / 128, 128, 0, st>>>(
-                hp.Ne, C, pl->mesh_nodes.p, pl->mesh_elements.p, pl->cons.p, owner.p, geom.p, pl->ke64.p, Ac.p);
+                hp.Ne, C, pl->mesh_nodes.p, pl->mesh_elements.p, pl->cons.p, owner.p, geom.p, pl->ke64.p, Ac);
         CK(cudaGetLastError());
     }
     // the blocked factorisation when its panels fit in shared memory
@@ -585,8 +588,8 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
     const void* ffn = blocked ? (const void*)pg::coarse_factor_kernel : (const void*)pg::coarse_factor_tiles_kernel;
     if (fsm > 48 * 1024) CK(cudaFuncSetAttribute(ffn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
     {
-        const double* acp = Ac.p;
-        double *lp = L.p, *ltp = Lt.p;
+        const double* acp = Ac;
+        double *lp = L, *ltp = Lt;
         int *kp = keep.p, *dp = dropped.p;
         void* fargs[] = {(void*)&C, (void*)&acp, (void*)&lp, (void*)&ltp, (void*)&kp, (void*)&dp};
         CK(cudaLaunchKernel(ffn, dim3(1), dim3(pg::kCoarseThreads), fargs, fsm, st));
@@ -594,7 +597,7 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
     CK(cudaGetLastError());
     // A_c^-1 = L^-T L^-1: one block per 32 x 32 tile of the lower triangle
     const int ntile = (C + 31) / 32;
-    pg::coarse_inverse_kernel<<<ntile * (ntile + 1) / 2, pg::kCoarseThreads, 0, st>>>(C, Lt.p, Ainv.p);
+    pg::coarse_inverse_kernel<<<ntile * (ntile + 1) / 2, pg::kCoarseThreads, 0, st>>>(C, Lt, Ainv);
     CK(cudaGetLastError());
     const int rows = (int)hp.ainv_src.size();
     pl->ainv64.alloc((size_t)rows * C);
@@ -602,7 +605,7 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
     if (rows > 0) {
         const long tot = (long)rows * C;
         pg::coarse_rows_kernel<<<(int)std::min<long>((tot + 255) / 256, 4096), 256, 0, st>>>(
-            rows, C, src.p, Ainv.p, pl->ainv64.p, pl->ainv32.p);
+            rows, C, src.p, Ainv, pl->ainv64.p, pl->ainv32.p);
         CK(cudaGetLastError());
     }
     int nd = 0;
