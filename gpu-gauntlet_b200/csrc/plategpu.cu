@@ -8,12 +8,14 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <list>
 #include <memory>
 #include <mutex>
 #include <atomic>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "coarse.cuh"
@@ -40,10 +42,14 @@ struct Fail {
                        std::string(#call) + ": " + cudaGetErrorString(e_)};               \
     } while (0)
 
+// Device array.  view() points it into memory owned elsewhere (a plan's
+// arena), which it then does not free.
 template <typename T>
 struct DevBuf {
+    using value_type = T;
     T* p = nullptr;
     size_t n = 0;
+    bool own = true;
     void alloc(size_t count) {
         release();
         n = count;
@@ -53,10 +59,17 @@ struct DevBuf {
         alloc(count);
         if (count) CK(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, st));
     }
+    void view(T* ptr, size_t count) {
+        release();
+        p = ptr;
+        n = count;
+        own = false;
+    }
     void release() {
-        if (p) cudaFree(p);
+        if (p && own) cudaFree(p);
         p = nullptr;
         n = 0;
+        own = true;
     }
     ~DevBuf() { release(); }
 };
@@ -98,6 +111,8 @@ struct Plan {
     DevBuf<int> abort_flag;
     DevBuf<unsigned long long> trace;
     DevBuf<pg::PcgResult> res;
+    // one allocation holding the arrays above that build_plan creates
+    DevBuf<unsigned char> arena;
     // load cases solved together (NR cases per launch): their loads,
     // solutions, exchange buffers and result records
     int m_nr = 0;
@@ -326,40 +341,57 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G, int ring
     cudaStream_t st = c->stream;
     const size_t Nn = p.node_count, Ne = p.element_count, npe = p.nodes_per_element;
     const size_t kk = 9 * npe * npe;
-    pl->node_off.upload(hp.node_off.data(), hp.node_off.size(), st);
-    pl->nown.upload(hp.nown.data(), hp.nown.size(), st);
-    pl->nodes.upload(hp.nodes.data(), hp.nodes.size(), st);
-    pl->task_off.upload(hp.task_off.data(), hp.task_off.size(), st);
-    pl->tp_off.upload(hp.tp_off.data(), hp.tp_off.size(), st);
-    pl->tptr.upload(hp.tptr.data(), hp.tptr.size(), st);
-    pl->n1.upload(hp.n1.data(), hp.n1.size(), st);
-    pl->task_elem.upload(hp.task_elem.data(), hp.task_elem.size(), st);
-    pl->task_pos.upload(hp.task_pos.data(), hp.task_pos.size(), st);
-    pl->task_nodes.upload(hp.task_nodes.data(), hp.task_nodes.size(), st);
-    pl->inc_ptr.upload(hp.inc_ptr.data(), hp.inc_ptr.size(), st);
-    pl->inc_idx.upload(hp.inc_idx.data(), hp.inc_idx.size(), st);
-    pl->mesh_nodes.upload(p.nodes, 2 * Nn, st);
-    pl->mesh_elements.upload(p.elements, npe * Ne, st);
-    pl->cob_off.upload(hp.color_offsets.data(), hp.color_offsets.size(), st);
-    pl->cob_list.upload(hp.elements_by_color.data(), hp.elements_by_color.size(), st);
-    pl->cons.upload(p.constrained, 3 * Nn, st);
-    pl->has_elem_t = p.elem_t != nullptr;
-    if (p.elem_t) pl->elem_t.upload(p.elem_t, Ne, st);
-    pl->F.alloc(3 * Nn);
     const size_t NT = hp.task_elem.size();
-    pl->ke64.alloc(std::max<size_t>(1, Ne * kk));
-    pl->ke32.alloc(std::max<size_t>(1, Ne * kk));
-    pl->kt64.alloc(std::max<size_t>(1, NT * 9 * npe));
-    pl->kt32.alloc(std::max<size_t>(1, NT * 9 * npe));
-    pl->binv64.alloc(9 * Nn);
-    pl->binv32.alloc(9 * Nn);
-    pl->x.alloc(3 * Nn);
-    pl->llv.alloc(12 * Nn);
-    pl->llx.alloc(6 * Nn);
-    pl->llp.alloc(32 * (size_t)pg::kRep * pl->G + 2);
-    pl->abort_flag.alloc(1);
-    pl->trace.alloc(4 * (size_t)pl->G);
-    pl->res.alloc(1);
+    // every device array of the plan in one allocation, each 256-byte
+    // aligned: one cudaMalloc instead of about thirty (each costs the first
+    // solve of a new mesh a driver call with page mapping)
+    size_t total = 0;
+    std::vector<std::function<void(unsigned char*)>> bind;
+    auto carve = [&](auto& buf, size_t count, const void* host) {
+        using T = typename std::remove_reference_t<decltype(buf)>::value_type;
+        const size_t off = total;
+        total += (count * sizeof(T) + 255) & ~size_t(255);
+        auto* b = &buf;
+        bind.push_back([b, off, count, host, st](unsigned char* base) {
+            b->view(reinterpret_cast<T*>(base + off), count);
+            if (host && count) CK(cudaMemcpyAsync(b->p, host, count * sizeof(T), cudaMemcpyHostToDevice, st));
+        });
+    };
+    carve(pl->node_off, hp.node_off.size(), hp.node_off.data());
+    carve(pl->nown, hp.nown.size(), hp.nown.data());
+    carve(pl->nodes, hp.nodes.size(), hp.nodes.data());
+    carve(pl->task_off, hp.task_off.size(), hp.task_off.data());
+    carve(pl->tp_off, hp.tp_off.size(), hp.tp_off.data());
+    carve(pl->tptr, hp.tptr.size(), hp.tptr.data());
+    carve(pl->n1, hp.n1.size(), hp.n1.data());
+    carve(pl->task_elem, hp.task_elem.size(), hp.task_elem.data());
+    carve(pl->task_pos, hp.task_pos.size(), hp.task_pos.data());
+    carve(pl->task_nodes, hp.task_nodes.size(), hp.task_nodes.data());
+    carve(pl->inc_ptr, hp.inc_ptr.size(), hp.inc_ptr.data());
+    carve(pl->inc_idx, hp.inc_idx.size(), hp.inc_idx.data());
+    carve(pl->mesh_nodes, 2 * Nn, p.nodes);
+    carve(pl->mesh_elements, npe * Ne, p.elements);
+    carve(pl->cob_off, hp.color_offsets.size(), hp.color_offsets.data());
+    carve(pl->cob_list, hp.elements_by_color.size(), hp.elements_by_color.data());
+    carve(pl->cons, 3 * Nn, p.constrained);
+    pl->has_elem_t = p.elem_t != nullptr;
+    if (p.elem_t) carve(pl->elem_t, Ne, p.elem_t);
+    carve(pl->F, 3 * Nn, nullptr);
+    carve(pl->ke64, std::max<size_t>(1, Ne * kk), nullptr);
+    carve(pl->ke32, std::max<size_t>(1, Ne * kk), nullptr);
+    carve(pl->kt64, std::max<size_t>(1, NT * 9 * npe), nullptr);
+    carve(pl->kt32, std::max<size_t>(1, NT * 9 * npe), nullptr);
+    carve(pl->binv64, 9 * Nn, nullptr);
+    carve(pl->binv32, 9 * Nn, nullptr);
+    carve(pl->x, 3 * Nn, nullptr);
+    carve(pl->llv, 12 * Nn, nullptr);
+    carve(pl->llx, 6 * Nn, nullptr);
+    carve(pl->llp, 32 * (size_t)pg::kRep * pl->G + 2, nullptr);
+    carve(pl->abort_flag, 1, nullptr);
+    carve(pl->trace, 4 * (size_t)pl->G, nullptr);
+    carve(pl->res, 1, nullptr);
+    pl->arena.alloc(total);
+    for (auto& f : bind) f(pl->arena.p);
     // synchronous: uploads read the host plan arrays
     CK(cudaStreamSynchronize(st));
     return pl;
