@@ -74,6 +74,32 @@ struct DevBuf {
     ~DevBuf() { release(); }
 };
 
+// Typed arrays carved out of one device allocation, each 256-byte aligned:
+// one cudaMalloc instead of one per array (each a driver call that maps
+// pages, which the first solve of a new mesh pays many times over).  add()
+// records an array (with the host data to copy into it, or none);
+// commit() allocates `store`, points the arrays into it and queues the
+// copies on `st`.
+struct Arena {
+    size_t total = 0;
+    std::vector<std::function<void(unsigned char*, cudaStream_t)>> bind;
+    template <typename B>
+    void add(B& buf, size_t count, const void* host) {
+        using T = typename B::value_type;
+        const size_t off = total;
+        total += (count * sizeof(T) + 255) & ~size_t(255);
+        B* b = &buf;
+        bind.push_back([b, off, count, host](unsigned char* base, cudaStream_t st) {
+            b->view(reinterpret_cast<T*>(base + off), count);
+            if (host && count) CK(cudaMemcpyAsync(b->p, host, count * sizeof(T), cudaMemcpyHostToDevice, st));
+        });
+    }
+    void commit(DevBuf<unsigned char>& store, cudaStream_t st) {
+        store.alloc(total);
+        for (auto& f : bind) f(store.p, st);
+    }
+};
+
 struct Plan {
     int G = 0;
     pg::HostPlan hp;
@@ -111,8 +137,9 @@ struct Plan {
     DevBuf<int> abort_flag;
     DevBuf<unsigned long long> trace;
     DevBuf<pg::PcgResult> res;
-    // one allocation holding the arrays above that build_plan creates
-    DevBuf<unsigned char> arena;
+    // one allocation holding the arrays above that build_plan creates, one
+    // for the coarse-space arrays
+    DevBuf<unsigned char> arena, coarse_arena;
     // load cases solved together (NR cases per launch): their loads,
     // solutions, exchange buffers and result records
     int m_nr = 0;
@@ -342,21 +369,9 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G, int ring
     const size_t Nn = p.node_count, Ne = p.element_count, npe = p.nodes_per_element;
     const size_t kk = 9 * npe * npe;
     const size_t NT = hp.task_elem.size();
-    // every device array of the plan in one allocation, each 256-byte
-    // aligned: one cudaMalloc instead of about thirty (each costs the first
-    // solve of a new mesh a driver call with page mapping)
-    size_t total = 0;
-    std::vector<std::function<void(unsigned char*)>> bind;
-    auto carve = [&](auto& buf, size_t count, const void* host) {
-        using T = typename std::remove_reference_t<decltype(buf)>::value_type;
-        const size_t off = total;
-        total += (count * sizeof(T) + 255) & ~size_t(255);
-        auto* b = &buf;
-        bind.push_back([b, off, count, host, st](unsigned char* base) {
-            b->view(reinterpret_cast<T*>(base + off), count);
-            if (host && count) CK(cudaMemcpyAsync(b->p, host, count * sizeof(T), cudaMemcpyHostToDevice, st));
-        });
-    };
+    // every device array of the plan in one allocation
+    Arena ar;
+    auto carve = [&](auto& buf, size_t count, const void* host) { ar.add(buf, count, host); };
     carve(pl->node_off, hp.node_off.size(), hp.node_off.data());
     carve(pl->nown, hp.nown.size(), hp.nown.data());
     carve(pl->nodes, hp.nodes.size(), hp.nodes.data());
@@ -390,8 +405,7 @@ std::unique_ptr<Plan> build_plan(pg_ctx* c, const pg_problem& p, int G, int ring
     carve(pl->abort_flag, 1, nullptr);
     carve(pl->trace, 4 * (size_t)pl->G, nullptr);
     carve(pl->res, 1, nullptr);
-    pl->arena.alloc(total);
-    for (auto& f : bind) f(pl->arena.p);
+    ar.commit(pl->arena, st);
     // synchronous: uploads read the host plan arrays
     CK(cudaStreamSynchronize(st));
     return pl;
@@ -576,7 +590,7 @@ int halo_rings(const pg_options& o) { return o.smoother == PG_SMOOTHER_CHEBYSHEV
 // on the device (coarse.cuh), from the element matrices already there.
 // Batches build the dense part on host threads (prepare_many, build_coarse).
 void upload_coarse(pg_ctx* c, Plan* pl);
-void upload_coarse_meta(pg_ctx* c, Plan* pl);
+void carve_coarse(Arena& ar, Plan* pl, size_t n, const double* a64, const float* a32);
 
 void ensure_coarse(pg_ctx* c, Plan* pl) {
     pg::HostPlan& hp = pl->hp;
@@ -587,21 +601,33 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
     cudaStream_t st = c->stream;
     const int C = hp.C;
     const size_t CC = (size_t)C * C;
+    const int rows = (int)hp.ainv_src.size();
+    // the set-up's scratch arrays in one allocation, freed on return; A_c,
+    // L, Lt and A_c^-1 ([C][C] each, consecutive) in `mats`: the first three
+    // start zeroed, every entry of A_c^-1 is written by coarse_inverse_kernel
+    DevBuf<unsigned char> scratch;
     DevBuf<int> owner, src, keep, dropped;
     DevBuf<double> geom, mats;
-    owner.upload(hp.coarse_owner.data(), hp.coarse_owner.size(), st);
-    geom.upload(hp.coarse_geom.data(), hp.coarse_geom.size(), st);
-    src.upload(hp.ainv_src.data(), hp.ainv_src.size(), st);
-    // A_c, L, Lt and A_c^-1 ([C][C] each) in one allocation; the first three
-    // start zeroed, every entry of A_c^-1 is written by coarse_inverse_kernel
-    mats.alloc(4 * CC);
+    {
+        Arena ar;
+        ar.add(owner, hp.coarse_owner.size(), hp.coarse_owner.data());
+        ar.add(geom, hp.coarse_geom.size(), hp.coarse_geom.data());
+        ar.add(src, hp.ainv_src.size(), hp.ainv_src.data());
+        ar.add(mats, 4 * CC, nullptr);
+        ar.add(keep, (size_t)C, nullptr);
+        ar.add(dropped, 1, nullptr);
+        ar.commit(scratch, st);
+    }
+    {
+        Arena ar;
+        carve_coarse(ar, pl, (size_t)rows * C, nullptr, nullptr);
+        ar.commit(pl->coarse_arena, st);
+    }
     double* const Ac = mats.p;
     double* const L = mats.p + CC;
     double* const Lt = mats.p + 2 * CC;
     double* const Ainv = mats.p + 3 * CC;
     CK(cudaMemsetAsync(mats.p, 0, 3 * CC * sizeof(double), st));
-    keep.alloc(C);
-    dropped.alloc(1);
     if (hp.Ne > 0) {
         if (hp.npe == 4)
             pg::coarse_assemble_kernel<4><<<(hp.Ne + 127) / 128, 128, 0, st>>>(
@@ -631,9 +657,6 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
     const int ntile = (C + 31) / 32;
     pg::coarse_inverse_kernel<<<ntile * (ntile + 1) / 2, pg::kCoarseThreads, 0, st>>>(C, Lt, Ainv);
     CK(cudaGetLastError());
-    const int rows = (int)hp.ainv_src.size();
-    pl->ainv64.alloc((size_t)rows * C);
-    pl->ainv32.alloc((size_t)rows * C);
     if (rows > 0) {
         const long tot = (long)rows * C;
         pg::coarse_rows_kernel<<<(int)std::min<long>((tot + 255) / 256, 4096), 256, 0, st>>>(
@@ -642,30 +665,32 @@ void ensure_coarse(pg_ctx* c, Plan* pl) {
     }
     int nd = 0;
     CK(cudaMemcpyAsync(&nd, dropped.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    upload_coarse_meta(c, pl);  // synchronises the stream
+    CK(cudaStreamSynchronize(st));  // nd; the scratch is freed on return
     hp.dropped_modes = nd;
     hp.coarse = true;
 }
 
-// Device copies of a plan's aggregate lists and node basis data.
-void upload_coarse_meta(pg_ctx* c, Plan* pl) {
+// The plan's device copies of its aggregate lists and node basis data and
+// of its A_c^-1 rows (n entries in FP64 and FP32, copied from a64 / a32
+// when given, else left for coarse_rows_kernel).
+void carve_coarse(Arena& ar, Plan* pl, size_t n, const double* a64, const float* a32) {
     const pg::HostPlan& hp = pl->hp;
-    cudaStream_t st = c->stream;
-    pl->cagg_off.upload(hp.cagg_off.data(), hp.cagg_off.size(), st);
-    pl->node_slot.upload(hp.node_slot.data(), hp.node_slot.size(), st);
-    pl->node_basis.upload(hp.node_basis.data(), hp.node_basis.size(), st);
-    pl->ainv_off.upload(hp.ainv_off.data(), hp.ainv_off.size(), st);
-    CK(cudaStreamSynchronize(st));
+    ar.add(pl->ainv64, n, a64);
+    ar.add(pl->ainv32, n, a32);
+    ar.add(pl->cagg_off, hp.cagg_off.size(), hp.cagg_off.data());
+    ar.add(pl->node_slot, hp.node_slot.size(), hp.node_slot.data());
+    ar.add(pl->node_basis, hp.node_basis.size(), hp.node_basis.data());
+    ar.add(pl->ainv_off, hp.ainv_off.size(), hp.ainv_off.data());
 }
 
 // Device copies of a plan's coarse data built on the host (build_coarse).
 void upload_coarse(pg_ctx* c, Plan* pl) {
     const pg::HostPlan& hp = pl->hp;
-    cudaStream_t st = c->stream;
-    pl->ainv64.upload(hp.ainv.data(), hp.ainv.size(), st);
     std::vector<float> a32(hp.ainv.begin(), hp.ainv.end());
-    pl->ainv32.upload(a32.data(), a32.size(), st);
-    upload_coarse_meta(c, pl);
+    Arena ar;
+    carve_coarse(ar, pl, hp.ainv.size(), hp.ainv.data(), a32.data());
+    ar.commit(pl->coarse_arena, c->stream);
+    CK(cudaStreamSynchronize(c->stream));  // a32 is read by the copy
 }
 
 // Largest eigenvalue of D^-1 K for the polynomial smoother, estimated once
