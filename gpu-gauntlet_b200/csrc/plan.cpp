@@ -132,7 +132,6 @@ std::string build_structure(const pg_problem& p, HostPlan& plan) {
 
 namespace {
 
-// Near-square partition of a node cloud into G parts (see plan.h).
 // Order-preserving map of a finite float to an unsigned key (-0 as +0, so
 // keys compare as the values do).
 inline uint32_t float_key(float v) {
@@ -154,6 +153,9 @@ void sort_keys(std::vector<SortKey>& v, size_t b, size_t e) {
     if (!std::is_sorted(v.begin() + b, v.begin() + e, less)) std::stable_sort(v.begin() + b, v.begin() + e, less);
 }
 
+}  // namespace
+
+// Near-square partition of a node cloud into G parts (see plan.h).
 void strip_partition(const float* xy, int Nn, int G, std::vector<int>& part_of) {
     part_of.assign(Nn, 0);
     if (G <= 1 || Nn == 0) return;
@@ -199,8 +201,6 @@ void strip_partition(const float* xy, int Nn, int G, std::vector<int>& part_of) 
         start = end;
     }
 }
-
-}  // namespace
 
 std::string build_partition(const pg_problem& p, int G, int rings, HostPlan& plan) {
     const int Nn = plan.Nn, npe = plan.npe;

@@ -69,6 +69,10 @@ std::string validate_problem(const pg_problem& p, bool need_rhs);
 // Builds the colouring (caller's or greedy) and node incidence.
 std::string build_structure(const pg_problem& p, HostPlan& plan);
 
+// The part (0 .. G - 1) of each of the Nn nodes (xy: [2 Nn]) under the
+// strip partition above: sorted by (y, x, node id) into R strips, each
+// strip sorted by (x, y, node id) and cut into its blocks; G >= 1.
+void strip_partition(const float* xy, int Nn, int G, std::vector<int>& part_of);
 // Partitions into G parts (G <= node_count) and fills the part arrays, with
 // a ghost halo of `rings` (1 or 2) element layers.
 std::string build_partition(const pg_problem& p, int G, int rings, HostPlan& plan);

@@ -2264,6 +2264,22 @@ int pg_batch_schedule(const uint32_t* node_counts, int count, int sms, int cap, 
     }
 }
 
+int pg_partition_nodes(const float* nodes, uint32_t node_count, int ctas, int32_t* part_of) {
+    if (node_count == 0) return PG_OK;
+    if (!nodes || !part_of || ctas < 1 || node_count > (uint32_t)INT32_MAX) return PG_EINVAL;
+    for (size_t i = 0; i < 2 * (size_t)node_count; i++)
+        if (!std::isfinite(nodes[i])) return PG_EINVAL;
+    try {
+        const int Nn = (int)node_count;
+        std::vector<int> part;
+        pg::strip_partition(nodes, Nn, std::min(ctas, Nn), part);
+        for (int n = 0; n < Nn; n++) part_of[n] = part[n];
+        return PG_OK;
+    } catch (...) {
+        return PG_ENOMEM;
+    }
+}
+
 int pg_moments(pg_ctx* c, const pg_problem* p, const double* x, double* Mx, double* My,
                           double* Mxy) {
     return guarded(c, nullptr, [&] {

@@ -31,7 +31,7 @@ EXPORTED = ("pg_options_default", "pg_is_available", "pg_create", "pg_destroy", 
             "pg_plan_destroy", "pg_apply_k", "pg_apply_k_static",
             "pg_block_jacobi", "pg_element_stiffness", "pg_plan_inspect",
             "pg_plan_inspect_halo", "pg_batch_create", "pg_batch_solve", "pg_batch_destroy",
-            "pg_solve_batch", "pg_batch_schedule", "pg_moments", "pg_plan_moments_device", "pg_solve_load_cases",
+            "pg_solve_batch", "pg_batch_schedule", "pg_partition_nodes", "pg_moments", "pg_plan_moments_device", "pg_solve_load_cases",
             "pg_net_create", "pg_net_destroy", "pg_net_param_count", "pg_net_set_params",
             "pg_net_get_params", "pg_net_forward", "pg_net_backward", "pg_net_adam_step",
             "pg_learned_create", "pg_learned_destroy", "pg_learned_make_pairs",
@@ -258,6 +258,8 @@ def load() -> C.CDLL:
     L.pg_solve_batch.restype = I
     L.pg_batch_schedule.argtypes = [P, I, I, I, P, P, P, P, P]
     L.pg_batch_schedule.restype = I
+    L.pg_partition_nodes.argtypes = [P, C.c_uint32, I, P]
+    L.pg_partition_nodes.restype = I
     L.pg_moments.argtypes = [P, C.POINTER(PgProblem), P, P, P, P]
     L.pg_moments.restype = I
     L.pg_plan_moments_device.argtypes = [P, P, P]
@@ -551,6 +553,18 @@ def batch_schedule(node_counts, sms: int, cap: int) -> dict:
         raise PlateGPUError(st, "batch schedule failed")
     return {"plate_phase": phase, "plate_size": size, "plate_team": team,
             "phase_grid": grid[:phases.value].copy(), "phases": phases.value}
+
+
+def partition_nodes(nodes, ctas: int) -> np.ndarray:
+    """pg_partition_nodes (host only): the part (thread block) of each node
+    in a solve over `ctas` blocks."""
+    xy = np.ascontiguousarray(nodes, np.float32).reshape(-1)
+    n = xy.size // 2
+    part = np.zeros(n, np.int32)
+    st = load().pg_partition_nodes(_ptr(xy), n, int(ctas), _ptr(part))
+    if st != PG_OK:
+        raise PlateGPUError(st, "partition failed")
+    return part
 
 
 class DevicePlan:

@@ -317,6 +317,14 @@ int pg_solve_batch(pg_ctx* ctx, const pg_problem* probs, int count, const pg_opt
 int pg_batch_schedule(const uint32_t* node_counts, int count, int sms, int cap, int32_t* plate_phase,
                       int32_t* plate_size, int32_t* plate_team, int32_t* phase_grid,
                       int32_t* phases_out);
+/* Host-only: the thread block (part) owning each node in a solve over
+ * `ctas` blocks (pg_info.ctas; at most node_count are used): nodes sorted
+ * by (y, x, node id) are cut into R = round(sqrt(ctas * height / width))
+ * strips, each strip sorted by (x, y, node id) is cut into its share of the
+ * blocks.  nodes: [2*node_count] x0,y0,...; part_of: [node_count].  No
+ * counterpart in the reference (its solver does not partition the mesh).
+ * PG_EINVAL for NULL arrays, ctas < 1, or coordinates that are not finite. */
+int pg_partition_nodes(const float* nodes, uint32_t node_count, int ctas, int32_t* part_of);
 
 /* Nodal bending moments of a solution, as computeMoments
  * (postprocess.ts:40-264): curvatures at each element's centroid (Q4
