@@ -865,7 +865,8 @@ def other_configs_bench(args, ctx, stream, flush, world, local, check):
                                          "global_path")}
             if r["global_path"]:
                 # flexible PCG over global memory: 16 FP32 vector words per DOF and
-                # iteration (SURVEY's minimal schedule) against the HBM copy peak
+                # iteration (the fewest vector reads and writes a PCG iteration
+                # needs) against the HBM copy peak
                 alg = 16.0 * 4 * wl.n_dof * max(1, r["iterations"])
                 ach = alg / (r["kernel_ms"] * 1e-3) / 1e9
                 rows[v]["roofline"] = {"achieved": ach, "peak": hbm_peak()[0], "unit": "GB/s",
