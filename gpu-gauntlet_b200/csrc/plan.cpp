@@ -272,6 +272,15 @@ std::string build_partition(const pg_problem& p, int G, int rings, HostPlan& pla
             o.nodes.insert(o.nodes.end(), ghosts.begin(), ghosts.end());
             o.nodes.insert(o.nodes.end(), ring2.begin(), ring2.end());
             const int ntn = o.n1;
+            size_t ntask = 0;
+            for (int i = 0; i < ntn; i++) {
+                const int n = i < (int)own.size() ? own[i] : ghosts[i - own.size()];
+                ntask += (size_t)(plan.inc_ptr[n + 1] - plan.inc_ptr[n]);
+            }
+            o.tptr.reserve(ntn + 1);
+            o.task_elem.reserve(ntask);
+            o.task_pos.reserve(ntask);
+            o.task_nodes.reserve(ntask * npe);
             for (int i = 0; i < ntn; i++) {
                 const int n = i < (int)own.size() ? own[i] : ghosts[i - own.size()];
                 if (i == (int)own.size()) o.ntask_own = (int)o.task_elem.size();
