@@ -277,24 +277,30 @@ std::string build_partition(const pg_problem& p, int G, int rings, HostPlan& pla
                 const int n = i < (int)own.size() ? own[i] : ghosts[i - own.size()];
                 ntask += (size_t)(plan.inc_ptr[n + 1] - plan.inc_ptr[n]);
             }
-            o.tptr.reserve(ntn + 1);
-            o.task_elem.reserve(ntask);
-            o.task_pos.reserve(ntask);
-            o.task_nodes.reserve(ntask * npe);
+            o.tptr.resize(ntn + 1);
+            o.task_elem.resize(ntask);
+            o.task_pos.resize(ntask);
+            o.task_nodes.resize(ntask * npe);
+            int* te = o.task_elem.data();
+            uint8_t* tpos = o.task_pos.data();
+            uint16_t* tnod = o.task_nodes.data();
+            int t = 0;
             for (int i = 0; i < ntn; i++) {
                 const int n = i < (int)own.size() ? own[i] : ghosts[i - own.size()];
-                if (i == (int)own.size()) o.ntask_own = (int)o.task_elem.size();
-                o.tptr.push_back((int)o.task_elem.size());
-                for (int q = plan.inc_ptr[n]; q < plan.inc_ptr[n + 1]; q++) {
+                if (i == (int)own.size()) o.ntask_own = t;
+                o.tptr[i] = t;
+                for (int q = plan.inc_ptr[n]; q < plan.inc_ptr[n + 1]; q++, t++) {
                     const int e = plan.inc_idx[q] / 4, k = plan.inc_idx[q] % 4;
-                    o.task_elem.push_back(e);
-                    o.task_pos.push_back((uint8_t)k);
-                    for (int j = 0; j < npe; j++)
-                        o.task_nodes.push_back((uint16_t)local[p.elements[(size_t)e * npe + (k + j) % npe]]);
+                    te[t] = e;
+                    tpos[t] = (uint8_t)k;
+                    const uint32_t* en = p.elements + (size_t)e * npe;
+                    uint16_t* dst = tnod + (size_t)t * npe;
+                    for (int j = 0, kj = k; j < npe; j++, kj = kj + 1 == npe ? 0 : kj + 1)
+                        dst[j] = (uint16_t)local[en[kj]];
                 }
             }
-            if (ntn == (int)own.size()) o.ntask_own = (int)o.task_elem.size();
-            o.tptr.push_back((int)o.task_elem.size());
+            if (ntn == (int)own.size()) o.ntask_own = t;
+            o.tptr[ntn] = t;
         }
         for (int n : own) local[n] = -1;
         for (int n : ghosts) local[n] = -1;
